@@ -1,0 +1,1586 @@
+// chatcarlo_b200 engine: photon transport for 1-150 keV on sm_100a.
+//
+// One persistent kernel runs the event loop of ChatCarlo's
+// transport_photons (chatcarlo/transport.py:98-233).  Every lane owns one
+// photon; when its history ends the lane takes the next history from a
+// warp-local pool that the warp refills from a global counter, so lanes
+// never wait for the longest history of their warp.  Per step a lane
+//   * finds its material at the segment start (geometry.py:205-212),
+//   * looks up mu in the material's union energy grid (materials.py:228-289),
+//   * finds the next analytic boundary (geometry.py:214-231),
+//   * decides between crossing and interacting with its optical depth tau
+//     (transport.py:137-158),
+//   * walks the segment through the voxel grid, scoring E*mu_en and
+//     h*(10)/Phi times the exact overlap length (tally.py:248-293 scores
+//     the same expectation with stratified points),
+//   * samples photoelectric absorption with K fluorescence, bound Compton
+//     or Rayleigh scattering (physics.py:95-367).
+// Tracking and sampling are FP32; tallies and the collision estimator are
+// FP64.  Batches of histories score into separate scratch grids that a
+// fold kernel turns into the batch statistics of VoxelGrid.end_batch
+// (tally.py:59-94).
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <string.h>
+#include <math.h>
+
+#include <algorithm>
+#include <cstdlib>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "philox.cuh"
+#include "../../include/chatcarlo_b200.h"
+
+namespace cc {
+
+constexpr int MAX_PRIMS = 64;
+constexpr int MAX_MATS = 16;
+constexpr int MAX_ELEMS_PER_MAT = 16;
+constexpr int MAX_ELEMS = 48;
+constexpr int TABLE_N = 2000;            // F, A, S tables (materials.py:376-496)
+constexpr int N_BUCKETS = 4096;          // uniform log-E index per material
+constexpr int MAX_SCRATCH = 64;          // batches per launch
+constexpr float LOG_E_MIN = 0.0f;        // ln(1 keV)
+constexpr float E_MIN_KEV = 1.0f;
+constexpr float E_MAX_KEV = 150.0f;
+constexpr float HC = 12.3984193f;        // keV Angstrom (physics.py:35)
+constexpr float MEC2 = 511.0f;           // keV (physics.py:34)
+constexpr float FLUOR_CUTOFF = 5.0f;     // keV (physics.py:38)
+constexpr float TWO_PI = 6.283185307179586f;
+
+// status bits
+constexpr unsigned ST_ENERGY = 1u, ST_RAYLEIGH_Q = 2u, ST_STEPS = 4u, ST_BOUNDS = 8u;
+
+struct DevPrim {
+    int type, material, axis, pad;
+    float c[3];
+    float h[3];     // box half sizes
+    float r2;       // radius^2
+    float hh;       // cylinder half height
+};
+
+struct DevMaterial {
+    float density;
+    int n_nodes, n_el, node_off;
+    int elem_off, muen_off, n_muen, bucket_off;
+    float bucket_scale;
+    int el_slot[MAX_ELEMS_PER_MAT];
+};
+
+struct DevElement {
+    float k_edge, k_prob, omega;
+    int n_lines, emits, pad;
+    float line_e[8];
+    float line_cum[8];
+};
+
+struct KTables {
+    const float* node_loge;
+    const float4* node_parts;
+    const float* elem_log;
+    const int* bucket;
+    const DevMaterial* mats;
+    const DevElement* elems;
+    const float* sq;       // [n_elem][TABLE_N] S/Z
+    const float* rx;       // [n_elem][TABLE_N]
+    const float* ra;       // [n_elem][TABLE_N]
+    const float* muen_x;
+    const float* muen_y;
+    const float* muen_d;
+    const float* h10_x;
+    const float* h10_y;
+    int n_mat, n_elem, n_h10;
+    float h10_lx_lo, h10_lx_hi;
+};
+
+struct KScene {
+    DevPrim prims[MAX_PRIMS];
+    int n_prims, background;
+    float wlo[3], whi[3];
+    float eps;        // geometric tolerance (cm) matched to the world's FP32 resolution
+};
+
+struct KGrid {
+    double* tally;          // [n_scratch][nvox] double2 (kerma, h10)
+    float o[3];
+    float h, inv_h;
+    int nx, ny, nz;
+    long long nvox;
+    int enabled;
+};
+
+struct KSource {
+    int field, rotation, rot_axis, n_angles;
+    float pos[3], dir[3], u[3], v[3];
+    float sid, su, sv, cos_half;
+    float iso[3];
+    float scan;
+    int n_e;
+    const float* e;          // energies
+    const float* alias_p;    // alias table
+    const int* alias_i;
+};
+
+struct KRun {
+    long long n;              // histories in this launch
+    long long first;          // global index of the first history
+    long long batch_size;     // histories per scratch buffer
+    int n_scratch;
+    int fluorescence;
+    unsigned long long seed;
+    long long max_steps;
+    // photon arrays (transport_photons mode)
+    double* pos;
+    double* dir;
+    double* energy;
+    int* n_scatter;
+    unsigned char* absorbed;
+    unsigned char* escaped;
+    // reductions
+    double* edep;             // [n_scratch][n_mat]
+    unsigned long long* counters;   // absorbed, escaped, scatter_sum, n_fluor, steps
+    unsigned long long* work;       // global history counter
+    unsigned* status;
+};
+
+// ---------------------------------------------------------------------------
+// geometry
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ float fmin3(float a, float b, float c) { return fminf(a, fminf(b, c)); }
+__device__ __forceinline__ float fmax3(float a, float b, float c) { return fmaxf(a, fmaxf(b, c)); }
+
+__device__ __forceinline__ bool contains(const DevPrim& g, float x, float y, float z) {
+    float dx = x - g.c[0], dy = y - g.c[1], dz = z - g.c[2];
+    if (g.type == CC_SHAPE_BOX) {
+        return fabsf(dx) <= g.h[0] && fabsf(dy) <= g.h[1] && fabsf(dz) <= g.h[2];
+    } else if (g.type == CC_SHAPE_SPHERE) {
+        return dx * dx + dy * dy + dz * dz <= g.r2;
+    } else {
+        float a, b, w;
+        if (g.axis == 0) { a = dy; b = dz; w = dx; }
+        else if (g.axis == 1) { a = dx; b = dz; w = dy; }
+        else { a = dx; b = dy; w = dz; }
+        return a * a + b * b <= g.r2 && fabsf(w) <= g.hh;
+    }
+}
+
+__device__ __forceinline__ int locate(const KScene& s, float x, float y, float z) {
+    int m = s.background;
+    for (int i = 0; i < s.n_prims; ++i)
+        if (contains(s.prims[i], x, y, z)) m = s.prims[i].material;
+    return m;
+}
+
+// Smallest root t > eps of primitive g along the ray, or +inf.
+__device__ __forceinline__ float slab_pair(float o, float d, float lo, float hi, float& tmin, float& tmax) {
+    // returns 0 when the ray misses the slab entirely (parallel and outside)
+    if (fabsf(d) < 1e-12f) {
+        if (o < lo || o > hi) return 0.0f;
+        return 1.0f;
+    }
+    float inv = 1.0f / d;
+    float ta = (lo - o) * inv, tb = (hi - o) * inv;
+    tmin = fmaxf(tmin, fminf(ta, tb));
+    tmax = fminf(tmax, fmaxf(ta, tb));
+    return 1.0f;
+}
+
+__device__ __forceinline__ void take_root(float t, float eps, float& best) {
+    if (t > eps && t < best) best = t;
+}
+
+__device__ float prim_next(const DevPrim& g, const float p[3], const float d[3], float eps, float best) {
+    float ox = p[0] - g.c[0], oy = p[1] - g.c[1], oz = p[2] - g.c[2];
+    if (g.type == CC_SHAPE_BOX) {
+        float tmin = -INFINITY, tmax = INFINITY;
+        if (slab_pair(ox, d[0], -g.h[0], g.h[0], tmin, tmax) == 0.0f) return best;
+        if (slab_pair(oy, d[1], -g.h[1], g.h[1], tmin, tmax) == 0.0f) return best;
+        if (slab_pair(oz, d[2], -g.h[2], g.h[2], tmin, tmax) == 0.0f) return best;
+        if (tmin <= tmax) { take_root(tmin, eps, best); take_root(tmax, eps, best); }
+        return best;
+    } else if (g.type == CC_SHAPE_SPHERE) {
+        float b = ox * d[0] + oy * d[1] + oz * d[2];
+        // squared distance of the line from the centre, computed without cancellation
+        float qx = ox - b * d[0], qy = oy - b * d[1], qz = oz - b * d[2];
+        float disc = g.r2 - (qx * qx + qy * qy + qz * qz);
+        if (disc < 0.0f) return best;
+        float sq = sqrtf(disc);
+        float c = ox * ox + oy * oy + oz * oz - g.r2;
+        float q = -(b + copysignf(sq, b));
+        float t1 = q, t2 = (q != 0.0f) ? c / q : 0.0f;
+        take_root(t1, eps, best);
+        take_root(t2, eps, best);
+        return best;
+    } else {
+        float ax, ay, aw, dx, dy, dw;
+        if (g.axis == 0) { ax = oy; ay = oz; aw = ox; dx = d[1]; dy = d[2]; dw = d[0]; }
+        else if (g.axis == 1) { ax = ox; ay = oz; aw = oy; dx = d[0]; dy = d[2]; dw = d[1]; }
+        else { ax = ox; ay = oy; aw = oz; dx = d[0]; dy = d[1]; dw = d[2]; }
+        float a = dx * dx + dy * dy;
+        float cc = ax * ax + ay * ay - g.r2;
+        float tmin, tmax;
+        if (a < 1e-12f) {
+            if (cc > 0.0f) return best;        // parallel to the axis, outside the radius
+            tmin = -INFINITY; tmax = INFINITY;
+        } else {
+            float b = ax * dx + ay * dy;
+            float inva = 1.0f / a;
+            float ex = ax - b * inva * dx, ey = ay - b * inva * dy;
+            float disc = (g.r2 - (ex * ex + ey * ey)) * a;   // b^2 - a c without cancellation
+            if (disc < 0.0f) return best;
+            float sq = sqrtf(disc);
+            float q = -(b + copysignf(sq, b));
+            float r1 = q * inva, r2 = (q != 0.0f) ? cc / q : 0.0f;
+            tmin = fminf(r1, r2); tmax = fmaxf(r1, r2);
+        }
+        if (slab_pair(aw, dw, -g.hh, g.hh, tmin, tmax) == 0.0f) return best;
+        if (tmin <= tmax) { take_root(tmin, eps, best); take_root(tmax, eps, best); }
+        return best;
+    }
+}
+
+// Distance to the world-box exit.
+__device__ __forceinline__ float world_exit(const KScene& s, const float p[3], const float d[3]) {
+    float t = INFINITY;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        if (d[k] > 1e-12f) t = fminf(t, (s.whi[k] - p[k]) / d[k]);
+        else if (d[k] < -1e-12f) t = fminf(t, (s.wlo[k] - p[k]) / d[k]);
+    }
+    return fmaxf(t, 0.0f);
+}
+
+// ---------------------------------------------------------------------------
+// tables
+// ---------------------------------------------------------------------------
+
+struct Lookup { int idx; float frac; };
+
+__device__ __forceinline__ Lookup energy_index(const KTables& T, const DevMaterial& m, float loge) {
+    int b = (int)(loge * m.bucket_scale);
+    b = max(0, min(N_BUCKETS - 1, b));
+    int i = __ldg(T.bucket + m.bucket_off + b);       // last node with log E <= bucket start
+    const float* x = T.node_loge + m.node_off;
+    int last = m.n_nodes - 2;
+    while (i < last && __ldg(x + i + 1) < loge) ++i;
+    float x0 = __ldg(x + i), x1 = __ldg(x + i + 1);
+    Lookup L;
+    L.idx = i;
+    L.frac = (loge - x0) / (x1 - x0);
+    return L;
+}
+
+__device__ __forceinline__ float mu_total(const KTables& T, const DevMaterial& m, const Lookup& L) {
+    float4 a = __ldg(T.node_parts + m.node_off + L.idx);
+    float4 b = __ldg(T.node_parts + m.node_off + L.idx + 1);
+    return m.density * __expf(a.w + L.frac * (b.w - a.w));
+}
+
+__device__ __forceinline__ void parts(const KTables& T, const DevMaterial& m, const Lookup& L,
+                                      float& ph, float& co, float& ra) {
+    float4 a = __ldg(T.node_parts + m.node_off + L.idx);
+    float4 b = __ldg(T.node_parts + m.node_off + L.idx + 1);
+    ph = __expf(a.x + L.frac * (b.x - a.x));
+    co = __expf(a.y + L.frac * (b.y - a.y));
+    ra = __expf(a.z + L.frac * (b.z - a.z));
+}
+
+// Element of the material that takes the interaction of kind k (0 photo,
+// 1 Compton, 2 Rayleigh), chosen with probability w_i sigma_i / sum
+// (physics.py:78-92, 138-152, 223-236).  Returns the element slot.
+__device__ int pick_element(const KTables& T, const DevMaterial& m, const Lookup& L, int k, float r) {
+    if (m.n_el == 1) return m.el_slot[0];
+    float w[MAX_ELEMS_PER_MAT];
+    float tot = 0.0f;
+    for (int i = 0; i < m.n_el; ++i) {
+        const float* y = T.elem_log + m.elem_off + (size_t)(i * 3 + k) * m.n_nodes;
+        float y0 = __ldg(y + L.idx), y1 = __ldg(y + L.idx + 1);
+        w[i] = __expf(y0 + L.frac * (y1 - y0));
+        tot += w[i];
+    }
+    float target = r * tot, acc = 0.0f;
+    for (int i = 0; i < m.n_el - 1; ++i) {
+        acc += w[i];
+        if (target <= acc) return m.el_slot[i];
+    }
+    return m.el_slot[m.n_el - 1];
+}
+
+// mu_en/rho by log-log cubic Hermite with the PCHIP node slopes (materials.py:310-335).
+__device__ float muen_rho(const KTables& T, const DevMaterial& m, float loge) {
+    const float* x = T.muen_x + m.muen_off;
+    const float* y = T.muen_y + m.muen_off;
+    const float* dd = T.muen_d + m.muen_off;
+    int lo = 0, hi = m.n_muen - 1;
+    while (hi - lo > 1) {
+        int mid = (lo + hi) >> 1;
+        if (__ldg(x + mid) <= loge) lo = mid; else hi = mid;
+    }
+    float x0 = __ldg(x + lo), x1 = __ldg(x + lo + 1);
+    float hgt = x1 - x0;
+    float t = (loge - x0) / hgt;
+    float y0 = __ldg(y + lo), y1 = __ldg(y + lo + 1);
+    float d0 = __ldg(dd + lo), d1 = __ldg(dd + lo + 1);
+    float t2 = t * t, t3 = t2 * t;
+    float h00 = 2.0f * t3 - 3.0f * t2 + 1.0f, h10 = t3 - 2.0f * t2 + t;
+    float h01 = -2.0f * t3 + 3.0f * t2, h11 = t3 - t2;
+    return __expf(h00 * y0 + h10 * hgt * d0 + h01 * y1 + h11 * hgt * d1);
+}
+
+// h*(10)/Phi: log-log linear, clamped to the table range (dose_coefficients.py:32-42).
+__device__ float h10_coeff(const KTables& T, float loge) {
+    float x = fminf(fmaxf(loge, T.h10_lx_lo), T.h10_lx_hi);
+    int lo = 0, hi = T.n_h10 - 1;
+    while (hi - lo > 1) {
+        int mid = (lo + hi) >> 1;
+        if (__ldg(T.h10_x + mid) <= x) lo = mid; else hi = mid;
+    }
+    float x0 = __ldg(T.h10_x + lo), x1 = __ldg(T.h10_x + lo + 1);
+    float y0 = __ldg(T.h10_y + lo), y1 = __ldg(T.h10_y + lo + 1);
+    return __expf(y0 + (x - x0) / (x1 - x0) * (y1 - y0));
+}
+
+// ---------------------------------------------------------------------------
+// interaction physics
+// ---------------------------------------------------------------------------
+
+// S(Z,q)/Z on q = {0} U linspace(1e-3, 20, 1999) (materials.py:484-496), np.interp.
+__device__ __forceinline__ float s_over_z(const float* s, float q) {
+    const float q1 = 1e-3f;
+    const float dq = (20.0f - 1e-3f) / 1998.0f;
+    if (q <= q1) return __ldg(s + 1) * (q / q1);
+    float u = (q - q1) / dq;
+    int j = (int)u;
+    if (j >= TABLE_N - 2) return __ldg(s + TABLE_N - 1);
+    float f = u - (float)j;
+    float a = __ldg(s + 1 + j), b = __ldg(s + 2 + j);
+    return a + f * (b - a);
+}
+
+// Bound Compton: Kahn-type KN proposal with S(Z,q)/Z rejection (physics.py:41-56, 95-135).
+__device__ void sample_compton(const float* sz, float E, HistoryRng& rng, float& eps_out, float& cos_out) {
+    float alpha = E / MEC2;
+    float emin = 1.0f / (1.0f + 2.0f * alpha);
+    float env = 1.0f / emin + emin;
+    float qscale = E / HC;
+    for (int trial = 0; trial < 100000; ++trial) {
+        float x1 = rng.uniform(), x2 = rng.uniform(), x3 = rng.uniform();
+        float eps = emin + x1 * (1.0f - emin);
+        float c = 1.0f - (1.0f / eps - 1.0f) / alpha;
+        float g = 1.0f / eps + eps - (1.0f - c * c);
+        if (x2 * env > g) continue;
+        float cc = fminf(fmaxf(c, -1.0f), 1.0f);
+        float q = qscale * sqrtf(0.5f * (1.0f - cc));
+        if (x3 <= s_over_z(sz, q)) { eps_out = eps; cos_out = c; return; }
+    }
+    eps_out = 1.0f; cos_out = 1.0f;
+}
+
+// Rayleigh: inverse of A(x) then (1+cos^2)/2 rejection (physics.py:281-351).
+__device__ bool sample_rayleigh(const float* rx, const float* ra, float E, HistoryRng& rng, float& cos_out) {
+    float xmax = (E / HC) * (E / HC);
+    if (xmax > __ldg(rx + TABLE_N - 1)) return false;
+    // A(x_max): x grid is q^2 with q uniform on [0, 20]
+    const float dq = 20.0f / (float)(TABLE_N - 1);
+    int j = (int)(sqrtf(xmax) / dq);
+    j = min(max(j, 0), TABLE_N - 2);
+    while (j > 0 && __ldg(rx + j) > xmax) --j;
+    while (j < TABLE_N - 2 && __ldg(rx + j + 1) < xmax) ++j;
+    float xa = __ldg(rx + j), xb = __ldg(rx + j + 1);
+    float aa = __ldg(ra + j), ab = __ldg(ra + j + 1);
+    float a_cut = aa + (xmax - xa) / (xb - xa) * (ab - aa);
+    int jmax = j + 1;
+    for (int trial = 0; trial < 100000; ++trial) {
+        float target = rng.uniform() * a_cut;
+        int lo = 0, hi = jmax;
+        while (hi - lo > 1) {
+            int mid = (lo + hi) >> 1;
+            if (__ldg(ra + mid) <= target) lo = mid; else hi = mid;
+        }
+        float a0 = __ldg(ra + lo), a1 = __ldg(ra + lo + 1);
+        float x0 = __ldg(rx + lo), x1 = __ldg(rx + lo + 1);
+        float x = (a1 > a0) ? x0 + (target - a0) / (a1 - a0) * (x1 - x0) : x0;
+        x = fminf(x, xmax);
+        float c = fminf(fmaxf(1.0f - 2.0f * x / xmax, -1.0f), 1.0f);
+        if (rng.uniform() <= 0.5f * (1.0f + c * c)) { cos_out = c; return true; }
+    }
+    cos_out = 1.0f;
+    return true;
+}
+
+// New direction from cos(theta) and a uniform azimuth (physics.py:354-367).
+__device__ void scatter_direction(float d[3], float cost, float phi) {
+    float sint = sqrtf(fmaxf(0.0f, 1.0f - cost * cost));
+    float upx, upy, upz;
+    if (fabsf(d[2]) < 0.999f) { upx = 0.f; upy = 0.f; upz = 1.f; } else { upx = 1.f; upy = 0.f; upz = 0.f; }
+    float ux = upy * d[2] - upz * d[1], uy = upz * d[0] - upx * d[2], uz = upx * d[1] - upy * d[0];
+    float inv = rsqrtf(ux * ux + uy * uy + uz * uz);
+    ux *= inv; uy *= inv; uz *= inv;
+    float vx = d[1] * uz - d[2] * uy, vy = d[2] * ux - d[0] * uz, vz = d[0] * uy - d[1] * ux;
+    float sp, cp;
+    __sincosf(phi, &sp, &cp);
+    float a = sint * cp, b = sint * sp;
+    float nx = a * ux + b * vx + cost * d[0];
+    float ny = a * uy + b * vy + cost * d[1];
+    float nz = a * uz + b * vz + cost * d[2];
+    float n = rsqrtf(nx * nx + ny * ny + nz * nz);
+    d[0] = nx * n; d[1] = ny * n; d[2] = nz * n;
+}
+
+__device__ void isotropic(float d[3], HistoryRng& rng) {
+    float c = 2.0f * rng.uniform() - 1.0f;
+    float s = sqrtf(fmaxf(0.0f, 1.0f - c * c));
+    float sp, cp;
+    __sincosf(TWO_PI * rng.uniform(), &sp, &cp);
+    d[0] = s * cp; d[1] = s * sp; d[2] = c;
+}
+
+// ---------------------------------------------------------------------------
+// track-length tally: exact voxel traversal (Amanatides & Woo)
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ void score(double* tally, long long v, double wk, double wh) {
+    atomicAdd(tally + 2 * v, wk);
+    atomicAdd(tally + 2 * v + 1, wh);
+}
+
+__device__ void tally_segment(const KGrid& G, double* tally, const float p[3], const float d[3],
+                              float s, float wk, float wh, unsigned* status) {
+    // clip the segment to the grid box
+    float t0 = 0.0f, t1 = s;
+    float lo[3], hi[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        lo[k] = G.o[k];
+        hi[k] = G.o[k] + G.h * (float)(k == 0 ? G.nx : (k == 1 ? G.ny : G.nz));
+        if (fabsf(d[k]) < 1e-12f) {
+            if (p[k] < lo[k] || p[k] >= hi[k]) return;
+        } else {
+            float inv = 1.0f / d[k];
+            float ta = (lo[k] - p[k]) * inv, tb = (hi[k] - p[k]) * inv;
+            t0 = fmaxf(t0, fminf(ta, tb));
+            t1 = fminf(t1, fmaxf(ta, tb));
+        }
+    }
+    if (!(t1 > t0)) return;
+    int n[3] = {G.nx, G.ny, G.nz};
+    int iv[3], step[3];
+    float tmax[3], tdel[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        // voxel of the clipped entry point; a point that rounds onto the far
+        // side of a face gets a zero-length first cell and steps back in
+        float x = (p[k] + d[k] * t0 - G.o[k]) * G.inv_h;
+        int i = max(0, min(n[k] - 1, (int)floorf(x)));
+        iv[k] = i;
+        if (d[k] > 1e-12f) {
+            step[k] = 1;
+            tmax[k] = (G.o[k] + (float)(i + 1) * G.h - p[k]) / d[k];
+            tdel[k] = G.h / d[k];
+        } else if (d[k] < -1e-12f) {
+            step[k] = -1;
+            tmax[k] = (G.o[k] + (float)i * G.h - p[k]) / d[k];
+            tdel[k] = -G.h / d[k];
+        } else {
+            step[k] = 0;
+            tmax[k] = INFINITY;
+            tdel[k] = INFINITY;
+        }
+    }
+    float t = t0;
+    const double dwk = (double)wk, dwh = (double)wh;
+    int guard = n[0] + n[1] + n[2] + 4;
+    while (t < t1 && guard-- > 0) {
+        int ax = (tmax[0] < tmax[1]) ? (tmax[0] < tmax[2] ? 0 : 2) : (tmax[1] < tmax[2] ? 1 : 2);
+        float tn = fminf(tmax[ax], t1);
+        float len = tn - t;
+        if (len > 0.0f) {
+            long long v = ((long long)iv[0] * G.ny + iv[1]) * G.nz + iv[2];
+            score(tally, v, dwk * len, dwh * len);
+        }
+        t = tn;
+        if (t >= t1) break;
+        iv[ax] += step[ax];
+        if (iv[ax] < 0 || iv[ax] >= n[ax]) break;
+        tmax[ax] += tdel[ax];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// source (source.py:67-210)
+// ---------------------------------------------------------------------------
+
+__device__ void rotate(float v[3], int axis, float ca, float sa) {
+    // Rodrigues rotation about a coordinate axis
+    float a0 = v[0], a1 = v[1], a2 = v[2];
+    if (axis == 0) { v[1] = a1 * ca - a2 * sa; v[2] = a1 * sa + a2 * ca; }
+    else if (axis == 1) { v[0] = a0 * ca + a2 * sa; v[2] = -a0 * sa + a2 * ca; }
+    else { v[0] = a0 * ca - a1 * sa; v[1] = a0 * sa + a1 * ca; }
+}
+
+__device__ void sample_source(const KSource& S, HistoryRng& rng, float p[3], float d[3], float& E) {
+    float pos[3] = {S.pos[0], S.pos[1], S.pos[2]};
+    float dir[3] = {S.dir[0], S.dir[1], S.dir[2]};
+    float u[3] = {S.u[0], S.u[1], S.u[2]};
+    float v[3] = {S.v[0], S.v[1], S.v[2]};
+    if (S.rotation) {
+        float ang;
+        if (S.n_angles > 0) {
+            uint32_t k = (uint32_t)(((uint64_t)rng.next_u32() * (uint64_t)S.n_angles) >> 32);
+            ang = TWO_PI * (float)k / (float)S.n_angles;
+        } else {
+            ang = TWO_PI * (rng.uniform() - 0.5f) + 3.14159265358979f;
+        }
+        float sa, ca;
+        __sincosf(ang, &sa, &ca);
+        float rel[3] = {pos[0] - S.iso[0], pos[1] - S.iso[1], pos[2] - S.iso[2]};
+        rotate(rel, S.rot_axis, ca, sa);
+        rotate(dir, S.rot_axis, ca, sa);
+        rotate(u, S.rot_axis, ca, sa);
+        rotate(v, S.rot_axis, ca, sa);
+        pos[0] = S.iso[0] + rel[0]; pos[1] = S.iso[1] + rel[1]; pos[2] = S.iso[2] + rel[2];
+        if (S.scan > 0.0f) {
+            float shift = S.scan * (rng.uniform() - 0.5f);
+            pos[S.rot_axis] += shift;
+        }
+    }
+    if (S.field == CC_FIELD_CONE) {
+        float c = S.cos_half + (1.0f - S.cos_half) * (1.0f - rng.uniform());
+        float sp, cp;
+        __sincosf(TWO_PI * rng.uniform(), &sp, &cp);
+        float s = sqrtf(fmaxf(0.0f, 1.0f - c * c));
+        for (int k = 0; k < 3; ++k) { p[k] = pos[k]; d[k] = c * dir[k] + s * cp * u[k] + s * sp * v[k]; }
+    } else if (S.field == CC_FIELD_PARALLEL) {
+        float a = S.su * (rng.uniform() - 0.5f), b = S.sv * (rng.uniform() - 0.5f);
+        for (int k = 0; k < 3; ++k) { p[k] = pos[k] + a * u[k] + b * v[k]; d[k] = dir[k]; }
+    } else {
+        float a = S.su * (rng.uniform() - 0.5f), b = S.sv * (rng.uniform() - 0.5f);
+        float t[3];
+        for (int k = 0; k < 3; ++k) t[k] = dir[k] * S.sid + a * u[k] + b * v[k];
+        float inv = rsqrtf(t[0] * t[0] + t[1] * t[1] + t[2] * t[2]);
+        for (int k = 0; k < 3; ++k) { p[k] = pos[k]; d[k] = t[k] * inv; }
+    }
+    // discrete spectrum by Walker's alias method
+    float r = rng.uniform() * (float)S.n_e;
+    int i = min((int)r, S.n_e - 1);
+    float f = r - (float)i;
+    int pick = (f <= __ldg(S.alias_p + i)) ? i : __ldg(S.alias_i + i);
+    E = __ldg(S.e + pick);
+}
+
+// ---------------------------------------------------------------------------
+// the transport kernel
+// ---------------------------------------------------------------------------
+
+constexpr int HIST_CHUNK = 256;     // histories a warp takes from the global counter at once
+
+template <bool FROM_SOURCE, bool TALLY>
+__global__ void __launch_bounds__(256)
+transport_kernel(const KTables T, const KScene S, const KGrid G, const KSource SRC, const KRun R) {
+    extern __shared__ double s_edep[];             // [n_scratch][n_mat]
+    __shared__ unsigned long long s_cnt[5];
+    const int n_acc = R.n_scratch * T.n_mat;
+    for (int i = threadIdx.x; i < n_acc; i += blockDim.x) s_edep[i] = 0.0;
+    if (threadIdx.x < 5) s_cnt[threadIdx.x] = 0ull;
+    __syncthreads();
+
+    const int lane = threadIdx.x & 31;
+    unsigned long long c_abs = 0, c_esc = 0, c_sc = 0, c_fl = 0, c_steps = 0;
+
+    // warp-local pool [pool_next, pool_end)
+    long long pool_next = 0, pool_end = 0;
+    bool live = false;
+    long long h = 0;
+    float p[3], d[3], E = 0.f, tau = 0.f;
+    int nsc = 0, mat = -1, batch = 0;
+    long long steps = 0;
+    HistoryRng rng;
+
+    while (true) {
+        // ---- regeneration: lanes without a photon take the next history ----
+        unsigned need = __ballot_sync(0xffffffffu, !live);
+        while (need) {
+            if (pool_next >= pool_end) {
+                long long base = 0;
+                if (lane == 0) base = (long long)atomicAdd(R.work, (unsigned long long)HIST_CHUNK);
+                base = __shfl_sync(0xffffffffu, base, 0);
+                if (base >= R.n) break;
+                pool_next = base;
+                pool_end = min(base + HIST_CHUNK, R.n);
+            }
+            int rank = __popc(need & ((1u << lane) - 1u));
+            long long avail = pool_end - pool_next;
+            int take = (int)min((long long)__popc(need), avail);
+            if (!live && rank < take) {
+                h = pool_next + rank;
+                live = true;
+                long long gh = R.first + h;
+                rng.init(R.seed, (unsigned long long)gh, 0u);
+                batch = (int)(h / R.batch_size);
+                if (batch >= R.n_scratch) batch = R.n_scratch - 1;
+                if (FROM_SOURCE) {
+                    sample_source(SRC, rng, p, d, E);
+                } else {
+                    for (int k = 0; k < 3; ++k) {
+                        p[k] = (float)R.pos[3 * h + k];
+                        d[k] = (float)R.dir[3 * h + k];
+                    }
+                    E = (float)R.energy[h];
+                }
+                tau = -__logf(rng.uniform());
+                nsc = 0;
+                mat = -1;
+                steps = 0;
+            }
+            pool_next += take;
+            need = __ballot_sync(0xffffffffu, !live);
+        }
+        if (__all_sync(0xffffffffu, !live)) break;
+        if (!live) continue;
+
+        // ---- one step ----
+        ++steps;
+        if (mat < 0) {
+            mat = locate(S, p[0] + d[0] * S.eps, p[1] + d[1] * S.eps, p[2] + d[2] * S.eps);
+        }
+        if (mat >= T.n_mat) {
+            atomicOr(R.status, ST_BOUNDS);
+            live = false;
+            continue;
+        }
+        const DevMaterial& M = T.mats[mat];
+        if (!(E >= E_MIN_KEV && E <= E_MAX_KEV)) {
+            atomicOr(R.status, ST_ENERGY);
+            live = false;
+            continue;
+        }
+        float loge = __logf(E);
+        Lookup L = energy_index(T, M, loge);
+        float mu = mu_total(T, M, L);
+
+        float tb = INFINITY;
+        for (int i = 0; i < S.n_prims; ++i) tb = prim_next(S.prims[i], p, d, S.eps, tb);
+        float tw = world_exit(S, p, d);
+        bool escape = tw <= tb;
+        tb = fminf(tb, tw);
+        float tau_b = mu * tb;
+        bool interact = tau < tau_b;
+        float s = interact ? tau / fmaxf(mu, 1e-30f) : tb;
+
+        if (TALLY) {
+            float wk = E * muen_rho(T, M, loge) * M.density;
+            float wh = h10_coeff(T, loge);
+            tally_segment(G, G.tally + (size_t)batch * 2 * G.nvox, p, d, s, wk, wh, R.status);
+        }
+        p[0] += d[0] * s; p[1] += d[1] * s; p[2] += d[2] * s;
+
+        bool done = false;
+        bool esc = false, absd = false;
+        if (!interact) {
+            tau -= tau_b;
+            if (escape) { esc = true; done = true; }
+            mat = -1;                      // re-locate after the crossing
+        } else {
+            float ph, co, ra;
+            parts(T, M, L, ph, co, ra);
+            float tot = ph + co + ra;
+            float r = rng.uniform() * tot;
+            ++nsc;
+            if (r < ph) {
+                // photoelectric, K fluorescence (physics.py:155-212, transport.py:174-198)
+                int slot = pick_element(T, M, L, 0, rng.uniform());
+                const DevElement& el = T.elems[slot];
+                float e_line = 0.0f;
+                bool emit = false;
+                if (R.fluorescence && el.emits && E > el.k_edge) {
+                    bool is_k = rng.uniform() < el.k_prob;
+                    bool is_rad = rng.uniform() < el.omega;
+                    if (is_k && is_rad) {
+                        float rl = rng.uniform();
+                        int li = el.n_lines - 1;
+                        for (int k = 0; k < el.n_lines; ++k) if (rl <= el.line_cum[k]) { li = k; break; }
+                        if (el.line_e[li] >= FLUOR_CUTOFF) { emit = true; e_line = el.line_e[li]; }
+                    }
+                }
+                atomicAdd(&s_edep[batch * T.n_mat + mat], (double)(emit ? E - e_line : E));
+                if (emit) {
+                    ++c_fl;
+                    E = e_line;
+                    isotropic(d, rng);
+                    tau = -__logf(rng.uniform());
+                } else {
+                    absd = true;
+                    done = true;
+                }
+            } else if (r < ph + co) {
+                int slot = pick_element(T, M, L, 1, rng.uniform());
+                float eps, cost;
+                sample_compton(T.sq + (size_t)slot * TABLE_N, E, rng, eps, cost);
+                float e_new = E * eps;
+                atomicAdd(&s_edep[batch * T.n_mat + mat], (double)(E - e_new));
+                scatter_direction(d, cost, TWO_PI * rng.uniform());
+                E = e_new;
+                tau = -__logf(rng.uniform());
+            } else {
+                int slot = pick_element(T, M, L, 2, rng.uniform());
+                float cost;
+                if (!sample_rayleigh(T.rx + (size_t)slot * TABLE_N, T.ra + (size_t)slot * TABLE_N, E, rng, cost)) {
+                    atomicOr(R.status, ST_RAYLEIGH_Q);
+                    live = false;
+                    continue;
+                }
+                scatter_direction(d, cost, TWO_PI * rng.uniform());
+                tau = -__logf(rng.uniform());
+            }
+            // the interaction point stays inside the same material
+        }
+        if (!done && steps >= R.max_steps) {
+            atomicOr(R.status, ST_STEPS);
+            done = true;
+        }
+        if (done) {
+            c_steps += steps;
+            c_sc += nsc;
+            if (esc) ++c_esc;
+            if (absd) ++c_abs;
+            if (!FROM_SOURCE) {
+                for (int k = 0; k < 3; ++k) {
+                    R.pos[3 * h + k] = (double)p[k] + (esc ? (double)d[k] * 1e-6 : 0.0);
+                    R.dir[3 * h + k] = (double)d[k];
+                }
+                R.energy[h] = (double)E;
+                if (R.n_scatter) R.n_scatter[h] = nsc;
+                if (R.absorbed) R.absorbed[h] = absd ? 1 : 0;
+                if (R.escaped) R.escaped[h] = esc ? 1 : 0;
+            }
+            live = false;
+        }
+    }
+    // ---- reductions ----
+    atomicAdd(&s_cnt[0], c_abs);
+    atomicAdd(&s_cnt[1], c_esc);
+    atomicAdd(&s_cnt[2], c_sc);
+    atomicAdd(&s_cnt[3], c_fl);
+    atomicAdd(&s_cnt[4], c_steps);
+    __syncthreads();
+    for (int i = threadIdx.x; i < n_acc; i += blockDim.x)
+        if (s_edep[i] != 0.0) atomicAdd(R.edep + i, s_edep[i]);
+    if (threadIdx.x < 5) atomicAdd(R.counters + threadIdx.x, s_cnt[threadIdx.x]);
+}
+
+// Batch statistics fold (tally.py:59-94): T += S, Q += S^2/n_b,
+// n_hit += (S_k != 0 or S_h != 0), S = 0.
+__global__ void fold_kernel(double2* __restrict__ total, double2* __restrict__ q,
+                            int* __restrict__ nhit, double2* __restrict__ scratch,
+                            long long nvox, double inv_nb) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    long long stride = (long long)gridDim.x * blockDim.x;
+    for (; i < nvox; i += stride) {
+        double2 s = scratch[i];
+        if (s.x != 0.0 || s.y != 0.0) {
+            double2 t = total[i];
+            t.x += s.x; t.y += s.y;
+            total[i] = t;
+            double2 qq = q[i];
+            qq.x += s.x * s.x * inv_nb;
+            qq.y += s.y * s.y * inv_nb;
+            q[i] = qq;
+            nhit[i] += 1;
+            scratch[i] = make_double2(0.0, 0.0);
+        }
+    }
+}
+
+__global__ void add_kernel(double2* __restrict__ out, const double2* __restrict__ a,
+                           const double2* __restrict__ b, long long nvox) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    long long stride = (long long)gridDim.x * blockDim.x;
+    for (; i < nvox; i += stride) {
+        double2 x = a[i];
+        if (b) { double2 y = b[i]; x.x += y.x; x.y += y.y; }
+        out[i] = x;
+    }
+}
+
+__global__ void sample_source_kernel(const KSource SRC, long long n, long long first,
+                                     unsigned long long seed, double* pos, double* dir, double* en) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    HistoryRng rng;
+    rng.init(seed, (unsigned long long)(first + i), 0u);
+    float p[3], d[3], E;
+    sample_source(SRC, rng, p, d, E);
+    for (int k = 0; k < 3; ++k) { pos[3 * i + k] = p[k]; dir[3 * i + k] = d[k]; }
+    en[i] = E;
+}
+
+}  // namespace cc
+
+// ===========================================================================
+// host side: objects and the C ABI
+// ===========================================================================
+
+using namespace cc;
+
+static thread_local std::string g_last_error;
+
+static int set_error(int code, const std::string& msg) {
+    g_last_error = msg;
+    return code;
+}
+
+#define CC_CUDA(call)                                                                 \
+    do {                                                                              \
+        cudaError_t _e = (call);                                                      \
+        if (_e != cudaSuccess)                                                        \
+            return set_error(CC_E_DEVICE, std::string(#call ": ") + cudaGetErrorString(_e)); \
+    } while (0)
+
+struct cc_ctx {
+    int device = 0;
+    int sm_count = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    unsigned* d_status = nullptr;
+    unsigned long long* d_counters = nullptr;   // [5] + work counter
+    int block = 256;
+    int blocks_per_sm = 0;                       // 0 = occupancy based
+    long long max_steps = 1000000;
+};
+
+struct cc_tables {
+    cc_ctx* ctx;
+    KTables k;
+    std::vector<void*> allocs;
+    int n_mat;
+};
+
+struct cc_scene {
+    cc_ctx* ctx;
+    KScene k;
+};
+
+struct cc_source {
+    cc_ctx* ctx;
+    KSource k;
+    std::vector<void*> allocs;
+};
+
+struct cc_grid {
+    cc_ctx* ctx;
+    KGrid k;
+    int flags;
+    double* d_total = nullptr;      // double2 per voxel
+    double* d_q = nullptr;
+    int* d_nhit = nullptr;
+    double* d_scratch = nullptr;    // [n_scratch][nvox] double2; slot 0 is the pending batch
+    int n_scratch = 0;
+    long long n_batches = 0;
+    long long n_histories = 0;
+};
+
+template <class T>
+static int dev_upload(std::vector<void*>& allocs, const std::vector<T>& v, const T** out) {
+    void* p = nullptr;
+    size_t bytes = std::max<size_t>(v.size() * sizeof(T), 16);
+    CC_CUDA(cudaMalloc(&p, bytes));
+    allocs.push_back(p);
+    if (!v.empty()) CC_CUDA(cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+    *out = (const T*)p;
+    return CC_OK;
+}
+
+template <bool FS, bool TL>
+static cudaError_t launch_transport(cc_ctx* c, const KTables& T, const KScene& S, const KGrid& G,
+                                    const KSource& SRC, const KRun& R, size_t smem, int grid_blocks) {
+    transport_kernel<FS, TL><<<grid_blocks, c->block, smem, c->stream>>>(T, S, G, SRC, R);
+    return cudaGetLastError();
+}
+
+extern "C" {
+
+int cc_version(void) { return CC_ABI_VERSION; }
+
+const char* cc_last_error(void) { return g_last_error.c_str(); }
+
+int cc_ctx_create(int device, cc_ctx** out) {
+    if (!out) return set_error(CC_E_INVALID, "out is NULL");
+    cc_ctx* c = new (std::nothrow) cc_ctx();
+    if (!c) return set_error(CC_E_NOMEM, "out of host memory");
+    c->device = device;
+    CC_CUDA(cudaSetDevice(device));
+    CC_CUDA(cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device));
+    CC_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    CC_CUDA(cudaEventCreate(&c->ev0));
+    CC_CUDA(cudaEventCreate(&c->ev1));
+    CC_CUDA(cudaMalloc(&c->d_status, sizeof(unsigned)));
+    CC_CUDA(cudaMalloc(&c->d_counters, 8 * sizeof(unsigned long long)));
+    *out = c;
+    return CC_OK;
+}
+
+int cc_ctx_destroy(cc_ctx* c) {
+    if (!c) return CC_OK;
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    cudaFree(c->d_status);
+    cudaFree(c->d_counters);
+    cudaEventDestroy(c->ev0);
+    cudaEventDestroy(c->ev1);
+    cudaStreamDestroy(c->stream);
+    delete c;
+    return CC_OK;
+}
+
+int cc_ctx_set_launch(cc_ctx* c, int block_size, int blocks_per_sm) {
+    if (!c) return set_error(CC_E_INVALID, "ctx is NULL");
+    if (block_size != 0 && (block_size % 32 != 0 || block_size > 256 || block_size < 32))
+        return set_error(CC_E_INVALID, "block_size must be a multiple of 32 in [32, 256]");
+    if (blocks_per_sm < 0 || blocks_per_sm > 64) return set_error(CC_E_INVALID, "blocks_per_sm out of range");
+    c->block = block_size ? block_size : 256;
+    c->blocks_per_sm = blocks_per_sm;
+    return CC_OK;
+}
+
+int cc_ctx_set_step_limit(cc_ctx* c, int64_t max_steps) {
+    if (!c || max_steps <= 0) return set_error(CC_E_INVALID, "invalid step limit");
+    c->max_steps = max_steps;
+    return CC_OK;
+}
+
+// ---------------------------------------------------------------------------
+
+int cc_tables_create(cc_ctx* ctx, const cc_table_desc* desc, cc_tables** out) {
+    if (!ctx || !desc || !out) return set_error(CC_E_INVALID, "NULL argument");
+    if (desc->n_materials < 1 || desc->n_materials > MAX_MATS)
+        return set_error(CC_E_INVALID, "n_materials must be in [1, 16]");
+    if (desc->n_elements < 1 || desc->n_elements > MAX_ELEMS)
+        return set_error(CC_E_INVALID, "n_elements must be in [1, 48]");
+    if (desc->n_h10 < 2) return set_error(CC_E_INVALID, "h10 table needs >= 2 rows");
+    CC_CUDA(cudaSetDevice(ctx->device));
+    std::vector<float> loge, elem_log, mx, my, md;
+    std::vector<float4> nparts;
+    std::vector<int> bucket;
+    std::vector<DevMaterial> mats(desc->n_materials);
+    for (int m = 0; m < desc->n_materials; ++m) {
+        const cc_material_desc& md_ = desc->materials[m];
+        if (md_.n_nodes < 2 || md_.n_elements < 1 || md_.n_elements > MAX_ELEMS_PER_MAT || md_.n_muen < 2)
+            return set_error(CC_E_INVALID, "material " + std::to_string(m) + ": bad sizes");
+        DevMaterial& dm = mats[m];
+        memset(&dm, 0, sizeof(dm));
+        dm.density = (float)md_.density;
+        dm.n_nodes = md_.n_nodes;
+        dm.n_el = md_.n_elements;
+        dm.node_off = (int)loge.size();
+        dm.elem_off = (int)elem_log.size();
+        dm.muen_off = (int)mx.size();
+        dm.n_muen = md_.n_muen;
+        dm.bucket_off = (int)bucket.size();
+        double lmax = log(150.0);
+        dm.bucket_scale = (float)(N_BUCKETS / lmax);
+        for (int i = 0; i < md_.n_nodes; ++i) {
+            if (i > 0 && !(md_.log_e[i] > md_.log_e[i - 1]))
+                return set_error(CC_E_INVALID, "material " + std::to_string(m) + ": log_e not increasing");
+            loge.push_back((float)md_.log_e[i]);
+            const double* q = md_.log_parts + 4 * (size_t)i;
+            nparts.push_back(make_float4((float)q[0], (float)q[1], (float)q[2], (float)q[3]));
+        }
+        // node index per bucket: last node whose float log E <= the bucket start
+        int node = 0;
+        const float* lf = loge.data() + dm.node_off;
+        for (int b = 0; b < N_BUCKETS; ++b) {
+            float start = (float)b / dm.bucket_scale;
+            while (node + 1 < md_.n_nodes - 1 && lf[node + 1] <= start) ++node;
+            bucket.push_back(node);
+        }
+        for (size_t i = 0; i < (size_t)md_.n_elements * 3 * md_.n_nodes; ++i)
+            elem_log.push_back((float)md_.log_elem[i]);
+        for (int e = 0; e < md_.n_elements; ++e) {
+            int slot = md_.element_slot[e];
+            if (slot < 0 || slot >= desc->n_elements)
+                return set_error(CC_E_INVALID, "material element slot out of range");
+            dm.el_slot[e] = slot;
+        }
+        for (int i = 0; i < md_.n_muen; ++i) {
+            mx.push_back((float)md_.muen_log_e[i]);
+            my.push_back((float)md_.muen_log_v[i]);
+            md.push_back((float)md_.muen_slope[i]);
+        }
+    }
+    std::vector<DevElement> els(desc->n_elements);
+    std::vector<float> sq, rx, ra;
+    for (int e = 0; e < desc->n_elements; ++e) {
+        const cc_element_desc& ed = desc->elements[e];
+        if (ed.n_lines < 0 || ed.n_lines > 8) return set_error(CC_E_INVALID, "n_lines must be <= 8");
+        DevElement& de = els[e];
+        memset(&de, 0, sizeof(de));
+        de.k_edge = (float)ed.k_edge_kev;
+        de.k_prob = (float)ed.k_shell_prob;
+        de.omega = (float)ed.omega_k;
+        de.n_lines = ed.n_lines;
+        de.emits = ed.emits && ed.n_lines > 0;
+        double cum = 0.0;
+        for (int k = 0; k < ed.n_lines; ++k) {
+            cum += ed.line_p[k];
+            de.line_e[k] = (float)ed.line_e[k];
+            de.line_cum[k] = (float)cum;
+        }
+        for (int i = 0; i < TABLE_N; ++i) {
+            sq.push_back((float)ed.s_over_z[i]);
+            rx.push_back((float)ed.ray_x[i]);
+            ra.push_back((float)ed.ray_a[i]);
+        }
+    }
+    std::vector<float> hx(desc->n_h10), hy(desc->n_h10);
+    for (int i = 0; i < desc->n_h10; ++i) { hx[i] = (float)desc->h10_log_e[i]; hy[i] = (float)desc->h10_log_v[i]; }
+
+    cc_tables* t = new (std::nothrow) cc_tables();
+    if (!t) return set_error(CC_E_NOMEM, "out of host memory");
+    t->ctx = ctx;
+    t->n_mat = desc->n_materials;
+    KTables& k = t->k;
+    int rc;
+#define UP(vec, field) if ((rc = dev_upload(t->allocs, vec, &k.field)) != CC_OK) { cc_tables_destroy(t); return rc; }
+    UP(loge, node_loge);
+    UP(nparts, node_parts);
+    UP(elem_log, elem_log);
+    UP(bucket, bucket);
+    UP(mats, mats);
+    UP(els, elems);
+    UP(sq, sq);
+    UP(rx, rx);
+    UP(ra, ra);
+    UP(mx, muen_x);
+    UP(my, muen_y);
+    UP(md, muen_d);
+    UP(hx, h10_x);
+    UP(hy, h10_y);
+#undef UP
+    k.n_mat = desc->n_materials;
+    k.n_elem = desc->n_elements;
+    k.n_h10 = desc->n_h10;
+    k.h10_lx_lo = (float)log(desc->h10_e_min);
+    k.h10_lx_hi = (float)log(desc->h10_e_max);
+    *out = t;
+    return CC_OK;
+}
+
+int cc_tables_destroy(cc_tables* t) {
+    if (!t) return CC_OK;
+    cudaSetDevice(t->ctx->device);
+    for (void* p : t->allocs) cudaFree(p);
+    delete t;
+    return CC_OK;
+}
+
+int cc_scene_create(cc_ctx* ctx, const cc_primitive* prims, int32_t n_prims, int32_t background,
+                    const double world_lo[3], const double world_hi[3], cc_scene** out) {
+    if (!ctx || !out || !world_lo || !world_hi || (n_prims > 0 && !prims))
+        return set_error(CC_E_INVALID, "NULL argument");
+    if (n_prims < 0 || n_prims > MAX_PRIMS) return set_error(CC_E_INVALID, "n_prims must be in [0, 64]");
+    if (background < 0 || background >= MAX_MATS) return set_error(CC_E_UNKNOWN_MATERIAL, "background material out of range");
+    cc_scene* s = new (std::nothrow) cc_scene();
+    if (!s) return set_error(CC_E_NOMEM, "out of host memory");
+    s->ctx = ctx;
+    KScene& k = s->k;
+    memset(&k, 0, sizeof(k));
+    k.n_prims = n_prims;
+    k.background = background;
+    double extent = 1.0;
+    for (int a = 0; a < 3; ++a) {
+        k.wlo[a] = (float)world_lo[a];
+        k.whi[a] = (float)world_hi[a];
+        extent = std::max(extent, std::max(fabs(world_lo[a]), fabs(world_hi[a])));
+    }
+    // 8 ulps of the largest world coordinate, and at least the 1e-6 cm of
+    // transport.py:155 / geometry.py:214
+    k.eps = (float)std::max(1e-6, 8.0 * extent * 5.960464477539063e-08);
+    for (int i = 0; i < n_prims; ++i) {
+        const cc_primitive& p = prims[i];
+        DevPrim& g = k.prims[i];
+        if (p.type < 0 || p.type > 2) { delete s; return set_error(CC_E_BAD_SHAPE, "unknown primitive type " + std::to_string(p.type)); }
+        if (p.material < 0 || p.material >= MAX_MATS) { delete s; return set_error(CC_E_UNKNOWN_MATERIAL, "primitive material out of range"); }
+        if (p.type == CC_SHAPE_CYLINDER && (p.axis < 0 || p.axis > 2)) { delete s; return set_error(CC_E_INVALID, "cylinder axis must be 0, 1 or 2"); }
+        g.type = p.type;
+        g.material = p.material;
+        g.axis = p.axis;
+        for (int a = 0; a < 3; ++a) { g.c[a] = (float)p.center[a]; g.h[a] = (float)(0.5 * p.size[a]); }
+        g.r2 = (float)(p.radius * p.radius);
+        g.hh = (float)(0.5 * p.height);
+    }
+    *out = s;
+    return CC_OK;
+}
+
+int cc_scene_destroy(cc_scene* s) {
+    delete s;
+    return CC_OK;
+}
+
+int cc_source_create(cc_ctx* ctx, const cc_source_desc* d, cc_source** out) {
+    if (!ctx || !d || !out) return set_error(CC_E_INVALID, "NULL argument");
+    if (d->n_energies < 1 || !d->energies_kev || !d->weights) return set_error(CC_E_INVALID, "empty spectrum");
+    if (d->field < 0 || d->field > 2) return set_error(CC_E_INVALID, "unknown field shape");
+    CC_CUDA(cudaSetDevice(ctx->device));
+    // Walker alias table built in FP64
+    int n = d->n_energies;
+    double tot = 0.0;
+    for (int i = 0; i < n; ++i) {
+        if (!(d->weights[i] >= 0.0)) return set_error(CC_E_INVALID, "negative spectrum weight");
+        if (!(d->energies_kev[i] >= 1.0 && d->energies_kev[i] <= 150.0))
+            return set_error(CC_E_ENERGY_RANGE, "spectrum energy outside [1, 150] keV");
+        tot += d->weights[i];
+    }
+    if (!(tot > 0.0)) return set_error(CC_E_INVALID, "spectrum weights sum to zero");
+    std::vector<double> q(n);
+    std::vector<int> alias(n);
+    std::vector<int> small, large;
+    for (int i = 0; i < n; ++i) {
+        q[i] = d->weights[i] / tot * n;
+        alias[i] = i;
+        (q[i] < 1.0 ? small : large).push_back(i);
+    }
+    while (!small.empty() && !large.empty()) {
+        int s = small.back(); small.pop_back();
+        int l = large.back();
+        alias[s] = l;
+        q[l] = q[l] + q[s] - 1.0;
+        if (q[l] < 1.0) { large.pop_back(); small.push_back(l); }
+    }
+    for (int i : large) q[i] = 1.0;
+    for (int i : small) q[i] = 1.0;
+    std::vector<float> qf(n), ef(n);
+    for (int i = 0; i < n; ++i) { qf[i] = (float)q[i]; ef[i] = (float)d->energies_kev[i]; }
+    cc_source* s = new (std::nothrow) cc_source();
+    if (!s) return set_error(CC_E_NOMEM, "out of host memory");
+    s->ctx = ctx;
+    KSource& k = s->k;
+    k.field = d->field;
+    k.rotation = d->rotation;
+    k.rot_axis = d->rot_axis;
+    k.n_angles = d->n_angles;
+    for (int a = 0; a < 3; ++a) {
+        k.pos[a] = (float)d->position[a];
+        k.dir[a] = (float)d->direction[a];
+        k.u[a] = (float)d->u[a];
+        k.v[a] = (float)d->v[a];
+        k.iso[a] = (float)d->isocenter[a];
+    }
+    k.sid = (float)d->sid_cm;
+    k.su = (float)d->size_u;
+    k.sv = (float)d->size_v;
+    k.cos_half = (float)d->cos_half_angle;
+    k.scan = (float)d->scan_length_cm;
+    k.n_e = n;
+    int rc;
+    if ((rc = dev_upload(s->allocs, ef, &k.e)) != CC_OK) { cc_source_destroy(s); return rc; }
+    if ((rc = dev_upload(s->allocs, qf, &k.alias_p)) != CC_OK) { cc_source_destroy(s); return rc; }
+    if ((rc = dev_upload(s->allocs, alias, &k.alias_i)) != CC_OK) { cc_source_destroy(s); return rc; }
+    *out = s;
+    return CC_OK;
+}
+
+int cc_source_destroy(cc_source* s) {
+    if (!s) return CC_OK;
+    cudaSetDevice(s->ctx->device);
+    for (void* p : s->allocs) cudaFree(p);
+    delete s;
+    return CC_OK;
+}
+
+static int grid_alloc_scratch(cc_grid* g, int n) {
+    if (g->n_scratch >= n) return CC_OK;
+    double* p = nullptr;
+    size_t bytes = (size_t)n * 2 * g->k.nvox * sizeof(double);
+    CC_CUDA(cudaMalloc(&p, bytes));
+    CC_CUDA(cudaMemsetAsync(p, 0, bytes, g->ctx->stream));
+    if (g->d_scratch) {
+        CC_CUDA(cudaMemcpyAsync(p, g->d_scratch, (size_t)g->n_scratch * 2 * g->k.nvox * sizeof(double),
+                                cudaMemcpyDeviceToDevice, g->ctx->stream));
+        CC_CUDA(cudaStreamSynchronize(g->ctx->stream));
+        cudaFree(g->d_scratch);
+    }
+    g->d_scratch = p;
+    g->n_scratch = n;
+    return CC_OK;
+}
+
+int cc_grid_create(cc_ctx* ctx, const double origin[3], int32_t nx, int32_t ny, int32_t nz,
+                   double voxel_cm, int32_t flags, cc_grid** out) {
+    if (!ctx || !origin || !out) return set_error(CC_E_INVALID, "NULL argument");
+    if (nx < 1 || ny < 1 || nz < 1 || !(voxel_cm > 0.0)) return set_error(CC_E_INVALID, "bad grid shape");
+    CC_CUDA(cudaSetDevice(ctx->device));
+    cc_grid* g = new (std::nothrow) cc_grid();
+    if (!g) return set_error(CC_E_NOMEM, "out of host memory");
+    g->ctx = ctx;
+    g->flags = flags;
+    KGrid& k = g->k;
+    for (int a = 0; a < 3; ++a) k.o[a] = (float)origin[a];
+    k.h = (float)voxel_cm;
+    k.inv_h = (float)(1.0 / voxel_cm);
+    k.nx = nx; k.ny = ny; k.nz = nz;
+    k.nvox = (long long)nx * ny * nz;
+    k.enabled = 1;
+    size_t b2 = (size_t)k.nvox * 2 * sizeof(double);
+    if (cudaMalloc(&g->d_total, b2) != cudaSuccess) { delete g; return set_error(CC_E_NOMEM, "device allocation of the grid failed"); }
+    if (flags & CC_GRID_STATS) {
+        if (cudaMalloc(&g->d_q, b2) != cudaSuccess || cudaMalloc(&g->d_nhit, (size_t)k.nvox * sizeof(int)) != cudaSuccess) {
+            cc_grid_destroy(g);
+            return set_error(CC_E_NOMEM, "device allocation of the statistics grids failed");
+        }
+        int rc = grid_alloc_scratch(g, 1);
+        if (rc != CC_OK) { cc_grid_destroy(g); return rc; }
+    }
+    int rc = cc_grid_reset(g);
+    if (rc != CC_OK) { cc_grid_destroy(g); return rc; }
+    *out = g;
+    return CC_OK;
+}
+
+int cc_grid_destroy(cc_grid* g) {
+    if (!g) return CC_OK;
+    cudaSetDevice(g->ctx->device);
+    cudaFree(g->d_total);
+    cudaFree(g->d_q);
+    cudaFree(g->d_nhit);
+    cudaFree(g->d_scratch);
+    delete g;
+    return CC_OK;
+}
+
+int cc_grid_reset(cc_grid* g) {
+    if (!g) return set_error(CC_E_INVALID, "grid is NULL");
+    cudaStream_t st = g->ctx->stream;
+    size_t b2 = (size_t)g->k.nvox * 2 * sizeof(double);
+    CC_CUDA(cudaMemsetAsync(g->d_total, 0, b2, st));
+    if (g->d_q) CC_CUDA(cudaMemsetAsync(g->d_q, 0, b2, st));
+    if (g->d_nhit) CC_CUDA(cudaMemsetAsync(g->d_nhit, 0, (size_t)g->k.nvox * sizeof(int), st));
+    if (g->d_scratch) CC_CUDA(cudaMemsetAsync(g->d_scratch, 0, (size_t)g->n_scratch * b2, st));
+    CC_CUDA(cudaStreamSynchronize(st));
+    g->n_batches = 0;
+    g->n_histories = 0;
+    return CC_OK;
+}
+
+static int fold_batches(cc_grid* g, int n_slots, const long long* counts) {
+    cc_ctx* c = g->ctx;
+    int threads = 256;
+    int blocks = std::max(1, std::min((int)((g->k.nvox + threads - 1) / threads), c->sm_count * 8));
+    for (int s = 0; s < n_slots; ++s) {
+        if (counts[s] <= 0) continue;
+        fold_kernel<<<blocks, threads, 0, c->stream>>>(
+            (double2*)g->d_total, (double2*)g->d_q, g->d_nhit,
+            (double2*)(g->d_scratch + (size_t)s * 2 * g->k.nvox), g->k.nvox, 1.0 / (double)counts[s]);
+        CC_CUDA(cudaGetLastError());
+        g->n_batches += 1;
+        g->n_histories += counts[s];
+    }
+    return CC_OK;
+}
+
+int cc_grid_end_batch(cc_grid* g, int64_t n_hist) {
+    if (!g) return set_error(CC_E_INVALID, "grid is NULL");
+    if (!(g->flags & CC_GRID_STATS) || n_hist <= 0) return CC_OK;
+    long long cnt = n_hist;
+    int rc = fold_batches(g, 1, &cnt);
+    if (rc != CC_OK) return rc;
+    CC_CUDA(cudaStreamSynchronize(g->ctx->stream));
+    return CC_OK;
+}
+
+int cc_grid_download(cc_grid* g, double* kerma, double* h10, double* k2, double* h2, int32_t* nhit,
+                     int64_t* n_batches, int64_t* n_histories) {
+    if (!g) return set_error(CC_E_INVALID, "grid is NULL");
+    cc_ctx* c = g->ctx;
+    CC_CUDA(cudaSetDevice(c->device));
+    long long nv = g->k.nvox;
+    std::vector<double> buf((size_t)nv * 2);
+    if (kerma || h10) {
+        // totals include a pending (not yet folded) batch, as VoxelGrid.kerma_keV does
+        double* tmp = nullptr;
+        CC_CUDA(cudaMalloc(&tmp, (size_t)nv * 2 * sizeof(double)));
+        int threads = 256;
+        int blocks = std::max(1, std::min((int)((nv + threads - 1) / threads), c->sm_count * 8));
+        add_kernel<<<blocks, threads, 0, c->stream>>>((double2*)tmp, (const double2*)g->d_total,
+                                                      (const double2*)g->d_scratch, nv);
+        cudaError_t e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaMemcpyAsync(buf.data(), tmp, (size_t)nv * 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+        cudaFree(tmp);
+        if (e != cudaSuccess) return set_error(CC_E_DEVICE, std::string("grid download: ") + cudaGetErrorString(e));
+        for (long long i = 0; i < nv; ++i) {
+            if (kerma) kerma[i] = buf[2 * i];
+            if (h10) h10[i] = buf[2 * i + 1];
+        }
+    }
+    if ((k2 || h2) && g->d_q) {
+        CC_CUDA(cudaMemcpyAsync(buf.data(), g->d_q, (size_t)nv * 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+        CC_CUDA(cudaStreamSynchronize(c->stream));
+        for (long long i = 0; i < nv; ++i) {
+            if (k2) k2[i] = buf[2 * i];
+            if (h2) h2[i] = buf[2 * i + 1];
+        }
+    }
+    if (nhit && g->d_nhit) {
+        CC_CUDA(cudaMemcpyAsync(nhit, g->d_nhit, (size_t)nv * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+        CC_CUDA(cudaStreamSynchronize(c->stream));
+    }
+    if (n_batches) *n_batches = g->n_batches;
+    if (n_histories) *n_histories = g->n_histories;
+    return CC_OK;
+}
+
+// ---------------------------------------------------------------------------
+
+static int status_to_error(unsigned st) {
+    if (st & ST_ENERGY) return set_error(CC_E_ENERGY_RANGE, "photon energy left the cross-section table range [1, 150] keV");
+    if (st & ST_RAYLEIGH_Q) return set_error(CC_E_RAYLEIGH_Q_RANGE, "q(E) beyond the Rayleigh form-factor table");
+    if (st & ST_STEPS) return set_error(CC_E_TIMEOUT, "a photon exceeded the step limit");
+    if (st & ST_BOUNDS) return set_error(CC_E_BOUNDS, "an index check failed inside the kernel");
+    return CC_OK;
+}
+
+static int grid_blocks_for(cc_ctx* c, size_t smem, bool fs, bool tl) {
+    int per_sm = c->blocks_per_sm;
+    if (per_sm == 0) {
+        int occ = 0;
+        cudaError_t e;
+        if (fs && tl) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, transport_kernel<true, true>, c->block, smem);
+        else if (fs) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, transport_kernel<true, false>, c->block, smem);
+        else if (tl) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, transport_kernel<false, true>, c->block, smem);
+        else e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, transport_kernel<false, false>, c->block, smem);
+        if (e != cudaSuccess || occ < 1) occ = 1;
+        per_sm = occ;
+    }
+    return c->sm_count * per_sm;
+}
+
+// One launch of the transport kernel plus its reductions.
+static int run_launch(cc_ctx* c, const cc_scene* scene, const cc_tables* tables, const KSource* src,
+                      cc_grid* grid, double* tally_base, int n_slots, long long batch_size,
+                      KRun R, std::vector<double>& edep_slots, unsigned long long* counters_out) {
+    const KTables& T = tables->k;
+    R.n_scratch = n_slots;
+    R.batch_size = batch_size;
+    R.max_steps = c->max_steps;
+    R.status = c->d_status;
+    R.counters = c->d_counters;
+    R.work = c->d_counters + 5;
+    double* d_edep = nullptr;
+    size_t n_acc = (size_t)n_slots * T.n_mat;
+    CC_CUDA(cudaMalloc(&d_edep, n_acc * sizeof(double)));
+    cudaStream_t st = c->stream;
+    cudaMemsetAsync(d_edep, 0, n_acc * sizeof(double), st);
+    cudaMemsetAsync(c->d_counters, 0, 8 * sizeof(unsigned long long), st);
+    cudaMemsetAsync(c->d_status, 0, sizeof(unsigned), st);
+    R.edep = d_edep;
+    KGrid G;
+    memset(&G, 0, sizeof(G));
+    bool tl = grid != nullptr;
+    if (tl) { G = grid->k; G.tally = tally_base; }
+    KSource S;
+    memset(&S, 0, sizeof(S));
+    bool fs = src != nullptr;
+    if (fs) S = *src;
+    size_t smem = n_acc * sizeof(double);
+    if (smem > 48 * 1024) { cudaFree(d_edep); return set_error(CC_E_INVALID, "too many batches x materials per launch"); }
+    int blocks = grid_blocks_for(c, smem, fs, tl);
+    cudaError_t e;
+    if (fs && tl) e = launch_transport<true, true>(c, T, scene->k, G, S, R, smem, blocks);
+    else if (fs) e = launch_transport<true, false>(c, T, scene->k, G, S, R, smem, blocks);
+    else if (tl) e = launch_transport<false, true>(c, T, scene->k, G, S, R, smem, blocks);
+    else e = launch_transport<false, false>(c, T, scene->k, G, S, R, smem, blocks);
+    if (e != cudaSuccess) { cudaFree(d_edep); return set_error(CC_E_DEVICE, std::string("transport launch: ") + cudaGetErrorString(e)); }
+    edep_slots.assign(n_acc, 0.0);
+    unsigned st_h = 0;
+    e = cudaMemcpyAsync(edep_slots.data(), d_edep, n_acc * sizeof(double), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(counters_out, c->d_counters, 5 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&st_h, c->d_status, sizeof(unsigned), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaFree(d_edep);
+    if (e != cudaSuccess) return set_error(CC_E_DEVICE, std::string("transport: ") + cudaGetErrorString(e));
+    return status_to_error(st_h);
+}
+
+static int transport_common(cc_ctx* c, const cc_scene* scene, const cc_tables* tables, cc_grid* grid,
+                            int64_t n, double* d_pos, double* d_dir, double* d_en, uint64_t seed,
+                            uint64_t stream_offset, int32_t fluorescence, int32_t* d_nsc,
+                            uint8_t* d_abs, uint8_t* d_esc, double* edep, int64_t* n_fluor) {
+    KRun R;
+    memset(&R, 0, sizeof(R));
+    R.n = n;
+    R.first = (long long)stream_offset;
+    R.fluorescence = fluorescence;
+    R.seed = seed;
+    R.pos = d_pos; R.dir = d_dir; R.energy = d_en;
+    R.n_scatter = d_nsc; R.absorbed = d_abs; R.escaped = d_esc;
+    double* tally = nullptr;
+    if (grid) tally = (grid->flags & CC_GRID_STATS) ? grid->d_scratch : grid->d_total;
+    std::vector<double> slots;
+    unsigned long long cnt[5] = {0, 0, 0, 0, 0};
+    int rc = run_launch(c, scene, tables, nullptr, grid, tally, 1, std::max<long long>(n, 1), R, slots, cnt);
+    if (rc != CC_OK) return rc;
+    if (edep) for (int m = 0; m < tables->n_mat; ++m) edep[m] += slots[m];
+    if (n_fluor) *n_fluor = (int64_t)cnt[3];
+    return CC_OK;
+}
+
+int cc_transport_photons_device(cc_ctx* c, const cc_scene* scene, const cc_tables* tables, cc_grid* grid,
+                                int64_t n, double* d_pos, double* d_dir, double* d_en, uint64_t seed,
+                                uint64_t stream_offset, int32_t fluorescence, int32_t* d_nsc,
+                                uint8_t* d_abs, uint8_t* d_esc, double* edep, int64_t* n_fluor) {
+    if (!c || !scene || !tables) return set_error(CC_E_INVALID, "NULL argument");
+    if (n < 0) return set_error(CC_E_INVALID, "n < 0");
+    if (n == 0) { if (n_fluor) *n_fluor = 0; return CC_OK; }
+    if (!d_pos || !d_dir || !d_en) return set_error(CC_E_INVALID, "photon arrays are NULL");
+    CC_CUDA(cudaSetDevice(c->device));
+    return transport_common(c, scene, tables, grid, n, d_pos, d_dir, d_en, seed, stream_offset,
+                            fluorescence, d_nsc, d_abs, d_esc, edep, n_fluor);
+}
+
+int cc_transport_photons(cc_ctx* c, const cc_scene* scene, const cc_tables* tables, cc_grid* grid,
+                         int64_t n, double* pos, double* dir, double* energy, uint64_t seed,
+                         uint64_t stream_offset, int32_t fluorescence, int32_t* n_scatter,
+                         uint8_t* absorbed, uint8_t* escaped, double* edep, int64_t* n_fluor) {
+    if (!c || !scene || !tables) return set_error(CC_E_INVALID, "NULL argument");
+    if (n < 0) return set_error(CC_E_INVALID, "n < 0");
+    if (n == 0) { if (n_fluor) *n_fluor = 0; return CC_OK; }
+    if (!pos || !dir || !energy) return set_error(CC_E_INVALID, "photon arrays are NULL");
+    CC_CUDA(cudaSetDevice(c->device));
+    cudaStream_t st = c->stream;
+    size_t b3 = (size_t)n * 3 * sizeof(double), b1 = (size_t)n * sizeof(double);
+    char* buf = nullptr;
+    size_t total = 2 * b3 + b1 + (size_t)n * (sizeof(int32_t) + 2);
+    CC_CUDA(cudaMalloc(&buf, total));
+    double* d_pos = (double*)buf;
+    double* d_dir = (double*)(buf + b3);
+    double* d_en = (double*)(buf + 2 * b3);
+    int32_t* d_nsc = (int32_t*)(buf + 2 * b3 + b1);
+    uint8_t* d_abs = (uint8_t*)(d_nsc + n);
+    uint8_t* d_esc = d_abs + n;
+    cudaError_t e = cudaMemcpyAsync(d_pos, pos, b3, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_dir, dir, b3, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_en, energy, b1, cudaMemcpyHostToDevice, st);
+    if (e != cudaSuccess) { cudaFree(buf); return set_error(CC_E_DEVICE, std::string("upload: ") + cudaGetErrorString(e)); }
+    int rc = transport_common(c, scene, tables, grid, n, d_pos, d_dir, d_en, seed, stream_offset,
+                              fluorescence, n_scatter ? d_nsc : nullptr, absorbed ? d_abs : nullptr,
+                              escaped ? d_esc : nullptr, edep, n_fluor);
+    if (rc == CC_OK) {
+        e = cudaMemcpyAsync(pos, d_pos, b3, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(dir, d_dir, b3, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(energy, d_en, b1, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess && n_scatter) e = cudaMemcpyAsync(n_scatter, d_nsc, (size_t)n * sizeof(int32_t), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess && absorbed) e = cudaMemcpyAsync(absorbed, d_abs, (size_t)n, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess && escaped) e = cudaMemcpyAsync(escaped, d_esc, (size_t)n, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) rc = set_error(CC_E_DEVICE, std::string("download: ") + cudaGetErrorString(e));
+    }
+    cudaFree(buf);
+    return rc;
+}
+
+int cc_run(cc_ctx* c, const cc_scene* scene, const cc_tables* tables, const cc_source* src, cc_grid* grid,
+           int64_t n_hist, int64_t batch_size, uint64_t seed, int64_t first_history, int32_t fluorescence,
+           double* edep, double* edep_sum2, cc_run_out* out) {
+    if (!c || !scene || !tables || !src) return set_error(CC_E_INVALID, "NULL argument");
+    if (n_hist < 0 || batch_size <= 0) return set_error(CC_E_INVALID, "n_histories < 0 or batch_size <= 0");
+    CC_CUDA(cudaSetDevice(c->device));
+    const int n_mat = tables->n_mat;
+    bool stats = grid && (grid->flags & CC_GRID_STATS);
+    // batches per launch: enough histories per launch to hide the tail of
+    // the longest histories, bounded by the scratch memory
+    long long per_launch_target = 1LL << 22;
+    int slots = (int)std::min<long long>(MAX_SCRATCH, std::max<long long>(1, per_launch_target / batch_size));
+    slots = std::min(slots, std::max(1, (int)((48 * 1024) / (sizeof(double) * n_mat))));
+    if (stats) {
+        size_t per = (size_t)grid->k.nvox * 2 * sizeof(double);
+        size_t budget = (size_t)8 << 30;
+        slots = (int)std::max<size_t>(1, std::min<size_t>(slots, budget / per));
+        int rc = grid_alloc_scratch(grid, slots);
+        if (rc != CC_OK) return rc;
+    }
+    long long done = 0;
+    long long launches = 0;
+    unsigned long long tot[5] = {0, 0, 0, 0, 0};
+    float ms_total = 0.0f;
+    while (done < n_hist) {
+        int ns = slots;
+        long long n_launch = std::min<long long>(n_hist - done, (long long)ns * batch_size);
+        ns = (int)((n_launch + batch_size - 1) / batch_size);
+        KRun R;
+        memset(&R, 0, sizeof(R));
+        R.n = n_launch;
+        R.first = first_history + done;
+        R.fluorescence = fluorescence;
+        R.seed = seed;
+        double* tally = nullptr;
+        if (grid) tally = stats ? grid->d_scratch : grid->d_total;
+        std::vector<double> slot_edep;
+        unsigned long long cnt[5];
+        CC_CUDA(cudaEventRecord(c->ev0, c->stream));
+        int rc = run_launch(c, scene, tables, &src->k, grid, tally, stats ? ns : 1,
+                            stats ? batch_size : std::max<long long>(n_launch, 1), R, slot_edep, cnt);
+        if (rc != CC_OK) return rc;
+        ++launches;
+        // per-batch collision-estimator moments (ScalarMoments.add_batch, tally.py:204-213)
+        for (int b = 0; b < ns; ++b) {
+            long long nb = std::min<long long>(batch_size, n_launch - (long long)b * batch_size);
+            for (int m = 0; m < n_mat; ++m) {
+                double v = stats ? slot_edep[(size_t)b * n_mat + m] : (b == 0 ? slot_edep[m] : 0.0);
+                if (edep) edep[m] += v;
+                if (edep_sum2 && stats) edep_sum2[m] += v * v / (double)nb;
+            }
+        }
+        if (stats) {
+            std::vector<long long> counts(ns);
+            for (int b = 0; b < ns; ++b) counts[b] = std::min<long long>(batch_size, n_launch - (long long)b * batch_size);
+            rc = fold_batches(grid, ns, counts.data());
+            if (rc != CC_OK) return rc;
+            launches += ns;
+        }
+        CC_CUDA(cudaEventRecord(c->ev1, c->stream));
+        CC_CUDA(cudaEventSynchronize(c->ev1));
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+        ms_total += ms;
+        for (int k = 0; k < 5; ++k) tot[k] += cnt[k];
+        done += n_launch;
+    }
+    if (out) {
+        out->n_histories = n_hist;
+        out->n_absorbed = (int64_t)tot[0];
+        out->n_escaped = (int64_t)tot[1];
+        out->scatter_sum = (int64_t)tot[2];
+        out->n_fluorescence = (int64_t)tot[3];
+        out->n_batches = (n_hist + batch_size - 1) / batch_size;
+        out->gpu_launches = launches;
+        out->elapsed_ms = ms_total;
+    }
+    return CC_OK;
+}
+
+int cc_sample_source(cc_ctx* c, const cc_source* src, int64_t n, uint64_t seed, int64_t first,
+                     double* pos, double* dir, double* energy) {
+    if (!c || !src || !pos || !dir || !energy) return set_error(CC_E_INVALID, "NULL argument");
+    if (n <= 0) return CC_OK;
+    CC_CUDA(cudaSetDevice(c->device));
+    double* buf = nullptr;
+    CC_CUDA(cudaMalloc(&buf, (size_t)n * 7 * sizeof(double)));
+    int threads = 256;
+    long long blocks = (n + threads - 1) / threads;
+    sample_source_kernel<<<(unsigned)blocks, threads, 0, c->stream>>>(src->k, n, first, seed, buf, buf + 3 * n, buf + 6 * n);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(pos, buf, (size_t)n * 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dir, buf + 3 * n, (size_t)n * 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(energy, buf + 6 * n, (size_t)n * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    cudaFree(buf);
+    if (e != cudaSuccess) return set_error(CC_E_DEVICE, std::string("sample_source: ") + cudaGetErrorString(e));
+    return CC_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,294 @@
+"""The transport entry points, backed by the sm_100a engine.
+
+``transport_photons`` and ``run_transport`` keep the signatures and result
+types of ChatCarlo's NumPy implementation (chatcarlo/transport.py:88-95,
+98-103, 236-254, 358-361).  Every photon is transported by the CUDA engine
+through the C ABI of include/chatcarlo_b200.h; there is no CPU path.  The
+random streams are Philox4x32-10 streams keyed by a 64-bit seed and the
+history index, so results are reproducible for a given seed and
+independent of the launch shape, but not bit-identical to NumPy's PCG64.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _native as N
+from .devtables import TableSet, build_table_set
+from .geometry import Geometry
+from .source import SourceSpec
+from .tally import ScalarMoments, VoxelGrid
+
+
+@dataclass
+class BatchResult:
+    n_scatter: np.ndarray
+    absorbed: np.ndarray
+    escaped: np.ndarray
+    final_energy: np.ndarray
+    energy_deposited: dict = field(default_factory=dict)
+    n_fluorescence: int = 0
+
+
+@dataclass
+class TransportResult:
+    n_histories: int
+    energy_deposited_MeV: dict
+    fraction_absorbed: float
+    fraction_escaped: float
+    mean_scatter_events: float
+    grid: VoxelGrid | None = None
+    n_photons_real: float | None = None
+    n_fluorescence: int = 0
+    n_batches: int = 0
+    energy_deposited_sem_MeV: dict = field(default_factory=dict)
+    energy_deposited_rel_err: dict = field(default_factory=dict)
+    # engine bookkeeping (not in the NumPy result)
+    device_ms: float = 0.0
+    gpu_launches: int = 0
+
+
+class DeviceGrid:
+    """A cc_grid with the geometry of a host VoxelGrid."""
+
+    def __init__(self, engine: "Engine", grid: VoxelGrid, stats: bool):
+        self.engine = engine
+        self.shape = tuple(grid.shape)
+        self.handle = C.c_void_p()
+        origin = np.ascontiguousarray(grid.origin_cm, dtype=float)
+        nx, ny, nz = self.shape
+        N.check(N.lib().cc_grid_create(engine.ctx, N.dptr(origin), nx, ny, nz, float(grid.voxel_size_cm),
+                                       N.CC_GRID_STATS if stats else 0, C.byref(self.handle)))
+        self.stats = stats
+
+    def download(self, grid: VoxelGrid, accumulate: bool = False) -> None:
+        k = np.empty(self.shape)
+        h = np.empty(self.shape)
+        k2 = np.empty(self.shape) if self.stats else None
+        h2 = np.empty(self.shape) if self.stats else None
+        nh = np.empty(self.shape, dtype=np.int32) if self.stats else None
+        nb = C.c_int64()
+        nhist = C.c_int64()
+        N.check(N.lib().cc_grid_download(
+            self.handle, N.dptr(k), N.dptr(h), N.dptr(k2) if k2 is not None else None,
+            N.dptr(h2) if h2 is not None else None,
+            nh.ctypes.data_as(C.POINTER(C.c_int32)) if nh is not None else None,
+            C.byref(nb), C.byref(nhist)))
+        if accumulate:
+            grid.kerma_keV += k
+            grid.h10_track_pSv_cm3 += h
+        else:
+            grid.kerma_keV[...] = k
+            grid.h10_track_pSv_cm3[...] = h
+        if self.stats and grid.track_uncertainty:
+            grid.kerma_sum2[...] = k2
+            grid.h10_sum2[...] = h2
+            grid.n_batches_hit[...] = nh
+            grid.n_batches = int(nb.value)
+            grid.n_histories = int(nhist.value)
+
+    def reset(self):
+        N.check(N.lib().cc_grid_reset(self.handle))
+
+    def close(self):
+        if self.handle:
+            N.lib().cc_grid_destroy(self.handle)
+            self.handle = C.c_void_p()
+
+
+class Engine:
+    """A device context plus cached device tables per material set."""
+
+    def __init__(self, device: int = 0):
+        self.lib = N.lib()
+        self.ctx = C.c_void_p()
+        N.check(self.lib.cc_ctx_create(int(device), C.byref(self.ctx)))
+        self.device = device
+        self._tables: dict = {}
+        self._lock = threading.Lock()
+
+    def set_launch(self, block_size: int = 256, blocks_per_sm: int = 0) -> None:
+        N.check(self.lib.cc_ctx_set_launch(self.ctx, block_size, blocks_per_sm))
+
+    def tables(self, names: list[str], need_muen: bool) -> tuple[TableSet, C.c_void_p]:
+        key = (tuple(names), need_muen)
+        with self._lock:
+            hit = self._tables.get(key)
+            if hit is None:
+                ts = build_table_set(list(names), need_muen=need_muen)
+                h = C.c_void_p()
+                N.check(self.lib.cc_tables_create(self.ctx, C.byref(ts.desc), C.byref(h)))
+                hit = (ts, h)
+                self._tables[key] = hit
+            return hit
+
+    def scene(self, geometry: Geometry, ts: TableSet) -> C.c_void_p:
+        idx = {n: i for i, n in enumerate(ts.names)}
+        prims = geometry.primitives(idx)
+        lo = np.ascontiguousarray(geometry.bbox_min, dtype=float)
+        hi = np.ascontiguousarray(geometry.bbox_max, dtype=float)
+        h = C.c_void_p()
+        N.check(self.lib.cc_scene_create(self.ctx, prims, len(geometry.geoms), idx[geometry.background],
+                                         N.dptr(lo), N.dptr(hi), C.byref(h)))
+        return h
+
+    def source(self, spec: SourceSpec) -> C.c_void_p:
+        h = C.c_void_p()
+        N.check(self.lib.cc_source_create(self.ctx, C.byref(spec.desc), C.byref(h)))
+        return h
+
+    def close(self):
+        for ts, h in self._tables.values():
+            self.lib.cc_tables_destroy(h)
+        self._tables.clear()
+        if self.ctx:
+            self.lib.cc_ctx_destroy(self.ctx)
+            self.ctx = C.c_void_p()
+
+
+_engines: dict = {}
+
+
+def default_engine(device: int | None = None) -> Engine:
+    dev = int(os.environ.get("CHATCARLO_B200_DEVICE", "0")) if device is None else device
+    if dev not in _engines:
+        _engines[dev] = Engine(dev)
+    return _engines[dev]
+
+
+def _seed_from(rng, seed):
+    if seed is not None:
+        return int(seed) & 0xFFFFFFFFFFFFFFFF
+    if rng is not None:
+        return int(rng.integers(0, 2 ** 63))
+    return int.from_bytes(os.urandom(8), "little")
+
+
+def transport_photons(pos: np.ndarray, dirv: np.ndarray, energy: np.ndarray, geometry: Geometry,
+                      rng: np.random.Generator | None = None, grid: VoxelGrid | None = None,
+                      recorder=None, tally_rng=None, fluorescence_enabled: bool = True,
+                      seed: int | None = None, stream_offset: int = 0,
+                      engine: Engine | None = None) -> BatchResult:
+    """Transport the given photons to absorption or escape on the GPU.
+
+    Same contract as chatcarlo/transport.py:98-233: pos/dirv/energy are
+    updated in place with the final state, grid (if given) accumulates the
+    track-length kerma and H*(10) tallies.  The photon streams are keyed by
+    ``seed`` (or one draw of ``rng``).  ``recorder`` (trajectory capture for
+    visualisation) is not supported by the engine.
+    """
+    if recorder is not None:
+        raise NotImplementedError("trajectory recording is not part of the GPU engine")
+    eng = engine or default_engine()
+    n = int(pos.shape[0])
+    names = geometry.materials()
+    ts, th = eng.tables(names, need_muen=grid is not None)
+    sh = eng.scene(geometry, ts)
+    try:
+        p = np.ascontiguousarray(pos, dtype=np.float64)
+        d = np.ascontiguousarray(dirv, dtype=np.float64)
+        e = np.ascontiguousarray(energy, dtype=np.float64)
+        nsc = np.zeros(n, dtype=np.int32)
+        absd = np.zeros(n, dtype=np.uint8)
+        esc = np.zeros(n, dtype=np.uint8)
+        edep = np.zeros(len(names))
+        nfl = C.c_int64(0)
+        dg = None
+        if grid is not None:
+            dg = DeviceGrid(eng, grid, stats=False)
+        try:
+            N.check(eng.lib.cc_transport_photons(
+                eng.ctx, sh, th, dg.handle if dg else None, n, N.dptr(p), N.dptr(d), N.dptr(e),
+                _seed_from(rng, seed), int(stream_offset), int(bool(fluorescence_enabled)),
+                nsc.ctypes.data_as(C.POINTER(C.c_int32)), absd.ctypes.data_as(C.POINTER(C.c_uint8)),
+                esc.ctypes.data_as(C.POINTER(C.c_uint8)), N.dptr(edep), C.byref(nfl)))
+            if dg is not None:
+                dg.download(grid, accumulate=True)
+        finally:
+            if dg is not None:
+                dg.close()
+    finally:
+        eng.lib.cc_scene_destroy(sh)
+    if p is not pos:
+        pos[...] = p
+    if d is not dirv:
+        dirv[...] = d
+    if e is not energy:
+        energy[...] = e
+    dep = {name: float(edep[i]) for i, name in enumerate(names) if edep[i] != 0.0}
+    return BatchResult(n_scatter=nsc.astype(int), absorbed=absd.astype(bool), escaped=esc.astype(bool),
+                       final_energy=energy, energy_deposited=dep, n_fluorescence=int(nfl.value))
+
+
+def run_transport(scene, n_histories: int = 100_000, seed: int | None = None,
+                  batch_size: int = 200_000, dose_grid: bool = False,
+                  grid_resolution_cm: float = 5.0, n_workers: int = 1,
+                  track_uncertainty: bool = True, engine: Engine | None = None,
+                  first_history: int = 0, grid: VoxelGrid | None = None) -> TransportResult:
+    """run_transport (chatcarlo/transport.py:358-474) on the GPU.
+
+    ``n_workers`` is accepted for signature compatibility; the histories run
+    on one device.  The source is sampled on the device, histories are
+    grouped into batches of ``batch_size`` for the batch statistics.
+    """
+    raw = scene.raw if hasattr(scene, "raw") else scene
+    src = raw["source"]
+    if src.get("mas") is not None or src.get("ctdi_vol_mGy") is not None:
+        raise RuntimeError("absolute calibration (mas / ctdi_vol_mGy) needs SpekPy, which is not available")
+    eng = engine or default_engine()
+    geometry = Geometry(raw["geometry"])
+    if dose_grid and grid is None:
+        grid = VoxelGrid.from_bbox(geometry.bbox_min, geometry.bbox_max, grid_resolution_cm,
+                                   track_uncertainty=track_uncertainty)
+    if not dose_grid:
+        grid = None
+    fluorescence = raw.get("physics", {}).get("fluorescence", True)
+    names = geometry.materials()
+    ts, th = eng.tables(names, need_muen=grid is not None)
+    spec = SourceSpec(src)
+    sh = eng.scene(geometry, ts)
+    srch = eng.source(spec)
+    dg = DeviceGrid(eng, grid, stats=track_uncertainty) if grid is not None else None
+    edep = np.zeros(len(names))
+    edep2 = np.zeros(len(names))
+    out = N.RunOut()
+    try:
+        N.check(eng.lib.cc_run(eng.ctx, sh, th, srch, dg.handle if dg else None, int(n_histories),
+                               int(batch_size), _seed_from(None, seed), int(first_history),
+                               int(bool(fluorescence)), N.dptr(edep), N.dptr(edep2), C.byref(out)))
+        if dg is not None:
+            dg.download(grid)
+    finally:
+        if dg is not None:
+            dg.close()
+        eng.lib.cc_source_destroy(srch)
+        eng.lib.cc_scene_destroy(sh)
+    n_batches = int(out.n_batches)
+    dep = {name: float(edep[i]) for i, name in enumerate(names) if edep[i] != 0.0}
+    sem, rel = {}, {}
+    if track_uncertainty:
+        mom = ScalarMoments()
+        mom.add_moments(dep, {name: float(edep2[i]) for i, name in enumerate(names) if edep[i] != 0.0},
+                        n_batches, int(n_histories))
+        sem = {k: v / 1000.0 for k, v in mom.standard_errors().items()}
+        rel = mom.relative_errors()
+    nh = max(int(n_histories), 1)
+    return TransportResult(
+        n_histories=int(n_histories),
+        energy_deposited_MeV={k: v / 1000.0 for k, v in dep.items()},
+        fraction_absorbed=out.n_absorbed / nh,
+        fraction_escaped=out.n_escaped / nh,
+        mean_scatter_events=out.scatter_sum / nh,
+        grid=grid,
+        n_photons_real=None,
+        n_fluorescence=int(out.n_fluorescence),
+        n_batches=n_batches if track_uncertainty else (grid.n_batches if grid is not None else 0),
+        energy_deposited_sem_MeV=sem,
+        energy_deposited_rel_err=rel,
+        device_ms=float(out.elapsed_ms),
+        gpu_launches=int(out.gpu_launches),
+    )

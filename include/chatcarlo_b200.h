@@ -1,0 +1,219 @@
+/*
+ * chatcarlo_b200 -- C ABI of the B200 photon-transport engine.
+ *
+ * The entry points replace the NumPy hot path of ChatCarlo:
+ *   cc_transport_photons  <- chatcarlo/transport.py:98-233  transport_photons(pos, dirv,
+ *                            energy, geometry, rng, grid, recorder, tally_rng,
+ *                            fluorescence_enabled) -> BatchResult
+ *   cc_run                <- chatcarlo/transport.py:257-312,358-474  _run_batches /
+ *                            run_transport(scene, n_histories, seed, batch_size, dose_grid, ...)
+ *   cc_grid_*             <- chatcarlo/tally.py:27-132  VoxelGrid (+ end_batch 59-94)
+ *   cc_scene_create       <- chatcarlo/geometry.py:121-231  Geometry
+ *   cc_tables_create      <- chatcarlo/materials.py:202-496 (element tables, mu_en, S, F, K data)
+ *                            and chatcarlo/dose_coefficients.py:32-42 (h*(10)/fluence)
+ *   cc_source_create      <- chatcarlo/source.py:67-210 and chatcarlo/spectrum.py:73-82
+ *
+ * Conventions: every call returns 0 on success or a negative CC_E_* code;
+ * cc_last_error() gives the message of the calling thread's last failure.
+ * All sizes are explicit; the library copies what it needs to the device
+ * and never keeps a caller pointer after a call returns.  Calls on one
+ * context are synchronous at return.  Lengths in cm, energies in keV.
+ */
+#ifndef CHATCARLO_B200_H
+#define CHATCARLO_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CC_ABI_VERSION 1
+
+/* error codes (mirroring the ValueError cases of the NumPy path) */
+#define CC_OK                   0
+#define CC_E_INVALID          (-1)  /* bad argument */
+#define CC_E_ENERGY_RANGE     (-2)  /* energy outside the cross-section tables: materials.py:234-237 */
+#define CC_E_RAYLEIGH_Q_RANGE (-3)  /* q(E) beyond the form-factor table: physics.py:333-337 */
+#define CC_E_UNKNOWN_MATERIAL (-4)  /* material index outside the table set: materials.py:66-69 */
+#define CC_E_BAD_SHAPE        (-5)  /* unknown primitive type: geometry.py:158 */
+#define CC_E_DEVICE           (-6)  /* CUDA runtime failure */
+#define CC_E_TIMEOUT          (-7)  /* a photon exceeded the step limit */
+#define CC_E_BOUNDS           (-8)  /* an index check failed inside a kernel */
+#define CC_E_NOMEM            (-9)
+
+/* primitive types (scene.py:14 VALID_SHAPES) */
+#define CC_SHAPE_BOX      0
+#define CC_SHAPE_SPHERE   1
+#define CC_SHAPE_CYLINDER 2
+
+/* grid flags */
+#define CC_GRID_STATS 1   /* batch statistics (kerma_sum2, h10_sum2, n_batches_hit) */
+
+/* source field shapes (source.py:151-194) */
+#define CC_FIELD_RECT     0
+#define CC_FIELD_CONE     1
+#define CC_FIELD_PARALLEL 2
+
+typedef struct cc_ctx cc_ctx;
+typedef struct cc_tables cc_tables;
+typedef struct cc_scene cc_scene;
+typedef struct cc_grid cc_grid;
+typedef struct cc_source cc_source;
+
+/* One analytic primitive; list order is kept (a later one overrides an
+ * earlier one where they overlap: geometry.py:205-212). */
+typedef struct {
+    int32_t type;          /* CC_SHAPE_* */
+    int32_t material;      /* index into the material set of cc_tables */
+    int32_t axis;          /* cylinder axis 0=x 1=y 2=z */
+    int32_t pad;
+    double center[3];
+    double size[3];        /* box full edge lengths */
+    double radius;         /* sphere, cylinder */
+    double height;         /* cylinder full length */
+} cc_primitive;
+
+/* Per-material tables.  Energies share one union grid per material. */
+typedef struct {
+    double density;               /* g/cm^3 */
+    int32_t n_nodes;              /* union energy grid */
+    int32_t n_elements;
+    const double* log_e;          /* [n_nodes] ln(E/keV), strictly increasing */
+    const double* log_parts;      /* [n_nodes][4] ln(photo), ln(compt), ln(rayl), ln(sum) of the
+                                     mass-fraction mix, cm^2/g */
+    const double* log_elem;       /* [n_elements][3][n_nodes] ln(w_i * sigma_i) for photo, compt, rayl */
+    const int32_t* element_slot;  /* [n_elements] index into the element table array */
+    int32_t n_muen;               /* NIST rows for mu_en/rho */
+    int32_t pad;
+    const double* muen_log_e;     /* [n_muen] */
+    const double* muen_log_v;     /* [n_muen] ln(mu_en/rho) */
+    const double* muen_slope;     /* [n_muen] PCHIP node slopes in log-log */
+} cc_material_desc;
+
+/* Per-element angular and fluorescence tables. */
+typedef struct {
+    int32_t z;
+    int32_t n_lines;              /* <= 8 */
+    const double* s_over_z;       /* [2000] S(Z,q)/Z on q = {0} U linspace(1e-3, 20, 1999) */
+    const double* ray_x;          /* [2000] x = q^2, q = linspace(0, 20, 2000) */
+    const double* ray_a;          /* [2000] A(x) = int_0^x F^2 dx' */
+    double k_edge_kev;
+    double k_shell_prob;          /* CS_Photo_Partial(K)/CS_Photo above the K edge */
+    double omega_k;
+    double line_e[8];             /* keV */
+    double line_p[8];             /* probabilities, summing to 1 */
+    int32_t emits;                /* 1 when some line reaches the 5 keV cut-off */
+    int32_t pad;
+} cc_element_desc;
+
+typedef struct {
+    int32_t n_materials;
+    int32_t n_elements;
+    const cc_material_desc* materials;
+    const cc_element_desc* elements;
+    int32_t n_h10;
+    int32_t pad;
+    const double* h10_log_e;      /* [n_h10] */
+    const double* h10_log_v;      /* [n_h10] ln(h*(10)/Phi) pSv cm^2 */
+    double h10_e_min, h10_e_max;  /* clamp range keV */
+} cc_table_desc;
+
+/* Point source into a field, with optional CT rotation (source.py:67-210). */
+typedef struct {
+    int32_t field;                /* CC_FIELD_* */
+    int32_t rotation;             /* 0 = none, 1 = rotation about rot_axis */
+    int32_t rot_axis;             /* 0/1/2 */
+    int32_t n_angles;             /* 0 = continuous */
+    double position[3];
+    double direction[3];          /* unit */
+    double u[3], v[3];            /* beam basis (source.py:28-35) */
+    double sid_cm;
+    double size_u, size_v;        /* rect/parallel field edge lengths */
+    double cos_half_angle;        /* cone */
+    double isocenter[3];
+    double scan_length_cm;
+    int32_t n_energies;           /* discrete spectrum */
+    int32_t pad;
+    const double* energies_kev;   /* [n_energies] */
+    const double* weights;        /* [n_energies], not necessarily normalised */
+} cc_source_desc;
+
+typedef struct {
+    int64_t n_histories;
+    int64_t n_absorbed;
+    int64_t n_escaped;
+    int64_t scatter_sum;
+    int64_t n_fluorescence;
+    int64_t n_batches;
+    int64_t gpu_launches;
+    double elapsed_ms;            /* device time of the run (CUDA events) */
+} cc_run_out;
+
+/* -- context and error handling ------------------------------------------ */
+int cc_version(void);
+const char* cc_last_error(void);
+int cc_ctx_create(int device, cc_ctx** out);
+int cc_ctx_destroy(cc_ctx* ctx);
+int cc_ctx_set_launch(cc_ctx* ctx, int block_size, int blocks_per_sm);
+int cc_ctx_set_step_limit(cc_ctx* ctx, int64_t max_steps_per_photon);
+
+/* -- tables, scene, source, grid -------------------------------------------- */
+int cc_tables_create(cc_ctx* ctx, const cc_table_desc* desc, cc_tables** out);
+int cc_tables_destroy(cc_tables* t);
+int cc_scene_create(cc_ctx* ctx, const cc_primitive* prims, int32_t n_prims,
+                    int32_t background_material, const double world_lo[3],
+                    const double world_hi[3], cc_scene** out);
+int cc_scene_destroy(cc_scene* s);
+int cc_source_create(cc_ctx* ctx, const cc_source_desc* desc, cc_source** out);
+int cc_source_destroy(cc_source* s);
+int cc_grid_create(cc_ctx* ctx, const double origin[3], int32_t nx, int32_t ny, int32_t nz,
+                   double voxel_cm, int32_t flags, cc_grid** out);
+int cc_grid_destroy(cc_grid* g);
+int cc_grid_reset(cc_grid* g);
+/* Any output pointer may be NULL.  Arrays are C-ordered (nx, ny, nz). */
+int cc_grid_download(cc_grid* g, double* kerma_keV, double* h10_track_pSv_cm3,
+                     double* kerma_sum2, double* h10_sum2, int32_t* n_batches_hit,
+                     int64_t* n_batches, int64_t* n_histories);
+/* VoxelGrid.end_batch (tally.py:59-94) for photons scored outside cc_run:
+ * folds the batch accumulated since the previous fold. */
+int cc_grid_end_batch(cc_grid* g, int64_t n_histories_in_batch);
+
+/* -- transport ----------------------------------------------------------------
+ * cc_transport_photons: transport_photons() on caller-provided photons.
+ * pos/dir ([n][3]) and energy ([n]) are host arrays, updated in place with the
+ * final state like the NumPy path does.  grid may be NULL.  Per-photon
+ * outputs may be NULL.  edep_by_material has n_materials entries (keV),
+ * accumulated into (not overwritten).  The photons' random streams are
+ * Philox4x32-10 keyed by seed, counter (history index + stream_offset). */
+int cc_transport_photons(cc_ctx* ctx, const cc_scene* scene, const cc_tables* tables,
+                         cc_grid* grid, int64_t n, double* pos, double* dir, double* energy,
+                         uint64_t seed, uint64_t stream_offset, int32_t fluorescence,
+                         int32_t* n_scatter, uint8_t* absorbed, uint8_t* escaped,
+                         double* edep_by_material, int64_t* n_fluorescence);
+
+/* Same on device-resident arrays (pointers into this device's memory). */
+int cc_transport_photons_device(cc_ctx* ctx, const cc_scene* scene, const cc_tables* tables,
+                                cc_grid* grid, int64_t n, double* d_pos, double* d_dir,
+                                double* d_energy, uint64_t seed, uint64_t stream_offset,
+                                int32_t fluorescence, int32_t* d_n_scatter, uint8_t* d_absorbed,
+                                uint8_t* d_escaped, double* edep_by_material,
+                                int64_t* n_fluorescence);
+
+/* cc_run: _run_batches() with the source sampled on the device.  Histories
+ * [first_history, first_history + n_histories) of the run keyed by seed are
+ * simulated in batches of batch_size (the last batch may be smaller); with a
+ * CC_GRID_STATS grid each batch is folded into the batch statistics. */
+int cc_run(cc_ctx* ctx, const cc_scene* scene, const cc_tables* tables, const cc_source* src,
+           cc_grid* grid, int64_t n_histories, int64_t batch_size, uint64_t seed,
+           int64_t first_history, int32_t fluorescence, double* edep_by_material,
+           double* edep_sum2_by_material, cc_run_out* out);
+
+/* Sample source photons only (tests of source.py parity). */
+int cc_sample_source(cc_ctx* ctx, const cc_source* src, int64_t n, uint64_t seed,
+                     int64_t first_history, double* pos, double* dir, double* energy);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
