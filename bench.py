@@ -1,0 +1,350 @@
+"""Throughput of the room-scale plain Monte Carlo workload (histories/s).
+
+Workload: 400x400x300 cm air room with a water torso, two bone cylinders, a
+0.05 cm lead sheet and a 20 cm concrete wall; 80 kVp spectrum in 1 keV bins,
+35x43 cm field at SID 180 cm; kerma and H*(10) on 5 cm voxels over the room
+(80x80x60) with batch statistics (batches of 200,000 histories).  One step
+is one call of the run driver over --histories-per-step histories (default
+1e7, so the default 10 steps are the 1e8-history run of the
+configuration).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
+
+Under torchrun every rank simulates its own history range (weak scaling)
+and the tallies are summed with one NCCL all-reduce at the end of the
+timed region.  ``--impl reference`` times the CPU restatement of ChatCarlo's
+NumPy path on all host cores instead (the reference arm).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "histories/s"
+BATCH = 200_000
+WORKLOAD = ("room-scale plain MC: 400x400x300 cm air room, water torso 35x25x20 cm, 2 bone cylinders "
+            "r1.5x20 cm, 0.05 cm lead 30x30 cm at 150 cm, 20 cm concrete wall; 80 kVp W spectrum 2.5 mm Al "
+            "(Kramers model, 1 keV bins); rect field 35x43 cm at SID 180 cm; kerma + H*(10) on 5 cm voxels "
+            "80x80x60 with batch statistics")
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic():
+    """DRAM bytes per history of the transport kernel from the committed ncu summary."""
+    p = ROOT / "profiles" / "transport_kernel_room.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return d.get("dram_bytes_per_history")
+    return None
+
+
+class ClockSampler:
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return None
+        rows = []
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) >= 9:
+                rows.append(f)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower().startswith("active")})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ---------------------------------------------------------------------------
+# reference arm: the CPU oracle on all host cores
+# ---------------------------------------------------------------------------
+
+def _ref_worker(n, seed):
+    import cc_oracle as O
+    from chatcarlo_b200 import workloads as W
+    raw = W.room()
+    agg = O.run_transport(raw, n_histories=n, seed=seed, batch_size=BATCH, grid_spec=W.ROOM_GRID,
+                          n_workers=1, track_uncertainty=True)
+    g = agg["grid"]
+    return n, g.kerma_keV, g.h10_track_pSv_cm3
+
+
+def _ref_warm(_):
+    _ref_worker(200, 0)      # builds the element tables in this process
+    return os.getpid()
+
+
+def run_cpu_reference(steps: int, warmup: int, per_core: int, cores: int | None = None):
+    """Times the oracle's run_transport on the workload with one process per
+    host core (spawned), per_core histories per process per step."""
+    import concurrent.futures
+    import multiprocessing as mp
+    sys.path.insert(0, str(ROOT / "oracle"))
+    cores = cores or os.cpu_count() or 1
+    ctx = mp.get_context("spawn")
+    times, total = [], 0
+    with concurrent.futures.ProcessPoolExecutor(max_workers=cores, mp_context=ctx,
+                                                initializer=_ref_init, initargs=(str(ROOT),)) as pool:
+        list(pool.map(_ref_warm, range(cores)))
+        for s in range(warmup + steps):
+            t0 = time.perf_counter()
+            futs = [pool.submit(_ref_worker, per_core, 1000 * s + i) for i in range(cores)]
+            kerma = None
+            n = 0
+            for f in futs:
+                k, a, b = f.result()
+                n += k
+                kerma = a if kerma is None else kerma + a
+            dt = time.perf_counter() - t0
+            if s >= warmup:
+                times.append(dt)
+                total += n
+    return total / sum(times), cores, times
+
+
+def _ref_init(root):
+    sys.path.insert(0, root)
+    sys.path.insert(0, os.path.join(root, "oracle"))
+
+
+# ---------------------------------------------------------------------------
+# engine arm
+# ---------------------------------------------------------------------------
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--histories-per-step", type=float, default=1e7)
+    ap.add_argument("--e2e-histories", type=float, default=4e6)
+    ap.add_argument("--cpu-per-core", type=int, default=25_000)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        per_core = max(2000, args.cpu_per_core // 5)
+        value, cores, times = run_cpu_reference(args.steps, args.warmup, per_core)
+        line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "histories/s",
+                "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": 1000.0 * float(np.mean(times)), "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": WORKLOAD, "histories_per_step": per_core * cores,
+                           "batch_size": BATCH, "l2": "n/a (CPU)"},
+                "cpu_baseline": {"value": value, "unit": "histories/s", "cores": cores, "kind": "port",
+                                 "sample": f"{per_core} histories per process x {cores} processes per step"},
+                "e2e": {"value": value, "unit": "histories/s", "h2d_bytes_per_step": 0,
+                        "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return 0
+
+    import torch
+    import torch.distributed as dist
+    if world > 1:
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", init_method="env://",
+                                timeout=__import__("datetime").timedelta(seconds=120))
+    import ctypes as C
+    from chatcarlo_b200 import _native as N
+    from chatcarlo_b200 import workloads as W
+    from chatcarlo_b200.geometry import Geometry
+    from chatcarlo_b200.source import SourceSpec
+    from chatcarlo_b200.transport import DeviceGrid, Engine, transport_photons
+
+    device = local if world > 1 else 0
+    torch.cuda.set_device(device)
+    eng = Engine(device)
+    raw = W.room()
+    geom = Geometry(raw["geometry"])
+    ts, th = eng.tables(geom.materials(), need_muen=True)
+    sh = eng.scene(geom, ts)
+    spec = SourceSpec(raw["source"])
+    srch = eng.source(spec)
+    grid = W.make_grid(W.ROOM_GRID, track_uncertainty=True)
+    dg = DeviceGrid(eng, grid, stats=True)
+    S = int(args.histories_per_step)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    edep = np.zeros(len(ts.names))
+    edep2 = np.zeros(len(ts.names))
+    seed = 20261203
+    base = rank << 40
+
+    def step(i):
+        out = N.RunOut()
+        N.check(eng.lib.cc_run(eng.ctx, sh, th, srch, dg.handle, S, BATCH, seed, base + i * S, 1,
+                               N.dptr(edep), N.dptr(edep2), C.byref(out)))
+        return out
+
+    for i in range(args.warmup):
+        step(i)
+    N.check(eng.lib.cc_grid_reset(dg.handle))
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    step_ms, outs = [], []
+    with ClockSampler(device) as clk:
+        for i in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            ev0.record()
+            outs.append(step(args.warmup + i))
+            ev1.record()
+            torch.cuda.synchronize()
+            step_ms.append(ev0.elapsed_time(ev1))
+        red_ms = 0.0
+        if world > 1:
+            # the one exchange step: sum the tally grids over ranks
+            dg.download(grid)
+            t = torch.from_numpy(np.stack([grid.kerma_keV, grid.h10_track_pSv_cm3])).cuda()
+            ev0.record()
+            dist.all_reduce(t)
+            ev1.record()
+            torch.cuda.synchronize()
+            red_ms = ev0.elapsed_time(ev1)
+    clocks = clk.summary()
+    total_ms = float(np.sum(step_ms)) + red_ms
+    if world > 1:
+        tt = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        total_ms = float(tt.item())
+        dist.barrier()
+    hist = S * args.steps * world
+    value = hist / (total_ms / 1e3)
+
+    n_h = S * args.steps
+    n_seg = sum(o.n_steps for o in outs) / n_h
+    n_vox = sum(o.n_voxel_visits for o in outs) / n_h
+    b_hist = 96.0 * n_seg + 32.0 * n_vox + 32.0
+    tr_ms = sum(o.transport_ms for o in outs)
+    tr_launch = sum(o.transport_launches for o in outs)
+    launches = sum(o.gpu_launches for o in outs)
+    peak, peak_kind = peaks()
+    achieved = b_hist * n_h / (tr_ms / 1e3) / 1e9
+    traffic_per_hist = profile_traffic()
+    hist_per_launch = n_h / max(tr_launch, 1)
+
+    # e2e: the public transport_photons API on host buffers (pinned), each
+    # step copies its photons in and the per-photon results and tallies out
+    e2e = None
+    if rank == 0:
+        ne = int(args.e2e_histories)
+        pin = lambda shape: torch.empty(shape, dtype=torch.float64, pin_memory=True).numpy()  # noqa: E731
+        p0, d0, e0 = pin((ne, 3)), pin((ne, 3)), pin((ne,))
+        N.check(eng.lib.cc_sample_source(eng.ctx, srch, ne, seed + 7, 1 << 50, N.dptr(p0), N.dptr(d0), N.dptr(e0)))
+        p, d, e = pin((ne, 3)), pin((ne, 3)), pin((ne,))
+        egrid = W.make_grid(W.ROOM_GRID, track_uncertainty=False)
+        e_ms = []
+        for i in range(args.warmup + min(args.steps, 5)):
+            np.copyto(p, p0)
+            np.copyto(d, d0)
+            np.copyto(e, e0)
+            flush.zero_()
+            torch.cuda.synchronize()
+            ev0.record()
+            transport_photons(p, d, e, geom, seed=seed + i, grid=egrid, engine=eng)
+            ev1.record()
+            torch.cuda.synchronize()
+            if i >= args.warmup:
+                e_ms.append(ev0.elapsed_time(ev1))
+        nvox = int(np.prod(grid.shape))
+        e2e = {"value": ne * len(e_ms) / (float(np.sum(e_ms)) / 1e3), "unit": "histories/s",
+               "h2d_bytes_per_step": ne * (3 + 3 + 1) * 8,
+               "d2h_bytes_per_step": ne * (3 + 3 + 1) * 8 + ne * (4 + 1 + 1) + 2 * nvox * 8,
+               "api": "chatcarlo_b200.transport.transport_photons (C ABI cc_transport_photons, host buffers)"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        per_core = max(1000, args.cpu_per_core // 5)
+        v, cores, times = run_cpu_reference(1, 0, per_core)
+        cpu = {"value": v, "unit": "histories/s", "cores": cores, "kind": "port",
+               "sample": f"room workload, {per_core} histories in each of {cores} spawned processes "
+                         f"({per_core * cores} histories, {times[0]:.1f} s wall incl. pool start)"}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "histories/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": {"workload": WORKLOAD, "histories_per_step_per_gpu": S, "batch_size": BATCH,
+                           "grid": list(grid.shape), "voxel_cm": 5.0, "tally_dtype": "f64",
+                           "l2": "flushed between steps (256 MiB write)",
+                           "parallelism": f"history shards x{world}"},
+                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                             "frac": achieved / peak, "peak_kind": peak_kind,
+                             "traffic": (traffic_per_hist * hist_per_launch) if traffic_per_hist else None,
+                             "kernel": "transport_kernel<true,true>",
+                             "bytes_per_history": b_hist, "segments_per_history": n_seg,
+                             "voxel_visits_per_history": n_vox,
+                             "avg_launch_ms": tr_ms / max(tr_launch, 1),
+                             "histories_per_launch": hist_per_launch},
+                "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks, "gpu_launches": int(launches),
+                "reduce_ms": red_ms}
+        print(json.dumps(line))
+    dg.close()
+    eng.lib.cc_source_destroy(srch)
+    eng.lib.cc_scene_destroy(sh)
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -90,7 +90,9 @@ class SourceDesc(C.Structure):
 class RunOut(C.Structure):
     _fields_ = [("n_histories", C.c_int64), ("n_absorbed", C.c_int64), ("n_escaped", C.c_int64),
                 ("scatter_sum", C.c_int64), ("n_fluorescence", C.c_int64), ("n_batches", C.c_int64),
-                ("gpu_launches", C.c_int64), ("elapsed_ms", C.c_double)]
+                ("gpu_launches", C.c_int64), ("elapsed_ms", C.c_double), ("n_steps", C.c_int64),
+                ("n_voxel_visits", C.c_int64), ("transport_ms", C.c_double),
+                ("transport_launches", C.c_int64)]
 
 
 P = C.c_void_p

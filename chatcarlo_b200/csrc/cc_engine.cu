@@ -141,7 +141,7 @@ struct KRun {
     unsigned char* escaped;
     // reductions
     double* edep;             // [n_scratch][n_mat]
-    unsigned long long* counters;   // absorbed, escaped, scatter_sum, n_fluor, steps
+    unsigned long long* counters;   // absorbed, escaped, scatter_sum, n_fluor, steps, voxel visits
     unsigned long long* work;       // global history counter
     unsigned* status;
 };
@@ -448,8 +448,8 @@ __device__ __forceinline__ void score(double* tally, long long v, double wk, dou
     atomicAdd(tally + 2 * v + 1, wh);
 }
 
-__device__ void tally_segment(const KGrid& G, double* tally, const float p[3], const float d[3],
-                              float s, float wk, float wh, unsigned* status) {
+__device__ int tally_segment(const KGrid& G, double* tally, const float p[3], const float d[3],
+                             float s, float wk, float wh) {
     // clip the segment to the grid box
     float t0 = 0.0f, t1 = s;
     float lo[3], hi[3];
@@ -458,7 +458,7 @@ __device__ void tally_segment(const KGrid& G, double* tally, const float p[3], c
         lo[k] = G.o[k];
         hi[k] = G.o[k] + G.h * (float)(k == 0 ? G.nx : (k == 1 ? G.ny : G.nz));
         if (fabsf(d[k]) < 1e-12f) {
-            if (p[k] < lo[k] || p[k] >= hi[k]) return;
+            if (p[k] < lo[k] || p[k] >= hi[k]) return 0;
         } else {
             float inv = 1.0f / d[k];
             float ta = (lo[k] - p[k]) * inv, tb = (hi[k] - p[k]) * inv;
@@ -466,7 +466,7 @@ __device__ void tally_segment(const KGrid& G, double* tally, const float p[3], c
             t1 = fminf(t1, fmaxf(ta, tb));
         }
     }
-    if (!(t1 > t0)) return;
+    if (!(t1 > t0)) return 0;
     int n[3] = {G.nx, G.ny, G.nz};
     int iv[3], step[3];
     float tmax[3], tdel[3];
@@ -494,6 +494,7 @@ __device__ void tally_segment(const KGrid& G, double* tally, const float p[3], c
     float t = t0;
     const double dwk = (double)wk, dwh = (double)wh;
     int guard = n[0] + n[1] + n[2] + 4;
+    int visits = 0;
     while (t < t1 && guard-- > 0) {
         int ax = (tmax[0] < tmax[1]) ? (tmax[0] < tmax[2] ? 0 : 2) : (tmax[1] < tmax[2] ? 1 : 2);
         float tn = fminf(tmax[ax], t1);
@@ -501,6 +502,7 @@ __device__ void tally_segment(const KGrid& G, double* tally, const float p[3], c
         if (len > 0.0f) {
             long long v = ((long long)iv[0] * G.ny + iv[1]) * G.nz + iv[2];
             score(tally, v, dwk * len, dwh * len);
+            ++visits;
         }
         t = tn;
         if (t >= t1) break;
@@ -508,6 +510,7 @@ __device__ void tally_segment(const KGrid& G, double* tally, const float p[3], c
         if (iv[ax] < 0 || iv[ax] >= n[ax]) break;
         tmax[ax] += tdel[ax];
     }
+    return visits;
 }
 
 // ---------------------------------------------------------------------------
@@ -582,14 +585,14 @@ template <bool FROM_SOURCE, bool TALLY>
 __global__ void __launch_bounds__(256)
 transport_kernel(const KTables T, const KScene S, const KGrid G, const KSource SRC, const KRun R) {
     extern __shared__ double s_edep[];             // [n_scratch][n_mat]
-    __shared__ unsigned long long s_cnt[5];
+    __shared__ unsigned long long s_cnt[6];
     const int n_acc = R.n_scratch * T.n_mat;
     for (int i = threadIdx.x; i < n_acc; i += blockDim.x) s_edep[i] = 0.0;
-    if (threadIdx.x < 5) s_cnt[threadIdx.x] = 0ull;
+    if (threadIdx.x < 6) s_cnt[threadIdx.x] = 0ull;
     __syncthreads();
 
     const int lane = threadIdx.x & 31;
-    unsigned long long c_abs = 0, c_esc = 0, c_sc = 0, c_fl = 0, c_steps = 0;
+    unsigned long long c_abs = 0, c_esc = 0, c_sc = 0, c_fl = 0, c_steps = 0, c_vox = 0;
 
     // warp-local pool [pool_next, pool_end)
     long long pool_next = 0, pool_end = 0;
@@ -674,7 +677,7 @@ transport_kernel(const KTables T, const KScene S, const KGrid G, const KSource S
         if (TALLY) {
             float wk = E * muen_rho(T, M, loge) * M.density;
             float wh = h10_coeff(T, loge);
-            tally_segment(G, G.tally + (size_t)batch * 2 * G.nvox, p, d, s, wk, wh, R.status);
+            c_vox += tally_segment(G, G.tally + (size_t)batch * 2 * G.nvox, p, d, s, wk, wh);
         }
         p[0] += d[0] * s; p[1] += d[1] * s; p[2] += d[2] * s;
 
@@ -766,10 +769,11 @@ transport_kernel(const KTables T, const KScene S, const KGrid G, const KSource S
     atomicAdd(&s_cnt[2], c_sc);
     atomicAdd(&s_cnt[3], c_fl);
     atomicAdd(&s_cnt[4], c_steps);
+    atomicAdd(&s_cnt[5], c_vox);
     __syncthreads();
     for (int i = threadIdx.x; i < n_acc; i += blockDim.x)
         if (s_edep[i] != 0.0) atomicAdd(R.edep + i, s_edep[i]);
-    if (threadIdx.x < 5) atomicAdd(R.counters + threadIdx.x, s_cnt[threadIdx.x]);
+    if (threadIdx.x < 6) atomicAdd(R.counters + threadIdx.x, s_cnt[threadIdx.x]);
 }
 
 // Batch statistics fold (tally.py:59-94): T += S, Q += S^2/n_b,
@@ -845,6 +849,8 @@ struct cc_ctx {
     int sm_count = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaEvent_t kev0 = nullptr, kev1 = nullptr;     // around the transport kernel alone
+    double* d_edep = nullptr;                       // [MAX_SCRATCH * MAX_MATS] per-launch reductions
     unsigned* d_status = nullptr;
     unsigned long long* d_counters = nullptr;   // [5] + work counter
     int block = 256;
@@ -917,6 +923,9 @@ int cc_ctx_create(int device, cc_ctx** out) {
     CC_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
     CC_CUDA(cudaEventCreate(&c->ev0));
     CC_CUDA(cudaEventCreate(&c->ev1));
+    CC_CUDA(cudaEventCreate(&c->kev0));
+    CC_CUDA(cudaEventCreate(&c->kev1));
+    CC_CUDA(cudaMalloc(&c->d_edep, (size_t)MAX_SCRATCH * MAX_MATS * sizeof(double)));
     CC_CUDA(cudaMalloc(&c->d_status, sizeof(unsigned)));
     CC_CUDA(cudaMalloc(&c->d_counters, 8 * sizeof(unsigned long long)));
     *out = c;
@@ -929,8 +938,11 @@ int cc_ctx_destroy(cc_ctx* c) {
     cudaStreamSynchronize(c->stream);
     cudaFree(c->d_status);
     cudaFree(c->d_counters);
+    cudaFree(c->d_edep);
     cudaEventDestroy(c->ev0);
     cudaEventDestroy(c->ev1);
+    cudaEventDestroy(c->kev0);
+    cudaEventDestroy(c->kev1);
     cudaStreamDestroy(c->stream);
     delete c;
     return CC_OK;
@@ -1362,22 +1374,22 @@ static int grid_blocks_for(cc_ctx* c, size_t smem, bool fs, bool tl) {
 // One launch of the transport kernel plus its reductions.
 static int run_launch(cc_ctx* c, const cc_scene* scene, const cc_tables* tables, const KSource* src,
                       cc_grid* grid, double* tally_base, int n_slots, long long batch_size,
-                      KRun R, std::vector<double>& edep_slots, unsigned long long* counters_out) {
+                      KRun R, std::vector<double>& edep_slots, unsigned long long* counters_out,
+                      float* kernel_ms) {
     const KTables& T = tables->k;
     R.n_scratch = n_slots;
     R.batch_size = batch_size;
     R.max_steps = c->max_steps;
     R.status = c->d_status;
     R.counters = c->d_counters;
-    R.work = c->d_counters + 5;
-    double* d_edep = nullptr;
+    R.work = c->d_counters + 6;
     size_t n_acc = (size_t)n_slots * T.n_mat;
-    CC_CUDA(cudaMalloc(&d_edep, n_acc * sizeof(double)));
+    if (n_acc > (size_t)MAX_SCRATCH * MAX_MATS) return set_error(CC_E_INVALID, "too many batches x materials per launch");
     cudaStream_t st = c->stream;
-    cudaMemsetAsync(d_edep, 0, n_acc * sizeof(double), st);
-    cudaMemsetAsync(c->d_counters, 0, 8 * sizeof(unsigned long long), st);
-    cudaMemsetAsync(c->d_status, 0, sizeof(unsigned), st);
-    R.edep = d_edep;
+    CC_CUDA(cudaMemsetAsync(c->d_edep, 0, n_acc * sizeof(double), st));
+    CC_CUDA(cudaMemsetAsync(c->d_counters, 0, 8 * sizeof(unsigned long long), st));
+    CC_CUDA(cudaMemsetAsync(c->d_status, 0, sizeof(unsigned), st));
+    R.edep = c->d_edep;
     KGrid G;
     memset(&G, 0, sizeof(G));
     bool tl = grid != nullptr;
@@ -1387,22 +1399,27 @@ static int run_launch(cc_ctx* c, const cc_scene* scene, const cc_tables* tables,
     bool fs = src != nullptr;
     if (fs) S = *src;
     size_t smem = n_acc * sizeof(double);
-    if (smem > 48 * 1024) { cudaFree(d_edep); return set_error(CC_E_INVALID, "too many batches x materials per launch"); }
     int blocks = grid_blocks_for(c, smem, fs, tl);
+    CC_CUDA(cudaEventRecord(c->kev0, st));
     cudaError_t e;
     if (fs && tl) e = launch_transport<true, true>(c, T, scene->k, G, S, R, smem, blocks);
     else if (fs) e = launch_transport<true, false>(c, T, scene->k, G, S, R, smem, blocks);
     else if (tl) e = launch_transport<false, true>(c, T, scene->k, G, S, R, smem, blocks);
     else e = launch_transport<false, false>(c, T, scene->k, G, S, R, smem, blocks);
-    if (e != cudaSuccess) { cudaFree(d_edep); return set_error(CC_E_DEVICE, std::string("transport launch: ") + cudaGetErrorString(e)); }
+    if (e != cudaSuccess) return set_error(CC_E_DEVICE, std::string("transport launch: ") + cudaGetErrorString(e));
+    CC_CUDA(cudaEventRecord(c->kev1, st));
     edep_slots.assign(n_acc, 0.0);
     unsigned st_h = 0;
-    e = cudaMemcpyAsync(edep_slots.data(), d_edep, n_acc * sizeof(double), cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(counters_out, c->d_counters, 5 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st);
+    e = cudaMemcpyAsync(edep_slots.data(), c->d_edep, n_acc * sizeof(double), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(counters_out, c->d_counters, 6 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(&st_h, c->d_status, sizeof(unsigned), cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    cudaFree(d_edep);
     if (e != cudaSuccess) return set_error(CC_E_DEVICE, std::string("transport: ") + cudaGetErrorString(e));
+    if (kernel_ms) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, c->kev0, c->kev1);
+        *kernel_ms = ms;
+    }
     return status_to_error(st_h);
 }
 
@@ -1421,8 +1438,8 @@ static int transport_common(cc_ctx* c, const cc_scene* scene, const cc_tables* t
     double* tally = nullptr;
     if (grid) tally = (grid->flags & CC_GRID_STATS) ? grid->d_scratch : grid->d_total;
     std::vector<double> slots;
-    unsigned long long cnt[5] = {0, 0, 0, 0, 0};
-    int rc = run_launch(c, scene, tables, nullptr, grid, tally, 1, std::max<long long>(n, 1), R, slots, cnt);
+    unsigned long long cnt[6] = {0, 0, 0, 0, 0, 0};
+    int rc = run_launch(c, scene, tables, nullptr, grid, tally, 1, std::max<long long>(n, 1), R, slots, cnt, nullptr);
     if (rc != CC_OK) return rc;
     if (edep) for (int m = 0; m < tables->n_mat; ++m) edep[m] += slots[m];
     if (n_fluor) *n_fluor = (int64_t)cnt[3];
@@ -1505,8 +1522,10 @@ int cc_run(cc_ctx* c, const cc_scene* scene, const cc_tables* tables, const cc_s
     }
     long long done = 0;
     long long launches = 0;
-    unsigned long long tot[5] = {0, 0, 0, 0, 0};
+    unsigned long long tot[6] = {0, 0, 0, 0, 0, 0};
     float ms_total = 0.0f;
+    double ms_transport = 0.0;
+    long long transport_launches = 0;
     while (done < n_hist) {
         int ns = slots;
         long long n_launch = std::min<long long>(n_hist - done, (long long)ns * batch_size);
@@ -1520,12 +1539,15 @@ int cc_run(cc_ctx* c, const cc_scene* scene, const cc_tables* tables, const cc_s
         double* tally = nullptr;
         if (grid) tally = stats ? grid->d_scratch : grid->d_total;
         std::vector<double> slot_edep;
-        unsigned long long cnt[5];
+        unsigned long long cnt[6];
         CC_CUDA(cudaEventRecord(c->ev0, c->stream));
+        float kms = 0.f;
         int rc = run_launch(c, scene, tables, &src->k, grid, tally, stats ? ns : 1,
-                            stats ? batch_size : std::max<long long>(n_launch, 1), R, slot_edep, cnt);
+                            stats ? batch_size : std::max<long long>(n_launch, 1), R, slot_edep, cnt, &kms);
         if (rc != CC_OK) return rc;
         ++launches;
+        ++transport_launches;
+        ms_transport += kms;
         // per-batch collision-estimator moments (ScalarMoments.add_batch, tally.py:204-213)
         for (int b = 0; b < ns; ++b) {
             long long nb = std::min<long long>(batch_size, n_launch - (long long)b * batch_size);
@@ -1547,7 +1569,7 @@ int cc_run(cc_ctx* c, const cc_scene* scene, const cc_tables* tables, const cc_s
         float ms = 0.f;
         cudaEventElapsedTime(&ms, c->ev0, c->ev1);
         ms_total += ms;
-        for (int k = 0; k < 5; ++k) tot[k] += cnt[k];
+        for (int k = 0; k < 6; ++k) tot[k] += cnt[k];
         done += n_launch;
     }
     if (out) {
@@ -1559,6 +1581,10 @@ int cc_run(cc_ctx* c, const cc_scene* scene, const cc_tables* tables, const cc_s
         out->n_batches = (n_hist + batch_size - 1) / batch_size;
         out->gpu_launches = launches;
         out->elapsed_ms = ms_total;
+        out->n_steps = (int64_t)tot[4];
+        out->n_voxel_visits = (int64_t)tot[5];
+        out->transport_ms = ms_transport;
+        out->transport_launches = transport_launches;
     }
     return CC_OK;
 }

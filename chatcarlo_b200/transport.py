@@ -50,6 +50,10 @@ class TransportResult:
     # engine bookkeeping (not in the NumPy result)
     device_ms: float = 0.0
     gpu_launches: int = 0
+    transport_ms: float = 0.0
+    transport_launches: int = 0
+    n_steps: int = 0
+    n_voxel_visits: int = 0
 
 
 class DeviceGrid:
@@ -291,4 +295,8 @@ def run_transport(scene, n_histories: int = 100_000, seed: int | None = None,
         energy_deposited_rel_err=rel,
         device_ms=float(out.elapsed_ms),
         gpu_launches=int(out.gpu_launches),
+        transport_ms=float(out.transport_ms),
+        transport_launches=int(out.transport_launches),
+        n_steps=int(out.n_steps),
+        n_voxel_visits=int(out.n_voxel_visits),
     )

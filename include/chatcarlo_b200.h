@@ -146,8 +146,12 @@ typedef struct {
     int64_t scatter_sum;
     int64_t n_fluorescence;
     int64_t n_batches;
-    int64_t gpu_launches;
+    int64_t gpu_launches;         /* kernels launched (transport + batch folds) */
     double elapsed_ms;            /* device time of the run (CUDA events) */
+    int64_t n_steps;              /* transport steps (track segments) of all histories */
+    int64_t n_voxel_visits;       /* voxel scores of the track-length tally walk */
+    double transport_ms;          /* device time of the transport kernel launches alone */
+    int64_t transport_launches;
 } cc_run_out;
 
 /* -- context and error handling ------------------------------------------ */

@@ -1,0 +1,43 @@
+"""The C-ABI library loads on a machine without a GPU and exports every
+entry point that include/chatcarlo_b200.h declares."""
+import ctypes as C
+import re
+from pathlib import Path
+
+import pytest
+
+from chatcarlo_b200 import _native as N
+
+HEADER = Path(__file__).resolve().parent.parent / "include" / "chatcarlo_b200.h"
+
+
+def declared_functions():
+    text = HEADER.read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(cc_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_header_and_binding_agree():
+    assert declared_functions() == sorted(N.EXPORTED)
+
+
+def test_library_exports_every_declared_symbol():
+    lib = C.CDLL(str(N.LIB_PATH))
+    missing = [f for f in declared_functions() if not hasattr(lib, f)]
+    assert not missing, missing
+
+
+def test_version_and_error_string_without_gpu():
+    lib = N.lib()
+    assert lib.cc_version() == 1
+    assert isinstance(lib.cc_last_error(), bytes)
+
+
+def test_invalid_arguments_are_rejected_before_any_device_work():
+    lib = N.lib()
+    assert lib.cc_ctx_create(0, None) == N.CC_E_INVALID
+    assert lib.cc_scene_create(None, None, 0, 0, None, None, None) == N.CC_E_INVALID
+    assert lib.cc_transport_photons(None, None, None, None, 0, None, None, None, 0, 0, 1,
+                                    None, None, None, None, None) == N.CC_E_INVALID
+    with pytest.raises(ValueError):
+        N.check(N.CC_E_ENERGY_RANGE)
