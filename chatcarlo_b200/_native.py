@@ -8,7 +8,10 @@ from __future__ import annotations
 import ctypes as C
 from pathlib import Path
 
-LIB_PATH = Path(__file__).resolve().parent / "lib" / "libccb200.so"
+import os
+
+LIB_PATH = Path(os.environ.get("CHATCARLO_B200_LIB") or
+                Path(__file__).resolve().parent / "lib" / "libccb200.so")
 
 CC_OK = 0
 CC_E_INVALID = -1

@@ -59,6 +59,7 @@ struct DevPrim {
     float c[3];
     float h[3];     // box half sizes
     float r2;       // radius^2
+    float r;        // radius
     float hh;       // cylinder half height
 };
 
@@ -100,7 +101,7 @@ struct KScene {
     DevPrim prims[MAX_PRIMS];
     int n_prims, background;
     float wlo[3], whi[3];
-    float eps;        // geometric tolerance (cm) matched to the world's FP32 resolution
+    float eps;        // surface band half-width and smallest root (cm): 8 ulps of the world's FP32 extent
 };
 
 struct KGrid {
@@ -153,53 +154,83 @@ struct KRun {
 __device__ __forceinline__ float fmin3(float a, float b, float c) { return fminf(a, fminf(b, c)); }
 __device__ __forceinline__ float fmax3(float a, float b, float c) { return fmaxf(a, fmaxf(b, c)); }
 
-__device__ __forceinline__ bool contains(const DevPrim& g, float x, float y, float z) {
-    float dx = x - g.c[0], dy = y - g.c[1], dz = z - g.c[2];
+// Positions are FP32, so a photon that has just reached a surface sits
+// within a few ulps (of the world's largest coordinate) of it on either
+// side.  Points inside that band, of half-width tol, are classified by
+// their direction: on a surface, a photon is inside the primitive when it
+// moves inwards.  For planar faces (box faces, cylinder caps) the root of
+// the face the photon sits on is dropped as well: a photon grazing a face
+// would otherwise find that face again a fraction of an ulp ahead on every
+// step and never leave it.
+
+// Inside the slab |o| <= h, deciding points on a face by the direction d.
+__device__ __forceinline__ bool slab_inside(float o, float d, float h, float tol) {
+    float a = fabsf(o);
+    if (a < h - tol) return true;
+    if (a > h + tol) return false;
+    return o * d <= 0.0f;
+}
+
+// Inside the ball |o| <= r (o with n components folded into o2 = |o|^2 and od = o.d).
+__device__ __forceinline__ bool ball_inside(float o2, float od, float r, float tol) {
+    float lo = fmaxf(r - tol, 0.0f), hi = r + tol;
+    if (o2 < lo * lo) return true;
+    if (o2 > hi * hi) return false;
+    return od <= 0.0f;
+}
+
+__device__ __forceinline__ bool contains(const DevPrim& g, const float p[3], const float d[3], float tol) {
+    float o0 = p[0] - g.c[0], o1 = p[1] - g.c[1], o2 = p[2] - g.c[2];
     if (g.type == CC_SHAPE_BOX) {
-        return fabsf(dx) <= g.h[0] && fabsf(dy) <= g.h[1] && fabsf(dz) <= g.h[2];
+        return slab_inside(o0, d[0], g.h[0], tol) && slab_inside(o1, d[1], g.h[1], tol) &&
+               slab_inside(o2, d[2], g.h[2], tol);
     } else if (g.type == CC_SHAPE_SPHERE) {
-        return dx * dx + dy * dy + dz * dz <= g.r2;
+        return ball_inside(o0 * o0 + o1 * o1 + o2 * o2, o0 * d[0] + o1 * d[1] + o2 * d[2], g.r, tol);
     } else {
-        float a, b, w;
-        if (g.axis == 0) { a = dy; b = dz; w = dx; }
-        else if (g.axis == 1) { a = dx; b = dz; w = dy; }
-        else { a = dx; b = dy; w = dz; }
-        return a * a + b * b <= g.r2 && fabsf(w) <= g.hh;
+        const int ax = g.axis;
+        const int i0 = ax == 0 ? 1 : 0, i1 = ax == 2 ? 1 : 2;
+        float oa = p[i0] - g.c[i0], ob = p[i1] - g.c[i1], ow = p[ax] - g.c[ax];
+        return ball_inside(oa * oa + ob * ob, oa * d[i0] + ob * d[i1], g.r, tol) &&
+               slab_inside(ow, d[ax], g.hh, tol);
     }
 }
 
-__device__ __forceinline__ int locate(const KScene& s, float x, float y, float z) {
+__device__ __forceinline__ int locate(const KScene& s, const float p[3], const float d[3]) {
     int m = s.background;
     for (int i = 0; i < s.n_prims; ++i)
-        if (contains(s.prims[i], x, y, z)) m = s.prims[i].material;
+        if (contains(s.prims[i], p, d, s.eps)) m = s.prims[i].material;
     return m;
 }
 
-// Smallest root t > eps of primitive g along the ray, or +inf.
-__device__ __forceinline__ float slab_pair(float o, float d, float lo, float hi, float& tmin, float& tmax) {
-    // returns 0 when the ray misses the slab entirely (parallel and outside)
-    if (fabsf(d) < 1e-12f) {
-        if (o < lo || o > hi) return 0.0f;
-        return 1.0f;
-    }
+// Interval of t where p + t d lies inside the slab [lo, hi] of one axis
+// (o = p - c relative coordinate, tol the band of this face); a face the
+// point sits on contributes t = 0.  Returns false for a ray parallel to the
+// slab outside it.
+__device__ __forceinline__ bool slab_pair(float o, float d, float lo, float hi, float tol,
+                                          float& tmin, float& tmax) {
+    float dlo = lo - o, dhi = hi - o;
+    if (fabsf(dlo) <= tol) dlo = 0.0f;
+    if (fabsf(dhi) <= tol) dhi = 0.0f;
+    if (fabsf(d) < 1e-12f) return dlo <= 0.0f && dhi >= 0.0f;
     float inv = 1.0f / d;
-    float ta = (lo - o) * inv, tb = (hi - o) * inv;
+    float ta = dlo * inv, tb = dhi * inv;
     tmin = fmaxf(tmin, fminf(ta, tb));
     tmax = fminf(tmax, fmaxf(ta, tb));
-    return 1.0f;
+    return true;
 }
 
 __device__ __forceinline__ void take_root(float t, float eps, float& best) {
     if (t > eps && t < best) best = t;
 }
 
+// Smallest root t > eps of primitive g along the ray (geometry.py:20-99), or best.
 __device__ float prim_next(const DevPrim& g, const float p[3], const float d[3], float eps, float best) {
     float ox = p[0] - g.c[0], oy = p[1] - g.c[1], oz = p[2] - g.c[2];
     if (g.type == CC_SHAPE_BOX) {
         float tmin = -INFINITY, tmax = INFINITY;
-        if (slab_pair(ox, d[0], -g.h[0], g.h[0], tmin, tmax) == 0.0f) return best;
-        if (slab_pair(oy, d[1], -g.h[1], g.h[1], tmin, tmax) == 0.0f) return best;
-        if (slab_pair(oz, d[2], -g.h[2], g.h[2], tmin, tmax) == 0.0f) return best;
+        if (!slab_pair(ox, d[0], -g.h[0], g.h[0], eps, tmin, tmax)) return best;
+        if (!slab_pair(oy, d[1], -g.h[1], g.h[1], eps, tmin, tmax)) return best;
+        if (!slab_pair(oz, d[2], -g.h[2], g.h[2], eps, tmin, tmax)) return best;
         if (tmin <= tmax) { take_root(tmin, eps, best); take_root(tmax, eps, best); }
         return best;
     } else if (g.type == CC_SHAPE_SPHERE) {
@@ -216,20 +247,20 @@ __device__ float prim_next(const DevPrim& g, const float p[3], const float d[3],
         take_root(t2, eps, best);
         return best;
     } else {
-        float ax, ay, aw, dx, dy, dw;
-        if (g.axis == 0) { ax = oy; ay = oz; aw = ox; dx = d[1]; dy = d[2]; dw = d[0]; }
-        else if (g.axis == 1) { ax = ox; ay = oz; aw = oy; dx = d[0]; dy = d[2]; dw = d[1]; }
-        else { ax = ox; ay = oy; aw = oz; dx = d[0]; dy = d[1]; dw = d[2]; }
+        const int ax = g.axis;
+        const int i0 = ax == 0 ? 1 : 0, i1 = ax == 2 ? 1 : 2;
+        float a0 = p[i0] - g.c[i0], a1 = p[i1] - g.c[i1], aw = p[ax] - g.c[ax];
+        float dx = d[i0], dy = d[i1], dw = d[ax];
         float a = dx * dx + dy * dy;
-        float cc = ax * ax + ay * ay - g.r2;
+        float cc = a0 * a0 + a1 * a1 - g.r2;
         float tmin, tmax;
         if (a < 1e-12f) {
             if (cc > 0.0f) return best;        // parallel to the axis, outside the radius
             tmin = -INFINITY; tmax = INFINITY;
         } else {
-            float b = ax * dx + ay * dy;
+            float b = a0 * dx + a1 * dy;
             float inva = 1.0f / a;
-            float ex = ax - b * inva * dx, ey = ay - b * inva * dy;
+            float ex = a0 - b * inva * dx, ey = a1 - b * inva * dy;
             float disc = (g.r2 - (ex * ex + ey * ey)) * a;   // b^2 - a c without cancellation
             if (disc < 0.0f) return best;
             float sq = sqrtf(disc);
@@ -237,7 +268,7 @@ __device__ float prim_next(const DevPrim& g, const float p[3], const float d[3],
             float r1 = q * inva, r2 = (q != 0.0f) ? cc / q : 0.0f;
             tmin = fminf(r1, r2); tmax = fmaxf(r1, r2);
         }
-        if (slab_pair(aw, dw, -g.hh, g.hh, tmin, tmax) == 0.0f) return best;
+        if (!slab_pair(aw, dw, -g.hh, g.hh, eps, tmin, tmax)) return best;
         if (tmin <= tmax) { take_root(tmin, eps, best); take_root(tmax, eps, best); }
         return best;
     }
@@ -292,22 +323,25 @@ __device__ __forceinline__ void parts(const KTables& T, const DevMaterial& m, co
 // Element of the material that takes the interaction of kind k (0 photo,
 // 1 Compton, 2 Rayleigh), chosen with probability w_i sigma_i / sum
 // (physics.py:78-92, 138-152, 223-236).  Returns the element slot.
-__device__ int pick_element(const KTables& T, const DevMaterial& m, const Lookup& L, int k, float r) {
-    if (m.n_el == 1) return m.el_slot[0];
-    float w[MAX_ELEMS_PER_MAT];
+__device__ __noinline__ int pick_element(const KTables& T, const DevMaterial& m, const Lookup& L, int k, float r) {
+    const int n_el = m.n_el;
+    if (n_el == 1) return m.el_slot[0];
+    const float* base = T.elem_log + m.elem_off + (size_t)k * m.n_nodes;
+    const size_t stride = (size_t)3 * m.n_nodes;
     float tot = 0.0f;
-    for (int i = 0; i < m.n_el; ++i) {
-        const float* y = T.elem_log + m.elem_off + (size_t)(i * 3 + k) * m.n_nodes;
+    for (int i = 0; i < n_el; ++i) {
+        const float* y = base + i * stride;
         float y0 = __ldg(y + L.idx), y1 = __ldg(y + L.idx + 1);
-        w[i] = __expf(y0 + L.frac * (y1 - y0));
-        tot += w[i];
+        tot += __expf(y0 + L.frac * (y1 - y0));
     }
     float target = r * tot, acc = 0.0f;
-    for (int i = 0; i < m.n_el - 1; ++i) {
-        acc += w[i];
+    for (int i = 0; i < n_el - 1; ++i) {
+        const float* y = base + i * stride;
+        float y0 = __ldg(y + L.idx), y1 = __ldg(y + L.idx + 1);
+        acc += __expf(y0 + L.frac * (y1 - y0));
         if (target <= acc) return m.el_slot[i];
     }
-    return m.el_slot[m.n_el - 1];
+    return m.el_slot[n_el - 1];
 }
 
 // mu_en/rho by log-log cubic Hermite with the PCHIP node slopes (materials.py:310-335).
@@ -443,39 +477,61 @@ __device__ void isotropic(float d[3], HistoryRng& rng) {
 // track-length tally: exact voxel traversal (Amanatides & Woo)
 // ---------------------------------------------------------------------------
 
-__device__ __forceinline__ void score(double* tally, long long v, double wk, double wh) {
-    atomicAdd(tally + 2 * v, wk);
-    atomicAdd(tally + 2 * v + 1, wh);
+__device__ __forceinline__ void score(double* tally, long long v, float wk_len, float wh_len) {
+    atomicAdd(tally + 2 * v, (double)wk_len);
+    atomicAdd(tally + 2 * v + 1, (double)wh_len);
 }
 
-__device__ int tally_segment(const KGrid& G, double* tally, const float p[3], const float d[3],
-                             float s, float wk, float wh) {
-    // clip the segment to the grid box
-    float t0 = 0.0f, t1 = s;
-    float lo[3], hi[3];
+// Clip the ray p + t d, t in [0, s], to the grid box.  Returns false when
+// no part of it lies inside.
+__device__ __forceinline__ bool clip_to_grid(const KGrid& G, const float p[3], const float d[3], float s,
+                                             float& t0, float& t1) {
+    t0 = 0.0f;
+    t1 = s;
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-        lo[k] = G.o[k];
-        hi[k] = G.o[k] + G.h * (float)(k == 0 ? G.nx : (k == 1 ? G.ny : G.nz));
+        float lo = G.o[k];
+        float hi = G.o[k] + G.h * (float)(k == 0 ? G.nx : (k == 1 ? G.ny : G.nz));
         if (fabsf(d[k]) < 1e-12f) {
-            if (p[k] < lo[k] || p[k] >= hi[k]) return 0;
+            if (p[k] < lo || p[k] >= hi) return false;
         } else {
             float inv = 1.0f / d[k];
-            float ta = (lo[k] - p[k]) * inv, tb = (hi[k] - p[k]) * inv;
+            float ta = (lo - p[k]) * inv, tb = (hi - p[k]) * inv;
             t0 = fmaxf(t0, fminf(ta, tb));
             t1 = fminf(t1, fmaxf(ta, tb));
         }
     }
-    if (!(t1 > t0)) return 0;
-    int n[3] = {G.nx, G.ny, G.nz};
+    return t1 > t0;
+}
+
+__device__ __forceinline__ int grid_dim(const KGrid& G, int k) { return k == 0 ? G.nx : (k == 1 ? G.ny : G.nz); }
+
+// Number of voxels the clipped range [t0, t1] crosses (for load balancing).
+__device__ __forceinline__ int visit_estimate(const KGrid& G, const float p[3], const float d[3], float t0, float t1) {
+    int n = 1;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        int nk = grid_dim(G, k);
+        int a = max(0, min(nk - 1, (int)floorf((p[k] + d[k] * t0 - G.o[k]) * G.inv_h)));
+        int b = max(0, min(nk - 1, (int)floorf((p[k] + d[k] * t1 - G.o[k]) * G.inv_h)));
+        n += abs(b - a);
+    }
+    return n;
+}
+
+// Exact voxel traversal (Amanatides & Woo) of p + t d over [t0, t1], which
+// lies inside the grid box; scores weight x overlap length per voxel.
+__device__ int walk_range(const KGrid& G, double* tally, const float p[3], const float d[3],
+                          float t0, float t1, float wk, float wh) {
     int iv[3], step[3];
     float tmax[3], tdel[3];
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-        // voxel of the clipped entry point; a point that rounds onto the far
-        // side of a face gets a zero-length first cell and steps back in
+        // voxel of the entry point; a point that rounds onto the far side of
+        // a face gets a zero-length first cell and steps back in
+        int nk = grid_dim(G, k);
         float x = (p[k] + d[k] * t0 - G.o[k]) * G.inv_h;
-        int i = max(0, min(n[k] - 1, (int)floorf(x)));
+        int i = max(0, min(nk - 1, (int)floorf(x)));
         iv[k] = i;
         if (d[k] > 1e-12f) {
             step[k] = 1;
@@ -492,8 +548,7 @@ __device__ int tally_segment(const KGrid& G, double* tally, const float p[3], co
         }
     }
     float t = t0;
-    const double dwk = (double)wk, dwh = (double)wh;
-    int guard = n[0] + n[1] + n[2] + 4;
+    int guard = G.nx + G.ny + G.nz + 4;
     int visits = 0;
     while (t < t1 && guard-- > 0) {
         int ax = (tmax[0] < tmax[1]) ? (tmax[0] < tmax[2] ? 0 : 2) : (tmax[1] < tmax[2] ? 1 : 2);
@@ -501,17 +556,25 @@ __device__ int tally_segment(const KGrid& G, double* tally, const float p[3], co
         float len = tn - t;
         if (len > 0.0f) {
             long long v = ((long long)iv[0] * G.ny + iv[1]) * G.nz + iv[2];
-            score(tally, v, dwk * len, dwh * len);
+            score(tally, v, wk * len, wh * len);
             ++visits;
         }
         t = tn;
         if (t >= t1) break;
         iv[ax] += step[ax];
-        if (iv[ax] < 0 || iv[ax] >= n[ax]) break;
+        if (iv[ax] < 0 || iv[ax] >= grid_dim(G, ax)) break;
         tmax[ax] += tdel[ax];
     }
     return visits;
 }
+
+// Track segments of one warp, shared so that the warp can split long ones.
+struct SegRec {
+    float p[3], d[3];
+    float t0, t1;
+    float wk, wh;
+    int batch, m;
+};
 
 // ---------------------------------------------------------------------------
 // source (source.py:67-210)
@@ -580,18 +643,51 @@ __device__ void sample_source(const KSource& S, HistoryRng& rng, float p[3], flo
 // ---------------------------------------------------------------------------
 
 constexpr int HIST_CHUNK = 256;     // histories a warp takes from the global counter at once
+constexpr int BLOCK = 256;
+constexpr int WARPS_PER_BLOCK = BLOCK / 32;
+constexpr unsigned FULL = 0xffffffffu;
+
+__device__ __forceinline__ int warp_sum(int v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
+    return v;
+}
+
+__device__ __forceinline__ int warp_inclusive_scan(int v, int lane) {
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        int t = __shfl_up_sync(FULL, v, o);
+        if (lane >= o) v += t;
+    }
+    return v;
+}
+
+// Each loop iteration is one transport step of every lane, in three
+// warp-synchronous phases:
+//   1. lanes without a photon start the next history; every lane finds its
+//      material, mu and next boundary and decides its segment;
+//   2. the warp scores all its segments together: long segments are cut
+//      into equal-length pieces so that every lane walks about the same
+//      number of voxels (the pieces' partial voxel lengths add up exactly);
+//   3. lanes move their photon and sample the interaction, if any.
+#ifndef CC_MIN_BLOCKS
+#define CC_MIN_BLOCKS 2
+#endif
 
 template <bool FROM_SOURCE, bool TALLY>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(BLOCK, CC_MIN_BLOCKS)
 transport_kernel(const KTables T, const KScene S, const KGrid G, const KSource SRC, const KRun R) {
     extern __shared__ double s_edep[];             // [n_scratch][n_mat]
     __shared__ unsigned long long s_cnt[6];
+    __shared__ SegRec s_seg[TALLY ? WARPS_PER_BLOCK : 1][32];
+    __shared__ int s_pre[TALLY ? WARPS_PER_BLOCK : 1][33];
     const int n_acc = R.n_scratch * T.n_mat;
     for (int i = threadIdx.x; i < n_acc; i += blockDim.x) s_edep[i] = 0.0;
     if (threadIdx.x < 6) s_cnt[threadIdx.x] = 0ull;
     __syncthreads();
 
     const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
     unsigned long long c_abs = 0, c_esc = 0, c_sc = 0, c_fl = 0, c_steps = 0, c_vox = 0;
 
     // warp-local pool [pool_next, pool_end)
@@ -604,13 +700,13 @@ transport_kernel(const KTables T, const KScene S, const KGrid G, const KSource S
     HistoryRng rng;
 
     while (true) {
-        // ---- regeneration: lanes without a photon take the next history ----
-        unsigned need = __ballot_sync(0xffffffffu, !live);
+        // ---- phase 1a: regeneration ----
+        unsigned need = __ballot_sync(FULL, !live);
         while (need) {
             if (pool_next >= pool_end) {
                 long long base = 0;
                 if (lane == 0) base = (long long)atomicAdd(R.work, (unsigned long long)HIST_CHUNK);
-                base = __shfl_sync(0xffffffffu, base, 0);
+                base = __shfl_sync(FULL, base, 0);
                 if (base >= R.n) break;
                 pool_next = base;
                 pool_end = min(base + HIST_CHUNK, R.n);
@@ -640,47 +736,88 @@ transport_kernel(const KTables T, const KScene S, const KGrid G, const KSource S
                 steps = 0;
             }
             pool_next += take;
-            need = __ballot_sync(0xffffffffu, !live);
+            need = __ballot_sync(FULL, !live);
         }
-        if (__all_sync(0xffffffffu, !live)) break;
-        if (!live) continue;
+        if (__all_sync(FULL, !live)) break;
 
-        // ---- one step ----
-        ++steps;
-        if (mat < 0) {
-            mat = locate(S, p[0] + d[0] * S.eps, p[1] + d[1] * S.eps, p[2] + d[2] * S.eps);
+        // ---- phase 1b: material, mu, next boundary ----
+        bool go = live;
+        bool interact = false, escape = false;
+        float s = 0.f, tau_b = 0.f, loge = 0.f;
+        float t0 = 0.f, t1 = 0.f, wk = 0.f, wh = 0.f;
+        int tal_n = 0;
+        Lookup L;
+        L.idx = 0;
+        L.frac = 0.f;
+        if (go) {
+            ++steps;
+            if (mat < 0) mat = locate(S, p, d);
+            if (mat >= T.n_mat) {
+                atomicOr(R.status, ST_BOUNDS);
+                go = live = false;
+            } else if (!(E >= E_MIN_KEV && E <= E_MAX_KEV)) {
+                atomicOr(R.status, ST_ENERGY);
+                go = live = false;
+            }
         }
-        if (mat >= T.n_mat) {
-            atomicOr(R.status, ST_BOUNDS);
-            live = false;
-            continue;
+        if (go) {
+            const DevMaterial& M = T.mats[mat];
+            loge = __logf(E);
+            L = energy_index(T, M, loge);
+            float mu = mu_total(T, M, L);
+            float tb = INFINITY;
+            for (int i = 0; i < S.n_prims; ++i) tb = prim_next(S.prims[i], p, d, S.eps, tb);
+            float tw = world_exit(S, p, d);
+            escape = tw <= tb;
+            tb = fminf(tb, tw);
+            tau_b = mu * tb;
+            interact = tau < tau_b;
+            s = interact ? tau / fmaxf(mu, 1e-30f) : tb;
+            if (TALLY && clip_to_grid(G, p, d, s, t0, t1)) {
+                wk = E * muen_rho(T, M, loge) * M.density;
+                wh = h10_coeff(T, loge);
+                tal_n = visit_estimate(G, p, d, t0, t1);
+            }
         }
-        const DevMaterial& M = T.mats[mat];
-        if (!(E >= E_MIN_KEV && E <= E_MAX_KEV)) {
-            atomicOr(R.status, ST_ENERGY);
-            live = false;
-            continue;
-        }
-        float loge = __logf(E);
-        Lookup L = energy_index(T, M, loge);
-        float mu = mu_total(T, M, L);
 
-        float tb = INFINITY;
-        for (int i = 0; i < S.n_prims; ++i) tb = prim_next(S.prims[i], p, d, S.eps, tb);
-        float tw = world_exit(S, p, d);
-        bool escape = tw <= tb;
-        tb = fminf(tb, tw);
-        float tau_b = mu * tb;
-        bool interact = tau < tau_b;
-        float s = interact ? tau / fmaxf(mu, 1e-30f) : tb;
-
+        // ---- phase 2: the warp scores its segments together ----
         if (TALLY) {
-            float wk = E * muen_rho(T, M, loge) * M.density;
-            float wh = h10_coeff(T, loge);
-            c_vox += tally_segment(G, G.tally + (size_t)batch * 2 * G.nvox, p, d, s, wk, wh);
+            int V = warp_sum(tal_n);
+            if (V > 0) {
+                int C = max((V + 31) >> 5, 2);
+                int m = (tal_n + C - 1) / C;
+                if (m > 0) {
+                    SegRec& r = s_seg[warp][lane];
+                    r.p[0] = p[0]; r.p[1] = p[1]; r.p[2] = p[2];
+                    r.d[0] = d[0]; r.d[1] = d[1]; r.d[2] = d[2];
+                    r.t0 = t0; r.t1 = t1; r.wk = wk; r.wh = wh; r.batch = batch; r.m = m;
+                }
+                int incl = warp_inclusive_scan(m, lane);
+                s_pre[warp][lane] = incl - m;
+                if (lane == 31) s_pre[warp][32] = incl;
+                __syncwarp();
+                const int U = s_pre[warp][32];
+                for (int u = lane; u < U; u += 32) {
+                    int lo = 0, hi = 32;            // s_pre[lo] <= u < s_pre[hi]
+                    while (hi - lo > 1) {
+                        int mid = (lo + hi) >> 1;
+                        if (s_pre[warp][mid] <= u) lo = mid; else hi = mid;
+                    }
+                    const SegRec& q = s_seg[warp][lo];
+                    int k = u - s_pre[warp][lo];
+                    float dt = (q.t1 - q.t0) / (float)q.m;
+                    float ta = q.t0 + dt * (float)k;
+                    float tz = (k == q.m - 1) ? q.t1 : ta + dt;
+                    c_vox += walk_range(G, G.tally + (size_t)q.batch * 2 * G.nvox, q.p, q.d, ta, tz, q.wk, q.wh);
+                }
+                __syncwarp();
+            }
         }
-        p[0] += d[0] * s; p[1] += d[1] * s; p[2] += d[2] * s;
+        if (!go) continue;
 
+        // ---- phase 3: move, cross or interact ----
+        const DevMaterial& M = T.mats[mat];
+        p[0] += d[0] * s; p[1] += d[1] * s; p[2] += d[2] * s;
         bool done = false;
         bool esc = false, absd = false;
         if (!interact) {
@@ -739,7 +876,7 @@ transport_kernel(const KTables T, const KScene S, const KGrid G, const KSource S
                 scatter_direction(d, cost, TWO_PI * rng.uniform());
                 tau = -__logf(rng.uniform());
             }
-            // the interaction point stays inside the same material
+            mat = -1;                      // new direction: re-locate (material_at every round)
         }
         if (!done && steps >= R.max_steps) {
             atomicOr(R.status, ST_STEPS);
@@ -855,7 +992,7 @@ struct cc_ctx {
     unsigned long long* d_counters = nullptr;   // [5] + work counter
     int block = 256;
     int blocks_per_sm = 0;                       // 0 = occupancy based
-    long long max_steps = 1000000;
+    long long max_steps = 100000;
 };
 
 struct cc_tables {
@@ -1122,6 +1259,7 @@ int cc_scene_create(cc_ctx* ctx, const cc_primitive* prims, int32_t n_prims, int
         g.axis = p.axis;
         for (int a = 0; a < 3; ++a) { g.c[a] = (float)p.center[a]; g.h[a] = (float)(0.5 * p.size[a]); }
         g.r2 = (float)(p.radius * p.radius);
+        g.r = (float)p.radius;
         g.hh = (float)(0.5 * p.height);
     }
     *out = s;

@@ -118,6 +118,10 @@ class Engine:
     def set_launch(self, block_size: int = 256, blocks_per_sm: int = 0) -> None:
         N.check(self.lib.cc_ctx_set_launch(self.ctx, block_size, blocks_per_sm))
 
+    def set_step_limit(self, max_steps: int = 100_000) -> None:
+        """Transport steps a single photon may take before the run fails with CC_E_TIMEOUT."""
+        N.check(self.lib.cc_ctx_set_step_limit(self.ctx, int(max_steps)))
+
     def tables(self, names: list[str], need_muen: bool) -> tuple[TableSet, C.c_void_p]:
         key = (tuple(names), need_muen)
         with self._lock:

@@ -236,3 +236,35 @@ def test_source_sampling_matches_oracle(engine):
         np.testing.assert_allclose(a.std(axis=0), b.std(axis=0), rtol=0.01, atol=1e-3)
     for ek in (30.0, 60.0, 90.0):
         assert abs(np.mean(en == ek) - np.mean(eo == ek)) < 0.005
+
+
+def test_grazing_photons_on_a_thin_sheet(engine):
+    """Photons starting on the face of a 0.05 cm lead sheet at a grazing
+    angle: FP32 positions cannot resolve their normal motion per step, yet
+    they must enter the sheet like the FP64 oracle's photons do."""
+    geoms = [{"name": "air", "shape": "box", "material": "air", "center": [0, 0, 50], "size_cm": [100, 100, 100]},
+             {"name": "pb", "shape": "box", "material": "lead", "center": [0, 0, 40], "size_cm": [30, 30, 0.05]}]
+    d = np.array([0.995934, -0.09004128, -0.00283073])
+    d /= np.linalg.norm(d)
+    start = [0.8246886, -11.880426, 40.025]
+    engine.set_step_limit(2000)
+    try:
+        _, _, _, rg = _gpu_tp(engine, geoms, start, d, 59.0, 200_000, seed=6)
+    finally:
+        engine.set_step_limit(100_000)
+    pos, dirv, eo = W.pencil_beam_arrays(20_000, start, d, 59.0)
+    ro = O.transport_photons(pos, dirv, eo, O.OracleGeometry(geoms), np.random.default_rng(6))
+    z = _z(rg.absorbed.mean(), 200_000, ro.absorbed.mean(), 20_000)
+    assert abs(z) < 4, (rg.absorbed.mean(), ro.absorbed.mean())
+
+
+def test_room_scene_has_no_runaway_histories(engine):
+    """Regression: with seed 6 one history of the room scene used to slide
+    along the lead sheet's face for 28,404 steps."""
+    from chatcarlo_b200.transport import run_transport
+    engine.set_step_limit(2000)
+    try:
+        r = run_transport(W.room(), n_histories=8_000_000, seed=6, batch_size=200_000, engine=engine)
+    finally:
+        engine.set_step_limit(100_000)
+    assert r.n_steps / 8e6 < 10
