@@ -168,7 +168,8 @@ def main():
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--histories-per-step", type=float, default=1e7)
     ap.add_argument("--e2e-histories", type=float, default=4e6)
-    ap.add_argument("--cpu-per-core", type=int, default=25_000)
+    ap.add_argument("--cpu-per-core", type=int, default=40_000,
+                    help="CPU sample: histories per host process is a fifth of this")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -282,10 +283,32 @@ def main():
     traffic_per_hist = profile_traffic()
     hist_per_launch = n_h / max(tr_launch, 1)
 
-    # e2e: the public transport_photons API on host buffers (pinned), each
-    # step copies its photons in and the per-photon results and tallies out
+    # e2e: the public run_transport call a user makes, once per step: scene,
+    # source and spectrum descriptors go to the device, the five tally grids
+    # (kerma, H*(10), their batch sums of squares, batches hit) come back
     e2e = None
+    e2e_photons = None
     if rank == 0:
+        from chatcarlo_b200.transport import run_transport
+        eg = W.make_grid(W.ROOM_GRID, track_uncertainty=True)
+        e_ms = []
+        for i in range(args.warmup + min(args.steps, 5)):
+            flush.zero_()
+            torch.cuda.synchronize()
+            ev0.record()
+            run_transport(raw, n_histories=S, seed=seed + 100 + i, batch_size=BATCH, dose_grid=True, grid=eg,
+                          engine=eng, first_history=(1 << 44) + i * S)
+            ev1.record()
+            torch.cuda.synchronize()
+            if i >= args.warmup:
+                e_ms.append(ev0.elapsed_time(ev1))
+        nvox = int(np.prod(grid.shape))
+        h2d = (len(raw["geometry"]) * C.sizeof(N.Primitive) + C.sizeof(N.SourceDesc)
+               + 2 * 8 * len(raw["source"]["spectrum"]) + 6 * 8)
+        e2e = {"value": S * len(e_ms) / (float(np.sum(e_ms)) / 1e3), "unit": "histories/s",
+               "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(nvox * (4 * 8 + 4) + C.sizeof(N.RunOut)),
+               "api": "chatcarlo_b200.transport.run_transport (C ABI cc_run + cc_grid_download)"}
+        # the same through transport_photons on pinned host photon arrays
         ne = int(args.e2e_histories)
         pin = lambda shape: torch.empty(shape, dtype=torch.float64, pin_memory=True).numpy()  # noqa: E731
         p0, d0, e0 = pin((ne, 3)), pin((ne, 3)), pin((ne,))
@@ -305,11 +328,10 @@ def main():
             torch.cuda.synchronize()
             if i >= args.warmup:
                 e_ms.append(ev0.elapsed_time(ev1))
-        nvox = int(np.prod(grid.shape))
-        e2e = {"value": ne * len(e_ms) / (float(np.sum(e_ms)) / 1e3), "unit": "histories/s",
-               "h2d_bytes_per_step": ne * (3 + 3 + 1) * 8,
-               "d2h_bytes_per_step": ne * (3 + 3 + 1) * 8 + ne * (4 + 1 + 1) + 2 * nvox * 8,
-               "api": "chatcarlo_b200.transport.transport_photons (C ABI cc_transport_photons, host buffers)"}
+        e2e_photons = {"value": ne * len(e_ms) / (float(np.sum(e_ms)) / 1e3), "unit": "histories/s",
+                       "h2d_bytes_per_step": ne * (3 + 3 + 1) * 8,
+                       "d2h_bytes_per_step": ne * (3 + 3 + 1) * 8 + ne * (4 + 1 + 1) + 2 * nvox * 8,
+                       "api": "chatcarlo_b200.transport.transport_photons (C ABI cc_transport_photons, pinned host arrays)"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -335,7 +357,8 @@ def main():
                              "voxel_visits_per_history": n_vox,
                              "avg_launch_ms": tr_ms / max(tr_launch, 1),
                              "histories_per_launch": hist_per_launch},
-                "cpu_baseline": cpu, "e2e": e2e, "clocks": clocks, "gpu_launches": int(launches),
+                "cpu_baseline": cpu, "e2e": e2e, "e2e_photons": e2e_photons, "clocks": clocks,
+                "gpu_launches": int(launches),
                 "reduce_ms": red_ms}
         print(json.dumps(line))
     dg.close()

@@ -1,0 +1,171 @@
+"""Host-side logic that needs no GPU: scene schema, tables handed to the
+engine, statistics helpers, history sharding and the tally reduction over
+ranks (world size 2 over gloo)."""
+import os
+import socket
+
+import numpy as np
+import pytest
+
+import cc_oracle as O
+from chatcarlo_b200 import devtables, tables as tb, workloads as W
+from chatcarlo_b200.scene import validate_scene
+from chatcarlo_b200.tally import VoxelGrid, relative_error, standard_error
+
+
+def test_benchmark_scenes_validate():
+    for raw in (W.plain_mc(), W.room()):
+        sc = validate_scene(raw)
+        assert sc.ok, sc.errors
+
+
+@pytest.mark.parametrize("mutate,path", [
+    (lambda r: r["geometry"][0].update(shape="cone"), "geometry[0].shape"),
+    (lambda r: r["geometry"][1].update(material="unobtanium"), "geometry[1].material"),
+    (lambda r: r["source"].update(spectrum=[{"energy_keV": 200.0, "weight": 1.0}]), "source.spectrum"),
+    (lambda r: r["source"].update(kvp=80), "source"),
+    (lambda r: r["geometry"][2].update(axis="w"), "geometry[2].axis"),
+    (lambda r: r["source"]["field"].update(size_cm=[35.0]), "source.field.size_cm"),
+])
+def test_scene_errors_name_the_entry(mutate, path):
+    raw = W.room()
+    mutate(raw)
+    sc = validate_scene(raw)
+    assert not sc.ok
+    assert any(e.path == path for e in sc.errors), [str(e) for e in sc.errors]
+
+
+def test_voxel_grid_from_bbox_matches_reference_rule():
+    g = VoxelGrid.from_bbox(np.array([-250.0, -250.0, -50.0]), np.array([250.0, 250.0, 350.0]), 5.0)
+    assert g.shape == (100, 100, 80)
+    og = O.OracleGrid.from_bbox(np.array([-250.0, -250.0, -50.0]), np.array([250.0, 250.0, 350.0]), 5.0)
+    assert og.shape == g.shape
+    pts = np.array([[-250.0, -250.0, -50.0], [249.99, 0.0, 0.0], [250.0, 0.0, 0.0]])
+    idx, ok = g.voxel_index(pts)
+    assert ok.tolist() == [True, True, False]
+
+
+def test_statistics_helpers_match_oracle_moments():
+    rng = np.random.default_rng(0)
+    m = O.Moments()
+    batches = []
+    for n_b in (100, 250, 80, 400):
+        s_b = float(rng.normal(10.0, 2.0)) * n_b
+        batches.append((s_b, n_b))
+        m.add_batch({"x": s_b}, n_b)
+    T = sum(s for s, _ in batches)
+    Q = sum(s * s / n for s, n in batches)
+    N = sum(n for _, n in batches)
+    assert m.sums["x"] == pytest.approx(T) and m.sum2s["x"] == pytest.approx(Q)
+    se = standard_error(T, Q, 4, N)
+    assert se == pytest.approx(np.sqrt((Q - T * T / N) / 3 / N))
+    assert relative_error(T, Q, 4, N) == pytest.approx(se / (T / N))
+    assert np.isnan(relative_error(T, Q, 1, N))
+
+
+@pytest.mark.parametrize("material", ["bone", "concrete", "lead", "air"])
+def test_union_grid_reproduces_element_interpolation(material):
+    """Per element, interpolating the union-grid table gives the element's own
+    interpolation (materials.py:248-262); the mixed total differs from the sum
+    of interpolated parts only at second order."""
+    mt = devtables.build_material(material)
+    rng = np.random.default_rng(1)
+    e = np.exp(rng.uniform(0.0, np.log(150.0), 3000))
+    le = np.log(e)
+    idx = np.clip(np.searchsorted(mt.log_e, le), 1, len(mt.log_e) - 1)
+    fr = (le - mt.log_e[idx - 1]) / (mt.log_e[idx] - mt.log_e[idx - 1])
+    for i, z in enumerate(mt.zs):
+        for k, kind in enumerate(("photo", "compt", "rayl")):
+            y = mt.log_elem[i, k]
+            got = np.exp(y[idx - 1] + fr * (y[idx] - y[idx - 1]))
+            want = mt.fractions[i] * O.element_cs(int(z), e, kind)
+            np.testing.assert_allclose(got, want, rtol=1e-10)
+    y = mt.log_parts[:, 3]
+    tot = np.exp(y[idx - 1] + fr * (y[idx] - y[idx - 1]))
+    np.testing.assert_allclose(tot, O.mu_rho(material, e), rtol=2e-5)
+
+
+def test_element_tables_for_the_engine():
+    el = devtables.build_element(82)
+    assert el.emits and el.k_edge == pytest.approx(88.0045)
+    assert el.s_over_z[0] == 0.0 and el.s_over_z[-1] == pytest.approx(1.0, rel=0.01)
+    assert np.all(np.diff(el.ray_a) > 0)
+    assert devtables.build_element(8).emits is False
+
+
+def test_source_spec_fields():
+    from chatcarlo_b200.source import SourceSpec, beam_basis
+    for d in ([0, 0, 1.0], [0, 1.0, 0], [0.6, 0.0, -0.8]):
+        u, v = beam_basis(np.array(d))
+        m = np.stack([u, v, np.array(d)])
+        np.testing.assert_allclose(m @ m.T, np.eye(3), atol=1e-12)
+    spec = SourceSpec(W.room()["source"])
+    assert spec.desc.n_energies == 75 and spec.desc.sid_cm == 180.0
+    with pytest.raises(RuntimeError):
+        SourceSpec(dict(W.room()["source"], heel_effect=True))
+
+
+def test_cli_parser():
+    from chatcarlo_b200.__main__ import build_parser
+    a = build_parser().parse_args(["run", "s.yaml", "-n", "1e6", "--seed", "3", "--dose-grid",
+                                   "--resolution", "2.5", "--dose-out", "d.npz"])
+    assert a.n_histories == 1e6 and a.seed == 3 and a.dose_grid and a.resolution == 2.5
+
+
+def test_shard_ranges_partition_the_histories():
+    from chatcarlo_b200.distributed import shard_range
+    for n, w in ((10, 3), (1000003, 8), (5, 8)):
+        parts = [shard_range(n, r, w) for r in range(w)]
+        assert sum(c for _, c in parts) == n
+        firsts = [f for f, _ in parts]
+        assert firsts == sorted(firsts)
+        for (f, c), (g, _) in zip(parts, parts[1:]):
+            assert f + c == g
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    p = s.getsockname()[1]
+    s.close()
+    return p
+
+
+def _rank_main(rank, world, port, q):
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    from chatcarlo_b200.distributed import reduce_result
+    from chatcarlo_b200.transport import TransportResult
+    g = VoxelGrid(origin_cm=np.zeros(3), shape=(4, 3, 2), voxel_size_cm=1.0, track_uncertainty=True)
+    g.kerma_keV += rank + 1.0
+    g.h10_track_pSv_cm3 += 10.0 * (rank + 1)
+    g.kerma_sum2 += 0.5
+    g.h10_sum2 += 0.25
+    g.n_batches_hit += 1
+    g.n_batches, g.n_histories = 3, 300
+    res = TransportResult(n_histories=1000, energy_deposited_MeV={}, fraction_absorbed=0.25 * (rank + 1),
+                          fraction_escaped=0.5, mean_scatter_events=2.0, grid=g, n_fluorescence=7)
+    reduce_result(res)
+    q.put((rank, float(g.kerma_keV.sum()), float(g.h10_track_pSv_cm3[0, 0, 0]), int(g.n_batches_hit.max()),
+           g.n_batches, g.n_histories, res.n_histories, res.fraction_absorbed, res.n_fluorescence))
+    dist.destroy_process_group()
+
+
+def test_tally_reduction_over_two_ranks():
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank_main, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    out = [q.get(timeout=120) for _ in procs]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    for rank, ksum, h0, nhit, nb, nh, n, fa, nfl in out:
+        assert ksum == pytest.approx(24 * 3.0)
+        assert h0 == pytest.approx(30.0)
+        assert nhit == 2 and nb == 6 and nh == 600 and n == 2000 and nfl == 14
+        assert fa == pytest.approx((250 + 500) / 2000)
