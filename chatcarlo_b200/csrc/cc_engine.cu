@@ -27,6 +27,7 @@
 
 #include <algorithm>
 #include <cstdlib>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -1745,6 +1746,100 @@ int cc_sample_source(cc_ctx* c, const cc_source* src, int64_t n, uint64_t seed, 
     cudaFree(buf);
     if (e != cudaSuccess) return set_error(CC_E_DEVICE, std::string("sample_source: ") + cudaGetErrorString(e));
     return CC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free transport of device-resident photons.
+//
+// Some callers cannot let the engine allocate device memory: a host process
+// that hands every library a fixed slice of a pre-sized memory pool, a
+// real-time pipeline that forbids allocation once it runs (cudaMalloc and
+// cudaFree synchronise the device and can stall its other streams), or a
+// plug-in whose host application owns all allocations.  For them this entry
+// point keeps the per-call scratch -- the reduction counters, the history
+// work counter, the status word and the per-material deposited energy -- in
+// one file-scope __device__ array instead of the context's buffers.  Every
+// GPU that loads this library holds that array (NOALLOC_SCRATCH_WORDS 64-bit
+// words, 512 bytes) until the process exits.
+// ---------------------------------------------------------------------------
+
+constexpr int NOALLOC_SCRATCH_WORDS = 64;
+// word layout: [0, 6) counters, 6 history work counter, 7 status, [8, 8 + MAX_MATS) deposited energy
+static_assert(8 + MAX_MATS <= NOALLOC_SCRATCH_WORDS, "scratch too small for the material limit");
+static __device__ __align__(256) unsigned long long g_noalloc_scratch[NOALLOC_SCRATCH_WORDS];
+
+static std::mutex g_noalloc_mutex;
+static unsigned long long* g_noalloc_addr[64];   // device address of the array, per device ordinal
+
+int cc_transport_photons_device_noalloc(const cc_scene* scene, const cc_tables* tables, int64_t n,
+                                        double* d_pos, double* d_dir, double* d_en, uint64_t seed,
+                                        uint64_t stream_offset, int32_t fluorescence, int32_t* d_nsc,
+                                        uint8_t* d_abs, uint8_t* d_esc, double* edep,
+                                        int64_t* n_fluor, void* stream) {
+    if (!scene || !tables) return set_error(CC_E_INVALID, "NULL argument");
+    if (n < 0) return set_error(CC_E_INVALID, "n < 0");
+    if (tables->n_mat > MAX_MATS)
+        return set_error(CC_E_INVALID, "the allocation-free entry point handles at most 16 materials "
+                                       "(its static scratch holds 16 deposited-energy sums)");
+    if (n == 0) { if (n_fluor) *n_fluor = 0; return CC_OK; }
+    if (!d_pos || !d_dir || !d_en) return set_error(CC_E_INVALID, "photon arrays are NULL");
+    const int dev = tables->ctx->device;
+    if (dev < 0 || dev >= 64) return set_error(CC_E_INVALID, "device ordinal out of range");
+    CC_CUDA(cudaSetDevice(dev));
+    unsigned long long* scratch = nullptr;
+    {
+        // first call on this device: resolve the array's device address with
+        // the device current (the host-side symbol is not a device address)
+        std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+        if (!g_noalloc_addr[dev]) {
+            void* ptr = nullptr;
+            cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
+            if (e != cudaSuccess || !ptr)
+                return set_error(CC_E_DEVICE, std::string("cudaGetSymbolAddress of the scratch array: ") +
+                                                  cudaGetErrorString(e));
+            g_noalloc_addr[dev] = (unsigned long long*)ptr;
+        }
+        scratch = g_noalloc_addr[dev];
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    // the array keeps the previous call's contents: clear it
+    CC_CUDA(cudaMemsetAsync(scratch, 0, NOALLOC_SCRATCH_WORDS * sizeof(unsigned long long), st));
+    KRun R;
+    memset(&R, 0, sizeof(R));
+    R.n = n;
+    R.first = (long long)stream_offset;
+    R.fluorescence = fluorescence;
+    R.seed = seed;
+    R.pos = d_pos; R.dir = d_dir; R.energy = d_en;
+    R.n_scatter = d_nsc; R.absorbed = d_abs; R.escaped = d_esc;
+    R.n_scratch = 1;
+    R.batch_size = n;
+    R.max_steps = tables->ctx->max_steps;
+    R.counters = scratch;
+    R.work = scratch + 6;
+    R.status = (unsigned*)(scratch + 7);
+    R.edep = (double*)(scratch + 8);
+    KGrid G;
+    memset(&G, 0, sizeof(G));
+    KSource S;
+    memset(&S, 0, sizeof(S));
+    const size_t smem = (size_t)tables->n_mat * sizeof(double);
+    int sms = 0, occ = 0;
+    CC_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, transport_kernel<false, false>, BLOCK, smem) != cudaSuccess ||
+        occ < 1)
+        occ = 1;
+    transport_kernel<false, false><<<sms * occ, BLOCK, smem, st>>>(tables->k, scene->k, G, S, R);
+    CC_CUDA(cudaGetLastError());
+    unsigned long long words[8 + MAX_MATS];
+    CC_CUDA(cudaMemcpyAsync(words, scratch, sizeof(words), cudaMemcpyDeviceToHost, st));
+    CC_CUDA(cudaStreamSynchronize(st));
+    if (edep) {
+        const double* dep = (const double*)(words + 8);
+        for (int m = 0; m < tables->n_mat; ++m) edep[m] += dep[m];
+    }
+    if (n_fluor) *n_fluor = (int64_t)words[3];
+    return status_to_error((unsigned)words[7]);
 }
 
 }  // extern "C"

@@ -213,6 +213,27 @@ int cc_run(cc_ctx* ctx, const cc_scene* scene, const cc_tables* tables, const cc
            int64_t first_history, int32_t fluorescence, double* edep_by_material,
            double* edep_sum2_by_material, cc_run_out* out);
 
+/* Allocation-free variant of cc_transport_photons_device.  It has no
+ * counterpart in the reference.  It is for callers that cannot let the
+ * library allocate device memory: an application that owns every device
+ * allocation (a fixed memory pool per library), or a pipeline that forbids
+ * cudaMalloc/cudaFree once it runs because they synchronise the device.
+ * The scene, tables and all photon arrays are the caller's; the per-call
+ * scratch (counters, work counter, status, deposited energy of up to 16
+ * materials) lives in one static 512-byte __device__ array that each GPU
+ * loading the library keeps until exit.  No tally grid.  The first call on
+ * a device resolves that array's address (cudaGetSymbolAddress); make that
+ * first call before any stream capture.  Every call clears and reuses the
+ * same array, so calls that overlap on the GPU (other streams, other host
+ * threads) race: serialise them.  stream is a cudaStream_t (NULL = the
+ * legacy default stream); the call returns after the stream has finished
+ * its work. */
+int cc_transport_photons_device_noalloc(const cc_scene* scene, const cc_tables* tables, int64_t n,
+                                        double* d_pos, double* d_dir, double* d_energy,
+                                        uint64_t seed, uint64_t stream_offset, int32_t fluorescence,
+                                        int32_t* d_n_scatter, uint8_t* d_absorbed, uint8_t* d_escaped,
+                                        double* edep_by_material, int64_t* n_fluorescence, void* stream);
+
 /* Sample source photons only (tests of source.py parity). */
 int cc_sample_source(cc_ctx* ctx, const cc_source* src, int64_t n, uint64_t seed,
                      int64_t first_history, double* pos, double* dir, double* energy);
