@@ -168,8 +168,8 @@ def main():
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--histories-per-step", type=float, default=1e7)
     ap.add_argument("--e2e-histories", type=float, default=4e6)
-    ap.add_argument("--cpu-per-core", type=int, default=40_000,
-                    help="CPU sample: histories per host process is a fifth of this")
+    ap.add_argument("--cpu-histories-per-process", type=int, default=120_000,
+                    help="CPU sample per step: histories in each of the host-core processes")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
@@ -181,7 +181,7 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return 0
-        per_core = max(2000, args.cpu_per_core // 5)
+        per_core = args.cpu_histories_per_process // 2
         value, cores, times = run_cpu_reference(args.steps, args.warmup, per_core)
         line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "histories/s",
                 "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
@@ -335,7 +335,7 @@ def main():
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        per_core = max(1000, args.cpu_per_core // 5)
+        per_core = args.cpu_histories_per_process
         v, cores, times = run_cpu_reference(1, 0, per_core)
         cpu = {"value": v, "unit": "histories/s", "cores": cores, "kind": "port",
                "sample": f"room workload, {per_core} histories in each of {cores} spawned processes "

@@ -59,9 +59,7 @@ class MaterialDesc(C.Structure):
     _fields_ = [("density", C.c_double), ("n_nodes", C.c_int32), ("n_elements", C.c_int32),
                 ("log_e", C.POINTER(C.c_double)), ("log_parts", C.POINTER(C.c_double)),
                 ("log_elem", C.POINTER(C.c_double)), ("element_slot", C.POINTER(C.c_int32)),
-                ("n_muen", C.c_int32), ("pad", C.c_int32),
-                ("muen_log_e", C.POINTER(C.c_double)), ("muen_log_v", C.POINTER(C.c_double)),
-                ("muen_slope", C.POINTER(C.c_double))]
+                ("log_tally", C.POINTER(C.c_double))]
 
 
 class ElementDesc(C.Structure):
@@ -75,10 +73,7 @@ class ElementDesc(C.Structure):
 
 class TableDesc(C.Structure):
     _fields_ = [("n_materials", C.c_int32), ("n_elements", C.c_int32),
-                ("materials", C.POINTER(MaterialDesc)), ("elements", C.POINTER(ElementDesc)),
-                ("n_h10", C.c_int32), ("pad", C.c_int32),
-                ("h10_log_e", C.POINTER(C.c_double)), ("h10_log_v", C.POINTER(C.c_double)),
-                ("h10_e_min", C.c_double), ("h10_e_max", C.c_double)]
+                ("materials", C.POINTER(MaterialDesc)), ("elements", C.POINTER(ElementDesc))]
 
 
 class SourceDesc(C.Structure):

@@ -43,6 +43,7 @@ constexpr int MAX_ELEMS_PER_MAT = 16;
 constexpr int MAX_ELEMS = 48;
 constexpr int TABLE_N = 2000;            // F, A, S tables (materials.py:376-496)
 constexpr int N_BUCKETS = 4096;          // uniform log-E index per material
+constexpr int RAY_BUCKETS = 1024;        // uniform-in-A index of each Rayleigh A(x) table
 constexpr int MAX_SCRATCH = 64;          // batches per launch
 constexpr float LOG_E_MIN = 0.0f;        // ln(1 keV)
 constexpr float E_MIN_KEV = 1.0f;
@@ -67,7 +68,7 @@ struct DevPrim {
 struct DevMaterial {
     float density;
     int n_nodes, n_el, node_off;
-    int elem_off, muen_off, n_muen, bucket_off;
+    int elem_off, bucket_off;
     float bucket_scale;
     int el_slot[MAX_ELEMS_PER_MAT];
 };
@@ -75,6 +76,7 @@ struct DevMaterial {
 struct DevElement {
     float k_edge, k_prob, omega;
     int n_lines, emits, pad;
+    float ray_scale;        // RAY_BUCKETS / A(x_end)
     float line_e[8];
     float line_cum[8];
 };
@@ -89,13 +91,9 @@ struct KTables {
     const float* sq;       // [n_elem][TABLE_N] S/Z
     const float* rx;       // [n_elem][TABLE_N]
     const float* ra;       // [n_elem][TABLE_N]
-    const float* muen_x;
-    const float* muen_y;
-    const float* muen_d;
-    const float* h10_x;
-    const float* h10_y;
-    int n_mat, n_elem, n_h10;
-    float h10_lx_lo, h10_lx_hi;
+    const int* ray_bucket; // [n_elem][RAY_BUCKETS + 1] last row with A <= bucket start
+    const float2* node_tally;   // per node ln(mu_en/rho), ln(h*(10)/Phi)
+    int n_mat, n_elem;
 };
 
 struct KScene {
@@ -207,13 +205,12 @@ __device__ __forceinline__ int locate(const KScene& s, const float p[3], const f
 // (o = p - c relative coordinate, tol the band of this face); a face the
 // point sits on contributes t = 0.  Returns false for a ray parallel to the
 // slab outside it.
-__device__ __forceinline__ bool slab_pair(float o, float d, float lo, float hi, float tol,
+__device__ __forceinline__ bool slab_pair(float o, float d, float inv, float lo, float hi, float tol,
                                           float& tmin, float& tmax) {
     float dlo = lo - o, dhi = hi - o;
     if (fabsf(dlo) <= tol) dlo = 0.0f;
     if (fabsf(dhi) <= tol) dhi = 0.0f;
     if (fabsf(d) < 1e-12f) return dlo <= 0.0f && dhi >= 0.0f;
-    float inv = 1.0f / d;
     float ta = dlo * inv, tb = dhi * inv;
     tmin = fmaxf(tmin, fminf(ta, tb));
     tmax = fminf(tmax, fmaxf(ta, tb));
@@ -225,13 +222,14 @@ __device__ __forceinline__ void take_root(float t, float eps, float& best) {
 }
 
 // Smallest root t > eps of primitive g along the ray (geometry.py:20-99), or best.
-__device__ float prim_next(const DevPrim& g, const float p[3], const float d[3], float eps, float best) {
+__device__ float prim_next(const DevPrim& g, const float p[3], const float d[3], const float inv[3], float eps,
+                           float best) {
     float ox = p[0] - g.c[0], oy = p[1] - g.c[1], oz = p[2] - g.c[2];
     if (g.type == CC_SHAPE_BOX) {
         float tmin = -INFINITY, tmax = INFINITY;
-        if (!slab_pair(ox, d[0], -g.h[0], g.h[0], eps, tmin, tmax)) return best;
-        if (!slab_pair(oy, d[1], -g.h[1], g.h[1], eps, tmin, tmax)) return best;
-        if (!slab_pair(oz, d[2], -g.h[2], g.h[2], eps, tmin, tmax)) return best;
+        if (!slab_pair(ox, d[0], inv[0], -g.h[0], g.h[0], eps, tmin, tmax)) return best;
+        if (!slab_pair(oy, d[1], inv[1], -g.h[1], g.h[1], eps, tmin, tmax)) return best;
+        if (!slab_pair(oz, d[2], inv[2], -g.h[2], g.h[2], eps, tmin, tmax)) return best;
         if (tmin <= tmax) { take_root(tmin, eps, best); take_root(tmax, eps, best); }
         return best;
     } else if (g.type == CC_SHAPE_SPHERE) {
@@ -269,19 +267,20 @@ __device__ float prim_next(const DevPrim& g, const float p[3], const float d[3],
             float r1 = q * inva, r2 = (q != 0.0f) ? cc / q : 0.0f;
             tmin = fminf(r1, r2); tmax = fmaxf(r1, r2);
         }
-        if (!slab_pair(aw, dw, -g.hh, g.hh, eps, tmin, tmax)) return best;
+        if (!slab_pair(aw, dw, inv[ax], -g.hh, g.hh, eps, tmin, tmax)) return best;
         if (tmin <= tmax) { take_root(tmin, eps, best); take_root(tmax, eps, best); }
         return best;
     }
 }
 
 // Distance to the world-box exit.
-__device__ __forceinline__ float world_exit(const KScene& s, const float p[3], const float d[3]) {
+__device__ __forceinline__ float world_exit(const KScene& s, const float p[3], const float d[3],
+                                            const float inv[3]) {
     float t = INFINITY;
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-        if (d[k] > 1e-12f) t = fminf(t, (s.whi[k] - p[k]) / d[k]);
-        else if (d[k] < -1e-12f) t = fminf(t, (s.wlo[k] - p[k]) / d[k]);
+        if (d[k] > 1e-12f) t = fminf(t, (s.whi[k] - p[k]) * inv[k]);
+        else if (d[k] < -1e-12f) t = fminf(t, (s.wlo[k] - p[k]) * inv[k]);
     }
     return fmaxf(t, 0.0f);
 }
@@ -345,38 +344,15 @@ __device__ __noinline__ int pick_element(const KTables& T, const DevMaterial& m,
     return m.el_slot[n_el - 1];
 }
 
-// mu_en/rho by log-log cubic Hermite with the PCHIP node slopes (materials.py:310-335).
-__device__ float muen_rho(const KTables& T, const DevMaterial& m, float loge) {
-    const float* x = T.muen_x + m.muen_off;
-    const float* y = T.muen_y + m.muen_off;
-    const float* dd = T.muen_d + m.muen_off;
-    int lo = 0, hi = m.n_muen - 1;
-    while (hi - lo > 1) {
-        int mid = (lo + hi) >> 1;
-        if (__ldg(x + mid) <= loge) lo = mid; else hi = mid;
-    }
-    float x0 = __ldg(x + lo), x1 = __ldg(x + lo + 1);
-    float hgt = x1 - x0;
-    float t = (loge - x0) / hgt;
-    float y0 = __ldg(y + lo), y1 = __ldg(y + lo + 1);
-    float d0 = __ldg(dd + lo), d1 = __ldg(dd + lo + 1);
-    float t2 = t * t, t3 = t2 * t;
-    float h00 = 2.0f * t3 - 3.0f * t2 + 1.0f, h10 = t3 - 2.0f * t2 + t;
-    float h01 = -2.0f * t3 + 3.0f * t2, h11 = t3 - t2;
-    return __expf(h00 * y0 + h10 * hgt * d0 + h01 * y1 + h11 * hgt * d1);
-}
-
-// h*(10)/Phi: log-log linear, clamped to the table range (dose_coefficients.py:32-42).
-__device__ float h10_coeff(const KTables& T, float loge) {
-    float x = fminf(fmaxf(loge, T.h10_lx_lo), T.h10_lx_hi);
-    int lo = 0, hi = T.n_h10 - 1;
-    while (hi - lo > 1) {
-        int mid = (lo + hi) >> 1;
-        if (__ldg(T.h10_x + mid) <= x) lo = mid; else hi = mid;
-    }
-    float x0 = __ldg(T.h10_x + lo), x1 = __ldg(T.h10_x + lo + 1);
-    float y0 = __ldg(T.h10_y + lo), y1 = __ldg(T.h10_y + lo + 1);
-    return __expf(y0 + (x - x0) / (x1 - x0) * (y1 - y0));
+// Track-length weights at the segment energy: E mu_en (materials.py:310-335,
+// transport.py:59-64) and h*(10)/Phi (dose_coefficients.py:32-42), both
+// linear in ln E between the material's nodes.
+__device__ __forceinline__ void tally_weights(const KTables& T, const DevMaterial& m, const Lookup& L,
+                                              float E, float& wk, float& wh) {
+    float2 a = __ldg(T.node_tally + m.node_off + L.idx);
+    float2 b = __ldg(T.node_tally + m.node_off + L.idx + 1);
+    wk = E * m.density * __expf(a.x + L.frac * (b.x - a.x));
+    wh = __expf(a.y + L.frac * (b.y - a.y));
 }
 
 // ---------------------------------------------------------------------------
@@ -416,7 +392,10 @@ __device__ void sample_compton(const float* sz, float E, HistoryRng& rng, float&
 }
 
 // Rayleigh: inverse of A(x) then (1+cos^2)/2 rejection (physics.py:281-351).
-__device__ bool sample_rayleigh(const float* rx, const float* ra, float E, HistoryRng& rng, float& cos_out) {
+// The row of a target A comes from a uniform-in-A bucket index, then a
+// short binary search inside the bucket.
+__device__ __noinline__ bool sample_rayleigh(const float* rx, const float* ra, const int* bucket, float scale,
+                                             float E, HistoryRng& rng, float& cos_out) {
     float xmax = (E / HC) * (E / HC);
     if (xmax > __ldg(rx + TABLE_N - 1)) return false;
     // A(x_max): x grid is q^2 with q uniform on [0, 20]
@@ -428,11 +407,11 @@ __device__ bool sample_rayleigh(const float* rx, const float* ra, float E, Histo
     float xa = __ldg(rx + j), xb = __ldg(rx + j + 1);
     float aa = __ldg(ra + j), ab = __ldg(ra + j + 1);
     float a_cut = aa + (xmax - xa) / (xb - xa) * (ab - aa);
-    int jmax = j + 1;
     for (int trial = 0; trial < 100000; ++trial) {
         float target = rng.uniform() * a_cut;
-        int lo = 0, hi = jmax;
-        while (hi - lo > 1) {
+        int bk = min((int)(target * scale), RAY_BUCKETS - 1);
+        int lo = __ldg(bucket + bk), hi = min(__ldg(bucket + bk + 1) + 1, TABLE_N - 1);
+        while (hi - lo > 1) {                    // ra[lo] <= target < ra[hi]
             int mid = (lo + hi) >> 1;
             if (__ldg(ra + mid) <= target) lo = mid; else hi = mid;
         }
@@ -448,7 +427,8 @@ __device__ bool sample_rayleigh(const float* rx, const float* ra, float E, Histo
 }
 
 // New direction from cos(theta) and a uniform azimuth (physics.py:354-367).
-__device__ void scatter_direction(float d[3], float cost, float phi) {
+__device__ __noinline__ float3 scatter_dir(float dx, float dy, float dz, float cost, float phi) {
+    const float d[3] = {dx, dy, dz};
     float sint = sqrtf(fmaxf(0.0f, 1.0f - cost * cost));
     float upx, upy, upz;
     if (fabsf(d[2]) < 0.999f) { upx = 0.f; upy = 0.f; upz = 1.f; } else { upx = 1.f; upy = 0.f; upz = 0.f; }
@@ -463,7 +443,12 @@ __device__ void scatter_direction(float d[3], float cost, float phi) {
     float ny = a * uy + b * vy + cost * d[1];
     float nz = a * uz + b * vz + cost * d[2];
     float n = rsqrtf(nx * nx + ny * ny + nz * nz);
-    d[0] = nx * n; d[1] = ny * n; d[2] = nz * n;
+    return make_float3(nx * n, ny * n, nz * n);
+}
+
+__device__ __forceinline__ void scatter_direction(float d[3], float cost, float phi) {
+    float3 r = scatter_dir(d[0], d[1], d[2], cost, phi);
+    d[0] = r.x; d[1] = r.y; d[2] = r.z;
 }
 
 __device__ void isotropic(float d[3], HistoryRng& rng) {
@@ -485,8 +470,8 @@ __device__ __forceinline__ void score(double* tally, long long v, float wk_len, 
 
 // Clip the ray p + t d, t in [0, s], to the grid box.  Returns false when
 // no part of it lies inside.
-__device__ __forceinline__ bool clip_to_grid(const KGrid& G, const float p[3], const float d[3], float s,
-                                             float& t0, float& t1) {
+__device__ __forceinline__ bool clip_to_grid(const KGrid& G, const float p[3], const float d[3],
+                                             const float invd[3], float s, float& t0, float& t1) {
     t0 = 0.0f;
     t1 = s;
 #pragma unroll
@@ -496,8 +481,7 @@ __device__ __forceinline__ bool clip_to_grid(const KGrid& G, const float p[3], c
         if (fabsf(d[k]) < 1e-12f) {
             if (p[k] < lo || p[k] >= hi) return false;
         } else {
-            float inv = 1.0f / d[k];
-            float ta = (lo - p[k]) * inv, tb = (hi - p[k]) * inv;
+            float ta = (lo - p[k]) * invd[k], tb = (hi - p[k]) * invd[k];
             t0 = fmaxf(t0, fminf(ta, tb));
             t1 = fminf(t1, fmaxf(ta, tb));
         }
@@ -535,13 +519,15 @@ __device__ int walk_range(const KGrid& G, double* tally, const float p[3], const
         int i = max(0, min(nk - 1, (int)floorf(x)));
         iv[k] = i;
         if (d[k] > 1e-12f) {
+            float inv = 1.0f / d[k];
             step[k] = 1;
-            tmax[k] = (G.o[k] + (float)(i + 1) * G.h - p[k]) / d[k];
-            tdel[k] = G.h / d[k];
+            tmax[k] = (G.o[k] + (float)(i + 1) * G.h - p[k]) * inv;
+            tdel[k] = G.h * inv;
         } else if (d[k] < -1e-12f) {
+            float inv = 1.0f / d[k];
             step[k] = -1;
-            tmax[k] = (G.o[k] + (float)i * G.h - p[k]) / d[k];
-            tdel[k] = -G.h / d[k];
+            tmax[k] = (G.o[k] + (float)i * G.h - p[k]) * inv;
+            tdel[k] = -G.h * inv;
         } else {
             step[k] = 0;
             tmax[k] = INFINITY;
@@ -671,8 +657,10 @@ __device__ __forceinline__ int warp_inclusive_scan(int v, int lane) {
 //      into equal-length pieces so that every lane walks about the same
 //      number of voxels (the pieces' partial voxel lengths add up exactly);
 //   3. lanes move their photon and sample the interaction, if any.
+// Three 256-thread blocks per SM: the register budget (<= 80) that this
+// asks for costs no spills and hides more latency than two blocks.
 #ifndef CC_MIN_BLOCKS
-#define CC_MIN_BLOCKS 2
+#define CC_MIN_BLOCKS 3
 #endif
 
 template <bool FROM_SOURCE, bool TALLY>
@@ -766,17 +754,17 @@ transport_kernel(const KTables T, const KScene S, const KGrid G, const KSource S
             loge = __logf(E);
             L = energy_index(T, M, loge);
             float mu = mu_total(T, M, L);
+            const float invd[3] = {1.0f / d[0], 1.0f / d[1], 1.0f / d[2]};
             float tb = INFINITY;
-            for (int i = 0; i < S.n_prims; ++i) tb = prim_next(S.prims[i], p, d, S.eps, tb);
-            float tw = world_exit(S, p, d);
+            for (int i = 0; i < S.n_prims; ++i) tb = prim_next(S.prims[i], p, d, invd, S.eps, tb);
+            float tw = world_exit(S, p, d, invd);
             escape = tw <= tb;
             tb = fminf(tb, tw);
             tau_b = mu * tb;
             interact = tau < tau_b;
             s = interact ? tau / fmaxf(mu, 1e-30f) : tb;
-            if (TALLY && clip_to_grid(G, p, d, s, t0, t1)) {
-                wk = E * muen_rho(T, M, loge) * M.density;
-                wh = h10_coeff(T, loge);
+            if (TALLY && clip_to_grid(G, p, d, invd, s, t0, t1)) {
+                tally_weights(T, M, L, E, wk, wh);
                 tal_n = visit_estimate(G, p, d, t0, t1);
             }
         }
@@ -869,7 +857,9 @@ transport_kernel(const KTables T, const KScene S, const KGrid G, const KSource S
             } else {
                 int slot = pick_element(T, M, L, 2, rng.uniform());
                 float cost;
-                if (!sample_rayleigh(T.rx + (size_t)slot * TABLE_N, T.ra + (size_t)slot * TABLE_N, E, rng, cost)) {
+                if (!sample_rayleigh(T.rx + (size_t)slot * TABLE_N, T.ra + (size_t)slot * TABLE_N,
+                                     T.ray_bucket + (size_t)slot * (RAY_BUCKETS + 1), T.elems[slot].ray_scale,
+                                     E, rng, cost)) {
                     atomicOr(R.status, ST_RAYLEIGH_Q);
                     live = false;
                     continue;
@@ -989,6 +979,8 @@ struct cc_ctx {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     cudaEvent_t kev0 = nullptr, kev1 = nullptr;     // around the transport kernel alone
     double* d_edep = nullptr;                       // [MAX_SCRATCH * MAX_MATS] per-launch reductions
+    char* d_io = nullptr;                           // staging of cc_transport_photons (grow-only)
+    size_t io_bytes = 0;
     unsigned* d_status = nullptr;
     unsigned long long* d_counters = nullptr;   // [5] + work counter
     int block = 256;
@@ -1077,6 +1069,7 @@ int cc_ctx_destroy(cc_ctx* c) {
     cudaFree(c->d_status);
     cudaFree(c->d_counters);
     cudaFree(c->d_edep);
+    cudaFree(c->d_io);
     cudaEventDestroy(c->ev0);
     cudaEventDestroy(c->ev1);
     cudaEventDestroy(c->kev0);
@@ -1110,15 +1103,15 @@ int cc_tables_create(cc_ctx* ctx, const cc_table_desc* desc, cc_tables** out) {
         return set_error(CC_E_INVALID, "n_materials must be in [1, 16]");
     if (desc->n_elements < 1 || desc->n_elements > MAX_ELEMS)
         return set_error(CC_E_INVALID, "n_elements must be in [1, 48]");
-    if (desc->n_h10 < 2) return set_error(CC_E_INVALID, "h10 table needs >= 2 rows");
     CC_CUDA(cudaSetDevice(ctx->device));
-    std::vector<float> loge, elem_log, mx, my, md;
+    std::vector<float> loge, elem_log;
     std::vector<float4> nparts;
+    std::vector<float2> ntally;
     std::vector<int> bucket;
     std::vector<DevMaterial> mats(desc->n_materials);
     for (int m = 0; m < desc->n_materials; ++m) {
         const cc_material_desc& md_ = desc->materials[m];
-        if (md_.n_nodes < 2 || md_.n_elements < 1 || md_.n_elements > MAX_ELEMS_PER_MAT || md_.n_muen < 2)
+        if (md_.n_nodes < 2 || md_.n_elements < 1 || md_.n_elements > MAX_ELEMS_PER_MAT || !md_.log_tally)
             return set_error(CC_E_INVALID, "material " + std::to_string(m) + ": bad sizes");
         DevMaterial& dm = mats[m];
         memset(&dm, 0, sizeof(dm));
@@ -1127,8 +1120,6 @@ int cc_tables_create(cc_ctx* ctx, const cc_table_desc* desc, cc_tables** out) {
         dm.n_el = md_.n_elements;
         dm.node_off = (int)loge.size();
         dm.elem_off = (int)elem_log.size();
-        dm.muen_off = (int)mx.size();
-        dm.n_muen = md_.n_muen;
         dm.bucket_off = (int)bucket.size();
         double lmax = log(150.0);
         dm.bucket_scale = (float)(N_BUCKETS / lmax);
@@ -1138,6 +1129,7 @@ int cc_tables_create(cc_ctx* ctx, const cc_table_desc* desc, cc_tables** out) {
             loge.push_back((float)md_.log_e[i]);
             const double* q = md_.log_parts + 4 * (size_t)i;
             nparts.push_back(make_float4((float)q[0], (float)q[1], (float)q[2], (float)q[3]));
+            ntally.push_back(make_float2((float)md_.log_tally[2 * (size_t)i], (float)md_.log_tally[2 * (size_t)i + 1]));
         }
         // node index per bucket: last node whose float log E <= the bucket start
         int node = 0;
@@ -1155,14 +1147,10 @@ int cc_tables_create(cc_ctx* ctx, const cc_table_desc* desc, cc_tables** out) {
                 return set_error(CC_E_INVALID, "material element slot out of range");
             dm.el_slot[e] = slot;
         }
-        for (int i = 0; i < md_.n_muen; ++i) {
-            mx.push_back((float)md_.muen_log_e[i]);
-            my.push_back((float)md_.muen_log_v[i]);
-            md.push_back((float)md_.muen_slope[i]);
-        }
     }
     std::vector<DevElement> els(desc->n_elements);
     std::vector<float> sq, rx, ra;
+    std::vector<int> rbk;
     for (int e = 0; e < desc->n_elements; ++e) {
         const cc_element_desc& ed = desc->elements[e];
         if (ed.n_lines < 0 || ed.n_lines > 8) return set_error(CC_E_INVALID, "n_lines must be <= 8");
@@ -1179,14 +1167,25 @@ int cc_tables_create(cc_ctx* ctx, const cc_table_desc* desc, cc_tables** out) {
             de.line_e[k] = (float)ed.line_e[k];
             de.line_cum[k] = (float)cum;
         }
+        size_t ra_off = ra.size();
         for (int i = 0; i < TABLE_N; ++i) {
+            if (i > 0 && !(ed.ray_a[i] >= ed.ray_a[i - 1]))
+                return set_error(CC_E_INVALID, "Rayleigh A(x) table must not decrease");
             sq.push_back((float)ed.s_over_z[i]);
             rx.push_back((float)ed.ray_x[i]);
             ra.push_back((float)ed.ray_a[i]);
         }
+        // bucket index on the FP32 table the kernel searches
+        const float a_end = ra[ra_off + TABLE_N - 1];
+        if (!(a_end > 0.0f)) return set_error(CC_E_INVALID, "Rayleigh A(x) table is empty");
+        de.ray_scale = (float)RAY_BUCKETS / a_end;
+        int row = 0;
+        for (int b = 0; b <= RAY_BUCKETS; ++b) {
+            float start = (float)b / de.ray_scale;
+            while (row + 1 < TABLE_N - 1 && ra[ra_off + row + 1] <= start) ++row;
+            rbk.push_back(row);
+        }
     }
-    std::vector<float> hx(desc->n_h10), hy(desc->n_h10);
-    for (int i = 0; i < desc->n_h10; ++i) { hx[i] = (float)desc->h10_log_e[i]; hy[i] = (float)desc->h10_log_v[i]; }
 
     cc_tables* t = new (std::nothrow) cc_tables();
     if (!t) return set_error(CC_E_NOMEM, "out of host memory");
@@ -1204,17 +1203,11 @@ int cc_tables_create(cc_ctx* ctx, const cc_table_desc* desc, cc_tables** out) {
     UP(sq, sq);
     UP(rx, rx);
     UP(ra, ra);
-    UP(mx, muen_x);
-    UP(my, muen_y);
-    UP(md, muen_d);
-    UP(hx, h10_x);
-    UP(hy, h10_y);
+    UP(ntally, node_tally);
+    UP(rbk, ray_bucket);
 #undef UP
     k.n_mat = desc->n_materials;
     k.n_elem = desc->n_elements;
-    k.n_h10 = desc->n_h10;
-    k.h10_lx_lo = (float)log(desc->h10_e_min);
-    k.h10_lx_hi = (float)log(desc->h10_e_max);
     *out = t;
     return CC_OK;
 }
@@ -1609,9 +1602,15 @@ int cc_transport_photons(cc_ctx* c, const cc_scene* scene, const cc_tables* tabl
     CC_CUDA(cudaSetDevice(c->device));
     cudaStream_t st = c->stream;
     size_t b3 = (size_t)n * 3 * sizeof(double), b1 = (size_t)n * sizeof(double);
-    char* buf = nullptr;
     size_t total = 2 * b3 + b1 + (size_t)n * (sizeof(int32_t) + 2);
-    CC_CUDA(cudaMalloc(&buf, total));
+    if (total > c->io_bytes) {
+        cudaFree(c->d_io);
+        c->d_io = nullptr;
+        c->io_bytes = 0;
+        CC_CUDA(cudaMalloc(&c->d_io, total));
+        c->io_bytes = total;
+    }
+    char* buf = c->d_io;
     double* d_pos = (double*)buf;
     double* d_dir = (double*)(buf + b3);
     double* d_en = (double*)(buf + 2 * b3);
@@ -1621,7 +1620,7 @@ int cc_transport_photons(cc_ctx* c, const cc_scene* scene, const cc_tables* tabl
     cudaError_t e = cudaMemcpyAsync(d_pos, pos, b3, cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(d_dir, dir, b3, cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(d_en, energy, b1, cudaMemcpyHostToDevice, st);
-    if (e != cudaSuccess) { cudaFree(buf); return set_error(CC_E_DEVICE, std::string("upload: ") + cudaGetErrorString(e)); }
+    if (e != cudaSuccess) return set_error(CC_E_DEVICE, std::string("upload: ") + cudaGetErrorString(e));
     int rc = transport_common(c, scene, tables, grid, n, d_pos, d_dir, d_en, seed, stream_offset,
                               fluorescence, n_scatter ? d_nsc : nullptr, absorbed ? d_abs : nullptr,
                               escaped ? d_esc : nullptr, edep, n_fluor);
@@ -1635,7 +1634,6 @@ int cc_transport_photons(cc_ctx* c, const cc_scene* scene, const cc_tables* tabl
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
         if (e != cudaSuccess) rc = set_error(CC_E_DEVICE, std::string("download: ") + cudaGetErrorString(e));
     }
-    cudaFree(buf);
     return rc;
 }
 

@@ -8,8 +8,10 @@
 
 #ifdef __CUDACC__
 #define CC_HD __host__ __device__ __forceinline__
+#define CC_HD_NOINLINE __host__ __device__ __noinline__
 #else
 #define CC_HD inline
+#define CC_HD_NOINLINE inline
 #endif
 
 namespace cc {
@@ -51,6 +53,15 @@ CC_HD u32x4 philox4x32_10(u32x4 c, uint32_t k0, uint32_t k1) {
     return c;
 }
 
+// One counter block, kept out of line: the generator is drawn from at many
+// places of the transport kernel and each inlined copy of the ten rounds
+// would cost instruction-cache space.
+CC_HD_NOINLINE u32x4 philox_block(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t k0,
+                                  uint32_t k1) {
+    u32x4 c = {c0, c1, c2, c3};
+    return philox4x32_10(c, k0, k1);
+}
+
 // (0, 1] with 2^-32 resolution; safe for -log().
 CC_HD float u01_oc(uint32_t x) { return ((float)x + 1.0f) * 2.3283064365386963e-10f; }
 
@@ -74,8 +85,7 @@ struct HistoryRng {
     }
     CC_HD uint32_t next_u32() {
         if (avail == 0) {
-            u32x4 c = {block, tag, h0, h1};
-            buf = philox4x32_10(c, k0, k1);
+            buf = philox_block(block, tag, h0, h1, k0, k1);
             ++block;
             avail = 4;
         }

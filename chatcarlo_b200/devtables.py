@@ -14,6 +14,7 @@ import ctypes as C
 from dataclasses import dataclass, field
 
 import numpy as np
+from scipy.interpolate import PchipInterpolator
 
 from . import _native as N
 from . import physdata as pd
@@ -39,9 +40,7 @@ class MaterialTables:
     log_e: np.ndarray
     log_parts: np.ndarray           # (n, 4)
     log_elem: np.ndarray            # (n_el, 3, n)
-    muen_x: np.ndarray
-    muen_y: np.ndarray
-    muen_d: np.ndarray
+    log_tally: np.ndarray           # (n, 2) ln(mu_en/rho), ln(h*(10)/Phi)
 
 
 @dataclass
@@ -58,11 +57,47 @@ class ElementTables:
     emits: bool
 
 
+def _muen_rows(name: str):
+    """NIST rows and PCHIP of mu_en/rho, or None without a bundled table."""
+    try:
+        key = tb.muen_key(name)
+    except tb.UnknownMaterialError:
+        return None
+    e, _, muen = pd.load_xaamdi(key)
+    return e, PchipInterpolator(np.log(e), np.log(muen))
+
+
+def _refine_for_pchip(grid: np.ndarray, pchip, tol: float = 2e-6, rounds: int = 8) -> np.ndarray:
+    """Bisect (in ln E) every interval where linear interpolation of the
+    mu_en PCHIP misses its midpoint by more than tol (relative)."""
+    for _ in range(rounds):
+        le = np.log(grid)
+        mid = 0.5 * (le[1:] + le[:-1])
+        lin = 0.5 * (pchip(le[1:]) + pchip(le[:-1]))
+        bad = np.abs(lin - pchip(mid)) > tol
+        if not np.any(bad):
+            break
+        grid = np.unique(np.concatenate([grid, np.exp(mid[bad])]))
+    return grid
+
+
 def build_material(name: str, need_muen: bool = True) -> MaterialTables:
     comp = tb.element_composition(name)
     zs = np.array([z for z, _ in comp], dtype=np.int32)
     fr = np.array([f for _, f in comp], dtype=float)
-    grid = np.unique(np.concatenate([tb.element_energy_grid_kev(int(z)) for z in zs]))
+    lo, hi = tb.XS_GRID_MIN_KEV, tb.XS_GRID_MAX_KEV
+    muen = _muen_rows(name)
+    if muen is None and need_muen:
+        raise tb.UnknownMaterialError(
+            f"no mu_en/rho table for material '{name}'; available: {sorted(tb.XAAMDI_FILES)}")
+    he, hv = tb.h10_table()
+    parts = [tb.element_energy_grid_kev(int(z)) for z in zs]
+    parts.append(he[(he > lo) & (he < hi)])           # h*(10) rows: exact log-log interpolation
+    if muen is not None:
+        parts.append(muen[0][(muen[0] > lo) & (muen[0] < hi)])
+    grid = np.unique(np.concatenate(parts))
+    if muen is not None:
+        grid = _refine_for_pchip(grid, muen[1])
     log_e = np.log(grid)
     n = len(grid)
     log_elem = np.empty((len(zs), 3, n))
@@ -75,19 +110,12 @@ def build_material(name: str, need_muen: bool = True) -> MaterialTables:
     log_parts = np.empty((n, 4))
     log_parts[:, :3] = np.log(sums.T)
     log_parts[:, 3] = np.log(sums.sum(axis=0))
-    try:
-        key = tb.muen_key(name)
-        x, y, d = pd.muen_pchip(key)
-        # rows up to the first one at or above the table's 150 keV end
-        last = int(np.searchsorted(x, np.log(tb.XS_GRID_MAX_KEV))) + 1
-        x, y, d = x[:last + 1], y[:last + 1], d[:last + 1]
-    except tb.UnknownMaterialError:
-        if need_muen:
-            raise
-        x = np.log(np.array([1.0, 150.0]))
-        y = np.zeros(2)
-        d = np.zeros(2)
-    return MaterialTables(name, tb.density(name), zs, fr, log_e, log_parts, log_elem, x, y, d)
+    log_tally = np.zeros((n, 2))
+    if muen is not None:
+        log_tally[:, 0] = muen[1](log_e)                # materials.py:315-335
+    ec = np.clip(grid, he[0], he[-1])                    # dose_coefficients.py:32-42
+    log_tally[:, 1] = np.interp(np.log(ec), np.log(he), np.log(hv))
+    return MaterialTables(name, tb.density(name), zs, fr, log_e, log_parts, log_elem, log_tally)
 
 
 def build_element(z: int) -> ElementTables:
@@ -135,10 +163,7 @@ def build_table_set(names: list[str], need_muen: bool = True) -> TableSet:
         d.log_elem = N.dptr(arr(m.log_elem))
         slots = arr([zs.index(int(z)) for z in m.zs], np.int32)
         d.element_slot = slots.ctypes.data_as(C.POINTER(C.c_int32))
-        d.n_muen = len(m.muen_x)
-        d.muen_log_e = N.dptr(arr(m.muen_x))
-        d.muen_log_v = N.dptr(arr(m.muen_y))
-        d.muen_slope = N.dptr(arr(m.muen_d))
+        d.log_tally = N.dptr(arr(m.log_tally))
     ed = (N.ElementDesc * len(elems))()
     for i, e in enumerate(elems):
         d = ed[i]
@@ -154,17 +179,11 @@ def build_table_set(names: list[str], need_muen: bool = True) -> TableSet:
             d.line_e[k] = float(e.line_e[k])
             d.line_p[k] = float(e.line_p[k])
         d.emits = int(e.emits)
-    he, hv = tb.h10_table()
     desc = N.TableDesc()
     desc.n_materials = len(mats)
     desc.n_elements = len(elems)
     desc.materials = md
     desc.elements = ed
-    desc.n_h10 = len(he)
-    desc.h10_log_e = N.dptr(arr(np.log(he)))
-    desc.h10_log_v = N.dptr(arr(np.log(hv)))
-    desc.h10_e_min = float(he[0])
-    desc.h10_e_max = float(he[-1])
     keep.extend([md, ed])
     ts.desc = desc
     return ts

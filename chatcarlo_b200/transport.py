@@ -113,6 +113,7 @@ class Engine:
         N.check(self.lib.cc_ctx_create(int(device), C.byref(self.ctx)))
         self.device = device
         self._tables: dict = {}
+        self._grids: dict = {}
         self._lock = threading.Lock()
 
     def set_launch(self, block_size: int = 256, blocks_per_sm: int = 0) -> None:
@@ -144,12 +145,30 @@ class Engine:
                                          N.dptr(lo), N.dptr(hi), C.byref(h)))
         return h
 
+    def device_grid(self, grid: VoxelGrid, stats: bool) -> DeviceGrid:
+        """A zeroed device grid of this shape, reused between calls."""
+        key = (tuple(grid.shape), tuple(np.asarray(grid.origin_cm, dtype=float).tolist()),
+               float(grid.voxel_size_cm), bool(stats))
+        dg = self._grids.get(key)
+        if dg is None:
+            if len(self._grids) >= 4:
+                _, old = self._grids.popitem()
+                old.close()
+            dg = DeviceGrid(self, grid, stats)
+            self._grids[key] = dg
+        else:
+            dg.reset()
+        return dg
+
     def source(self, spec: SourceSpec) -> C.c_void_p:
         h = C.c_void_p()
         N.check(self.lib.cc_source_create(self.ctx, C.byref(spec.desc), C.byref(h)))
         return h
 
     def close(self):
+        for dg in self._grids.values():
+            dg.close()
+        self._grids.clear()
         for ts, h in self._tables.values():
             self.lib.cc_tables_destroy(h)
         self._tables.clear()
@@ -205,20 +224,14 @@ def transport_photons(pos: np.ndarray, dirv: np.ndarray, energy: np.ndarray, geo
         esc = np.zeros(n, dtype=np.uint8)
         edep = np.zeros(len(names))
         nfl = C.c_int64(0)
-        dg = None
-        if grid is not None:
-            dg = DeviceGrid(eng, grid, stats=False)
-        try:
-            N.check(eng.lib.cc_transport_photons(
-                eng.ctx, sh, th, dg.handle if dg else None, n, N.dptr(p), N.dptr(d), N.dptr(e),
-                _seed_from(rng, seed), int(stream_offset), int(bool(fluorescence_enabled)),
-                nsc.ctypes.data_as(C.POINTER(C.c_int32)), absd.ctypes.data_as(C.POINTER(C.c_uint8)),
-                esc.ctypes.data_as(C.POINTER(C.c_uint8)), N.dptr(edep), C.byref(nfl)))
-            if dg is not None:
-                dg.download(grid, accumulate=True)
-        finally:
-            if dg is not None:
-                dg.close()
+        dg = eng.device_grid(grid, stats=False) if grid is not None else None
+        N.check(eng.lib.cc_transport_photons(
+            eng.ctx, sh, th, dg.handle if dg else None, n, N.dptr(p), N.dptr(d), N.dptr(e),
+            _seed_from(rng, seed), int(stream_offset), int(bool(fluorescence_enabled)),
+            nsc.ctypes.data_as(C.POINTER(C.c_int32)), absd.ctypes.data_as(C.POINTER(C.c_uint8)),
+            esc.ctypes.data_as(C.POINTER(C.c_uint8)), N.dptr(edep), C.byref(nfl)))
+        if dg is not None:
+            dg.download(grid, accumulate=True)
     finally:
         eng.lib.cc_scene_destroy(sh)
     if p is not pos:
@@ -260,7 +273,7 @@ def run_transport(scene, n_histories: int = 100_000, seed: int | None = None,
     spec = SourceSpec(src)
     sh = eng.scene(geometry, ts)
     srch = eng.source(spec)
-    dg = DeviceGrid(eng, grid, stats=track_uncertainty) if grid is not None else None
+    dg = eng.device_grid(grid, stats=track_uncertainty) if grid is not None else None
     edep = np.zeros(len(names))
     edep2 = np.zeros(len(names))
     out = N.RunOut()
@@ -271,8 +284,6 @@ def run_transport(scene, n_histories: int = 100_000, seed: int | None = None,
         if dg is not None:
             dg.download(grid)
     finally:
-        if dg is not None:
-            dg.close()
         eng.lib.cc_source_destroy(srch)
         eng.lib.cc_scene_destroy(sh)
     n_batches = int(out.n_batches)

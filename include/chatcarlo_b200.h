@@ -84,11 +84,11 @@ typedef struct {
                                      mass-fraction mix, cm^2/g */
     const double* log_elem;       /* [n_elements][3][n_nodes] ln(w_i * sigma_i) for photo, compt, rayl */
     const int32_t* element_slot;  /* [n_elements] index into the element table array */
-    int32_t n_muen;               /* NIST rows for mu_en/rho */
-    int32_t pad;
-    const double* muen_log_e;     /* [n_muen] */
-    const double* muen_log_v;     /* [n_muen] ln(mu_en/rho) */
-    const double* muen_slope;     /* [n_muen] PCHIP node slopes in log-log */
+    const double* log_tally;      /* [n_nodes][2] ln(mu_en/rho) (log-log PCHIP through the NIST rows,
+                                     materials.py:310-335) and ln(h*(10)/Phi) (dose_coefficients.py:
+                                     32-42) at the nodes; the grid contains every mu_en and h*(10) row
+                                     in range, so interpolating linearly in ln E reproduces h*(10)
+                                     exactly and the PCHIP to ~1e-6 */
 } cc_material_desc;
 
 /* Per-element angular and fluorescence tables. */
@@ -112,11 +112,6 @@ typedef struct {
     int32_t n_elements;
     const cc_material_desc* materials;
     const cc_element_desc* elements;
-    int32_t n_h10;
-    int32_t pad;
-    const double* h10_log_e;      /* [n_h10] */
-    const double* h10_log_v;      /* [n_h10] ln(h*(10)/Phi) pSv cm^2 */
-    double h10_e_min, h10_e_max;  /* clamp range keV */
 } cc_table_desc;
 
 /* Point source into a field, with optional CT rotation (source.py:67-210). */

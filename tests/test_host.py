@@ -85,6 +85,23 @@ def test_union_grid_reproduces_element_interpolation(material):
     np.testing.assert_allclose(tot, O.mu_rho(material, e), rtol=2e-5)
 
 
+@pytest.mark.parametrize("material", ["water", "bone", "lead", "concrete", "air"])
+def test_node_tally_weights_match_reference_interpolants(material):
+    """ln(mu_en/rho) and ln(h*(10)/Phi) interpolated linearly between the
+    nodes vs the reference's PCHIP (materials.py:315-335) and log-log
+    h*(10) interpolation (dose_coefficients.py:32-42)."""
+    mt = devtables.build_material(material)
+    e = np.exp(np.random.default_rng(2).uniform(0.0, np.log(150.0), 4000))
+    le = np.log(e)
+    idx = np.clip(np.searchsorted(mt.log_e, le), 1, len(mt.log_e) - 1)
+    fr = (le - mt.log_e[idx - 1]) / (mt.log_e[idx] - mt.log_e[idx - 1])
+    y = mt.log_tally
+    muen = np.exp(y[idx - 1, 0] + fr * (y[idx, 0] - y[idx - 1, 0]))
+    h10 = np.exp(y[idx - 1, 1] + fr * (y[idx, 1] - y[idx - 1, 1]))
+    np.testing.assert_allclose(muen, O.mu_en_rho(material, e), rtol=2e-5)
+    np.testing.assert_allclose(h10, O.h10_per_fluence(e), rtol=1e-12)
+
+
 def test_element_tables_for_the_engine():
     el = devtables.build_element(82)
     assert el.emits and el.k_edge == pytest.approx(88.0045)
