@@ -35,7 +35,7 @@ EXPORTED = [
     "cc_scene_destroy", "cc_source_create", "cc_source_destroy", "cc_grid_create",
     "cc_grid_destroy", "cc_grid_reset", "cc_grid_download", "cc_grid_end_batch",
     "cc_transport_photons", "cc_transport_photons_device", "cc_run", "cc_sample_source",
-    "cc_transport_photons_device_noalloc",
+    "cc_transport_photons_device_noalloc", "cc_batch_create", "cc_batch_run", "cc_batch_destroy",
 ]
 
 
@@ -126,6 +126,10 @@ def _bind(lib):
         "cc_run": (C.c_int, [P, P, P, P, P, C.c_int64, C.c_int64, C.c_uint64, C.c_int64, C.c_int32, PD, PD,
                              C.POINTER(RunOut)]),
         "cc_sample_source": (C.c_int, [P, P, C.c_int64, C.c_uint64, C.c_int64, PD, PD, PD]),
+        "cc_batch_create": (C.c_int, [P, P, C.c_int32, C.POINTER(P), C.POINTER(P), C.POINTER(P),
+                                      C.POINTER(C.c_int64), C.c_int32, C.c_int32, C.POINTER(P)]),
+        "cc_batch_run": (C.c_int, [P, C.c_uint64, C.c_int32, C.POINTER(C.c_int64), C.POINTER(RunOut)]),
+        "cc_batch_destroy": (C.c_int, [P]),
         "cc_transport_photons_device_noalloc": (C.c_int, [P, P, C.c_int64, P, P, P, C.c_uint64, C.c_uint64,
                                                           C.c_int32, P, P, P, PD, C.POINTER(C.c_int64), P]),
     }

@@ -82,17 +82,15 @@ struct DevElement {
 };
 
 struct KTables {
-    const float* node_loge;
-    const float4* node_parts;
-    const float* elem_log;
-    const int* bucket;
+    const float4* nodes;        // 2 per node: {ln E, ln photo, ln Compton, ln Rayleigh}, {ln total, ln mu_en, ln h10, 0}
+    const float* elem_cum;      // per material [3][n_el - 1][n_nodes] normalised cumulative element weights
+    const unsigned short* bucket;
     const DevMaterial* mats;
     const DevElement* elems;
     const float* sq;       // [n_elem][TABLE_N] S/Z
     const float* rx;       // [n_elem][TABLE_N]
     const float* ra;       // [n_elem][TABLE_N]
     const int* ray_bucket; // [n_elem][RAY_BUCKETS + 1] last row with A <= bucket start
-    const float2* node_tally;   // per node ln(mu_en/rho), ln(h*(10)/Phi)
     int n_mat, n_elem;
 };
 
@@ -157,10 +155,15 @@ __device__ __forceinline__ float fmax3(float a, float b, float c) { return fmaxf
 // within a few ulps (of the world's largest coordinate) of it on either
 // side.  Points inside that band, of half-width tol, are classified by
 // their direction: on a surface, a photon is inside the primitive when it
-// moves inwards.  For planar faces (box faces, cylinder caps) the root of
-// the face the photon sits on is dropped as well: a photon grazing a face
-// would otherwise find that face again a fraction of an ulp ahead on every
-// step and never leave it.
+// moves inwards.  The root of the surface the photon sits on is dropped as
+// well: a photon grazing a face would otherwise find that face again a
+// fraction of an ulp ahead on every step and never leave it.  For planar
+// faces (box faces, cylinder caps) the face contributes t = 0; for the
+// curved surfaces (sphere, cylinder side) the near root is taken as 0 and
+// the far one as the chord -2 b / a of a point on the surface, so a
+// photon moving outwards finds no root ahead and one moving inwards finds
+// the far side -- the quadratic's own near root, off by rounding of
+// order ulp / |radial direction|, can be far above tol at grazing angles.
 
 // Inside the slab |o| <= h, deciding points on a face by the direction d.
 __device__ __forceinline__ bool slab_inside(float o, float d, float h, float tol) {
@@ -234,12 +237,18 @@ __device__ float prim_next(const DevPrim& g, const float p[3], const float d[3],
         return best;
     } else if (g.type == CC_SHAPE_SPHERE) {
         float b = ox * d[0] + oy * d[1] + oz * d[2];
+        float o2 = ox * ox + oy * oy + oz * oz;
+        float lo = fmaxf(g.r - eps, 0.0f), hi = g.r + eps;
+        if (o2 >= lo * lo && o2 <= hi * hi) {          // on the surface
+            if (b <= 0.0f) take_root(-2.0f * b, eps, best);
+            return best;
+        }
         // squared distance of the line from the centre, computed without cancellation
         float qx = ox - b * d[0], qy = oy - b * d[1], qz = oz - b * d[2];
         float disc = g.r2 - (qx * qx + qy * qy + qz * qz);
         if (disc < 0.0f) return best;
         float sq = sqrtf(disc);
-        float c = ox * ox + oy * oy + oz * oz - g.r2;
+        float c = o2 - g.r2;
         float q = -(b + copysignf(sq, b));
         float t1 = q, t2 = (q != 0.0f) ? c / q : 0.0f;
         take_root(t1, eps, best);
@@ -251,13 +260,19 @@ __device__ float prim_next(const DevPrim& g, const float p[3], const float d[3],
         float a0 = p[i0] - g.c[i0], a1 = p[i1] - g.c[i1], aw = p[ax] - g.c[ax];
         float dx = d[i0], dy = d[i1], dw = d[ax];
         float a = dx * dx + dy * dy;
-        float cc = a0 * a0 + a1 * a1 - g.r2;
+        float rho2 = a0 * a0 + a1 * a1;
+        float cc = rho2 - g.r2;
         float tmin, tmax;
-        if (a < 1e-12f) {
+        float b = a0 * dx + a1 * dy;
+        float lo = fmaxf(g.r - eps, 0.0f), hi = g.r + eps;
+        if (rho2 >= lo * lo && rho2 <= hi * hi) {      // on the side surface
+            if (b > 0.0f) return best;
+            tmin = 0.0f;
+            tmax = a < 1e-12f ? INFINITY : -2.0f * b / a;
+        } else if (a < 1e-12f) {
             if (cc > 0.0f) return best;        // parallel to the axis, outside the radius
             tmin = -INFINITY; tmax = INFINITY;
         } else {
-            float b = a0 * dx + a1 * dy;
             float inva = 1.0f / a;
             float ex = a0 - b * inva * dx, ey = a1 - b * inva * dy;
             float disc = (g.r2 - (ex * ex + ey * ey)) * a;   // b^2 - a c without cancellation
@@ -295,10 +310,14 @@ __device__ __forceinline__ Lookup energy_index(const KTables& T, const DevMateri
     int b = (int)(loge * m.bucket_scale);
     b = max(0, min(N_BUCKETS - 1, b));
     int i = __ldg(T.bucket + m.bucket_off + b);       // last node with log E <= bucket start
-    const float* x = T.node_loge + m.node_off;
+    const float4* x = T.nodes + 2 * (size_t)m.node_off;
     int last = m.n_nodes - 2;
-    while (i < last && __ldg(x + i + 1) < loge) ++i;
-    float x0 = __ldg(x + i), x1 = __ldg(x + i + 1);
+    float x0 = __ldg(&x[2 * i].x), x1 = __ldg(&x[2 * i + 2].x);
+    while (i < last && x1 < loge) {
+        ++i;
+        x0 = x1;
+        x1 = __ldg(&x[2 * i + 2].x);
+    }
     Lookup L;
     L.idx = i;
     L.frac = (loge - x0) / (x1 - x0);
@@ -306,18 +325,18 @@ __device__ __forceinline__ Lookup energy_index(const KTables& T, const DevMateri
 }
 
 __device__ __forceinline__ float mu_total(const KTables& T, const DevMaterial& m, const Lookup& L) {
-    float4 a = __ldg(T.node_parts + m.node_off + L.idx);
-    float4 b = __ldg(T.node_parts + m.node_off + L.idx + 1);
-    return m.density * __expf(a.w + L.frac * (b.w - a.w));
+    const float4* r = T.nodes + 2 * ((size_t)m.node_off + L.idx);
+    float a = __ldg(&r[1].x), b = __ldg(&r[3].x);
+    return m.density * __expf(a + L.frac * (b - a));
 }
 
 __device__ __forceinline__ void parts(const KTables& T, const DevMaterial& m, const Lookup& L,
                                       float& ph, float& co, float& ra) {
-    float4 a = __ldg(T.node_parts + m.node_off + L.idx);
-    float4 b = __ldg(T.node_parts + m.node_off + L.idx + 1);
-    ph = __expf(a.x + L.frac * (b.x - a.x));
-    co = __expf(a.y + L.frac * (b.y - a.y));
-    ra = __expf(a.z + L.frac * (b.z - a.z));
+    const float4* r = T.nodes + 2 * ((size_t)m.node_off + L.idx);
+    float4 a = __ldg(r), b = __ldg(r + 2);
+    ph = __expf(a.y + L.frac * (b.y - a.y));
+    co = __expf(a.z + L.frac * (b.z - a.z));
+    ra = __expf(a.w + L.frac * (b.w - a.w));
 }
 
 // Element of the material that takes the interaction of kind k (0 photo,
@@ -326,20 +345,13 @@ __device__ __forceinline__ void parts(const KTables& T, const DevMaterial& m, co
 __device__ __noinline__ int pick_element(const KTables& T, const DevMaterial& m, const Lookup& L, int k, float r) {
     const int n_el = m.n_el;
     if (n_el == 1) return m.el_slot[0];
-    const float* base = T.elem_log + m.elem_off + (size_t)k * m.n_nodes;
-    const size_t stride = (size_t)3 * m.n_nodes;
-    float tot = 0.0f;
-    for (int i = 0; i < n_el; ++i) {
-        const float* y = base + i * stride;
-        float y0 = __ldg(y + L.idx), y1 = __ldg(y + L.idx + 1);
-        tot += __expf(y0 + L.frac * (y1 - y0));
-    }
-    float target = r * tot, acc = 0.0f;
+    // cumulative sums of w_i sigma_i / sum_j w_j sigma_j, tabulated per node in
+    // FP64 on the host and interpolated linearly: first i with r <= cum_i
+    const float* c = T.elem_cum + m.elem_off + (size_t)k * (n_el - 1) * m.n_nodes + L.idx;
     for (int i = 0; i < n_el - 1; ++i) {
-        const float* y = base + i * stride;
-        float y0 = __ldg(y + L.idx), y1 = __ldg(y + L.idx + 1);
-        acc += __expf(y0 + L.frac * (y1 - y0));
-        if (target <= acc) return m.el_slot[i];
+        float c0 = __ldg(c), c1 = __ldg(c + 1);
+        if (r <= c0 + L.frac * (c1 - c0)) return m.el_slot[i];
+        c += m.n_nodes;
     }
     return m.el_slot[n_el - 1];
 }
@@ -349,10 +361,10 @@ __device__ __noinline__ int pick_element(const KTables& T, const DevMaterial& m,
 // linear in ln E between the material's nodes.
 __device__ __forceinline__ void tally_weights(const KTables& T, const DevMaterial& m, const Lookup& L,
                                               float E, float& wk, float& wh) {
-    float2 a = __ldg(T.node_tally + m.node_off + L.idx);
-    float2 b = __ldg(T.node_tally + m.node_off + L.idx + 1);
-    wk = E * m.density * __expf(a.x + L.frac * (b.x - a.x));
-    wh = __expf(a.y + L.frac * (b.y - a.y));
+    const float4* r = T.nodes + 2 * ((size_t)m.node_off + L.idx);
+    float4 a = __ldg(r + 1), b = __ldg(r + 3);
+    wk = E * m.density * __expf(a.y + L.frac * (b.y - a.y));
+    wh = __expf(a.z + L.frac * (b.z - a.z));
 }
 
 // ---------------------------------------------------------------------------
@@ -463,7 +475,7 @@ __device__ void isotropic(float d[3], HistoryRng& rng) {
 // track-length tally: exact voxel traversal (Amanatides & Woo)
 // ---------------------------------------------------------------------------
 
-__device__ __forceinline__ void score(double* tally, long long v, float wk_len, float wh_len) {
+__device__ __forceinline__ void score(double* tally, int v, float wk_len, float wh_len) {
     atomicAdd(tally + 2 * v, (double)wk_len);
     atomicAdd(tally + 2 * v + 1, (double)wh_len);
 }
@@ -537,12 +549,14 @@ __device__ int walk_range(const KGrid& G, double* tally, const float p[3], const
     float t = t0;
     int guard = G.nx + G.ny + G.nz + 4;
     int visits = 0;
+    // flat index (C order, tally.py:292) updated incrementally; grids are < 2^31 voxels
+    const int stride[3] = {G.ny * G.nz, G.nz, 1};
+    int v = (iv[0] * G.ny + iv[1]) * G.nz + iv[2];
     while (t < t1 && guard-- > 0) {
         int ax = (tmax[0] < tmax[1]) ? (tmax[0] < tmax[2] ? 0 : 2) : (tmax[1] < tmax[2] ? 1 : 2);
         float tn = fminf(tmax[ax], t1);
         float len = tn - t;
         if (len > 0.0f) {
-            long long v = ((long long)iv[0] * G.ny + iv[1]) * G.nz + iv[2];
             score(tally, v, wk * len, wh * len);
             ++visits;
         }
@@ -550,6 +564,7 @@ __device__ int walk_range(const KGrid& G, double* tally, const float p[3], const
         if (t >= t1) break;
         iv[ax] += step[ax];
         if (iv[ax] < 0 || iv[ax] >= grid_dim(G, ax)) break;
+        v += step[ax] * stride[ax];
         tmax[ax] += tdel[ax];
     }
     return visits;
@@ -630,15 +645,17 @@ __device__ void sample_source(const KSource& S, HistoryRng& rng, float p[3], flo
 // ---------------------------------------------------------------------------
 
 constexpr int HIST_CHUNK = 256;     // histories a warp takes from the global counter at once
+// Voxel visits per piece when a warp splits its track segments.  The split
+// of a segment depends on that segment alone, never on the warp's other
+// lanes, so every piece -- and every length it scores -- is the same
+// whichever histories share a warp; runs with one seed then differ only in
+// the order of the FP64 additions.
+#ifndef TALLY_PIECE
+#define TALLY_PIECE 8
+#endif
 constexpr int BLOCK = 256;
 constexpr int WARPS_PER_BLOCK = BLOCK / 32;
 constexpr unsigned FULL = 0xffffffffu;
-
-__device__ __forceinline__ int warp_sum(int v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
-    return v;
-}
 
 __device__ __forceinline__ int warp_inclusive_scan(int v, int lane) {
 #pragma unroll
@@ -654,13 +671,14 @@ __device__ __forceinline__ int warp_inclusive_scan(int v, int lane) {
 //   1. lanes without a photon start the next history; every lane finds its
 //      material, mu and next boundary and decides its segment;
 //   2. the warp scores all its segments together: long segments are cut
-//      into equal-length pieces so that every lane walks about the same
-//      number of voxels (the pieces' partial voxel lengths add up exactly);
+//      into equal-length pieces of at most TALLY_PIECE voxel visits, and the
+//      lanes walk the pieces round-robin, so every lane walks about the same
+//      number of voxels;
 //   3. lanes move their photon and sample the interaction, if any.
-// Three 256-thread blocks per SM: the register budget (<= 80) that this
-// asks for costs no spills and hides more latency than two blocks.
+// Four 256-thread blocks per SM: the register budget (<= 64) that this asks
+// for costs no spills and hides more latency than two or three blocks.
 #ifndef CC_MIN_BLOCKS
-#define CC_MIN_BLOCKS 3
+#define CC_MIN_BLOCKS 4
 #endif
 
 template <bool FROM_SOURCE, bool TALLY>
@@ -771,10 +789,8 @@ transport_kernel(const KTables T, const KScene S, const KGrid G, const KSource S
 
         // ---- phase 2: the warp scores its segments together ----
         if (TALLY) {
-            int V = warp_sum(tal_n);
-            if (V > 0) {
-                int C = max((V + 31) >> 5, 2);
-                int m = (tal_n + C - 1) / C;
+            if (__any_sync(FULL, tal_n > 0)) {
+                int m = (tal_n + TALLY_PIECE - 1) / TALLY_PIECE;
                 if (m > 0) {
                     SegRec& r = s_seg[warp][lane];
                     r.p[0] = p[0]; r.p[1] = p[1]; r.p[2] = p[2];
@@ -904,6 +920,280 @@ transport_kernel(const KTables T, const KScene S, const KGrid G, const KSource S
     if (threadIdx.x < 6) atomicAdd(R.counters + threadIdx.x, s_cnt[threadIdx.x]);
 }
 
+// ---------------------------------------------------------------------------
+// batched multi-scene transport (one launch over many scenes)
+// ---------------------------------------------------------------------------
+
+struct KBatch {
+    const KScene* scenes;           // [n_scenes]
+    const KSource* sources;         // [n_scenes]
+    const KGrid* grids;             // [n_scenes] (tally pointers at the first scratch slot)
+    const long long* chunk_first;   // [n_scenes + 1] first chunk of each scene
+    const long long* n_hist;        // [n_scenes]
+    unsigned long long* scene_cnt;  // [n_scenes][4] absorbed, escaped, scatter_sum, fluorescence
+    const unsigned long long* run;  // [2] seed, fluorescence (written before each replay)
+    int n_scenes;
+    int chunk;                      // histories per chunk (a chunk never spans two scenes)
+    int slots;                      // batch-statistics slots per scene (1 = totals only)
+    long long n_chunks;
+};
+
+static_assert(sizeof(KSource) % 8 == 0 && sizeof(KGrid) % 8 == 0, "device tables hold 8-byte fields");
+
+struct SegRecB {
+    float p[3], d[3];
+    float t0, t1;
+    float wk, wh;
+    int scene, slot, m;
+};
+
+__device__ __forceinline__ int scene_of_chunk(const KBatch& B, long long c) {
+    int lo = 0, hi = B.n_scenes;            // chunk_first[lo] <= c < chunk_first[hi]
+    while (hi - lo > 1) {
+        int mid = (lo + hi) >> 1;
+        if (__ldg(B.chunk_first + mid) <= c) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
+// Per-scene outcome counts, summed over the lanes of the warp that end a
+// history in this iteration with the same scene.
+__device__ __forceinline__ void add_scene_counts(const KBatch& B, bool ended, int sc, unsigned a, unsigned e,
+                                                 unsigned nsc, unsigned fl, int lane) {
+    unsigned enders = __ballot_sync(FULL, ended);
+    if (!ended) return;
+    unsigned grp = __match_any_sync(enders, sc);
+    int leader = __ffs(grp) - 1;
+    unsigned va = a, ve = e, vs = nsc, vf = fl;
+    // sum over the group with shuffles of the group members
+    unsigned sa = 0, se = 0, ss = 0, sf = 0;
+    for (unsigned m = grp; m; m &= m - 1) {
+        int src = __ffs(m) - 1;
+        sa += __shfl_sync(grp, va, src);
+        se += __shfl_sync(grp, ve, src);
+        ss += __shfl_sync(grp, vs, src);
+        sf += __shfl_sync(grp, vf, src);
+    }
+    if (lane == leader) {
+        unsigned long long* c = B.scene_cnt + 4 * (size_t)sc;
+        if (sa) atomicAdd(c + 0, (unsigned long long)sa);
+        if (se) atomicAdd(c + 1, (unsigned long long)se);
+        if (ss) atomicAdd(c + 2, (unsigned long long)ss);
+        if (sf) atomicAdd(c + 3, (unsigned long long)sf);
+    }
+}
+
+template <bool TALLY>
+__global__ void __launch_bounds__(BLOCK, CC_MIN_BLOCKS)
+batch_kernel(const KTables T, const KBatch B, const KRun R) {
+    __shared__ SegRecB s_seg[TALLY ? WARPS_PER_BLOCK : 1][32];
+    __shared__ int s_pre[TALLY ? WARPS_PER_BLOCK : 1][33];
+    __shared__ unsigned long long s_cnt[2];
+    if (threadIdx.x < 2) s_cnt[threadIdx.x] = 0ull;
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const unsigned long long seed = __ldg(B.run);
+    const int fluorescence = (int)__ldg(B.run + 1);
+    unsigned long long c_steps = 0, c_vox = 0;
+
+    long long pool_next = 0, pool_end = 0;
+    int pool_scene = 0;
+    bool live = false;
+    int sc = 0, slot = 0;
+    long long li = 0;
+    float p[3], d[3], E = 0.f, tau = 0.f;
+    int nsc = 0, mat = -1;
+    long long steps = 0;
+    HistoryRng rng;
+
+    while (true) {
+        // ---- regeneration ----
+        unsigned need = __ballot_sync(FULL, !live);
+        while (need) {
+            if (pool_next >= pool_end) {
+                long long c = 0;
+                if (lane == 0) c = (long long)atomicAdd(R.work, 1ull);
+                c = __shfl_sync(FULL, c, 0);
+                if (c >= B.n_chunks) break;
+                pool_scene = scene_of_chunk(B, c);
+                long long nh = __ldg(B.n_hist + pool_scene);
+                pool_next = (c - __ldg(B.chunk_first + pool_scene)) * (long long)B.chunk;
+                pool_end = min(pool_next + (long long)B.chunk, nh);
+            }
+            int rank = __popc(need & ((1u << lane) - 1u));
+            long long avail = pool_end - pool_next;
+            int take = (int)min((long long)__popc(need), avail);
+            if (!live && rank < take) {
+                li = pool_next + rank;
+                sc = pool_scene;
+                live = true;
+                rng.init(seed, ((unsigned long long)sc << 40) + (unsigned long long)li, 0u);
+                long long nh = __ldg(B.n_hist + sc);
+                slot = (int)((li * B.slots) / nh);
+                sample_source(B.sources[sc], rng, p, d, E);
+                tau = -__logf(rng.uniform());
+                nsc = 0;
+                mat = -1;
+                steps = 0;
+            }
+            pool_next += take;
+            need = __ballot_sync(FULL, !live);
+        }
+        if (__all_sync(FULL, !live)) break;
+
+        // ---- phase 1 ----
+        const KScene& S = B.scenes[sc];
+        bool go = live;
+        bool interact = false, escape = false;
+        float s = 0.f, tau_b = 0.f, loge = 0.f;
+        float t0 = 0.f, t1 = 0.f, wk = 0.f, wh = 0.f;
+        int tal_n = 0;
+        Lookup L;
+        L.idx = 0;
+        L.frac = 0.f;
+        if (go) {
+            ++steps;
+            if (mat < 0) mat = locate(S, p, d);
+            if (mat >= T.n_mat) {
+                atomicOr(R.status, ST_BOUNDS);
+                go = live = false;
+            } else if (!(E >= E_MIN_KEV && E <= E_MAX_KEV)) {
+                atomicOr(R.status, ST_ENERGY);
+                go = live = false;
+            }
+        }
+        if (go) {
+            const DevMaterial& M = T.mats[mat];
+            loge = __logf(E);
+            L = energy_index(T, M, loge);
+            float mu = mu_total(T, M, L);
+            const float invd[3] = {1.0f / d[0], 1.0f / d[1], 1.0f / d[2]};
+            float tb = INFINITY;
+            const int np = S.n_prims;
+            for (int i = 0; i < np; ++i) tb = prim_next(S.prims[i], p, d, invd, S.eps, tb);
+            float tw = world_exit(S, p, d, invd);
+            escape = tw <= tb;
+            tb = fminf(tb, tw);
+            tau_b = mu * tb;
+            interact = tau < tau_b;
+            s = interact ? tau / fmaxf(mu, 1e-30f) : tb;
+            if (TALLY && clip_to_grid(B.grids[sc], p, d, invd, s, t0, t1)) {
+                tally_weights(T, M, L, E, wk, wh);
+                tal_n = visit_estimate(B.grids[sc], p, d, t0, t1);
+            }
+        }
+
+        // ---- phase 2: the warp scores its segments together ----
+        if (TALLY) {
+            if (__any_sync(FULL, tal_n > 0)) {
+                int m = (tal_n + TALLY_PIECE - 1) / TALLY_PIECE;
+                if (m > 0) {
+                    SegRecB& r = s_seg[warp][lane];
+                    r.p[0] = p[0]; r.p[1] = p[1]; r.p[2] = p[2];
+                    r.d[0] = d[0]; r.d[1] = d[1]; r.d[2] = d[2];
+                    r.t0 = t0; r.t1 = t1; r.wk = wk; r.wh = wh; r.scene = sc; r.slot = slot; r.m = m;
+                }
+                int incl = warp_inclusive_scan(m, lane);
+                s_pre[warp][lane] = incl - m;
+                if (lane == 31) s_pre[warp][32] = incl;
+                __syncwarp();
+                const int U = s_pre[warp][32];
+                for (int u = lane; u < U; u += 32) {
+                    int lo = 0, hi = 32;
+                    while (hi - lo > 1) {
+                        int mid = (lo + hi) >> 1;
+                        if (s_pre[warp][mid] <= u) lo = mid; else hi = mid;
+                    }
+                    const SegRecB& q = s_seg[warp][lo];
+                    int k = u - s_pre[warp][lo];
+                    float dt = (q.t1 - q.t0) / (float)q.m;
+                    float ta = q.t0 + dt * (float)k;
+                    float tz = (k == q.m - 1) ? q.t1 : ta + dt;
+                    const KGrid& G = B.grids[q.scene];
+                    c_vox += walk_range(G, G.tally + (size_t)q.slot * 2 * G.nvox, q.p, q.d, ta, tz, q.wk, q.wh);
+                }
+                __syncwarp();
+            }
+        }
+
+        // ---- phase 3 ----
+        bool ended = false, esc = false, absd = false;
+        if (go) {
+            const DevMaterial& M = T.mats[mat];
+            p[0] += d[0] * s; p[1] += d[1] * s; p[2] += d[2] * s;
+            if (!interact) {
+                tau -= tau_b;
+                if (escape) { esc = true; ended = true; }
+                mat = -1;
+            } else {
+                float ph, co, ra;
+                parts(T, M, L, ph, co, ra);
+                float r = rng.uniform() * (ph + co + ra);
+                ++nsc;
+                if (r < ph) {
+                    int eslot = pick_element(T, M, L, 0, rng.uniform());
+                    const DevElement& el = T.elems[eslot];
+                    float e_line = 0.0f;
+                    bool emit = false;
+                    if (fluorescence && el.emits && E > el.k_edge) {
+                        bool is_k = rng.uniform() < el.k_prob;
+                        bool is_rad = rng.uniform() < el.omega;
+                        if (is_k && is_rad) {
+                            float rl = rng.uniform();
+                            int lidx = el.n_lines - 1;
+                            for (int k = 0; k < el.n_lines; ++k) if (rl <= el.line_cum[k]) { lidx = k; break; }
+                            if (el.line_e[lidx] >= FLUOR_CUTOFF) { emit = true; e_line = el.line_e[lidx]; }
+                        }
+                    }
+                    if (emit) {
+                        atomicAdd(B.scene_cnt + 4 * (size_t)sc + 3, 1ull);   // rare: K lines of heavy elements
+                        E = e_line;
+                        isotropic(d, rng);
+                        tau = -__logf(rng.uniform());
+                    } else {
+                        absd = true;
+                        ended = true;
+                    }
+                } else if (r < ph + co) {
+                    int eslot = pick_element(T, M, L, 1, rng.uniform());
+                    float eps, cost;
+                    sample_compton(T.sq + (size_t)eslot * TABLE_N, E, rng, eps, cost);
+                    scatter_direction(d, cost, TWO_PI * rng.uniform());
+                    E *= eps;
+                    tau = -__logf(rng.uniform());
+                } else {
+                    int eslot = pick_element(T, M, L, 2, rng.uniform());
+                    float cost;
+                    if (!sample_rayleigh(T.rx + (size_t)eslot * TABLE_N, T.ra + (size_t)eslot * TABLE_N,
+                                         T.ray_bucket + (size_t)eslot * (RAY_BUCKETS + 1), T.elems[eslot].ray_scale,
+                                         E, rng, cost)) {
+                        atomicOr(R.status, ST_RAYLEIGH_Q);
+                        ended = true;
+                    } else {
+                        scatter_direction(d, cost, TWO_PI * rng.uniform());
+                        tau = -__logf(rng.uniform());
+                    }
+                }
+                mat = -1;
+            }
+            if (!ended && steps >= R.max_steps) {
+                atomicOr(R.status, ST_STEPS);
+                ended = true;
+            }
+        }
+        add_scene_counts(B, ended, sc, absd ? 1u : 0u, esc ? 1u : 0u, ended ? (unsigned)nsc : 0u, 0u, lane);
+        if (ended) {
+            c_steps += steps;
+            live = false;
+        }
+    }
+    atomicAdd(&s_cnt[0], c_steps);
+    atomicAdd(&s_cnt[1], c_vox);
+    __syncthreads();
+    if (threadIdx.x < 2) atomicAdd(R.counters + 4 + threadIdx.x, s_cnt[threadIdx.x]);
+}
+
 // Batch statistics fold (tally.py:59-94): T += S, Q += S^2/n_b,
 // n_hit += (S_k != 0 or S_h != 0), S = 0.
 __global__ void fold_kernel(double2* __restrict__ total, double2* __restrict__ q,
@@ -927,14 +1217,20 @@ __global__ void fold_kernel(double2* __restrict__ total, double2* __restrict__ q
     }
 }
 
-__global__ void add_kernel(double2* __restrict__ out, const double2* __restrict__ a,
-                           const double2* __restrict__ b, long long nvox) {
+// Split the interleaved device grids into the caller's separate arrays
+// (totals include a pending, not yet folded batch, as VoxelGrid.kerma_keV does).
+__global__ void unpack_kernel(const double2* __restrict__ total, const double2* __restrict__ pending,
+                              const double2* __restrict__ q, const int* __restrict__ nhit,
+                              double* __restrict__ ok, double* __restrict__ oh, double* __restrict__ ok2,
+                              double* __restrict__ oh2, int* __restrict__ on, long long nvox) {
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     long long stride = (long long)gridDim.x * blockDim.x;
     for (; i < nvox; i += stride) {
-        double2 x = a[i];
-        if (b) { double2 y = b[i]; x.x += y.x; x.y += y.y; }
-        out[i] = x;
+        double2 x = total[i];
+        if (pending) { double2 y = pending[i]; x.x += y.x; x.y += y.y; }
+        ok[i] = x.x;
+        oh[i] = x.y;
+        if (q) { double2 z = q[i]; ok2[i] = z.x; oh2[i] = z.y; on[i] = nhit[i]; }
     }
 }
 
@@ -1015,6 +1311,8 @@ struct cc_grid {
     int* d_nhit = nullptr;
     double* d_scratch = nullptr;    // [n_scratch][nvox] double2; slot 0 is the pending batch
     int n_scratch = 0;
+    char* d_out = nullptr;          // download staging: kerma, h10, kerma_sum2, h10_sum2 (f64), n_hit (i32)
+    char* h_out = nullptr;          // pinned host copy of d_out
     long long n_batches = 0;
     long long n_histories = 0;
 };
@@ -1104,14 +1402,14 @@ int cc_tables_create(cc_ctx* ctx, const cc_table_desc* desc, cc_tables** out) {
     if (desc->n_elements < 1 || desc->n_elements > MAX_ELEMS)
         return set_error(CC_E_INVALID, "n_elements must be in [1, 48]");
     CC_CUDA(cudaSetDevice(ctx->device));
-    std::vector<float> loge, elem_log;
-    std::vector<float4> nparts;
-    std::vector<float2> ntally;
-    std::vector<int> bucket;
+    std::vector<float> loge, elem_cum;
+    std::vector<float4> nodes;
+    std::vector<unsigned short> bucket;
     std::vector<DevMaterial> mats(desc->n_materials);
     for (int m = 0; m < desc->n_materials; ++m) {
         const cc_material_desc& md_ = desc->materials[m];
-        if (md_.n_nodes < 2 || md_.n_elements < 1 || md_.n_elements > MAX_ELEMS_PER_MAT || !md_.log_tally)
+        if (md_.n_nodes < 2 || md_.n_nodes > 65535 || md_.n_elements < 1 || md_.n_elements > MAX_ELEMS_PER_MAT ||
+            !md_.log_tally)
             return set_error(CC_E_INVALID, "material " + std::to_string(m) + ": bad sizes");
         DevMaterial& dm = mats[m];
         memset(&dm, 0, sizeof(dm));
@@ -1119,7 +1417,7 @@ int cc_tables_create(cc_ctx* ctx, const cc_table_desc* desc, cc_tables** out) {
         dm.n_nodes = md_.n_nodes;
         dm.n_el = md_.n_elements;
         dm.node_off = (int)loge.size();
-        dm.elem_off = (int)elem_log.size();
+        dm.elem_off = (int)elem_cum.size();
         dm.bucket_off = (int)bucket.size();
         double lmax = log(150.0);
         dm.bucket_scale = (float)(N_BUCKETS / lmax);
@@ -1128,8 +1426,9 @@ int cc_tables_create(cc_ctx* ctx, const cc_table_desc* desc, cc_tables** out) {
                 return set_error(CC_E_INVALID, "material " + std::to_string(m) + ": log_e not increasing");
             loge.push_back((float)md_.log_e[i]);
             const double* q = md_.log_parts + 4 * (size_t)i;
-            nparts.push_back(make_float4((float)q[0], (float)q[1], (float)q[2], (float)q[3]));
-            ntally.push_back(make_float2((float)md_.log_tally[2 * (size_t)i], (float)md_.log_tally[2 * (size_t)i + 1]));
+            const double* t = md_.log_tally + 2 * (size_t)i;
+            nodes.push_back(make_float4((float)md_.log_e[i], (float)q[0], (float)q[1], (float)q[2]));
+            nodes.push_back(make_float4((float)q[3], (float)t[0], (float)t[1], 0.0f));
         }
         // node index per bucket: last node whose float log E <= the bucket start
         int node = 0;
@@ -1137,10 +1436,29 @@ int cc_tables_create(cc_ctx* ctx, const cc_table_desc* desc, cc_tables** out) {
         for (int b = 0; b < N_BUCKETS; ++b) {
             float start = (float)b / dm.bucket_scale;
             while (node + 1 < md_.n_nodes - 1 && lf[node + 1] <= start) ++node;
-            bucket.push_back(node);
+            bucket.push_back((unsigned short)node);
         }
-        for (size_t i = 0; i < (size_t)md_.n_elements * 3 * md_.n_nodes; ++i)
-            elem_log.push_back((float)md_.log_elem[i]);
+        {
+            // per kind k and node: normalised cumulative sums of w_i sigma_i (FP64)
+            const int ne = md_.n_elements, nn = md_.n_nodes;
+            std::vector<double> w(ne);
+            for (int k = 0; k < 3; ++k) {
+                size_t base = elem_cum.size();
+                elem_cum.resize(base + (size_t)(ne - 1) * nn);
+                for (int j = 0; j < nn; ++j) {
+                    double tot = 0.0;
+                    for (int e = 0; e < ne; ++e) {
+                        w[e] = exp(md_.log_elem[((size_t)e * 3 + k) * nn + j]);
+                        tot += w[e];
+                    }
+                    double acc = 0.0;
+                    for (int e = 0; e < ne - 1; ++e) {
+                        acc += w[e];
+                        elem_cum[base + (size_t)e * nn + j] = (float)(tot > 0.0 ? acc / tot : 1.0);
+                    }
+                }
+            }
+        }
         for (int e = 0; e < md_.n_elements; ++e) {
             int slot = md_.element_slot[e];
             if (slot < 0 || slot >= desc->n_elements)
@@ -1194,16 +1512,14 @@ int cc_tables_create(cc_ctx* ctx, const cc_table_desc* desc, cc_tables** out) {
     KTables& k = t->k;
     int rc;
 #define UP(vec, field) if ((rc = dev_upload(t->allocs, vec, &k.field)) != CC_OK) { cc_tables_destroy(t); return rc; }
-    UP(loge, node_loge);
-    UP(nparts, node_parts);
-    UP(elem_log, elem_log);
+    UP(nodes, nodes);
+    UP(elem_cum, elem_cum);
     UP(bucket, bucket);
     UP(mats, mats);
     UP(els, elems);
     UP(sq, sq);
     UP(rx, rx);
     UP(ra, ra);
-    UP(ntally, node_tally);
     UP(rbk, ray_bucket);
 #undef UP
     k.n_mat = desc->n_materials;
@@ -1357,6 +1673,7 @@ int cc_grid_create(cc_ctx* ctx, const double origin[3], int32_t nx, int32_t ny, 
                    double voxel_cm, int32_t flags, cc_grid** out) {
     if (!ctx || !origin || !out) return set_error(CC_E_INVALID, "NULL argument");
     if (nx < 1 || ny < 1 || nz < 1 || !(voxel_cm > 0.0)) return set_error(CC_E_INVALID, "bad grid shape");
+    if ((long long)nx * ny * nz >= (1LL << 31)) return set_error(CC_E_INVALID, "grids are limited to 2^31 - 1 voxels");
     CC_CUDA(cudaSetDevice(ctx->device));
     cc_grid* g = new (std::nothrow) cc_grid();
     if (!g) return set_error(CC_E_NOMEM, "out of host memory");
@@ -1392,6 +1709,8 @@ int cc_grid_destroy(cc_grid* g) {
     cudaFree(g->d_q);
     cudaFree(g->d_nhit);
     cudaFree(g->d_scratch);
+    cudaFree(g->d_out);
+    cudaFreeHost(g->h_out);
     delete g;
     return CC_OK;
 }
@@ -1441,37 +1760,38 @@ int cc_grid_download(cc_grid* g, double* kerma, double* h10, double* k2, double*
     if (!g) return set_error(CC_E_INVALID, "grid is NULL");
     cc_ctx* c = g->ctx;
     CC_CUDA(cudaSetDevice(c->device));
-    long long nv = g->k.nvox;
-    std::vector<double> buf((size_t)nv * 2);
-    if (kerma || h10) {
-        // totals include a pending (not yet folded) batch, as VoxelGrid.kerma_keV does
-        double* tmp = nullptr;
-        CC_CUDA(cudaMalloc(&tmp, (size_t)nv * 2 * sizeof(double)));
-        int threads = 256;
-        int blocks = std::max(1, std::min((int)((nv + threads - 1) / threads), c->sm_count * 8));
-        add_kernel<<<blocks, threads, 0, c->stream>>>((double2*)tmp, (const double2*)g->d_total,
-                                                      (const double2*)g->d_scratch, nv);
-        cudaError_t e = cudaGetLastError();
-        if (e == cudaSuccess) e = cudaMemcpyAsync(buf.data(), tmp, (size_t)nv * 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
-        cudaFree(tmp);
-        if (e != cudaSuccess) return set_error(CC_E_DEVICE, std::string("grid download: ") + cudaGetErrorString(e));
-        for (long long i = 0; i < nv; ++i) {
-            if (kerma) kerma[i] = buf[2 * i];
-            if (h10) h10[i] = buf[2 * i + 1];
+    const long long nv = g->k.nvox;
+    const bool stats = g->d_q != nullptr;
+    const size_t bytes = (size_t)nv * ((stats ? 4 : 2) * sizeof(double) + (stats ? sizeof(int) : 0));
+    if (!g->d_out) {
+        // staging allocated on the first download and kept with the grid
+        CC_CUDA(cudaMalloc(&g->d_out, bytes));
+        if (cudaHostAlloc((void**)&g->h_out, bytes, cudaHostAllocDefault) != cudaSuccess) {
+            cudaFree(g->d_out);
+            g->d_out = nullptr;
+            return set_error(CC_E_NOMEM, "pinned host staging for the grid download failed");
         }
     }
-    if ((k2 || h2) && g->d_q) {
-        CC_CUDA(cudaMemcpyAsync(buf.data(), g->d_q, (size_t)nv * 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-        CC_CUDA(cudaStreamSynchronize(c->stream));
-        for (long long i = 0; i < nv; ++i) {
-            if (k2) k2[i] = buf[2 * i];
-            if (h2) h2[i] = buf[2 * i + 1];
-        }
-    }
-    if (nhit && g->d_nhit) {
-        CC_CUDA(cudaMemcpyAsync(nhit, g->d_nhit, (size_t)nv * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-        CC_CUDA(cudaStreamSynchronize(c->stream));
+    double* ok = (double*)g->d_out;
+    double* oh = ok + nv;
+    double* ok2 = stats ? oh + nv : nullptr;
+    double* oh2 = stats ? ok2 + nv : nullptr;
+    int* on = stats ? (int*)(oh2 + nv) : nullptr;
+    int threads = 256;
+    int blocks = std::max(1, std::min((int)((nv + threads - 1) / threads), c->sm_count * 8));
+    unpack_kernel<<<blocks, threads, 0, c->stream>>>((const double2*)g->d_total, (const double2*)g->d_scratch,
+                                                     (const double2*)g->d_q, g->d_nhit, ok, oh, ok2, oh2, on, nv);
+    CC_CUDA(cudaGetLastError());
+    CC_CUDA(cudaMemcpyAsync(g->h_out, g->d_out, bytes, cudaMemcpyDeviceToHost, c->stream));
+    CC_CUDA(cudaStreamSynchronize(c->stream));
+    const double* hk = (const double*)g->h_out;
+    const size_t b8 = (size_t)nv * sizeof(double);
+    if (kerma) memcpy(kerma, hk, b8);
+    if (h10) memcpy(h10, hk + nv, b8);
+    if (stats) {
+        if (k2) memcpy(k2, hk + 2 * nv, b8);
+        if (h2) memcpy(h2, hk + 3 * nv, b8);
+        if (nhit) memcpy(nhit, hk + 4 * nv, (size_t)nv * sizeof(int));
     }
     if (n_batches) *n_batches = g->n_batches;
     if (n_histories) *n_histories = g->n_histories;
@@ -1838,6 +2158,240 @@ int cc_transport_photons_device_noalloc(const cc_scene* scene, const cc_tables* 
     }
     if (n_fluor) *n_fluor = (int64_t)words[3];
     return status_to_error((unsigned)words[7]);
+}
+
+// ---------------------------------------------------------------------------
+// Batched multi-scene runs: one persistent launch over many scenes, replayed
+// from a CUDA graph.
+// ---------------------------------------------------------------------------
+
+}  // extern "C"
+
+struct cc_batch {
+    cc_ctx* ctx = nullptr;
+    const cc_tables* tables = nullptr;
+    int n_scenes = 0;
+    int slots = 1;
+    int chunk = 256;
+    bool tally = false;
+    std::vector<cc_grid*> grids;
+    std::vector<long long> nhist;
+    std::vector<std::vector<long long>> slot_counts;
+    KBatch kb;
+    char* d_mem = nullptr;
+    unsigned long long* h_run = nullptr;      // pinned: seed, fluorescence
+    unsigned long long* d_counters = nullptr; // [8]: 4 steps, 5 voxel visits, 6 work
+    unsigned* d_status = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int blocks = 0;
+    long long launches = 0;                   // kernels per replay
+};
+
+static void batch_free(cc_batch* b) {
+    if (!b) return;
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    cudaFree(b->d_mem);
+    cudaFreeHost(b->h_run);
+    delete b;
+}
+
+extern "C" {
+
+int cc_batch_create(cc_ctx* c, const cc_tables* tables, int32_t n_scenes, const cc_scene* const* scenes,
+                    const cc_source* const* sources, cc_grid* const* grids, const int64_t* n_histories,
+                    int32_t slots, int32_t chunk, cc_batch** out) {
+    if (!c || !tables || !scenes || !sources || !n_histories || !out) return set_error(CC_E_INVALID, "NULL argument");
+    if (n_scenes < 1 || n_scenes > (1 << 20)) return set_error(CC_E_INVALID, "n_scenes out of range");
+    if (slots < 1 || slots > MAX_SCRATCH) return set_error(CC_E_INVALID, "slots must be in [1, 64]");
+    if (chunk < 32 || chunk > 4096) return set_error(CC_E_INVALID, "chunk must be in [32, 4096]");
+    CC_CUDA(cudaSetDevice(c->device));
+    cc_batch* b = new (std::nothrow) cc_batch();
+    if (!b) return set_error(CC_E_NOMEM, "out of host memory");
+    b->ctx = c;
+    b->tables = tables;
+    b->n_scenes = n_scenes;
+    b->slots = slots;
+    b->chunk = chunk;
+    b->tally = grids != nullptr;
+    std::vector<KScene> hs(n_scenes);
+    std::vector<KSource> hsrc(n_scenes);
+    std::vector<KGrid> hg(n_scenes);
+    std::vector<long long> cf(n_scenes + 1, 0);
+    b->nhist.resize(n_scenes);
+    b->slot_counts.resize(n_scenes);
+    for (int i = 0; i < n_scenes; ++i) {
+        if (!scenes[i] || !sources[i] || n_histories[i] < 1) { batch_free(b); return set_error(CC_E_INVALID, "scene " + std::to_string(i) + ": NULL handle or no histories"); }
+        hs[i] = scenes[i]->k;
+        hsrc[i] = sources[i]->k;
+        memset(&hg[i], 0, sizeof(KGrid));
+        if (b->tally) {
+            cc_grid* g = grids[i];
+            if (!g) { batch_free(b); return set_error(CC_E_INVALID, "scene " + std::to_string(i) + ": NULL grid"); }
+            if (slots > 1 && !(g->flags & CC_GRID_STATS)) { batch_free(b); return set_error(CC_E_INVALID, "batch statistics need CC_GRID_STATS grids"); }
+            if (slots > 1) { int rc = grid_alloc_scratch(g, slots); if (rc != CC_OK) { batch_free(b); return rc; } }
+            hg[i] = g->k;
+            hg[i].tally = slots > 1 ? g->d_scratch : g->d_total;
+            b->grids.push_back(g);
+        }
+        b->nhist[i] = n_histories[i];
+        cf[i + 1] = cf[i] + (n_histories[i] + chunk - 1) / chunk;
+        std::vector<long long>& sc = b->slot_counts[i];
+        sc.assign(slots, 0);
+        // histories li with floor(li * slots / n) == k
+        for (int k = 0; k < slots; ++k) {
+            long long lo = (k * n_histories[i] + slots - 1) / slots, hi = ((k + 1) * n_histories[i] + slots - 1) / slots;
+            sc[k] = hi - lo;
+        }
+    }
+    // one device block for every table of the batch
+    // every sub-array starts on a 256-byte boundary (KScene is 4-byte aligned,
+    // KSource and KGrid hold 8-byte pointers)
+    auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+    size_t o_sc = 0;
+    size_t o_src = al(o_sc + sizeof(KScene) * n_scenes);
+    size_t o_g = al(o_src + sizeof(KSource) * n_scenes);
+    size_t o_cf = al(o_g + sizeof(KGrid) * n_scenes);
+    size_t o_nh = al(o_cf + sizeof(long long) * (n_scenes + 1));
+    size_t o_cnt = al(o_nh + sizeof(long long) * n_scenes);
+    size_t o_run = al(o_cnt + sizeof(unsigned long long) * 4 * n_scenes);
+    size_t o_c8 = al(o_run + 2 * sizeof(unsigned long long));
+    size_t o_st = o_c8 + 8 * sizeof(unsigned long long);
+    size_t total = al(o_st + 16);
+    if (cudaMalloc(&b->d_mem, total) != cudaSuccess) { batch_free(b); return set_error(CC_E_NOMEM, "device allocation of the batch failed"); }
+    if (cudaHostAlloc((void**)&b->h_run, 2 * sizeof(unsigned long long), cudaHostAllocDefault) != cudaSuccess) {
+        batch_free(b);
+        return set_error(CC_E_NOMEM, "pinned host allocation failed");
+    }
+    cudaStream_t st = c->stream;
+    cudaError_t e = cudaMemcpy(b->d_mem + o_sc, hs.data(), sizeof(KScene) * n_scenes, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(b->d_mem + o_src, hsrc.data(), sizeof(KSource) * n_scenes, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && b->tally) e = cudaMemcpy(b->d_mem + o_g, hg.data(), sizeof(KGrid) * n_scenes, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(b->d_mem + o_cf, cf.data(), sizeof(long long) * (n_scenes + 1), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(b->d_mem + o_nh, b->nhist.data(), sizeof(long long) * n_scenes, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) { batch_free(b); return set_error(CC_E_DEVICE, std::string("batch upload: ") + cudaGetErrorString(e)); }
+    KBatch& k = b->kb;
+    k.scenes = (const KScene*)(b->d_mem + o_sc);
+    k.sources = (const KSource*)(b->d_mem + o_src);
+    k.grids = (const KGrid*)(b->d_mem + o_g);
+    k.chunk_first = (const long long*)(b->d_mem + o_cf);
+    k.n_hist = (const long long*)(b->d_mem + o_nh);
+    k.scene_cnt = (unsigned long long*)(b->d_mem + o_cnt);
+    k.run = (const unsigned long long*)(b->d_mem + o_run);
+    k.n_scenes = n_scenes;
+    k.chunk = chunk;
+    k.slots = slots;
+    k.n_chunks = cf[n_scenes];
+    b->d_counters = (unsigned long long*)(b->d_mem + o_c8);
+    b->d_status = (unsigned*)(b->d_mem + o_st);
+    KRun R;
+    memset(&R, 0, sizeof(R));
+    R.max_steps = c->max_steps;
+    R.status = b->d_status;
+    R.counters = b->d_counters;
+    R.work = b->d_counters + 6;
+    // launch shape: the context's block size and blocks per SM (the autotuner sets them)
+    int per_sm = c->blocks_per_sm;
+    if (per_sm == 0) {
+        int occ = 0;
+        cudaError_t oe = b->tally ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch_kernel<true>, c->block, 0)
+                                  : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, batch_kernel<false>, c->block, 0);
+        per_sm = (oe == cudaSuccess && occ > 0) ? occ : 1;
+    }
+    b->blocks = c->sm_count * per_sm;
+    // capture: clear the counters, take the seed, transport, fold the batches
+    e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) e = cudaMemsetAsync(b->d_mem + o_cnt, 0, sizeof(unsigned long long) * 4 * n_scenes, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(b->d_mem + o_c8, 0, total - o_c8, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(b->d_mem + o_run, b->h_run, 2 * sizeof(unsigned long long), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) {
+        if (b->tally) batch_kernel<true><<<b->blocks, c->block, 0, st>>>(tables->k, k, R);
+        else batch_kernel<false><<<b->blocks, c->block, 0, st>>>(tables->k, k, R);
+        e = cudaGetLastError();
+        b->launches = 1;
+    }
+    if (e == cudaSuccess && b->tally && slots > 1) {
+        int threads = 256;
+        for (int i = 0; i < n_scenes && e == cudaSuccess; ++i) {
+            cc_grid* g = grids[i];
+            int nb = std::max(1, std::min((int)((g->k.nvox + threads - 1) / threads), c->sm_count * 8));
+            for (int sl = 0; sl < slots; ++sl) {
+                long long cnt = b->slot_counts[i][sl];
+                if (cnt <= 0) continue;
+                fold_kernel<<<nb, threads, 0, st>>>((double2*)g->d_total, (double2*)g->d_q, g->d_nhit,
+                                                     (double2*)(g->d_scratch + (size_t)sl * 2 * g->k.nvox),
+                                                     g->k.nvox, 1.0 / (double)cnt);
+                ++b->launches;
+            }
+            e = cudaGetLastError();
+        }
+    }
+    cudaGraph_t graph = nullptr;
+    cudaError_t e2 = cudaStreamEndCapture(st, &graph);
+    if (e == cudaSuccess) e = e2;
+    b->graph = graph;
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&b->exec, graph, 0);
+    if (e != cudaSuccess) { batch_free(b); return set_error(CC_E_DEVICE, std::string("batch graph: ") + cudaGetErrorString(e)); }
+    *out = b;
+    return CC_OK;
+}
+
+int cc_batch_run(cc_batch* b, uint64_t seed, int32_t fluorescence, int64_t* scene_counts, cc_run_out* out) {
+    if (!b) return set_error(CC_E_INVALID, "batch is NULL");
+    cc_ctx* c = b->ctx;
+    CC_CUDA(cudaSetDevice(c->device));
+    b->h_run[0] = seed;
+    b->h_run[1] = (unsigned long long)(fluorescence != 0);
+    cudaStream_t st = c->stream;
+    CC_CUDA(cudaEventRecord(c->ev0, st));
+    CC_CUDA(cudaGraphLaunch(b->exec, st));
+    CC_CUDA(cudaEventRecord(c->ev1, st));
+    std::vector<unsigned long long> cnt(4 * (size_t)b->n_scenes);
+    unsigned long long c8[8];
+    unsigned status = 0;
+    CC_CUDA(cudaMemcpyAsync(cnt.data(), b->kb.scene_cnt, cnt.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+    CC_CUDA(cudaMemcpyAsync(c8, b->d_counters, sizeof(c8), cudaMemcpyDeviceToHost, st));
+    CC_CUDA(cudaMemcpyAsync(&status, b->d_status, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    CC_CUDA(cudaStreamSynchronize(st));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    long long tot = 0;
+    for (int i = 0; i < b->n_scenes; ++i) tot += b->nhist[i];
+    if (b->tally && b->slots > 1)
+        for (int i = 0; i < b->n_scenes; ++i) {
+            cc_grid* g = b->grids[i];
+            for (int sl = 0; sl < b->slots; ++sl)
+                if (b->slot_counts[i][sl] > 0) { g->n_batches += 1; g->n_histories += b->slot_counts[i][sl]; }
+        }
+    if (scene_counts)
+        for (size_t i = 0; i < cnt.size(); ++i) scene_counts[i] = (int64_t)cnt[i];
+    if (out) {
+        memset(out, 0, sizeof(*out));
+        out->n_histories = tot;
+        for (int i = 0; i < b->n_scenes; ++i) {
+            out->n_absorbed += (int64_t)cnt[4 * i];
+            out->n_escaped += (int64_t)cnt[4 * i + 1];
+            out->scatter_sum += (int64_t)cnt[4 * i + 2];
+            out->n_fluorescence += (int64_t)cnt[4 * i + 3];
+        }
+        out->n_batches = b->slots;
+        out->gpu_launches = b->launches;
+        out->elapsed_ms = ms;
+        out->n_steps = (int64_t)c8[4];
+        out->n_voxel_visits = (int64_t)c8[5];
+        out->transport_ms = ms;
+        out->transport_launches = 1;
+    }
+    return status_to_error(status);
+}
+
+int cc_batch_destroy(cc_batch* b) {
+    if (!b) return CC_OK;
+    cudaSetDevice(b->ctx->device);
+    cudaStreamSynchronize(b->ctx->stream);
+    batch_free(b);
+    return CC_OK;
 }
 
 }  // extern "C"

@@ -67,7 +67,7 @@ def _muen_rows(name: str):
     return e, PchipInterpolator(np.log(e), np.log(muen))
 
 
-def _refine_for_pchip(grid: np.ndarray, pchip, tol: float = 2e-6, rounds: int = 8) -> np.ndarray:
+def _refine_for_pchip(grid: np.ndarray, pchip, tol: float = 1e-5, rounds: int = 8) -> np.ndarray:
     """Bisect (in ln E) every interval where linear interpolation of the
     mu_en PCHIP misses its midpoint by more than tol (relative)."""
     for _ in range(rounds):

@@ -38,8 +38,11 @@ def linear_mu(material: str, energies_kev) -> np.ndarray:
     return total * tb.density(material)
 
 
-def kramers_spectrum(kvp: float, filtration_mm_al: float, n_bins: int = 60):
-    """Kramers' law with Al attenuation (spectrum.py:55-62)."""
+def kramers_spectrum(kvp: float, filtration_mm_al: float, n_bins: int | None = 60):
+    """Kramers' law with Al attenuation (spectrum.py:55-62); n_bins=None gives
+    1 keV bins from 5 keV to kVp."""
+    if n_bins is None:
+        n_bins = max(1, int(round(kvp - 5.0)))
     e = np.linspace(5.0, kvp, n_bins + 1)
     e_mid = 0.5 * (e[:-1] + e[1:])
     raw = np.clip(e_mid * (kvp - e_mid), 0, None)

@@ -114,6 +114,7 @@ class Engine:
         self.device = device
         self._tables: dict = {}
         self._grids: dict = {}
+        self._sources: dict = {}
         self._lock = threading.Lock()
 
     def set_launch(self, block_size: int = 256, blocks_per_sm: int = 0) -> None:
@@ -165,10 +166,26 @@ class Engine:
         N.check(self.lib.cc_source_create(self.ctx, C.byref(spec.desc), C.byref(h)))
         return h
 
+    def cached_source(self, src: dict) -> C.c_void_p:
+        """Device source for a scene's source section, built once per distinct section."""
+        key = repr(src)
+        with self._lock:
+            h = self._sources.get(key)
+            if h is None:
+                h = self.source(SourceSpec(src))
+                if len(self._sources) >= 16:
+                    _, old = self._sources.popitem()
+                    self.lib.cc_source_destroy(old)
+                self._sources[key] = h
+            return h
+
     def close(self):
         for dg in self._grids.values():
             dg.close()
         self._grids.clear()
+        for h in self._sources.values():
+            self.lib.cc_source_destroy(h)
+        self._sources.clear()
         for ts, h in self._tables.values():
             self.lib.cc_tables_destroy(h)
         self._tables.clear()
@@ -270,9 +287,8 @@ def run_transport(scene, n_histories: int = 100_000, seed: int | None = None,
     fluorescence = raw.get("physics", {}).get("fluorescence", True)
     names = geometry.materials()
     ts, th = eng.tables(names, need_muen=grid is not None)
-    spec = SourceSpec(src)
     sh = eng.scene(geometry, ts)
-    srch = eng.source(spec)
+    srch = eng.cached_source(src)
     dg = eng.device_grid(grid, stats=track_uncertainty) if grid is not None else None
     edep = np.zeros(len(names))
     edep2 = np.zeros(len(names))
@@ -284,7 +300,6 @@ def run_transport(scene, n_histories: int = 100_000, seed: int | None = None,
         if dg is not None:
             dg.download(grid)
     finally:
-        eng.lib.cc_source_destroy(srch)
         eng.lib.cc_scene_destroy(sh)
     n_batches = int(out.n_batches)
     dep = {name: float(edep[i]) for i, name in enumerate(names) if edep[i] != 0.0}

@@ -86,3 +86,60 @@ def pencil_beam_arrays(n: int, start, direction, energy_kev: float):
     pos = np.tile(np.asarray(start, dtype=float), (n, 1))
     dirv = np.tile(np.asarray(direction, dtype=float), (n, 1))
     return pos, dirv, np.full(n, float(energy_kev))
+
+
+BATCH_MATERIALS = ["air", "water", "bone", "muscle", "pmma", "lead", "concrete"]
+
+
+def batched_scenes(n_scenes: int = 256, seed: int = 2026, hist_lo: float = 1e5, hist_hi: float = 1e7):
+    """The batched configuration: n_scenes random scenes.
+
+    Per scene: 1-12 primitives of a uniformly drawn type (box / cylinder /
+    sphere) with dimensions U(1, 50) cm, materials drawn from
+    {air, water, ICRU bone, muscle, PMMA, lead, concrete} (a lead primitive
+    gets one dimension U(0.01, 0.2) cm); a source that is monoenergetic
+    U(20, 140) keV or a 60-140 kVp tungsten spectrum with 2-4 mm Al (the
+    Kramers model of spectrum.py:55-62 in 1 keV bins); its own 64^3 kerma
+    grid of U(0.5, 2) cm voxels centred on the scene; history counts
+    log-uniform in [hist_lo, hist_hi].  Returns (scenes, grid specs, counts).
+    """
+    rng = np.random.default_rng(seed)
+    scenes, grids, counts = [], [], []
+    for s in range(n_scenes):
+        voxel = float(rng.uniform(0.5, 2.0))
+        half = 32 * voxel
+        shape = str(rng.choice(["box", "cylinder", "sphere"]))
+        geoms = []
+        for i in range(int(rng.integers(1, 13))):
+            mat = str(rng.choice(BATCH_MATERIALS))
+            c = [float(x) for x in rng.uniform(-0.6 * half, 0.6 * half, 3)]
+            g = {"name": f"p{i}", "shape": shape, "material": mat, "center": c}
+            if shape == "box":
+                size = [float(x) for x in rng.uniform(1.0, 50.0, 3)]
+                if mat == "lead":
+                    size[int(rng.integers(0, 3))] = float(rng.uniform(0.01, 0.2))
+                g["size_cm"] = size
+            elif shape == "cylinder":
+                g["axis"] = str(rng.choice(["x", "y", "z"]))
+                g["radius_cm"] = float(rng.uniform(1.0, 50.0)) / 2.0
+                g["height_cm"] = float(rng.uniform(1.0, 50.0))
+                if mat == "lead":
+                    g["height_cm"] = float(rng.uniform(0.01, 0.2))
+            else:
+                g["radius_cm"] = float(rng.uniform(1.0, 50.0)) / 2.0
+                if mat == "lead":
+                    g["radius_cm"] = float(rng.uniform(0.01, 0.2))
+            geoms.append(g)
+        sid = 100.0 + half
+        src = {"position": [0.0, 0.0, -sid], "direction": [0.0, 0.0, 1.0],
+               "field": {"shape": "rect", "size_cm": [2 * half, 2 * half], "sid_cm": sid}}
+        if rng.random() < 0.5:
+            src["spectrum"] = [{"energy_keV": float(rng.uniform(20.0, 140.0)), "weight": 1.0}]
+        else:
+            e, w = kramers_spectrum(float(rng.uniform(60.0, 140.0)), float(rng.uniform(2.0, 4.0)),
+                                    n_bins=None)
+            src["spectrum"] = [{"energy_keV": float(a), "weight": float(b)} for a, b in zip(e, w)]
+        scenes.append({"source": src, "geometry": geoms, "physics": {"fluorescence": True}})
+        grids.append({"origin": (-half, -half, -half), "shape": (64, 64, 64), "voxel_cm": voxel})
+        counts.append(int(round(float(np.exp(rng.uniform(np.log(hist_lo), np.log(hist_hi)))))))
+    return scenes, grids, counts

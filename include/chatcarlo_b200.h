@@ -60,6 +60,7 @@ typedef struct cc_tables cc_tables;
 typedef struct cc_scene cc_scene;
 typedef struct cc_grid cc_grid;
 typedef struct cc_source cc_source;
+typedef struct cc_batch cc_batch;
 
 /* One analytic primitive; list order is kept (a later one overrides an
  * earlier one where they overlap: geometry.py:205-212). */
@@ -228,6 +229,24 @@ int cc_transport_photons_device_noalloc(const cc_scene* scene, const cc_tables* 
                                         uint64_t seed, uint64_t stream_offset, int32_t fluorescence,
                                         int32_t* d_n_scatter, uint8_t* d_absorbed, uint8_t* d_escaped,
                                         double* edep_by_material, int64_t* n_fluorescence, void* stream);
+
+/* Batched multi-scene runs (no counterpart in the reference, which runs one
+ * scene per run_transport call).  n_scenes scenes, each with its own source,
+ * grid (grids may be NULL: no tallies) and history count, share one table
+ * set and run in one persistent launch: warps take chunks of `chunk`
+ * histories that never span two scenes; history i of scene s draws the
+ * Philox stream of history (s << 40) + i.  With slots > 1 (grids created
+ * with CC_GRID_STATS) each scene's histories form `slots` batches for the
+ * batch statistics.  cc_batch_create captures the whole sequence (counter
+ * reset, transport, batch folds) in a CUDA graph; cc_batch_run replays it.
+ * The launch shape is the context's (cc_ctx_set_launch).  scene_counts gets
+ * [n_scenes][4] absorbed, escaped, interactions, fluorescence emissions. */
+int cc_batch_create(cc_ctx* ctx, const cc_tables* tables, int32_t n_scenes, const cc_scene* const* scenes,
+                    const cc_source* const* sources, cc_grid* const* grids, const int64_t* n_histories,
+                    int32_t slots, int32_t chunk, cc_batch** out);
+int cc_batch_run(cc_batch* batch, uint64_t seed, int32_t fluorescence, int64_t* scene_counts,
+                 cc_run_out* out);
+int cc_batch_destroy(cc_batch* batch);
 
 /* Sample source photons only (tests of source.py parity). */
 int cc_sample_source(cc_ctx* ctx, const cc_source* src, int64_t n, uint64_t seed,
