@@ -24,7 +24,7 @@ CC_E_TIMEOUT = -7
 CC_E_BOUNDS = -8
 CC_E_NOMEM = -9
 
-CC_SHAPE_BOX, CC_SHAPE_SPHERE, CC_SHAPE_CYLINDER = 0, 1, 2
+CC_SHAPE_BOX, CC_SHAPE_SPHERE, CC_SHAPE_CYLINDER, CC_SHAPE_ELLIPSOID = 0, 1, 2, 3
 CC_GRID_STATS = 1
 CC_FIELD_RECT, CC_FIELD_CONE, CC_FIELD_PARALLEL = 0, 1, 2
 

@@ -59,9 +59,9 @@ constexpr unsigned ST_ENERGY = 1u, ST_RAYLEIGH_Q = 2u, ST_STEPS = 4u, ST_BOUNDS 
 struct DevPrim {
     int type, material, axis, pad;
     float c[3];
-    float h[3];     // box half sizes
+    float h[3];     // box half sizes, ellipsoid semi-axes
     float r2;       // radius^2
-    float r;        // radius
+    float r;        // radius; ellipsoid: 1 / smallest semi-axis
     float hh;       // cylinder half height
 };
 
@@ -188,6 +188,12 @@ __device__ __forceinline__ bool contains(const DevPrim& g, const float p[3], con
                slab_inside(o2, d[2], g.h[2], tol);
     } else if (g.type == CC_SHAPE_SPHERE) {
         return ball_inside(o0 * o0 + o1 * o1 + o2 * o2, o0 * d[0] + o1 * d[1] + o2 * d[2], g.r, tol);
+    } else if (g.type == CC_SHAPE_ELLIPSOID) {
+        // the unit ball in coordinates scaled by the semi-axes; the band
+        // scaled by the smallest semi-axis covers the tol band everywhere
+        float u0 = o0 / g.h[0], u1 = o1 / g.h[1], u2 = o2 / g.h[2];
+        return ball_inside(u0 * u0 + u1 * u1 + u2 * u2,
+                           u0 * d[0] / g.h[0] + u1 * d[1] / g.h[1] + u2 * d[2] / g.h[2], 1.0f, tol * g.r);
     } else {
         const int ax = g.axis;
         const int i0 = ax == 0 ? 1 : 0, i1 = ax == 2 ? 1 : 2;
@@ -253,6 +259,27 @@ __device__ float prim_next(const DevPrim& g, const float p[3], const float d[3],
         float t1 = q, t2 = (q != 0.0f) ? c / q : 0.0f;
         take_root(t1, eps, best);
         take_root(t2, eps, best);
+        return best;
+    } else if (g.type == CC_SHAPE_ELLIPSOID) {
+        // |u + t v|^2 = 1 with u = o / h, v = d / h (componentwise)
+        float ux = ox / g.h[0], uy = oy / g.h[1], uz = oz / g.h[2];
+        float vx = d[0] / g.h[0], vy = d[1] / g.h[1], vz = d[2] / g.h[2];
+        float a = vx * vx + vy * vy + vz * vz;
+        float b = ux * vx + uy * vy + uz * vz;
+        float u2 = ux * ux + uy * uy + uz * uz;
+        float tl = eps * g.r;
+        float lo = fmaxf(1.0f - tl, 0.0f), hi = 1.0f + tl;
+        if (u2 >= lo * lo && u2 <= hi * hi) {            // on the surface
+            if (b <= 0.0f) take_root(-2.0f * b / a, eps, best);
+            return best;
+        }
+        float inva = 1.0f / a;
+        float ex = ux - b * inva * vx, ey = uy - b * inva * vy, ez = uz - b * inva * vz;
+        float disc = (1.0f - (ex * ex + ey * ey + ez * ez)) * a;   // b^2 - a c without cancellation
+        if (disc < 0.0f) return best;
+        float q = -(b + copysignf(sqrtf(disc), b));
+        take_root(q * inva, eps, best);
+        take_root((q != 0.0f) ? (u2 - 1.0f) / q : 0.0f, eps, best);
         return best;
     } else {
         const int ax = g.axis;
@@ -813,7 +840,8 @@ transport_kernel(const KTables T, const KScene S, const KGrid G, const KSource S
                     float dt = (q.t1 - q.t0) / (float)q.m;
                     float ta = q.t0 + dt * (float)k;
                     float tz = (k == q.m - 1) ? q.t1 : ta + dt;
-                    c_vox += walk_range(G, G.tally + (size_t)q.batch * 2 * G.nvox, q.p, q.d, ta, tz, q.wk, q.wh);
+                    int nv = walk_range(G, G.tally + (size_t)q.batch * 2 * G.nvox, q.p, q.d, ta, tz, q.wk, q.wh);
+                    c_vox += max(nv - (k > 0 ? 1 : 0), 0);   // a cut voxel is one visit
                 }
                 __syncwarp();
             }
@@ -1111,7 +1139,8 @@ batch_kernel(const KTables T, const KBatch B, const KRun R) {
                     float ta = q.t0 + dt * (float)k;
                     float tz = (k == q.m - 1) ? q.t1 : ta + dt;
                     const KGrid& G = B.grids[q.scene];
-                    c_vox += walk_range(G, G.tally + (size_t)q.slot * 2 * G.nvox, q.p, q.d, ta, tz, q.wk, q.wh);
+                    int nv = walk_range(G, G.tally + (size_t)q.slot * 2 * G.nvox, q.p, q.d, ta, tz, q.wk, q.wh);
+                    c_vox += max(nv - (k > 0 ? 1 : 0), 0);   // a cut voxel is one visit
                 }
                 __syncwarp();
             }
@@ -1561,7 +1590,11 @@ int cc_scene_create(cc_ctx* ctx, const cc_primitive* prims, int32_t n_prims, int
     for (int i = 0; i < n_prims; ++i) {
         const cc_primitive& p = prims[i];
         DevPrim& g = k.prims[i];
-        if (p.type < 0 || p.type > 2) { delete s; return set_error(CC_E_BAD_SHAPE, "unknown primitive type " + std::to_string(p.type)); }
+        if (p.type < 0 || p.type > 3) { delete s; return set_error(CC_E_BAD_SHAPE, "unknown primitive type " + std::to_string(p.type)); }
+        if (p.type == CC_SHAPE_ELLIPSOID && !(p.size[0] > 0 && p.size[1] > 0 && p.size[2] > 0)) {
+            delete s;
+            return set_error(CC_E_INVALID, "ellipsoid axes must be positive");
+        }
         if (p.material < 0 || p.material >= MAX_MATS) { delete s; return set_error(CC_E_UNKNOWN_MATERIAL, "primitive material out of range"); }
         if (p.type == CC_SHAPE_CYLINDER && (p.axis < 0 || p.axis > 2)) { delete s; return set_error(CC_E_INVALID, "cylinder axis must be 0, 1 or 2"); }
         g.type = p.type;
@@ -1571,6 +1604,8 @@ int cc_scene_create(cc_ctx* ctx, const cc_primitive* prims, int32_t n_prims, int
         g.r2 = (float)(p.radius * p.radius);
         g.r = (float)p.radius;
         g.hh = (float)(0.5 * p.height);
+        if (p.type == CC_SHAPE_ELLIPSOID)
+            g.r = (float)(2.0 / std::min(p.size[0], std::min(p.size[1], p.size[2])));
     }
     *out = s;
     return CC_OK;

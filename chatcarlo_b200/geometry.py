@@ -1,7 +1,9 @@
 """Scene geometry on the host: primitives in list order, world box, packing.
 
 Mirrors ChatCarlo's ``Geometry`` (chatcarlo/geometry.py:121-231): box,
-sphere and finite cylinder (axis x/y/z) primitives; where they overlap the
+sphere and finite cylinder (axis x/y/z) primitives, plus an axis-aligned
+``ellipsoid`` (``semi_axes_cm``) that the reference does not have and the
+learned-denoiser phantoms need; where they overlap the
 later one in the list wins; everything else is the background material;
 the world is the bounding box of all primitives grown by bbox_margin_cm
 (geometry.py:137-164).  Ray tracing happens in the engine; the host keeps
@@ -17,7 +19,8 @@ import numpy as np
 from . import _native as N
 
 AXES = {"x": 0, "y": 1, "z": 2}
-SHAPES = {"box": N.CC_SHAPE_BOX, "sphere": N.CC_SHAPE_SPHERE, "cylinder": N.CC_SHAPE_CYLINDER}
+SHAPES = {"box": N.CC_SHAPE_BOX, "sphere": N.CC_SHAPE_SPHERE, "cylinder": N.CC_SHAPE_CYLINDER,
+          "ellipsoid": N.CC_SHAPE_ELLIPSOID}
 
 
 def shape_bbox(g: dict) -> tuple[np.ndarray, np.ndarray]:
@@ -29,6 +32,9 @@ def shape_bbox(g: dict) -> tuple[np.ndarray, np.ndarray]:
     if shape == "sphere":
         r = g["radius_cm"]
         return c - r, c + r
+    if shape == "ellipsoid":
+        s = np.asarray(g["semi_axes_cm"], dtype=float)
+        return c - s, c + s
     if shape == "cylinder":
         ai = AXES[g.get("axis", "z")]
         r, h = g["radius_cm"], g["height_cm"]
@@ -49,6 +55,8 @@ def contains(g: dict, points: np.ndarray) -> np.ndarray:
         return np.all((points >= c - half) & (points <= c + half), axis=1)
     if shape == "sphere":
         return np.sum((points - c) ** 2, axis=1) <= g["radius_cm"] ** 2
+    if shape == "ellipsoid":
+        return np.sum(((points - c) / np.asarray(g["semi_axes_cm"], dtype=float)) ** 2, axis=1) <= 1.0
     if shape == "cylinder":
         ai = AXES[g.get("axis", "z")]
         oi = [k for k in range(3) if k != ai]
@@ -110,6 +118,9 @@ class Geometry:
             if g["shape"] == "box":
                 for k in range(3):
                     p.size[k] = float(g["size_cm"][k])
+            elif g["shape"] == "ellipsoid":
+                for k in range(3):
+                    p.size[k] = 2.0 * float(g["semi_axes_cm"][k])
             else:
                 p.radius = float(g["radius_cm"])
                 if g["shape"] == "cylinder":

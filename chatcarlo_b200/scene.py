@@ -3,7 +3,8 @@
 Checks the parts of the schema the transport path reads: the source
 (explicit spectrum or kvp 20-150, focus position and direction, rect /
 cone / parallel field, rotation), the geometry list (box / sphere /
-cylinder with positive sizes, axis x/y/z, a known material) and the
+cylinder with positive sizes, axis x/y/z, a known material; plus the
+axis-aligned ``ellipsoid`` with ``semi_axes_cm``, an extension) and the
 physics.fluorescence switch (scene.py:52-309).  Errors carry the path of
 the offending entry, like ChatCarlo's SceneError.
 """
@@ -16,7 +17,7 @@ import yaml
 
 from . import tables as tb
 
-VALID_SHAPES = {"box", "cylinder", "sphere"}
+VALID_SHAPES = {"box", "cylinder", "sphere", "ellipsoid"}
 VALID_AXES = {"x", "y", "z"}
 VALID_FIELDS = {"rect", "cone", "parallel"}
 
@@ -141,6 +142,10 @@ def validate_scene(raw) -> Scene:
                 sz = g.get("size_cm")
                 if not (isinstance(sz, (list, tuple)) and len(sz) == 3 and all(_num(x) and x > 0 for x in sz)):
                     errors.append(SceneError(f"{path}.size_cm", "expected three positive numbers"))
+            elif shape == "ellipsoid":
+                sa = g.get("semi_axes_cm")
+                if not (isinstance(sa, (list, tuple)) and len(sa) == 3 and all(_num(x) and x > 0 for x in sa)):
+                    errors.append(SceneError(f"{path}.semi_axes_cm", "expected three positive numbers"))
             else:
                 _positive(g, "radius_cm", path, errors)
                 if shape == "cylinder":

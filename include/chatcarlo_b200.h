@@ -46,6 +46,8 @@ extern "C" {
 #define CC_SHAPE_BOX      0
 #define CC_SHAPE_SPHERE   1
 #define CC_SHAPE_CYLINDER 2
+#define CC_SHAPE_ELLIPSOID 3  /* axis-aligned ellipsoid: an extension with no reference
+                                 counterpart (the reference has box/sphere/cylinder only) */
 
 /* grid flags */
 #define CC_GRID_STATS 1   /* batch statistics (kerma_sum2, h10_sum2, n_batches_hit) */
@@ -70,7 +72,7 @@ typedef struct {
     int32_t axis;          /* cylinder axis 0=x 1=y 2=z */
     int32_t pad;
     double center[3];
-    double size[3];        /* box full edge lengths */
+    double size[3];        /* box full edge lengths; ellipsoid full axis lengths (2 x semi-axes) */
     double radius;         /* sphere, cylinder */
     double height;         /* cylinder full length */
 } cc_primitive;
@@ -145,7 +147,8 @@ typedef struct {
     int64_t gpu_launches;         /* kernels launched (transport + batch folds) */
     double elapsed_ms;            /* device time of the run (CUDA events) */
     int64_t n_steps;              /* transport steps (track segments) of all histories */
-    int64_t n_voxel_visits;       /* voxel scores of the track-length tally walk */
+    int64_t n_voxel_visits;       /* voxels crossed by the track-length tally walk (a voxel cut
+                                     between two pieces of a split segment counts once) */
     double transport_ms;          /* device time of the transport kernel launches alone */
     int64_t transport_launches;
 } cc_run_out;

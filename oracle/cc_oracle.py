@@ -163,6 +163,23 @@ def _sphere(o, d, center, radius):
     return np.where(hit, np.minimum(t1, t2), np.nan), np.where(hit, np.maximum(t1, t2), np.nan)
 
 
+def _ellipsoid(o, d, center, semi):
+    """Axis-aligned ellipsoid: the project's extension primitive (the
+    reference has none), solved like _sphere in coordinates scaled by the
+    semi-axes."""
+    s = np.asarray(semi, dtype=float)
+    u = (o - np.asarray(center, dtype=float)) / s
+    v = d / s
+    a = np.einsum("ij,ij->i", v, v)
+    b = np.einsum("ij,ij->i", u, v)
+    c = np.einsum("ij,ij->i", u, u) - 1.0
+    disc = b * b - a * c
+    hit = disc >= 0
+    sq = np.sqrt(np.where(hit, disc, 0.0))
+    t1, t2 = (-b - sq) / a, (-b + sq) / a
+    return np.where(hit, t1, np.nan), np.where(hit, t2, np.nan)
+
+
 def _cylinder(o, d, center, radius, height, axis, eps=1e-12):
     """geometry.py:57-99."""
     ai = AXES[axis]
@@ -207,6 +224,8 @@ def _contains(g, p):
         return np.all((p >= c - s / 2) & (p <= c + s / 2), axis=1)
     if g["shape"] == "sphere":
         return np.sum((p - c) ** 2, axis=1) <= g["radius_cm"] ** 2
+    if g["shape"] == "ellipsoid":
+        return np.sum(((p - c) / np.asarray(g["semi_axes_cm"], dtype=float)) ** 2, axis=1) <= 1.0
     ai = AXES[g.get("axis", "z")]
     oi = [k for k in range(3) if k != ai]
     r2 = (p[:, oi[0]] - c[oi[0]]) ** 2 + (p[:, oi[1]] - c[oi[1]]) ** 2
@@ -237,6 +256,8 @@ class OracleGeometry:
             return _box(o, d, g["center"], g["size_cm"])
         if g["shape"] == "sphere":
             return _sphere(o, d, g["center"], g["radius_cm"])
+        if g["shape"] == "ellipsoid":
+            return _ellipsoid(o, d, g["center"], g["semi_axes_cm"])
         return _cylinder(o, d, g["center"], g["radius_cm"], g["height_cm"], g.get("axis", "z"))
 
     def next_boundary(self, o, d, eps=1e-6):

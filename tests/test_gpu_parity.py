@@ -308,3 +308,25 @@ def test_photons_on_a_curved_surface_moving_almost_tangentially(engine, shape, r
                          (rg.escaped, ro.escaped)):
         pg, po = np.mean(sel_g), np.mean(sel_o)
         assert abs(_z(pg, 200_000, po, 20_000)) < 4, (pg, po)
+
+
+def test_ellipsoid_transmission_and_oblique_rays(engine):
+    """The ellipsoid extension primitive: uncollided transmission along its
+    x axis vs exp(-sum mu t), and an oblique pencil beam vs the oracle."""
+    geoms = [{"name": "e", "shape": "ellipsoid", "material": "water", "center": [0, 0, 0],
+              "semi_axes_cm": [5.0, 8.0, 3.0]}]
+    n = 1_000_000
+    _, _, _, r = _gpu_tp(engine, geoms, [-15.0, 0, 0], [1, 0, 0], 60.0, n, seed=3)
+    unc = np.mean(r.escaped & (r.n_scatter == 0))
+    expect = float(np.exp(-O.linear_mu("water", 60.0)[0] * 10.0 - O.linear_mu("air", 60.0)[0] * 60.0))
+    assert abs(unc - expect) < 3.0 * np.sqrt(expect * (1 - expect) / n), (unc, expect)
+    d = np.array([0.8, 0.5, 0.33])
+    d /= np.linalg.norm(d)
+    start = np.array([1.0, 2.0, -0.5]) - 12.0 * d
+    _, _, _, rg = _gpu_tp(engine, geoms, start, d, 60.0, 400_000, seed=4)
+    pos, dirv, eo = W.pencil_beam_arrays(40_000, start, d, 60.0)
+    ro = O.transport_photons(pos, dirv, eo, O.OracleGeometry(geoms), np.random.default_rng(4))
+    for sel_g, sel_o in ((rg.escaped & (rg.n_scatter == 0), ro.escaped & (ro.n_scatter == 0)),
+                         (rg.absorbed, ro.absorbed)):
+        pg, po = np.mean(sel_g), np.mean(sel_o)
+        assert abs(_z(pg, 400_000, po, 40_000)) < 4, (pg, po)

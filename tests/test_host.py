@@ -26,6 +26,7 @@ def test_benchmark_scenes_validate():
     (lambda r: r["source"].update(kvp=80), "source"),
     (lambda r: r["geometry"][2].update(axis="w"), "geometry[2].axis"),
     (lambda r: r["source"]["field"].update(size_cm=[35.0]), "source.field.size_cm"),
+    (lambda r: r["geometry"][1].update(shape="ellipsoid", semi_axes_cm=[3.0, -1.0, 2.0]), "geometry[1].semi_axes_cm"),
 ])
 def test_scene_errors_name_the_entry(mutate, path):
     raw = W.room()
@@ -186,3 +187,30 @@ def test_tally_reduction_over_two_ranks():
         assert h0 == pytest.approx(30.0)
         assert nhit == 2 and nb == 6 and nh == 600 and n == 2000 and nfl == 14
         assert fa == pytest.approx((250 + 500) / 2000)
+
+
+def test_ellipsoid_extension_primitive():
+    """The axis-aligned ellipsoid (an extension for the denoiser phantoms):
+    the validator accepts it, the host packs full axis lengths, and the
+    oracle's roots lie on the surface and bracket the inside."""
+    from chatcarlo_b200.geometry import Geometry, contains
+    g = {"name": "e", "shape": "ellipsoid", "material": "water", "center": [1.0, -2.0, 3.0],
+         "semi_axes_cm": [4.0, 2.0, 7.0]}
+    raw = W.plain_mc()
+    raw["geometry"].append(g)
+    assert validate_scene(raw).ok
+    geo = Geometry(raw["geometry"])
+    prim = geo.primitives({"air": 0, "water": 1})[2]
+    assert prim.type == 3 and list(prim.size) == [8.0, 4.0, 14.0]
+    rng = np.random.default_rng(0)
+    o = rng.uniform(-12, 12, (2000, 3))
+    d = rng.normal(size=(2000, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    t1, t2 = O._ellipsoid(o, d, g["center"], g["semi_axes_cm"])
+    hit = ~np.isnan(t1)
+    assert hit.sum() > 100
+    for t in (t1, t2):
+        q = (o[hit] + t[hit, None] * d[hit] - np.array(g["center"])) / np.array(g["semi_axes_cm"])
+        np.testing.assert_allclose(np.sum(q * q, axis=1), 1.0, atol=1e-9)
+    mid = o[hit] + 0.5 * (t1[hit] + t2[hit])[:, None] * d[hit]
+    assert np.all(contains(g, mid)) and np.all(O._contains(g, mid))
