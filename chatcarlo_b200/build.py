@@ -1,8 +1,10 @@
-"""Compile the engine into chatcarlo_b200/lib/libccb200.so (sm_100a).
+"""Compile the engine into chatcarlo_b200/lib/libccb200.so and the learned
+denoiser's kernels into chatcarlo_b200/lib/libccunet.so (sm_100a).
 
-``python -m chatcarlo_b200.build`` rebuilds when a source is newer than the
-library.  The library links the CUDA runtime statically so it loads on any
-box with a driver, independent of the toolkit's library path.
+``python -m chatcarlo_b200.build`` rebuilds a library when one of its
+sources is newer than it.  The libraries link the CUDA runtime statically so
+they load on any box with a driver, independent of the toolkit's library
+path.
 """
 from __future__ import annotations
 
@@ -18,6 +20,9 @@ LIB_PATH = LIB_DIR / "libccb200.so"
 HEADER = PKG.parent / "include" / "chatcarlo_b200.h"
 SOURCES = [CSRC / "cc_engine.cu"]
 DEPS = SOURCES + [CSRC / "philox.cuh", HEADER]
+UNET_LIB_PATH = LIB_DIR / "libccunet.so"
+UNET_SOURCES = [CSRC / "cc_unet.cu"]
+UNET_DEPS = UNET_SOURCES + [PKG.parent / "include" / "chatcarlo_b200_unet.h"]
 
 # --use_fast_math: FP32 tracking tolerates approximate division, square root and
 # transcendentals (the surface band is 8 ulps of the world extent); tallies are
@@ -26,24 +31,31 @@ NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", 
               "--use_fast_math", "-Xcompiler", "-fPIC", "-shared", "-cudart", "static"]
 
 
+# the denoiser's kernels keep IEEE arithmetic (their gradients are checked
+# against an FP64 oracle)
+UNET_NVCC_FLAGS = [f for f in NVCC_FLAGS if f != "--use_fast_math"]
+
+
 def nvcc_path() -> str:
     cand = os.environ.get("NVCC") or "/usr/local/cuda/bin/nvcc"
     return cand if Path(cand).exists() else "nvcc"
 
 
-def needs_build() -> bool:
-    if not LIB_PATH.exists():
+def _stale(lib: Path, deps: list[Path]) -> bool:
+    if not lib.exists():
         return True
-    t = LIB_PATH.stat().st_mtime
-    return any(p.stat().st_mtime > t for p in DEPS if p.exists())
+    t = lib.stat().st_mtime
+    return any(p.stat().st_mtime > t for p in deps if p.exists())
 
 
-def build(force: bool = False, verbose: bool = False) -> Path:
-    if not force and not needs_build():
-        return LIB_PATH
+def needs_build() -> bool:
+    return _stale(LIB_PATH, DEPS) or _stale(UNET_LIB_PATH, UNET_DEPS)
+
+
+def _compile(lib: Path, sources: list[Path], flags: list[str], verbose: bool) -> None:
     LIB_DIR.mkdir(parents=True, exist_ok=True)
-    tmp = LIB_PATH.with_suffix(".so.tmp")
-    cmd = [nvcc_path(), *NVCC_FLAGS, "-o", str(tmp), *map(str, SOURCES)]
+    tmp = lib.with_suffix(".so.tmp")
+    cmd = [nvcc_path(), *flags, "-o", str(tmp), *map(str, sources)]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
         print(" ".join(cmd))
@@ -52,10 +64,19 @@ def build(force: bool = False, verbose: bool = False) -> Path:
         raise RuntimeError(f"nvcc failed ({res.returncode}):\n{res.stdout}\n{res.stderr}")
     if verbose:
         print(res.stderr)
-    os.replace(tmp, LIB_PATH)
+    os.replace(tmp, lib)
+
+
+def build(force: bool = False, verbose: bool = False) -> Path:
+    """Build both libraries where stale; returns the engine's path."""
+    if force or _stale(LIB_PATH, DEPS):
+        _compile(LIB_PATH, SOURCES, NVCC_FLAGS, verbose)
+    if force or _stale(UNET_LIB_PATH, UNET_DEPS):
+        _compile(UNET_LIB_PATH, UNET_SOURCES, UNET_NVCC_FLAGS, verbose)
     return LIB_PATH
 
 
 if __name__ == "__main__":
     build(force="--force" in sys.argv, verbose="-v" in sys.argv)
     print(LIB_PATH)
+    print(UNET_LIB_PATH)

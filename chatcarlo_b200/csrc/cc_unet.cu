@@ -1,0 +1,1032 @@
+// BF16 tensor-core kernels of the 3D U-Net kerma denoiser (sm_100a).
+//
+// Activations are channels-last BF16 tensors [B, D, H, W, C] with C a
+// multiple of 16.  Every 3x3x3 "same" convolution is an implicit GEMM on the
+// 5th-generation tensor cores:
+//
+//   D[v, co] = sum_{tap, ci} X[v + off(tap), ci] * W[tap, co, ci]
+//
+// M = 128 output voxels per CTA, N = output channels, K = 27 taps x input
+// channels.  All 256 threads of the CTA gather the A tile (neighbour voxel
+// rows, zero outside the volume) and the B tile (weights of one tap) into
+// shared memory in the K-major, no-swizzle canonical layout; one thread
+// issues tcgen05.mma (kind::f16, BF16 inputs, FP32 accumulator in tensor
+// memory) and commits to an mbarrier, so the gather of the next stage runs
+// while the tensor core works on the current one (two stages).  The
+// epilogue reads the accumulator back with tcgen05.ld and applies bias and
+// ReLU (forward) or the ReLU mask of the layer below (backward data).
+//
+// A convolution input may be the channel concatenation of a full-resolution
+// tensor a and a half-resolution tensor b read nearest-upsampled (the U-Net
+// decoder's skip + upsampled path), fused into the gather.
+//
+// The weight gradient is a second GEMM with M = 27 x C_in rows (tap, ci),
+// N = C_out and K = voxels, its operands MN-major in shared memory, split
+// over voxel ranges and reduced with FP32 atomics.
+//
+// Every mbarrier wait is bounded by the global timer; a wait that runs out
+// sets a status bit that the host reads, and the CTA still frees its tensor
+// memory before it returns.
+#include <cuda_runtime.h>
+#include <cuda_bf16.h>
+#include <stdint.h>
+#include <string.h>
+
+#include <string>
+
+#include "../../include/chatcarlo_b200_unet.h"
+
+namespace {
+
+constexpr int TILE_M = 128;
+constexpr int THREADS = 256;
+constexpr int KSTAGE = 64;                  // channels (conv) or voxels (weight grad) per stage
+constexpr unsigned long long WAIT_NS = 2000000000ull;   // 2 s bound on every mbarrier wait
+
+__device__ unsigned g_status;               // bit 0: an mbarrier wait ran out
+
+thread_local std::string t_err;
+
+int set_error(int code, const std::string& msg) {
+    t_err = msg;
+    return code;
+}
+
+#define CU_CHECK(call)                                                               \
+    do {                                                                            \
+        cudaError_t e_ = (call);                                                    \
+        if (e_ != cudaSuccess) return set_error(CCU_E_DEVICE, cudaGetErrorString(e_)); \
+    } while (0)
+
+// ---------------------------------------------------------------------------
+// PTX wrappers
+// ---------------------------------------------------------------------------
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_init_fence() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Wait for the completion of the phase with this parity, at most WAIT_NS.
+__device__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const unsigned long long t0 = global_ns();
+    while (true) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if (global_ns() - t0 > WAIT_NS) return false;
+    }
+}
+
+__device__ __forceinline__ void fence_proxy_async() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_before() {
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+
+// Tensor memory: a power of two >= 32 columns, allocated by one whole warp.
+__device__ __forceinline__ void tmem_alloc(uint32_t* dst, uint32_t ncols) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(dst)),
+                 "r"(ncols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols) : "memory");
+}
+
+// Shared-memory matrix descriptor, no swizzle: start, leading-dimension
+// byte offset (between core matrices adjacent in K), stride-dimension byte
+// offset (between core matrices adjacent in M/N), descriptor version 1.
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((addr & 0x3FFFFu) >> 4) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+// Instruction descriptor of kind::f16: FP32 accumulator, BF16 A and B,
+// A/B K-major (0) or MN-major (1), N >> 3, M >> 4.
+__host__ __device__ constexpr uint32_t idesc_bf16(int m, int n, int a_mn, int b_mn) {
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)a_mn << 15) | ((uint32_t)b_mn << 16) |
+           ((uint32_t)(n >> 3) << 17) | ((uint32_t)(m >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}"
+        ::"r"(d_tmem), "l"(a), "l"(b), "r"(idesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+
+__device__ __forceinline__ void mma_commit(uint64_t* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                     smem_u32(bar))
+                 : "memory");
+}
+
+// 32 lanes x 8 consecutive 32-bit columns; lane quarter in bits 31:16.
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, float f[8]) {
+    uint32_t r[8];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+                 : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int j = 0; j < 8; ++j) f[j] = __uint_as_float(r[j]);
+}
+
+__device__ __forceinline__ uint4 pack_bf16x8(const float f[8]) {
+    uint4 u;
+    __nv_bfloat162 h0 = __floats2bfloat162_rn(f[0], f[1]), h1 = __floats2bfloat162_rn(f[2], f[3]);
+    __nv_bfloat162 h2 = __floats2bfloat162_rn(f[4], f[5]), h3 = __floats2bfloat162_rn(f[6], f[7]);
+    memcpy(&u.x, &h0, 4);
+    memcpy(&u.y, &h1, 4);
+    memcpy(&u.z, &h2, 4);
+    memcpy(&u.w, &h3, 4);
+    return u;
+}
+
+__device__ __forceinline__ void unpack_bf16x8(uint4 u, float f[8]) {
+    __nv_bfloat162 h[4];
+    memcpy(&h[0], &u.x, 4);
+    memcpy(&h[1], &u.y, 4);
+    memcpy(&h[2], &u.z, 4);
+    memcpy(&h[3], &u.w, 4);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        float2 t = __bfloat1622float2(h[j]);
+        f[2 * j] = t.x;
+        f[2 * j + 1] = t.y;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// convolution input: a (full resolution) ++ b (half resolution, upsampled)
+// ---------------------------------------------------------------------------
+
+struct Src {
+    const __nv_bfloat16* a;
+    const __nv_bfloat16* b;
+    int ca, cb;
+    int B, D, H, W;
+};
+
+// 8 channels starting at ch (a multiple of 8) of input voxel (n, z, y, x);
+// zero outside the volume.
+__device__ __forceinline__ uint4 load_in8(const Src& s, int n, int z, int y, int x, int ch) {
+    if ((unsigned)z >= (unsigned)s.D || (unsigned)y >= (unsigned)s.H || (unsigned)x >= (unsigned)s.W)
+        return make_uint4(0u, 0u, 0u, 0u);
+    if (ch < s.ca) {
+        size_t v = (((size_t)n * s.D + z) * s.H + y) * s.W + x;
+        return __ldg(reinterpret_cast<const uint4*>(s.a + v * s.ca + ch));
+    }
+    const int D2 = s.D >> 1, H2 = s.H >> 1, W2 = s.W >> 1;
+    size_t v = (((size_t)n * D2 + (z >> 1)) * H2 + (y >> 1)) * W2 + (x >> 1);
+    return __ldg(reinterpret_cast<const uint4*>(s.b + v * s.cb + (ch - s.ca)));
+}
+
+__device__ __forceinline__ void voxel_coords(long long v, const Src& s, int& n, int& z, int& y, int& x) {
+    x = (int)(v % s.W);
+    long long t = v / s.W;
+    y = (int)(t % s.H);
+    t /= s.H;
+    z = (int)(t % s.D);
+    n = (int)(t / s.D);
+}
+
+// ---------------------------------------------------------------------------
+// forward / backward-data convolution
+// ---------------------------------------------------------------------------
+
+struct ConvP {
+    Src src;
+    int kc;                      // input channels per pipeline stage (divides ca + cb)
+    const __nv_bfloat16* w;      // [27][N][cin]
+    const float* bias;           // [N] or null
+    int relu;
+    long long n_vox;
+    // output channels [0, split) -> out0 [v][split], masked by mask0 (same
+    // layout) when given; channels [split, N) -> out1 [v][N - split]
+    __nv_bfloat16* out0;
+    const __nv_bfloat16* mask0;
+    int split;
+    __nv_bfloat16* out1;
+};
+
+__host__ __device__ constexpr uint32_t tmem_cols(int n) {
+    return n <= 32 ? 32u : (n <= 64 ? 64u : (n <= 128 ? 128u : 256u));
+}
+
+template <int N>
+__global__ void __launch_bounds__(THREADS) conv_kernel(const ConvP P) {
+    extern __shared__ __align__(128) uint8_t smem[];
+    __shared__ uint64_t bar[2];
+    __shared__ uint32_t s_tmem;
+    __shared__ int s_row[TILE_M][4];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int cin = P.src.ca + P.src.cb;
+    const int kc = P.kc;                             // 16, 32, 48 or 64
+    const int nkc = cin / kc;
+    const uint32_t a_bytes = TILE_M * kc * 2, b_bytes = N * kc * 2, stage_bytes = a_bytes + b_bytes;
+    const long long m0 = (long long)blockIdx.x * TILE_M;
+
+    if (tid < TILE_M) {
+        long long v = m0 + tid;
+        int n = -1, z = 0, y = 0, x = 0;
+        if (v < P.n_vox) voxel_coords(v, P.src, n, z, y, x);
+        s_row[tid][0] = n;
+        s_row[tid][1] = z;
+        s_row[tid][2] = y;
+        s_row[tid][3] = x;
+    }
+    if (warp == 0) tmem_alloc(&s_tmem, tmem_cols(N));
+    if (tid == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        mbar_init_fence();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = s_tmem;
+    constexpr uint32_t IDESC = idesc_bf16(TILE_M, N, 0, 0);
+
+    const int iters = 27 * nkc;
+    bool ok = true;
+    int issued = 0;                                  // stages whose MMAs were committed
+    for (int it = 0; it < iters && ok; ++it) {
+        const int st = it & 1;
+        if (it >= 2) ok = mbar_wait(&bar[st], ((it - 2) >> 1) & 1);
+        if (!__syncthreads_and(ok)) { ok = false; break; }
+        const int tap = it / nkc, kk = (it - tap * nkc) * kc;
+        const int dz = tap / 9 - 1, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
+        uint8_t* sA = smem + st * stage_bytes;
+        uint8_t* sB = sA + a_bytes;
+        // A: row m, channel chunk c8 at c8 * (TILE_M * 16) + (m / 8) * 128 + (m % 8) * 16
+        const int a_chunks = TILE_M * (kc >> 3);
+        for (int i = tid; i < a_chunks; i += THREADS) {
+            const int m = i & (TILE_M - 1), c8 = i >> 7;
+            uint4 val = make_uint4(0u, 0u, 0u, 0u);
+            const int n = s_row[m][0];
+            if (n >= 0) val = load_in8(P.src, n, s_row[m][1] + dz, s_row[m][2] + dy, s_row[m][3] + dx, kk + c8 * 8);
+            *reinterpret_cast<uint4*>(sA + c8 * (TILE_M * 16) + (m >> 3) * 128 + (m & 7) * 16) = val;
+        }
+        // B: output channel r, chunk c8 at c8 * (N * 16) + (r / 8) * 128 + (r % 8) * 16
+        const int b_chunks = N * (kc >> 3);
+        for (int i = tid; i < b_chunks; i += THREADS) {
+            const int r = i % N, c8 = i / N;
+            uint4 val = __ldg(reinterpret_cast<const uint4*>(P.w + ((size_t)tap * N + r) * cin + kk + c8 * 8));
+            *reinterpret_cast<uint4*>(sB + c8 * (N * 16) + (r >> 3) * 128 + (r & 7) * 16) = val;
+        }
+        fence_proxy_async();
+        __syncthreads();
+        if (tid == 0) {
+            tc_fence_after();
+            const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB);
+            for (int k = 0; k < (kc >> 4); ++k) {
+                uint64_t ad = smem_desc(a0 + k * 2 * (TILE_M * 16), TILE_M * 16, 128);
+                uint64_t bd = smem_desc(b0 + k * 2 * (N * 16), N * 16, 128);
+                mma_bf16(tmem, ad, bd, IDESC, (it > 0 || k > 0) ? 1u : 0u);
+            }
+            mma_commit(&bar[st]);
+        }
+        issued = it + 1;
+    }
+    // the last commit covers every earlier MMA of this thread; it is waited
+    // for on the error path too, before the tensor memory is freed
+    if (issued > 0 && !mbar_wait(&bar[(issued - 1) & 1], ((issued - 1) >> 1) & 1)) ok = false;
+    ok = __syncthreads_and(ok && issued == iters);
+    tc_fence_after();
+
+    if (ok) {
+        const int q = warp & 3, half = warp >> 2;
+        const int row = q * 32 + lane;
+        const long long v = m0 + row;
+        for (int c0 = half * 8; c0 < N; c0 += 16) {
+            float f[8];
+            tmem_ld8(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)c0, f);
+            if (v < P.n_vox) {
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    if (P.bias) f[j] += __ldg(P.bias + c0 + j);
+                    if (P.relu) f[j] = fmaxf(f[j], 0.0f);
+                }
+                if (c0 < P.split) {
+                    size_t o = (size_t)v * P.split + c0;
+                    if (P.mask0) {
+                        float mk[8];
+                        unpack_bf16x8(__ldg(reinterpret_cast<const uint4*>(P.mask0 + o)), mk);
+#pragma unroll
+                        for (int j = 0; j < 8; ++j) f[j] = mk[j] > 0.0f ? f[j] : 0.0f;
+                    }
+                    *reinterpret_cast<uint4*>(P.out0 + o) = pack_bf16x8(f);
+                } else {
+                    size_t o = (size_t)v * (N - P.split) + (c0 - P.split);
+                    *reinterpret_cast<uint4*>(P.out1 + o) = pack_bf16x8(f);
+                }
+            }
+        }
+    } else if (tid == 0) {
+        atomicOr(&g_status, 1u);
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) tmem_dealloc(tmem, tmem_cols(N));
+}
+
+// ---------------------------------------------------------------------------
+// weight gradient: dW[tap][co][ci] += sum_v dz[v][co] * X[v + off(tap)][ci]
+// ---------------------------------------------------------------------------
+
+struct WgradP {
+    Src src;
+    const __nv_bfloat16* dz;     // [n_vox][N]
+    long long n_vox;
+    long long vox_per_cta;       // multiple of KSTAGE
+    float* dw;                   // [27][N][cin], accumulated
+};
+
+template <int N>
+__global__ void __launch_bounds__(THREADS) wgrad_kernel(const WgradP P) {
+    extern __shared__ __align__(128) uint8_t smem[];
+    __shared__ uint64_t bar[2];
+    __shared__ uint32_t s_tmem;
+    __shared__ int s_vox[2][KSTAGE][4];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int cin = P.src.ca + P.src.cb;
+    const int rows = 27 * cin;
+    const int r0 = blockIdx.x * TILE_M;
+    const long long v_begin = (long long)blockIdx.y * P.vox_per_cta;
+    const long long v_end = v_begin + P.vox_per_cta < P.n_vox ? v_begin + P.vox_per_cta : P.n_vox;
+    constexpr uint32_t a_bytes = TILE_M * KSTAGE * 2, b_bytes = N * KSTAGE * 2, stage_bytes = a_bytes + b_bytes;
+
+    if (warp == 0) tmem_alloc(&s_tmem, tmem_cols(N));
+    if (tid == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        mbar_init_fence();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = s_tmem;
+    constexpr uint32_t IDESC = idesc_bf16(TILE_M, N, 1, 1);
+
+    const long long n_vox_cta = v_end > v_begin ? v_end - v_begin : 0;
+    const int iters = (int)((n_vox_cta + KSTAGE - 1) / KSTAGE);
+    bool ok = true;
+    int issued = 0;
+    for (int it = 0; it < iters && ok; ++it) {
+        const int st = it & 1;
+        const long long vk = v_begin + (long long)it * KSTAGE;
+        if (tid < KSTAGE) {
+            const long long v = vk + tid;
+            int n = -1, z = 0, y = 0, x = 0;
+            if (v < v_end) voxel_coords(v, P.src, n, z, y, x);
+            s_vox[st][tid][0] = n;
+            s_vox[st][tid][1] = z;
+            s_vox[st][tid][2] = y;
+            s_vox[st][tid][3] = x;
+        }
+        if (it >= 2) ok = mbar_wait(&bar[st], ((it - 2) >> 1) & 1);
+        if (!__syncthreads_and(ok)) { ok = false; break; }
+        uint8_t* sA = smem + st * stage_bytes;
+        uint8_t* sB = sA + a_bytes;
+        // A (MN-major): voxel k, row group g (8 rows = 8 input channels of one
+        // tap) at (k / 8) * (TILE_M * 16) + g * 128 + (k % 8) * 16
+        for (int i = tid; i < TILE_M / 8 * KSTAGE; i += THREADS) {
+            const int klo = i & 7, g = (i >> 3) & (TILE_M / 8 - 1), khi = i >> 7;
+            const int k = khi * 8 + klo;
+            const int r = r0 + g * 8;
+            const int n = s_vox[st][k][0];
+            uint4 val = make_uint4(0u, 0u, 0u, 0u);
+            if (r < rows && n >= 0) {
+                const int tap = r / cin, ci = r - tap * cin;
+                val = load_in8(P.src, n, s_vox[st][k][1] + tap / 9 - 1, s_vox[st][k][2] + (tap / 3) % 3 - 1,
+                               s_vox[st][k][3] + tap % 3 - 1, ci);
+            }
+            *reinterpret_cast<uint4*>(sA + khi * (TILE_M * 16) + g * 128 + klo * 16) = val;
+        }
+        // B (MN-major): voxel k, output-channel group g at (k / 8) * (N * 16) + g * 128 + (k % 8) * 16
+        for (int i = tid; i < N / 8 * KSTAGE; i += THREADS) {
+            const int klo = i & 7, g = (i >> 3) % (N / 8), khi = i / (N / 8 * 8);
+            const int k = khi * 8 + klo;
+            const long long v = vk + k;
+            uint4 val = make_uint4(0u, 0u, 0u, 0u);
+            if (v < v_end) val = __ldg(reinterpret_cast<const uint4*>(P.dz + (size_t)v * N + g * 8));
+            *reinterpret_cast<uint4*>(sB + khi * (N * 16) + g * 128 + klo * 16) = val;
+        }
+        fence_proxy_async();
+        __syncthreads();
+        if (tid == 0) {
+            tc_fence_after();
+            const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB);
+#pragma unroll
+            for (int k = 0; k < KSTAGE / 16; ++k) {
+                uint64_t ad = smem_desc(a0 + k * 2 * (TILE_M * 16), TILE_M * 16, 128);
+                uint64_t bd = smem_desc(b0 + k * 2 * (N * 16), N * 16, 128);
+                mma_bf16(tmem, ad, bd, IDESC, (it > 0 || k > 0) ? 1u : 0u);
+            }
+            mma_commit(&bar[st]);
+        }
+        issued = it + 1;
+    }
+    if (issued > 0 && !mbar_wait(&bar[(issued - 1) & 1], ((issued - 1) >> 1) & 1)) ok = false;
+    ok = __syncthreads_and(ok && issued == iters);
+    tc_fence_after();
+
+    if (ok && iters > 0) {
+        const int q = warp & 3, half = warp >> 2;
+        const int r = r0 + q * 32 + lane;
+        const int tap = r / cin, ci = r - tap * cin;
+        for (int c0 = half * 8; c0 < N; c0 += 16) {
+            float f[8];
+            tmem_ld8(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)c0, f);
+            if (r < rows) {
+#pragma unroll
+                for (int j = 0; j < 8; ++j) atomicAdd(P.dw + ((size_t)tap * N + c0 + j) * cin + ci, f[j]);
+            }
+        }
+    } else if (!ok && tid == 0) {
+        atomicOr(&g_status, 1u);
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) tmem_dealloc(tmem, tmem_cols(N));
+}
+
+// ---------------------------------------------------------------------------
+// memory-bound helpers (CUDA cores)
+// ---------------------------------------------------------------------------
+
+// db[c] += sum_v dz[v][c]
+__global__ void bias_grad_kernel(const __nv_bfloat16* __restrict__ dz, long long n_vox, int c,
+                                 float* __restrict__ db) {
+    extern __shared__ float s_acc[];
+    for (int i = threadIdx.x; i < c; i += blockDim.x) s_acc[i] = 0.0f;
+    __syncthreads();
+    const long long total = n_vox * c;
+    float acc = 0.0f;
+    int cur = -1;
+    // blockDim.x is a multiple of c, so every thread sums a single channel
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += stride) {
+        cur = (int)(i % c);
+        acc += __bfloat162float(dz[i]);
+    }
+    if (cur >= 0) atomicAdd(&s_acc[cur], acc);
+    __syncthreads();
+    for (int i = threadIdx.x; i < c; i += blockDim.x) atomicAdd(db + i, s_acc[i]);
+}
+
+// y[n, z, y, x, c] = mean of the 2x2x2 children (D, H, W of x even)
+__global__ void avgpool_kernel(const __nv_bfloat16* __restrict__ x, int B, int D, int H, int W, int c,
+                               __nv_bfloat16* __restrict__ y) {
+    const int D2 = D >> 1, H2 = H >> 1, W2 = W >> 1;
+    const long long total = (long long)B * D2 * H2 * W2 * (c >> 3);
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int c8 = (int)(i % (c >> 3));
+        long long v = i / (c >> 3);
+        const int xx = (int)(v % W2);
+        long long t = v / W2;
+        const int yy = (int)(t % H2);
+        t /= H2;
+        const int zz = (int)(t % D2);
+        const int n = (int)(t / D2);
+        float s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        for (int k = 0; k < 8; ++k) {
+            size_t src = ((((size_t)n * D + 2 * zz + (k >> 2)) * H + 2 * yy + ((k >> 1) & 1)) * W + 2 * xx + (k & 1)) * c +
+                         c8 * 8;
+            float f[8];
+            unpack_bf16x8(__ldg(reinterpret_cast<const uint4*>(x + src)), f);
+#pragma unroll
+            for (int j = 0; j < 8; ++j) s[j] += f[j];
+        }
+#pragma unroll
+        for (int j = 0; j < 8; ++j) s[j] *= 0.125f;
+        *reinterpret_cast<uint4*>(y + (size_t)v * c + c8 * 8) = pack_bf16x8(s);
+    }
+}
+
+// dz_x[v][c] += (x_act[v][c] > 0) * gy[parent(v)][c] / 8   (x at full resolution)
+__global__ void pool_backward_kernel(const __nv_bfloat16* __restrict__ gy, const __nv_bfloat16* __restrict__ x_act,
+                                     int B, int D, int H, int W, int c, __nv_bfloat16* __restrict__ dz_x) {
+    const long long total = (long long)B * D * H * W * (c >> 3);
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int c8 = (int)(i % (c >> 3));
+        long long v = i / (c >> 3);
+        const int xx = (int)(v % W);
+        long long t = v / W;
+        const int yy = (int)(t % H);
+        t /= H;
+        const int zz = (int)(t % D);
+        const int n = (int)(t / D);
+        size_t p = ((((size_t)n * (D >> 1) + (zz >> 1)) * (H >> 1) + (yy >> 1)) * (W >> 1) + (xx >> 1)) * c + c8 * 8;
+        size_t o = (size_t)v * c + c8 * 8;
+        float g[8], a[8], d[8];
+        unpack_bf16x8(__ldg(reinterpret_cast<const uint4*>(gy + p)), g);
+        unpack_bf16x8(__ldg(reinterpret_cast<const uint4*>(x_act + o)), a);
+        unpack_bf16x8(*reinterpret_cast<const uint4*>(dz_x + o), d);
+#pragma unroll
+        for (int j = 0; j < 8; ++j) d[j] += a[j] > 0.0f ? 0.125f * g[j] : 0.0f;
+        *reinterpret_cast<uint4*>(dz_x + o) = pack_bf16x8(d);
+    }
+}
+
+// dz_c[vc][c] = (coarse_act[vc][c] > 0) * sum over the 8 children of g_full
+// (g_full at full resolution D, H, W)
+__global__ void up_reduce_kernel(const __nv_bfloat16* __restrict__ g_full, const __nv_bfloat16* __restrict__ coarse,
+                                 int B, int D, int H, int W, int c, __nv_bfloat16* __restrict__ dz_c) {
+    const int D2 = D >> 1, H2 = H >> 1, W2 = W >> 1;
+    const long long total = (long long)B * D2 * H2 * W2 * (c >> 3);
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int c8 = (int)(i % (c >> 3));
+        long long v = i / (c >> 3);
+        const int xx = (int)(v % W2);
+        long long t = v / W2;
+        const int yy = (int)(t % H2);
+        t /= H2;
+        const int zz = (int)(t % D2);
+        const int n = (int)(t / D2);
+        float s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        for (int k = 0; k < 8; ++k) {
+            size_t src = ((((size_t)n * D + 2 * zz + (k >> 2)) * H + 2 * yy + ((k >> 1) & 1)) * W + 2 * xx + (k & 1)) * c +
+                         c8 * 8;
+            float f[8];
+            unpack_bf16x8(__ldg(reinterpret_cast<const uint4*>(g_full + src)), f);
+#pragma unroll
+            for (int j = 0; j < 8; ++j) s[j] += f[j];
+        }
+        float a[8];
+        size_t o = (size_t)v * c + c8 * 8;
+        unpack_bf16x8(__ldg(reinterpret_cast<const uint4*>(coarse + o)), a);
+#pragma unroll
+        for (int j = 0; j < 8; ++j) s[j] = a[j] > 0.0f ? s[j] : 0.0f;
+        *reinterpret_cast<uint4*>(dz_c + o) = pack_bf16x8(s);
+    }
+}
+
+// Head (1x1x1 conv, 16 -> 1, residual on the input log-kerma) with the
+// weighted squared-error loss and, when dz is given, its backward:
+//   out = xlog + hw . d0 + hb
+//   loss = sum_v wgt (out - tgt)^2 * inv_wsum
+//   dz_d0 = (d0 > 0) * dout * hw,  dout = 2 wgt (out - tgt) inv_wsum
+// acc[0..15] += dL/dhw, acc[16] += dL/dhb, acc[17] += loss.
+__global__ void head_kernel(const __nv_bfloat16* __restrict__ d0, const float* __restrict__ xlog,
+                            const float* __restrict__ tgt, const float* __restrict__ wgt, const float* __restrict__ hw,
+                            float hb, float inv_wsum, long long n_vox, float* __restrict__ out,
+                            __nv_bfloat16* __restrict__ dz, float* __restrict__ acc) {
+    __shared__ float s_acc[18];
+    if (threadIdx.x < 18) s_acc[threadIdx.x] = 0.0f;
+    __syncthreads();
+    float w[16];
+#pragma unroll
+    for (int j = 0; j < 16; ++j) w[j] = __ldg(hw + j);
+    float g[18];
+#pragma unroll
+    for (int j = 0; j < 18; ++j) g[j] = 0.0f;
+    for (long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x; v < n_vox;
+         v += (long long)gridDim.x * blockDim.x) {
+        float a[16];
+        unpack_bf16x8(__ldg(reinterpret_cast<const uint4*>(d0 + (size_t)v * 16)), a);
+        unpack_bf16x8(__ldg(reinterpret_cast<const uint4*>(d0 + (size_t)v * 16 + 8)), a + 8);
+        float o = xlog[v] + hb;
+#pragma unroll
+        for (int j = 0; j < 16; ++j) o += w[j] * a[j];
+        if (out) out[v] = o;
+        if (tgt) {
+            const float wv = wgt ? wgt[v] : 1.0f;
+            const float e = o - tgt[v];
+            g[17] += wv * e * e * inv_wsum;
+            const float dout = 2.0f * wv * e * inv_wsum;
+            if (dz) {
+                float d[16];
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                    d[j] = a[j] > 0.0f ? dout * w[j] : 0.0f;
+                    g[j] += dout * a[j];
+                }
+                *reinterpret_cast<uint4*>(dz + (size_t)v * 16) = pack_bf16x8(d);
+                *reinterpret_cast<uint4*>(dz + (size_t)v * 16 + 8) = pack_bf16x8(d + 8);
+                g[16] += dout;
+            }
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < 18; ++j) {
+        float t = g[j];
+        for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+        if ((threadIdx.x & 31) == 0 && t != 0.0f) atomicAdd(&s_acc[j], t);
+    }
+    __syncthreads();
+    if (threadIdx.x < 18 && s_acc[threadIdx.x] != 0.0f) atomicAdd(acc + threadIdx.x, s_acc[threadIdx.x]);
+}
+
+// Network input: 16 channels per voxel -- normalised log kerma, density,
+// material one-hot (n_mat <= 8), zero padding.
+__global__ void input_kernel(const float* __restrict__ xlog, const float* __restrict__ density,
+                             const uint8_t* __restrict__ mat, int n_mat, long long n_vox, __nv_bfloat16* __restrict__ x) {
+    for (long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x; v < n_vox;
+         v += (long long)gridDim.x * blockDim.x) {
+        float f[16];
+#pragma unroll
+        for (int j = 0; j < 16; ++j) f[j] = 0.0f;
+        f[0] = xlog[v];
+        f[1] = density[v];
+        const int m = mat[v];
+        if (m < n_mat && m < 14) f[2 + m] = 1.0f;
+        *reinterpret_cast<uint4*>(x + (size_t)v * 16) = pack_bf16x8(f);
+        *reinterpret_cast<uint4*>(x + (size_t)v * 16 + 8) = pack_bf16x8(f + 8);
+    }
+}
+
+// Adam with decoupled weight decay on a flat FP32 parameter vector.
+__global__ void adam_kernel(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m,
+                            float* __restrict__ v, long long n, float lr, float b1, float b2, float eps, float c1,
+                            float c2, float wd) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const float gi = g[i];
+        const float mi = b1 * m[i] + (1.0f - b1) * gi;
+        const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+        m[i] = mi;
+        v[i] = vi;
+        p[i] -= lr * ((mi * c1) / (sqrtf(vi * c2) + eps) + wd * p[i]);
+    }
+}
+
+// BF16 weights of one layer from its FP32 master copy: w[tap][co][ci] for
+// the forward pass and wt[26 - tap][ci][co] (flipped, transposed) for the
+// backward-data pass.
+__global__ void pack_weights_kernel(const float* __restrict__ w32, int cout, int cin, __nv_bfloat16* __restrict__ w,
+                                    __nv_bfloat16* __restrict__ wt) {
+    const long long total = 27LL * cout * cin;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int ci = (int)(i % cin);
+        long long t = i / cin;
+        const int co = (int)(t % cout);
+        const int tap = (int)(t / cout);
+        const __nv_bfloat16 h = __float2bfloat16_rn(w32[i]);
+        w[i] = h;
+        if (wt) wt[((size_t)(26 - tap) * cin + ci) * cout + co] = h;
+    }
+}
+
+// Plain tensor-core GEMM D[M][N] = A[M][K] . B[N][K]^T for the unit tests of
+// the descriptors (A, B K-major BF16; D FP32; M a multiple of 128, N of 16
+// up to 256, K of 64).
+__global__ void __launch_bounds__(THREADS) gemm_test_kernel(const __nv_bfloat16* A, const __nv_bfloat16* Bm,
+                                                            float* Dm, int M, int N, int K, int a_mn, int b_mn) {
+    extern __shared__ __align__(128) uint8_t smem[];
+    __shared__ uint64_t bar;
+    __shared__ uint32_t s_tmem;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int m0 = blockIdx.x * TILE_M;
+    if (warp == 0) tmem_alloc(&s_tmem, 256);
+    if (tid == 0) {
+        mbar_init(&bar, 1);
+        mbar_init_fence();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = s_tmem;
+    uint8_t* sA = smem;
+    uint8_t* sB = smem + TILE_M * 64 * 2;
+    bool ok = true;
+    const uint32_t idesc = idesc_bf16(TILE_M, N, a_mn, b_mn);
+    for (int k0 = 0; k0 < K && ok; k0 += 64) {
+        // K-major: row r, chunk c8 at c8 * (rows * 16) + (r / 8) * 128 + (r % 8) * 16
+        // MN-major: k, group g at (k / 8) * (rows * 16) + g * 128 + (k % 8) * 16 (A given as [K][M])
+        for (int i = tid; i < TILE_M * 8; i += THREADS) {
+            if (!a_mn) {
+                const int r = i & (TILE_M - 1), c8 = i >> 7;
+                *reinterpret_cast<uint4*>(sA + c8 * (TILE_M * 16) + (r >> 3) * 128 + (r & 7) * 16) =
+                    *reinterpret_cast<const uint4*>(A + (size_t)(m0 + r) * K + k0 + c8 * 8);
+            } else {
+                const int klo = i & 7, g = (i >> 3) & 15, khi = i >> 7;
+                *reinterpret_cast<uint4*>(sA + khi * (TILE_M * 16) + g * 128 + klo * 16) =
+                    *reinterpret_cast<const uint4*>(A + (size_t)(k0 + khi * 8 + klo) * M + m0 + g * 8);
+            }
+        }
+        for (int i = tid; i < N * 8; i += THREADS) {
+            if (!b_mn) {
+                const int r = i % N, c8 = i / N;
+                *reinterpret_cast<uint4*>(sB + c8 * (N * 16) + (r >> 3) * 128 + (r & 7) * 16) =
+                    *reinterpret_cast<const uint4*>(Bm + (size_t)r * K + k0 + c8 * 8);
+            } else {
+                const int klo = i & 7, g = (i >> 3) % (N / 8), khi = i / N;
+                *reinterpret_cast<uint4*>(sB + khi * (N * 16) + g * 128 + klo * 16) =
+                    *reinterpret_cast<const uint4*>(Bm + (size_t)(k0 + khi * 8 + klo) * N + g * 8);
+            }
+        }
+        fence_proxy_async();
+        __syncthreads();
+        if (tid == 0) {
+            tc_fence_after();
+            for (int k = 0; k < 4; ++k) {
+                uint64_t ad = smem_desc(smem_u32(sA) + k * 2 * (TILE_M * 16), TILE_M * 16, 128);
+                uint64_t bd = smem_desc(smem_u32(sB) + k * 2 * (N * 16), N * 16, 128);
+                mma_bf16(tmem, ad, bd, idesc, (k0 > 0 || k > 0) ? 1u : 0u);
+            }
+            mma_commit(&bar);
+        }
+        ok = mbar_wait(&bar, (k0 / 64) & 1);
+        ok = __syncthreads_and(ok);
+        tc_fence_after();
+    }
+    if (ok) {
+        const int q = warp & 3, half = warp >> 2;
+        for (int c0 = half * 8; c0 < N; c0 += 16) {
+            float f[8];
+            tmem_ld8(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)c0, f);
+            for (int j = 0; j < 8; ++j) Dm[(size_t)(m0 + q * 32 + lane) * N + c0 + j] = f[j];
+        }
+    } else if (tid == 0) {
+        atomicOr(&g_status, 1u);
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) tmem_dealloc(tmem, 256);
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+
+int g_sm_count = 0;
+
+int sm_count() {
+    if (g_sm_count == 0) {
+        int dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess) return 148;
+        cudaDeviceGetAttribute(&g_sm_count, cudaDevAttrMultiProcessorCount, dev);
+        if (g_sm_count <= 0) g_sm_count = 148;
+    }
+    return g_sm_count;
+}
+
+int grid_for(long long work, int threads) {
+    long long b = (work + threads - 1) / threads;
+    long long cap = (long long)sm_count() * 16;
+    if (b > cap) b = cap;
+    return (int)(b < 1 ? 1 : b);
+}
+
+bool aligned16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
+
+// Shared memory per CTA: the two stages, raised where needed so that the
+// CTAs resident on one SM never ask for more than its 512 tensor-memory
+// columns together (an allocation beyond that would wait for another CTA).
+template <typename K>
+int tc_launch_smem(K kernel, uint32_t stage_bytes, uint32_t cols, size_t& smem) {
+    smem = 2 * (size_t)stage_bytes;
+    const int max_ctas = (int)(512u / cols);
+    int dev = 0;
+    CU_CHECK(cudaGetDevice(&dev));
+    int per_sm = 0;
+    CU_CHECK(cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
+    const size_t floor_smem = (size_t)per_sm / (size_t)(max_ctas + 1) + 1024;
+    if (smem < floor_smem) smem = floor_smem;
+    if (smem > 200 * 1024) return set_error(CCU_E_INVALID, "stage too large for shared memory");
+    CU_CHECK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int occ = 0;
+    CU_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, THREADS, smem));
+    if (occ * (int)cols > 512) return set_error(CCU_E_INVALID, "tensor-memory budget per SM exceeded");
+    if (occ < 1) return set_error(CCU_E_INVALID, "kernel does not fit on an SM");
+    return CCU_OK;
+}
+
+int stage_channels(int cin) {
+    for (int k = KSTAGE; k >= 16; k -= 16)
+        if (cin % k == 0) return k;
+    return 16;
+}
+
+template <int N>
+int launch_conv(const ConvP& P, cudaStream_t st) {
+    const int kc = P.kc;
+    size_t smem = 0;
+    int rc = tc_launch_smem(conv_kernel<N>, (uint32_t)(TILE_M + N) * kc * 2, tmem_cols(N), smem);
+    if (rc != CCU_OK) return rc;
+    const long long blocks = (P.n_vox + TILE_M - 1) / TILE_M;
+    conv_kernel<N><<<(unsigned)blocks, THREADS, smem, st>>>(P);
+    CU_CHECK(cudaGetLastError());
+    return CCU_OK;
+}
+
+template <int N>
+int launch_wgrad(const WgradP& P, int slices, int cin, cudaStream_t st) {
+    size_t smem = 0;
+    int rc = tc_launch_smem(wgrad_kernel<N>, (uint32_t)(TILE_M + N) * KSTAGE * 2, tmem_cols(N), smem);
+    if (rc != CCU_OK) return rc;
+    dim3 grid((unsigned)((27 * cin + TILE_M - 1) / TILE_M), (unsigned)slices);
+    wgrad_kernel<N><<<grid, THREADS, smem, st>>>(P);
+    CU_CHECK(cudaGetLastError());
+    return CCU_OK;
+}
+
+int check_src(const void* a, int ca, const void* b, int cb, int batch, int d, int h, int w) {
+    if (!a || ca <= 0 || ca % 16 || cb < 0 || cb % 16 || (cb > 0 && !b))
+        return set_error(CCU_E_INVALID, "channels must be positive multiples of 16 (the second input optional)");
+    if (!aligned16(a) || (b && !aligned16(b))) return set_error(CCU_E_INVALID, "tensors must be 16-byte aligned");
+    if (batch <= 0 || d <= 0 || h <= 0 || w <= 0) return set_error(CCU_E_INVALID, "empty volume");
+    if (cb > 0 && (d % 2 || h % 2 || w % 2)) return set_error(CCU_E_INVALID, "upsampled input needs even dimensions");
+    return CCU_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ccu_version(void) { return CCU_VERSION; }
+
+const char* ccu_last_error(void) { return t_err.c_str(); }
+
+int ccu_status(unsigned* status, int reset) {
+    if (!status) return set_error(CCU_E_INVALID, "NULL argument");
+    CU_CHECK(cudaMemcpyFromSymbol(status, g_status, sizeof(unsigned)));
+    if (reset) {
+        unsigned z = 0;
+        CU_CHECK(cudaMemcpyToSymbol(g_status, &z, sizeof(unsigned)));
+    }
+    return CCU_OK;
+}
+
+int ccu_conv3d(const void* a, int ca, const void* b, int cb, int batch, int d, int h, int w, const void* weight,
+               const float* bias, int cout, int relu, void* out0, int split, const void* mask0, void* out1,
+               void* stream) {
+    int rc = check_src(a, ca, b, cb, batch, d, h, w);
+    if (rc != CCU_OK) return rc;
+    if (!weight || !out0 || split <= 0 || split > cout || split % 8 || (split < cout && !out1))
+        return set_error(CCU_E_INVALID, "bad output description");
+    if (!aligned16(weight) || !aligned16(out0) || (out1 && !aligned16(out1)) || (mask0 && !aligned16(mask0)))
+        return set_error(CCU_E_INVALID, "tensors must be 16-byte aligned");
+    ConvP P;
+    P.src = Src{(const __nv_bfloat16*)a, (const __nv_bfloat16*)b, ca, cb, batch, d, h, w};
+    P.kc = stage_channels(ca + cb);
+    P.w = (const __nv_bfloat16*)weight;
+    P.bias = bias;
+    P.relu = relu;
+    P.n_vox = (long long)batch * d * h * w;
+    P.out0 = (__nv_bfloat16*)out0;
+    P.mask0 = (const __nv_bfloat16*)mask0;
+    P.split = split;
+    P.out1 = (__nv_bfloat16*)out1;
+    cudaStream_t st = (cudaStream_t)stream;
+    switch (cout) {
+        case 16: return launch_conv<16>(P, st);
+        case 32: return launch_conv<32>(P, st);
+        case 48: return launch_conv<48>(P, st);
+        case 64: return launch_conv<64>(P, st);
+        case 96: return launch_conv<96>(P, st);
+        case 128: return launch_conv<128>(P, st);
+        case 192: return launch_conv<192>(P, st);
+        default: return set_error(CCU_E_INVALID, "output channels must be one of 16, 32, 48, 64, 96, 128, 192");
+    }
+}
+
+int ccu_conv3d_wgrad(const void* a, int ca, const void* b, int cb, int batch, int d, int h, int w, const void* dz,
+                     int cout, float* dw, int slices, void* stream) {
+    int rc = check_src(a, ca, b, cb, batch, d, h, w);
+    if (rc != CCU_OK) return rc;
+    if (!dz || !dw || !aligned16(dz) || slices <= 0) return set_error(CCU_E_INVALID, "bad gradient arguments");
+    WgradP P;
+    P.src = Src{(const __nv_bfloat16*)a, (const __nv_bfloat16*)b, ca, cb, batch, d, h, w};
+    P.dz = (const __nv_bfloat16*)dz;
+    P.n_vox = (long long)batch * d * h * w;
+    long long per = (P.n_vox + slices - 1) / slices;
+    per = (per + KSTAGE - 1) / KSTAGE * KSTAGE;
+    P.vox_per_cta = per;
+    slices = (int)((P.n_vox + per - 1) / per);
+    P.dw = dw;
+    cudaStream_t st = (cudaStream_t)stream;
+    const int cin = ca + cb;
+    switch (cout) {
+        case 16: return launch_wgrad<16>(P, slices, cin, st);
+        case 32: return launch_wgrad<32>(P, slices, cin, st);
+        case 64: return launch_wgrad<64>(P, slices, cin, st);
+        case 128: return launch_wgrad<128>(P, slices, cin, st);
+        default: return set_error(CCU_E_INVALID, "output channels must be one of 16, 32, 64, 128");
+    }
+}
+
+int ccu_bias_grad(const void* dz, long long n_vox, int c, float* db, void* stream) {
+    if (!dz || !db || c <= 0 || 256 % c) return set_error(CCU_E_INVALID, "bias gradient needs c dividing 256");
+    bias_grad_kernel<<<grid_for(n_vox * c, 256), 256, c * sizeof(float), (cudaStream_t)stream>>>(
+        (const __nv_bfloat16*)dz, n_vox, c, db);
+    CU_CHECK(cudaGetLastError());
+    return CCU_OK;
+}
+
+int ccu_avgpool(const void* x, int batch, int d, int h, int w, int c, void* y, void* stream) {
+    if (!x || !y || c % 8 || d % 2 || h % 2 || w % 2) return set_error(CCU_E_INVALID, "bad pooling arguments");
+    long long work = (long long)batch * (d / 2) * (h / 2) * (w / 2) * (c / 8);
+    avgpool_kernel<<<grid_for(work, 256), 256, 0, (cudaStream_t)stream>>>((const __nv_bfloat16*)x, batch, d, h, w, c,
+                                                                          (__nv_bfloat16*)y);
+    CU_CHECK(cudaGetLastError());
+    return CCU_OK;
+}
+
+int ccu_pool_backward(const void* gy, const void* x_act, int batch, int d, int h, int w, int c, void* dz_x,
+                      void* stream) {
+    if (!gy || !x_act || !dz_x || c % 8 || d % 2 || h % 2 || w % 2)
+        return set_error(CCU_E_INVALID, "bad pooling arguments");
+    long long work = (long long)batch * d * h * w * (c / 8);
+    pool_backward_kernel<<<grid_for(work, 256), 256, 0, (cudaStream_t)stream>>>(
+        (const __nv_bfloat16*)gy, (const __nv_bfloat16*)x_act, batch, d, h, w, c, (__nv_bfloat16*)dz_x);
+    CU_CHECK(cudaGetLastError());
+    return CCU_OK;
+}
+
+int ccu_up_reduce(const void* g_full, const void* coarse_act, int batch, int d, int h, int w, int c, void* dz_coarse,
+                  void* stream) {
+    if (!g_full || !coarse_act || !dz_coarse || c % 8 || d % 2 || h % 2 || w % 2)
+        return set_error(CCU_E_INVALID, "bad upsampling arguments");
+    long long work = (long long)batch * (d / 2) * (h / 2) * (w / 2) * (c / 8);
+    up_reduce_kernel<<<grid_for(work, 256), 256, 0, (cudaStream_t)stream>>>(
+        (const __nv_bfloat16*)g_full, (const __nv_bfloat16*)coarse_act, batch, d, h, w, c, (__nv_bfloat16*)dz_coarse);
+    CU_CHECK(cudaGetLastError());
+    return CCU_OK;
+}
+
+int ccu_head(const void* d0, const float* xlog, const float* target, const float* weight, const float* hw, float hb,
+             float inv_wsum, long long n_vox, float* out, void* dz, float* acc, void* stream) {
+    if (!d0 || !xlog || !hw || !acc || (dz && !target)) return set_error(CCU_E_INVALID, "bad head arguments");
+    head_kernel<<<grid_for(n_vox, 256), 256, 0, (cudaStream_t)stream>>>(
+        (const __nv_bfloat16*)d0, xlog, target, weight, hw, hb, inv_wsum, n_vox, out, (__nv_bfloat16*)dz, acc);
+    CU_CHECK(cudaGetLastError());
+    return CCU_OK;
+}
+
+int ccu_input(const float* xlog, const float* density, const uint8_t* mat, int n_mat, long long n_vox, void* x,
+              void* stream) {
+    if (!xlog || !density || !mat || !x || n_mat > 14) return set_error(CCU_E_INVALID, "bad input arguments");
+    input_kernel<<<grid_for(n_vox, 256), 256, 0, (cudaStream_t)stream>>>(xlog, density, mat, n_mat, n_vox,
+                                                                         (__nv_bfloat16*)x);
+    CU_CHECK(cudaGetLastError());
+    return CCU_OK;
+}
+
+int ccu_adam(float* p, const float* g, float* m, float* v, long long n, float lr, float b1, float b2, float eps,
+             int step, float wd, void* stream) {
+    if (!p || !g || !m || !v || step < 1) return set_error(CCU_E_INVALID, "bad optimizer arguments");
+    const float c1 = 1.0f / (1.0f - powf(b1, (float)step)), c2 = 1.0f / (1.0f - powf(b2, (float)step));
+    adam_kernel<<<grid_for(n, 256), 256, 0, (cudaStream_t)stream>>>(p, g, m, v, n, lr, b1, b2, eps, c1, c2, wd);
+    CU_CHECK(cudaGetLastError());
+    return CCU_OK;
+}
+
+int ccu_pack_weights(const float* w32, int cout, int cin, void* w, void* wt, void* stream) {
+    if (!w32 || !w || cout <= 0 || cin <= 0) return set_error(CCU_E_INVALID, "bad weight arguments");
+    pack_weights_kernel<<<grid_for(27LL * cout * cin, 256), 256, 0, (cudaStream_t)stream>>>(
+        w32, cout, cin, (__nv_bfloat16*)w, (__nv_bfloat16*)wt);
+    CU_CHECK(cudaGetLastError());
+    return CCU_OK;
+}
+
+int ccu_gemm_test(const void* a, const void* b, float* d, int m, int n, int k, int a_mn, int b_mn, void* stream) {
+    if (!a || !b || !d || m <= 0 || m % TILE_M || n < 16 || n > 256 || n % 16 || k <= 0 || k % 64)
+        return set_error(CCU_E_INVALID, "gemm test sizes: m % 128, 16 <= n <= 256 with n % 16, k % 64");
+    const size_t smem = (size_t)(TILE_M + n) * 64 * 2;
+    // one CTA per SM at most: 256 tensor-memory columns each
+    const size_t floor_smem = 120 * 1024;
+    const size_t use = smem < floor_smem ? floor_smem : smem;
+    CU_CHECK(cudaFuncSetAttribute(gemm_test_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)use));
+    gemm_test_kernel<<<m / TILE_M, THREADS, use, (cudaStream_t)stream>>>((const __nv_bfloat16*)a,
+                                                                         (const __nv_bfloat16*)b, d, m, n, k, a_mn, b_mn);
+    CU_CHECK(cudaGetLastError());
+    return CCU_OK;
+}
+
+}  // extern "C"

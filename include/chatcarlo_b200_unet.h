@@ -1,0 +1,102 @@
+/* C ABI of the learned kerma denoiser's kernels (libccunet.so).
+ *
+ * The reference has no learned part; these entry points implement the 3D
+ * U-Net denoiser that the engine's own Monte Carlo trains and that plain
+ * Monte Carlo judges.  Tensors are device pointers (16-byte aligned),
+ * channels-last BF16 [B, D, H, W, C] activations with C a multiple of 16,
+ * FP32 master weights and gradients.  Every call is asynchronous on the
+ * given CUDA stream (NULL = legacy default stream) and returns 0 or a
+ * negative CCU_E_* code with a message in ccu_last_error().
+ */
+#ifndef CHATCARLO_B200_UNET_H
+#define CHATCARLO_B200_UNET_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define CCU_VERSION 1
+
+#define CCU_OK          0
+#define CCU_E_INVALID (-1)   /* bad sizes, pointers or alignment */
+#define CCU_E_DEVICE  (-6)   /* CUDA runtime failure */
+
+int ccu_version(void);
+const char* ccu_last_error(void);
+
+/* Status bits set by the kernels (bit 0: a bounded tensor-core wait ran
+ * out); reset clears them. */
+int ccu_status(unsigned* status, int reset);
+
+/* 3x3x3 "same" convolution on the tensor cores (tcgen05, BF16 in, FP32
+ * accumulation).  The input is a [B, d, h, w, ca] concatenated on channels
+ * with b [B, d/2, h/2, w/2, cb] read nearest-upsampled (b NULL, cb 0 for a
+ * plain input).  weight [27][cout][ca + cb] BF16 (tap = (dz+1)*9 + (dy+1)*3
+ * + dx+1), bias [cout] FP32 or NULL, relu 0/1.  Output channels [0, split)
+ * go to out0 [.., split], multiplied by (mask0 > 0) when mask0 (same layout
+ * as out0) is given; channels [split, cout) go to out1 [.., cout - split].
+ * cout is one of 16, 32, 48, 64, 96, 128, 192. */
+int ccu_conv3d(const void* a, int ca, const void* b, int cb, int batch, int d, int h, int w, const void* weight,
+               const float* bias, int cout, int relu, void* out0, int split, const void* mask0, void* out1,
+               void* stream);
+
+/* Weight gradient of ccu_conv3d: dw[27][cout][ca + cb] (FP32) +=
+ * sum over voxels of dz[v][co] * input[v + tap][ci].  The voxels are split
+ * into `slices` ranges reduced with atomics.  cout in {16, 32, 64, 128}. */
+int ccu_conv3d_wgrad(const void* a, int ca, const void* b, int cb, int batch, int d, int h, int w, const void* dz,
+                     int cout, float* dw, int slices, void* stream);
+
+/* db[c] += sum over voxels of dz[v][c]; c divides 256. */
+int ccu_bias_grad(const void* dz, long long n_vox, int c, float* db, void* stream);
+
+/* 2x2x2 average pooling, [B, d, h, w, c] -> [B, d/2, h/2, w/2, c]. */
+int ccu_avgpool(const void* x, int batch, int d, int h, int w, int c, void* y, void* stream);
+
+/* Backward of the pooling into a ReLU output x_act (full resolution):
+ * dz_x += (x_act > 0) * gy[parent] / 8. */
+int ccu_pool_backward(const void* gy, const void* x_act, int batch, int d, int h, int w, int c, void* dz_x,
+                      void* stream);
+
+/* Backward of the nearest upsampling of a ReLU output coarse_act:
+ * dz_coarse = (coarse_act > 0) * sum over the 8 children of g_full
+ * (d, h, w are the full-resolution sizes). */
+int ccu_up_reduce(const void* g_full, const void* coarse_act, int batch, int d, int h, int w, int c, void* dz_coarse,
+                  void* stream);
+
+/* Output head (1x1x1 convolution 16 -> 1 with the input log kerma as
+ * residual) and the weighted squared-error loss:
+ *   out[v] = xlog[v] + hw . d0[v] + hb;  loss = sum wgt (out - target)^2 * inv_wsum
+ * target, weight, out and dz may be NULL (inference).  With dz, also the
+ * backward: dz[v] = (d0 > 0) * dloss/dout * hw; acc[0..15] += dloss/dhw,
+ * acc[16] += dloss/dhb, acc[17] += loss. */
+int ccu_head(const void* d0, const float* xlog, const float* target, const float* weight, const float* hw, float hb,
+             float inv_wsum, long long n_vox, float* out, void* dz, float* acc, void* stream);
+
+/* Network input [n_vox, 16] BF16: normalised log kerma, density, material
+ * one-hot (mat < n_mat <= 14), zeros. */
+int ccu_input(const float* xlog, const float* density, const uint8_t* mat, int n_mat, long long n_vox, void* x,
+              void* stream);
+
+/* One Adam step (bias-corrected, decoupled weight decay wd) on n FP32
+ * parameters; step counts from 1. */
+int ccu_adam(float* p, const float* g, float* m, float* v, long long n, float lr, float b1, float b2, float eps,
+             int step, float wd, void* stream);
+
+/* BF16 weights of a layer from its FP32 master copy w32[27][cout][cin]:
+ * w (same layout) and, when wt is not NULL, wt[26 - tap][cin][cout] for
+ * the backward-data convolution. */
+int ccu_pack_weights(const float* w32, int cout, int cin, void* w, void* wt, void* stream);
+
+/* Test GEMM of the tensor-core path: d[m][n] (FP32) = a . b^T with a
+ * [m][k] (a_mn = 0) or [k][m] (a_mn = 1) and b [n][k] (b_mn = 0) or
+ * [k][n] (b_mn = 1), BF16; m % 128 == 0, n % 16 == 0 with n <= 256,
+ * k % 64 == 0. */
+int ccu_gemm_test(const void* a, const void* b, float* d, int m, int n, int k, int a_mn, int b_mn, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -1,0 +1,152 @@
+"""Tensor-core kernels of the denoiser vs a plain PyTorch FP32 reference of the
+same operation on the same BF16 values (torch is only the reference here)."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+
+@pytest.fixture(scope="module")
+def U():
+    from chatcarlo_b200 import _unet_native as U
+    U.lib()
+    U.status(reset=True)
+    return U
+
+
+def _ptr(t):
+    return t.data_ptr()
+
+
+def _bf(shape, gen, scale=1.0):
+    return (torch.randn(*shape, generator=gen) * scale).to(torch.bfloat16).cuda()
+
+
+@pytest.mark.parametrize("n,a_mn,b_mn", [(16, 0, 0), (64, 0, 0), (256, 0, 0), (48, 1, 1), (128, 1, 1),
+                                         (32, 0, 1)])
+def test_gemm_descriptors(U, n, a_mn, b_mn):
+    gen = torch.Generator().manual_seed(n + 7 * a_mn)
+    m, k = 256, 192
+    a = _bf((m, k), gen)
+    b = _bf((n, k), gen)
+    d = torch.empty(m, n, dtype=torch.float32, device="cuda")
+    aa = a.t().contiguous() if a_mn else a
+    bb = b.t().contiguous() if b_mn else b
+    U.check(U.lib().ccu_gemm_test(_ptr(aa), _ptr(bb), _ptr(d), m, n, k, a_mn, b_mn, None))
+    torch.cuda.synchronize()
+    assert U.status() == 0
+    ref = a.float() @ b.float().t()
+    torch.testing.assert_close(d, ref, rtol=1e-4, atol=1e-3)
+
+
+def _torch_w(w_mine, cout, cin):
+    return w_mine.float().reshape(3, 3, 3, cout, cin).permute(3, 4, 0, 1, 2).contiguous()
+
+
+def _to_ncdhw(x):
+    return x.float().permute(0, 4, 1, 2, 3).contiguous()
+
+
+def _up(x):
+    return x.repeat_interleave(2, 2).repeat_interleave(2, 3).repeat_interleave(2, 4)
+
+
+@pytest.mark.parametrize("ca,cb,cout,dims", [(16, 0, 16, (2, 6, 8, 10)), (16, 32, 48, (1, 8, 8, 8)),
+                                             (64, 128, 64, (1, 4, 6, 8)), (32, 64, 96, (1, 6, 4, 4)),
+                                             (128, 0, 128, (1, 5, 3, 7)), (16, 0, 192, (1, 4, 4, 4))])
+def test_conv3d_forward(U, ca, cb, cout, dims):
+    gen = torch.Generator().manual_seed(ca * 1000 + cb * 10 + cout)
+    B, D, H, W = dims
+    a = _bf((B, D, H, W, ca), gen)
+    b = _bf((B, D // 2, H // 2, W // 2, cb), gen) if cb else None
+    w = _bf((27, cout, ca + cb), gen, scale=0.1)
+    bias = (torch.randn(cout, generator=gen) * 0.1).cuda()
+    split = ca if cb and cout == ca + cb else cout
+    out0 = torch.empty(B, D, H, W, split, dtype=torch.bfloat16, device="cuda")
+    out1 = torch.empty(B, D, H, W, cout - split, dtype=torch.bfloat16, device="cuda") if split < cout else None
+    U.check(U.lib().ccu_conv3d(_ptr(a), ca, _ptr(b) if b is not None else None, cb, B, D, H, W, _ptr(w),
+                               _ptr(bias), cout, 1, _ptr(out0), split, None,
+                               _ptr(out1) if out1 is not None else None, None))
+    torch.cuda.synchronize()
+    assert U.status() == 0
+    x = _to_ncdhw(a)
+    if cb:
+        x = torch.cat([x, _up(_to_ncdhw(b))], dim=1)
+    ref = torch.relu(torch.nn.functional.conv3d(x, _torch_w(w, cout, ca + cb), bias, padding=1))
+    ref = ref.permute(0, 2, 3, 4, 1)
+    got = out0.float() if out1 is None else torch.cat([out0.float(), out1.float()], dim=-1)
+    torch.testing.assert_close(got, ref, rtol=1.6e-2, atol=1e-2)
+
+
+@pytest.mark.parametrize("ca,cb,cout,dims", [(16, 0, 16, (2, 6, 8, 10)), (16, 32, 16, (1, 8, 8, 8)),
+                                             (64, 128, 64, (1, 4, 6, 8)), (64, 0, 128, (1, 5, 3, 7)),
+                                             (32, 0, 32, (3, 4, 4, 4))])
+def test_conv3d_weight_and_data_gradients(U, ca, cb, cout, dims):
+    """Weight gradient (tcgen05, MN-major operands) and the data gradient
+    (the forward kernel on flipped, transposed weights with the ReLU mask
+    of the input in its epilogue) vs torch autograd."""
+    gen = torch.Generator().manual_seed(ca + 3 * cb + 5 * cout)
+    B, D, H, W = dims
+    cin = ca + cb
+    a = torch.relu(_bf((B, D, H, W, ca), gen).float()).to(torch.bfloat16)
+    b = torch.relu(_bf((B, D // 2, H // 2, W // 2, cb), gen).float()).to(torch.bfloat16) if cb else None
+    dz = _bf((B, D, H, W, cout), gen)
+    w32 = (torch.randn(27 * cout * cin, generator=gen) * 0.1).cuda()
+    wbf = torch.empty(27 * cout * cin, dtype=torch.bfloat16, device="cuda")
+    wt = torch.empty_like(wbf)
+    U.check(U.lib().ccu_pack_weights(_ptr(w32), cout, cin, _ptr(wbf), _ptr(wt), None))
+    dw = torch.zeros(27 * cout * cin, dtype=torch.float32, device="cuda")
+    U.check(U.lib().ccu_conv3d_wgrad(_ptr(a), ca, _ptr(b) if b is not None else None, cb, B, D, H, W, _ptr(dz),
+                                     cout, _ptr(dw), 7, None))
+    # data gradient wrt the concatenated input, masked by the input's ReLU
+    # (the skip part) and written unmasked for the upsampled part
+    g0 = torch.empty(B, D, H, W, ca, dtype=torch.bfloat16, device="cuda")
+    g1 = torch.empty(B, D, H, W, cb, dtype=torch.bfloat16, device="cuda") if cb else None
+    U.check(U.lib().ccu_conv3d(_ptr(dz), cout, None, 0, B, D, H, W, _ptr(wt), None, cin, 0, _ptr(g0), ca,
+                               _ptr(a), _ptr(g1) if g1 is not None else None, None))
+    torch.cuda.synchronize()
+    assert U.status() == 0
+
+    x = _to_ncdhw(a).requires_grad_(True)
+    xb = _to_ncdhw(b).requires_grad_(True) if cb else None
+    xin = torch.cat([x, _up(xb)], dim=1) if cb else x
+    wt_ref = _torch_w(wbf, cout, cin).requires_grad_(True)
+    y = torch.nn.functional.conv3d(xin, wt_ref, None, padding=1)
+    y.backward(_to_ncdhw(dz))
+    dw_ref = wt_ref.grad.permute(2, 3, 4, 0, 1).reshape(-1)
+    torch.testing.assert_close(dw, dw_ref, rtol=2e-3, atol=2e-3 * float(dw_ref.abs().max()))
+    ga = (x.grad * (x > 0)).permute(0, 2, 3, 4, 1)
+    torch.testing.assert_close(g0.float(), ga, rtol=1.6e-2, atol=1e-2)
+    if cb:
+        # the upsampled part, before its 2x2x2 reduction
+        xin_up = _up(xb).detach().requires_grad_(True)
+        y2 = torch.nn.functional.conv3d(torch.cat([x.detach(), xin_up], dim=1), wt_ref.detach(), None, padding=1)
+        y2.backward(_to_ncdhw(dz))
+        torch.testing.assert_close(g1.float(), xin_up.grad.permute(0, 2, 3, 4, 1), rtol=1.6e-2, atol=1e-2)
+
+
+def test_pool_upsample_bias_helpers(U):
+    gen = torch.Generator().manual_seed(5)
+    B, D, H, W, c = 2, 4, 6, 8, 32
+    x = torch.relu(_bf((B, D, H, W, c), gen).float()).to(torch.bfloat16)
+    y = torch.empty(B, D // 2, H // 2, W // 2, c, dtype=torch.bfloat16, device="cuda")
+    U.check(U.lib().ccu_avgpool(_ptr(x), B, D, H, W, c, _ptr(y), None))
+    ref = torch.nn.functional.avg_pool3d(_to_ncdhw(x), 2).permute(0, 2, 3, 4, 1)
+    gy = _bf((B, D // 2, H // 2, W // 2, c), gen)
+    dz = torch.zeros(B, D, H, W, c, dtype=torch.bfloat16, device="cuda")
+    U.check(U.lib().ccu_pool_backward(_ptr(gy), _ptr(x), B, D, H, W, c, _ptr(dz), None))
+    gfull = _bf((B, D, H, W, c), gen)
+    coarse = torch.relu(_bf((B, D // 2, H // 2, W // 2, c), gen).float()).to(torch.bfloat16)
+    dzc = torch.empty_like(coarse)
+    U.check(U.lib().ccu_up_reduce(_ptr(gfull), _ptr(coarse), B, D, H, W, c, _ptr(dzc), None))
+    db = torch.zeros(c, dtype=torch.float32, device="cuda")
+    U.check(U.lib().ccu_bias_grad(_ptr(gfull), B * D * H * W, c, _ptr(db), None))
+    torch.cuda.synchronize()
+    torch.testing.assert_close(y.float(), ref, rtol=1.6e-2, atol=1e-2)
+    up = gy.float().repeat_interleave(2, 1).repeat_interleave(2, 2).repeat_interleave(2, 3) / 8
+    torch.testing.assert_close(dz.float(), up * (x.float() > 0), rtol=1.6e-2, atol=1e-2)
+    red = gfull.float().reshape(B, D // 2, 2, H // 2, 2, W // 2, 2, c).sum(dim=(2, 4, 6))
+    torch.testing.assert_close(dzc.float(), red * (coarse.float() > 0), rtol=1.6e-2, atol=2e-2)
+    torch.testing.assert_close(db, gfull.float().sum(dim=(0, 1, 2, 3)), rtol=1e-4, atol=1e-2)
