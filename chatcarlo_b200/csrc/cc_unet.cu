@@ -598,20 +598,21 @@ __global__ void up_reduce_kernel(const __nv_bfloat16* __restrict__ g_full, const
 
 // Head (1x1x1 conv, 16 -> 1, residual on the input log-kerma) with the
 // weighted squared-error loss and, when dz is given, its backward:
-//   out = xlog + hw . d0 + hb
+//   out = xlog + head[0:16] . d0 + head[16]
 //   loss = sum_v wgt (out - tgt)^2 * inv_wsum
-//   dz_d0 = (d0 > 0) * dout * hw,  dout = 2 wgt (out - tgt) inv_wsum
-// acc[0..15] += dL/dhw, acc[16] += dL/dhb, acc[17] += loss.
+//   dz_d0 = (d0 > 0) * dout * head[0:16],  dout = 2 wgt (out - tgt) inv_wsum
+// dhead[0..15] += dL/dweights, dhead[16] += dL/dbias, loss[0] += loss.
 __global__ void head_kernel(const __nv_bfloat16* __restrict__ d0, const float* __restrict__ xlog,
-                            const float* __restrict__ tgt, const float* __restrict__ wgt, const float* __restrict__ hw,
-                            float hb, float inv_wsum, long long n_vox, float* __restrict__ out,
-                            __nv_bfloat16* __restrict__ dz, float* __restrict__ acc) {
+                            const float* __restrict__ tgt, const float* __restrict__ wgt,
+                            const float* __restrict__ head, float inv_wsum, long long n_vox, float* __restrict__ out,
+                            __nv_bfloat16* __restrict__ dz, float* __restrict__ dhead, float* __restrict__ loss) {
     __shared__ float s_acc[18];
     if (threadIdx.x < 18) s_acc[threadIdx.x] = 0.0f;
     __syncthreads();
     float w[16];
 #pragma unroll
-    for (int j = 0; j < 16; ++j) w[j] = __ldg(hw + j);
+    for (int j = 0; j < 16; ++j) w[j] = __ldg(head + j);
+    const float hb = __ldg(head + 16);
     float g[18];
 #pragma unroll
     for (int j = 0; j < 18; ++j) g[j] = 0.0f;
@@ -649,7 +650,8 @@ __global__ void head_kernel(const __nv_bfloat16* __restrict__ d0, const float* _
         if ((threadIdx.x & 31) == 0 && t != 0.0f) atomicAdd(&s_acc[j], t);
     }
     __syncthreads();
-    if (threadIdx.x < 18 && s_acc[threadIdx.x] != 0.0f) atomicAdd(acc + threadIdx.x, s_acc[threadIdx.x]);
+    if (threadIdx.x < 17 && dhead && s_acc[threadIdx.x] != 0.0f) atomicAdd(dhead + threadIdx.x, s_acc[threadIdx.x]);
+    if (threadIdx.x == 17 && loss && s_acc[17] != 0.0f) atomicAdd(loss, s_acc[17]);
 }
 
 // Network input: 16 channels per voxel -- normalised log kerma, density,
@@ -980,11 +982,11 @@ int ccu_up_reduce(const void* g_full, const void* coarse_act, int batch, int d, 
     return CCU_OK;
 }
 
-int ccu_head(const void* d0, const float* xlog, const float* target, const float* weight, const float* hw, float hb,
-             float inv_wsum, long long n_vox, float* out, void* dz, float* acc, void* stream) {
-    if (!d0 || !xlog || !hw || !acc || (dz && !target)) return set_error(CCU_E_INVALID, "bad head arguments");
+int ccu_head(const void* d0, const float* xlog, const float* target, const float* weight, const float* head,
+             float inv_wsum, long long n_vox, float* out, void* dz, float* dhead, float* loss, void* stream) {
+    if (!d0 || !xlog || !head || (dz && (!target || !dhead))) return set_error(CCU_E_INVALID, "bad head arguments");
     head_kernel<<<grid_for(n_vox, 256), 256, 0, (cudaStream_t)stream>>>(
-        (const __nv_bfloat16*)d0, xlog, target, weight, hw, hb, inv_wsum, n_vox, out, (__nv_bfloat16*)dz, acc);
+        (const __nv_bfloat16*)d0, xlog, target, weight, head, inv_wsum, n_vox, out, (__nv_bfloat16*)dz, dhead, loss);
     CU_CHECK(cudaGetLastError());
     return CCU_OK;
 }
@@ -1012,6 +1014,12 @@ int ccu_pack_weights(const float* w32, int cout, int cin, void* w, void* wt, voi
     pack_weights_kernel<<<grid_for(27LL * cout * cin, 256), 256, 0, (cudaStream_t)stream>>>(
         w32, cout, cin, (__nv_bfloat16*)w, (__nv_bfloat16*)wt);
     CU_CHECK(cudaGetLastError());
+    return CCU_OK;
+}
+
+int ccu_zero(void* p, long long bytes, void* stream) {
+    if (!p || bytes < 0) return set_error(CCU_E_INVALID, "bad zero arguments");
+    CU_CHECK(cudaMemsetAsync(p, 0, (size_t)bytes, (cudaStream_t)stream));
     return CCU_OK;
 }
 

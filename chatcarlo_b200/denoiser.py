@@ -1,0 +1,318 @@
+"""Learned kerma denoiser: a 3D U-Net trained on the engine's own Monte Carlo.
+
+The network maps a low-history kerma map (plus density and material maps)
+to an estimate of the high-history map.  It works in log space: with s the
+mean input kerma per history inside the phantom,
+
+    x   = ln(k_in / s + EPS)         (input channel 0, and the residual)
+    out = x + head(U-Net(x, density, material one-hot))
+    k_denoised = s * (exp(out) - EPS)
+
+and is trained on ln(k_target / s + EPS) with a squared error weighted
+towards the phantom's voxels.  Plain Monte Carlo stays the fallback and
+the judge: the denoised map is only ever scored against a high-history
+Monte Carlo map.
+
+Architecture: 4 levels with 16, 32, 64 and 128 channels; two 3x3x3 ReLU
+convolutions per level; 2x2x2 average pooling down; nearest upsampling up,
+concatenated with the skip tensor inside the convolution's gather; a 1x1x1
+head.  Weights are BF16 copies of FP32 master weights; activations BF16;
+every convolution accumulates in FP32 on the tensor cores.  The forward,
+backward and optimizer steps are the kernels of libccunet.so; torch only
+allocates device memory and provides the stream.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _unet_native as U
+
+EPS = 0.05
+IN_CH = 16
+N_MAT = 4                       # air, water, bone, lead
+DENSITY_SCALE = 0.25
+
+
+@dataclass(frozen=True)
+class Conv:
+    name: str
+    ca: int          # channels of the full-resolution input
+    cb: int          # channels of the half-resolution input (upsampled), 0 if none
+    cout: int
+    level: int       # resolution level of input and output (0 = full)
+
+    @property
+    def cin(self) -> int:
+        return self.ca + self.cb
+
+
+LAYERS = [
+    Conv("e0a", 16, 0, 16, 0), Conv("e0", 16, 0, 16, 0),
+    Conv("e1a", 16, 0, 32, 1), Conv("e1", 32, 0, 32, 1),
+    Conv("e2a", 32, 0, 64, 2), Conv("e2", 64, 0, 64, 2),
+    Conv("b3a", 64, 0, 128, 3), Conv("b3", 128, 0, 128, 3),
+    Conv("d2a", 64, 128, 64, 2), Conv("d2", 64, 0, 64, 2),
+    Conv("d1a", 32, 64, 32, 1), Conv("d1", 32, 0, 32, 1),
+    Conv("d0a", 16, 32, 16, 0), Conv("d0", 16, 0, 16, 0),
+]
+HEAD_CH = 16
+
+
+def param_layout() -> dict[str, tuple[int, int, int, int]]:
+    """name -> (weight offset, weight size, bias offset, bias size) in the
+    flat FP32 parameter vector; the head ('head') is 16 weights + 1 bias."""
+    out, off = {}, 0
+    for L in LAYERS:
+        nw = 27 * L.cout * L.cin
+        out[L.name] = (off, nw, off + nw, L.cout)
+        off += nw + L.cout
+    out["head"] = (off, HEAD_CH, off + HEAD_CH, 1)
+    return out
+
+
+def n_params() -> int:
+    lay = param_layout()
+    o, n, bo, bn = lay["head"]
+    return bo + bn
+
+
+def init_params(seed: int = 0) -> np.ndarray:
+    """He-normal convolution weights, zero biases, zero head (the untrained
+    network returns its input)."""
+    rng = np.random.default_rng(seed)
+    p = np.zeros(n_params(), dtype=np.float32)
+    for L in LAYERS:
+        o, n, _, _ = param_layout()[L.name]
+        p[o:o + n] = rng.normal(0.0, np.sqrt(2.0 / (27 * L.cin)), n).astype(np.float32)
+    return p
+
+
+def conv_flops(B: int, S: int) -> float:
+    """Multiply-adds x 2 of one forward pass over B volumes of side S."""
+    return float(sum(2 * 27 * L.cin * L.cout * B * (S >> L.level) ** 3 for L in LAYERS))
+
+
+class UNet3D:
+    """Parameters, optimizer state and activation buffers on one device."""
+
+    def __init__(self, params: np.ndarray | None = None, seed: int = 0, device: str = "cuda"):
+        import torch
+        self.torch = torch
+        self.dev = torch.device(device)
+        U.lib()
+        p = init_params(seed) if params is None else np.asarray(params, dtype=np.float32)
+        if p.size != n_params():
+            raise ValueError(f"expected {n_params()} parameters, got {p.size}")
+        self.lay = param_layout()
+        self.p = torch.from_numpy(p.copy()).to(self.dev)
+        self.g = torch.zeros_like(self.p)
+        self.m = torch.zeros_like(self.p)
+        self.v = torch.zeros_like(self.p)
+        self.step_n = 0
+        self.w = {L.name: torch.empty(27 * L.cout * L.cin, dtype=torch.bfloat16, device=self.dev) for L in LAYERS}
+        self.wt = {L.name: torch.empty_like(self.w[L.name]) for L in LAYERS}
+        self.acc = torch.zeros(1, dtype=torch.float32, device=self.dev)      # loss
+        self.shape = None
+        self.launches = 0
+        self.pack()
+
+    # -- helpers ----------------------------------------------------------
+    def _stream(self):
+        return self.torch.cuda.current_stream(self.dev).cuda_stream
+
+    def _ptr(self, t, off: int = 0) -> int:
+        return t.data_ptr() + off * t.element_size()
+
+    def _call(self, fn, *args):
+        U.check(fn(*args))
+        self.launches += 1
+
+    def pack(self) -> None:
+        lib, st = U.lib(), self._stream()
+        for L in LAYERS:
+            o, _, _, _ = self.lay[L.name]
+            self._call(lib.ccu_pack_weights, self._ptr(self.p, o), L.cout, L.cin, self._ptr(self.w[L.name]),
+                       self._ptr(self.wt[L.name]), st)
+
+    def params_numpy(self) -> np.ndarray:
+        return self.p.detach().cpu().numpy()
+
+    def _alloc(self, B: int, S: int) -> None:
+        if self.shape == (B, S):
+            return
+        if S % 8:
+            raise ValueError("the volume side must be a multiple of 8 (three 2x2x2 poolings)")
+        torch = self.torch
+        bf = torch.bfloat16
+
+        def t(level, c, dtype=bf):
+            return torch.empty(B * (S >> level) ** 3 * c, dtype=dtype, device=self.dev)
+        a = {"x0": t(0, IN_CH), "p0": t(1, 16), "p1": t(2, 32), "p2": t(3, 64)}
+        for L in LAYERS:
+            a[L.name] = t(L.level, L.cout)
+        g = {}
+        for L in LAYERS:
+            g["dz_" + L.name] = t(L.level, L.cout)
+        g.update({"g_up1": t(0, 32), "g_up2": t(1, 64), "g_up3": t(2, 128),
+                  "g_p0": t(1, 16), "g_p1": t(2, 32), "g_p2": t(3, 64)})
+        self.a, self.gb = a, g
+        n0 = B * S ** 3
+        self.xlog = torch.empty(n0, dtype=torch.float32, device=self.dev)
+        self.out = torch.empty(n0, dtype=torch.float32, device=self.dev)
+        self.shape = (B, S)
+
+    def _dims(self, level: int):
+        B, S = self.shape
+        s = S >> level
+        return B, s, s, s
+
+    def _conv(self, L: Conv, a, b, out) -> None:
+        o, _, bo, _ = self.lay[L.name]
+        B, d, h, w = self._dims(L.level)
+        self._call(U.lib().ccu_conv3d, self._ptr(a), L.ca, self._ptr(b) if b is not None else None, L.cb, B, d, h, w,
+                   self._ptr(self.w[L.name]), self._ptr(self.p, bo), L.cout, 1, self._ptr(out), L.cout, None, None,
+                   self._stream())
+
+    # -- forward ----------------------------------------------------------
+    def set_input(self, xlog: np.ndarray | None, density: np.ndarray | None, mat: np.ndarray | None,
+                  B: int, S: int, device_xlog=None, device_density=None, device_mat=None) -> None:
+        """Input volumes [B, S, S, S] (host arrays, or device tensors)."""
+        torch = self.torch
+        self._alloc(B, S)
+        n0 = B * S ** 3
+        xl = device_xlog if device_xlog is not None else torch.from_numpy(
+            np.ascontiguousarray(xlog, dtype=np.float32).reshape(-1)).to(self.dev, non_blocking=True)
+        de = device_density if device_density is not None else torch.from_numpy(
+            np.ascontiguousarray(density, dtype=np.float32).reshape(-1) * DENSITY_SCALE).to(self.dev, non_blocking=True)
+        ma = device_mat if device_mat is not None else torch.from_numpy(
+            np.ascontiguousarray(mat, dtype=np.uint8).reshape(-1)).to(self.dev, non_blocking=True)
+        self.xlog.copy_(xl)
+        self._call(U.lib().ccu_input, self._ptr(self.xlog), self._ptr(de), self._ptr(ma), N_MAT, n0,
+                   self._ptr(self.a["x0"]), self._stream())
+        self._keep = (de, ma)
+
+    def forward(self) -> None:
+        a, lib, st = self.a, U.lib(), self._stream()
+        L = {x.name: x for x in LAYERS}
+        self._conv(L["e0a"], a["x0"], None, a["e0a"])
+        self._conv(L["e0"], a["e0a"], None, a["e0"])
+        B, S0, _, _ = self._dims(0)
+        self._call(lib.ccu_avgpool, self._ptr(a["e0"]), B, S0, S0, S0, 16, self._ptr(a["p0"]), st)
+        self._conv(L["e1a"], a["p0"], None, a["e1a"])
+        self._conv(L["e1"], a["e1a"], None, a["e1"])
+        _, S1, _, _ = self._dims(1)
+        self._call(lib.ccu_avgpool, self._ptr(a["e1"]), B, S1, S1, S1, 32, self._ptr(a["p1"]), st)
+        self._conv(L["e2a"], a["p1"], None, a["e2a"])
+        self._conv(L["e2"], a["e2a"], None, a["e2"])
+        _, S2, _, _ = self._dims(2)
+        self._call(lib.ccu_avgpool, self._ptr(a["e2"]), B, S2, S2, S2, 64, self._ptr(a["p2"]), st)
+        self._conv(L["b3a"], a["p2"], None, a["b3a"])
+        self._conv(L["b3"], a["b3a"], None, a["b3"])
+        self._conv(L["d2a"], a["e2"], a["b3"], a["d2a"])
+        self._conv(L["d2"], a["d2a"], None, a["d2"])
+        self._conv(L["d1a"], a["e1"], a["d2"], a["d1a"])
+        self._conv(L["d1"], a["d1a"], None, a["d1"])
+        self._conv(L["d0a"], a["e0"], a["d1"], a["d0a"])
+        self._conv(L["d0"], a["d0a"], None, a["d0"])
+
+    def _head(self, target=None, weight=None, inv_wsum: float = 0.0, backward: bool = False) -> None:
+        B, S = self.shape
+        ho, _, _, _ = self.lay["head"]
+        self._call(U.lib().ccu_head, self._ptr(self.a["d0"]), self._ptr(self.xlog),
+                   self._ptr(target) if target is not None else None,
+                   self._ptr(weight) if weight is not None else None, self._ptr(self.p, ho), inv_wsum,
+                   B * S ** 3, self._ptr(self.out), self._ptr(self.gb["dz_d0"]) if backward else None,
+                   self._ptr(self.g, ho) if backward else None, self._ptr(self.acc) if target is not None else None,
+                   self._stream())
+
+    def predict(self) -> "torch.Tensor":
+        """Forward pass and head; returns the predicted log map (device)."""
+        self.forward()
+        self._head()
+        return self.out
+
+    # -- backward ---------------------------------------------------------
+    def _layer_back(self, L: Conv, a, b, dz, out0=None, mask0=None, out1=None, slices: int | None = None) -> None:
+        lib, st = U.lib(), self._stream()
+        o, _, bo, _ = self.lay[L.name]
+        B, d, h, w = self._dims(L.level)
+        n = B * d * h * w
+        if slices is None:
+            slices = max(1, min(256, n // 2048))
+        self._call(lib.ccu_conv3d_wgrad, self._ptr(a), L.ca, self._ptr(b) if b is not None else None, L.cb, B, d, h, w,
+                   self._ptr(dz), L.cout, self._ptr(self.g, o), slices, st)
+        self._call(lib.ccu_bias_grad, self._ptr(dz), n, L.cout, self._ptr(self.g, bo), st)
+        if out0 is not None:
+            self._call(lib.ccu_conv3d, self._ptr(dz), L.cout, None, 0, B, d, h, w, self._ptr(self.wt[L.name]), None,
+                       L.cin, 0, self._ptr(out0), L.ca, self._ptr(mask0) if mask0 is not None else None,
+                       self._ptr(out1) if out1 is not None else None, st)
+
+    def backward(self, target, weight, inv_wsum: float) -> None:
+        a, g, lib, st = self.a, self.gb, U.lib(), self._stream()
+        L = {x.name: x for x in LAYERS}
+        self._call(lib.ccu_zero, self._ptr(self.g), self.g.numel() * 4, st)
+        self._call(lib.ccu_zero, self._ptr(self.acc), self.acc.numel() * 4, st)
+        self._head(target, weight, inv_wsum, backward=True)
+        B, S0, _, _ = self._dims(0)
+        _, S1, _, _ = self._dims(1)
+        _, S2, _, _ = self._dims(2)
+        self._layer_back(L["d0"], a["d0a"], None, g["dz_d0"], g["dz_d0a"], a["d0a"])
+        self._layer_back(L["d0a"], a["e0"], a["d1"], g["dz_d0a"], g["dz_e0"], a["e0"], g["g_up1"])
+        self._call(lib.ccu_up_reduce, self._ptr(g["g_up1"]), self._ptr(a["d1"]), B, S0, S0, S0, 32,
+                   self._ptr(g["dz_d1"]), st)
+        self._layer_back(L["d1"], a["d1a"], None, g["dz_d1"], g["dz_d1a"], a["d1a"])
+        self._layer_back(L["d1a"], a["e1"], a["d2"], g["dz_d1a"], g["dz_e1"], a["e1"], g["g_up2"])
+        self._call(lib.ccu_up_reduce, self._ptr(g["g_up2"]), self._ptr(a["d2"]), B, S1, S1, S1, 64,
+                   self._ptr(g["dz_d2"]), st)
+        self._layer_back(L["d2"], a["d2a"], None, g["dz_d2"], g["dz_d2a"], a["d2a"])
+        self._layer_back(L["d2a"], a["e2"], a["b3"], g["dz_d2a"], g["dz_e2"], a["e2"], g["g_up3"])
+        self._call(lib.ccu_up_reduce, self._ptr(g["g_up3"]), self._ptr(a["b3"]), B, S2, S2, S2, 128,
+                   self._ptr(g["dz_b3"]), st)
+        self._layer_back(L["b3"], a["b3a"], None, g["dz_b3"], g["dz_b3a"], a["b3a"])
+        self._layer_back(L["b3a"], a["p2"], None, g["dz_b3a"], g["g_p2"], None)
+        self._call(lib.ccu_pool_backward, self._ptr(g["g_p2"]), self._ptr(a["e2"]), B, S2, S2, S2, 64,
+                   self._ptr(g["dz_e2"]), st)
+        self._layer_back(L["e2"], a["e2a"], None, g["dz_e2"], g["dz_e2a"], a["e2a"])
+        self._layer_back(L["e2a"], a["p1"], None, g["dz_e2a"], g["g_p1"], None)
+        self._call(lib.ccu_pool_backward, self._ptr(g["g_p1"]), self._ptr(a["e1"]), B, S1, S1, S1, 32,
+                   self._ptr(g["dz_e1"]), st)
+        self._layer_back(L["e1"], a["e1a"], None, g["dz_e1"], g["dz_e1a"], a["e1a"])
+        self._layer_back(L["e1a"], a["p0"], None, g["dz_e1a"], g["g_p0"], None)
+        self._call(lib.ccu_pool_backward, self._ptr(g["g_p0"]), self._ptr(a["e0"]), B, S0, S0, S0, 16,
+                   self._ptr(g["dz_e0"]), st)
+        self._layer_back(L["e0"], a["e0a"], None, g["dz_e0"], g["dz_e0a"], a["e0a"])
+        self._layer_back(L["e0a"], a["x0"], None, g["dz_e0a"])
+    def loss(self) -> float:
+        """Loss of the last backward pass (synchronises the stream)."""
+        return float(self.acc[0].item())
+
+    def step(self, lr: float, b1: float = 0.9, b2: float = 0.999, eps: float = 1e-8, wd: float = 0.0) -> None:
+        self.step_n += 1
+        self._call(U.lib().ccu_adam, self._ptr(self.p), self._ptr(self.g), self._ptr(self.m), self._ptr(self.v),
+                   self.p.numel(), lr, b1, b2, eps, self.step_n, wd, self._stream())
+        self.pack()
+
+    def check_status(self) -> None:
+        st = U.status(reset=True)
+        if st:
+            raise RuntimeError(f"a tensor-core kernel reported status {st:#x} (a bounded wait ran out)")
+
+
+# ---------------------------------------------------------------------------
+# data normalisation
+# ---------------------------------------------------------------------------
+
+def kerma_scale(k_in: np.ndarray, inside: np.ndarray) -> float:
+    sel = k_in[inside]
+    s = float(sel.mean()) if sel.size else 0.0
+    return s if s > 0 else float(max(k_in.mean(), 1e-30))
+
+
+def to_log(k: np.ndarray, s: float) -> np.ndarray:
+    return np.log(np.maximum(k, 0.0) / s + EPS).astype(np.float32)
+
+
+def from_log(x: np.ndarray, s: float) -> np.ndarray:
+    return (s * (np.exp(x.astype(np.float64)) - EPS)).clip(min=0.0)

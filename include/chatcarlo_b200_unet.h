@@ -66,13 +66,15 @@ int ccu_up_reduce(const void* g_full, const void* coarse_act, int batch, int d, 
                   void* stream);
 
 /* Output head (1x1x1 convolution 16 -> 1 with the input log kerma as
- * residual) and the weighted squared-error loss:
- *   out[v] = xlog[v] + hw . d0[v] + hb;  loss = sum wgt (out - target)^2 * inv_wsum
- * target, weight, out and dz may be NULL (inference).  With dz, also the
- * backward: dz[v] = (d0 > 0) * dloss/dout * hw; acc[0..15] += dloss/dhw,
- * acc[16] += dloss/dhb, acc[17] += loss. */
-int ccu_head(const void* d0, const float* xlog, const float* target, const float* weight, const float* hw, float hb,
-             float inv_wsum, long long n_vox, float* out, void* dz, float* acc, void* stream);
+ * residual) and the weighted squared-error loss, head = 16 weights then the
+ * bias:
+ *   out[v] = xlog[v] + head[0:16] . d0[v] + head[16]
+ *   loss = sum wgt (out - target)^2 * inv_wsum   (wgt NULL: all ones)
+ * target, out, dz, dhead and loss may be NULL (inference).  With dz, also
+ * the backward: dz[v] = (d0 > 0) * dloss/dout * head[0:16];
+ * dhead[0..16] += dloss/dhead; loss[0] += loss. */
+int ccu_head(const void* d0, const float* xlog, const float* target, const float* weight, const float* head,
+             float inv_wsum, long long n_vox, float* out, void* dz, float* dhead, float* loss, void* stream);
 
 /* Network input [n_vox, 16] BF16: normalised log kerma, density, material
  * one-hot (mat < n_mat <= 14), zeros. */
@@ -88,6 +90,9 @@ int ccu_adam(float* p, const float* g, float* m, float* v, long long n, float lr
  * w (same layout) and, when wt is not NULL, wt[26 - tap][cin][cout] for
  * the backward-data convolution. */
 int ccu_pack_weights(const float* w32, int cout, int cin, void* w, void* wt, void* stream);
+
+/* cudaMemsetAsync(p, 0, bytes) on the stream (gradient buffers). */
+int ccu_zero(void* p, long long bytes, void* stream);
 
 /* Test GEMM of the tensor-core path: d[m][n] (FP32) = a . b^T with a
  * [m][k] (a_mn = 0) or [k][m] (a_mn = 1) and b [n][k] (b_mn = 0) or

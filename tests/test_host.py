@@ -214,3 +214,45 @@ def test_ellipsoid_extension_primitive():
         np.testing.assert_allclose(np.sum(q * q, axis=1), 1.0, atol=1e-9)
     mid = o[hit] + 0.5 * (t1[hit] + t2[hit])[:, None] * d[hit]
     assert np.all(contains(g, mid)) and np.all(O._contains(g, mid))
+
+
+def test_unet_oracle_gradients_match_finite_differences():
+    """The FP64 oracle's backward pass (no BF16 rounding) against central
+    differences of its own loss on an 8^3 volume."""
+    import unet_oracle as UO
+    from chatcarlo_b200 import denoiser as DN
+    rng = np.random.default_rng(0)
+    B, S = 1, 8
+    xlog = rng.normal(size=(B, S, S, S))
+    mat = rng.integers(0, 4, size=(B, S, S, S)).astype(np.uint8)
+    dens = np.array([0.0012, 1.0, 1.85, 11.35])[mat]
+    target = rng.normal(size=(B, S, S, S))
+    weight = np.where(mat > 0, 1.0, 0.1)
+    p = DN.init_params(1).astype(np.float64)
+    ho = DN.param_layout()["head"][0]
+    p[ho:ho + 17] = rng.normal(0, 0.3, 17)
+    for L in DN.LAYERS:
+        _, _, bo, bn = DN.param_layout()[L.name]
+        p[bo:bo + bn] = 0.05
+    _, g, _ = UO.loss_and_grads(p, xlog, dens, mat, target, weight, bf16_storage=False)
+    lay = DN.param_layout()
+    picks = [lay[n][0] + 3 for n in ("e0a", "e2", "b3", "d2a", "d0")] + [lay["d1a"][2], lay["head"][0] + 2, ho + 16]
+    for i in picks:
+        h = 1e-5
+        pp, pm = p.copy(), p.copy()
+        pp[i] += h
+        pm[i] -= h
+        fd = (UO.loss_and_grads(pp, xlog, dens, mat, target, weight, False)[0] -
+              UO.loss_and_grads(pm, xlog, dens, mat, target, weight, False)[0]) / (2 * h)
+        assert abs(fd - g[i]) < 1e-5 + 1e-3 * abs(fd), (i, fd, g[i])
+
+
+def test_denoiser_phantoms_validate_and_map_materials():
+    from chatcarlo_b200 import phantoms as PH
+    scenes, grids = PH.phantoms(4, 3, side=16, voxel_cm=1.0)
+    for sc, gr in zip(scenes, grids):
+        assert validate_scene(sc).ok
+        mat, dens = PH.voxel_maps(sc, gr)
+        assert mat.shape == (16, 16, 16) and mat.max() < 4
+        assert np.any(mat == 1)                       # the water body
+        np.testing.assert_allclose(dens[mat == 1], 1.0)

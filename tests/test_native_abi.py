@@ -41,3 +41,19 @@ def test_invalid_arguments_are_rejected_before_any_device_work():
                                     None, None, None, None, None) == N.CC_E_INVALID
     with pytest.raises(ValueError):
         N.check(N.CC_E_ENERGY_RANGE)
+
+
+UNET_HEADER = HEADER.parent / "chatcarlo_b200_unet.h"
+
+
+def test_denoiser_library_exports_every_declared_symbol():
+    from chatcarlo_b200 import _unet_native as U
+    text = re.sub(r"/\*.*?\*/", "", UNET_HEADER.read_text(), flags=re.S)
+    declared = sorted(set(re.findall(r"\b(ccu_[a-z0-9_]+)\s*\(", text)))
+    assert declared == sorted(U.EXPORTED)
+    lib = U.lib()
+    assert not [f for f in declared if not hasattr(lib, f)]
+    assert lib.ccu_version() == 1
+    # invalid sizes are rejected on the host
+    assert lib.ccu_conv3d(None, 16, None, 0, 1, 8, 8, 8, None, None, 16, 1, None, 16, None, None, None) == -1
+    assert lib.ccu_gemm_test(None, None, None, 100, 16, 64, 0, 0, None) == -1
