@@ -40,7 +40,7 @@ namespace {
 
 constexpr int TILE_M = 128;
 constexpr int THREADS = 256;
-constexpr int KSTAGE = 64;                  // channels (conv) or voxels (weight grad) per stage
+constexpr int KSTAGE = 64;                  // voxels per weight-gradient pipeline stage
 constexpr unsigned long long WAIT_NS = 2000000000ull;   // 2 s bound on every mbarrier wait
 
 __device__ unsigned g_status;               // bit 0: an mbarrier wait ran out
@@ -198,20 +198,6 @@ struct Src {
     int B, D, H, W;
 };
 
-// 8 channels starting at ch (a multiple of 8) of input voxel (n, z, y, x);
-// zero outside the volume.
-__device__ __forceinline__ uint4 load_in8(const Src& s, int n, int z, int y, int x, int ch) {
-    if ((unsigned)z >= (unsigned)s.D || (unsigned)y >= (unsigned)s.H || (unsigned)x >= (unsigned)s.W)
-        return make_uint4(0u, 0u, 0u, 0u);
-    if (ch < s.ca) {
-        size_t v = (((size_t)n * s.D + z) * s.H + y) * s.W + x;
-        return __ldg(reinterpret_cast<const uint4*>(s.a + v * s.ca + ch));
-    }
-    const int D2 = s.D >> 1, H2 = s.H >> 1, W2 = s.W >> 1;
-    size_t v = (((size_t)n * D2 + (z >> 1)) * H2 + (y >> 1)) * W2 + (x >> 1);
-    return __ldg(reinterpret_cast<const uint4*>(s.b + v * s.cb + (ch - s.ca)));
-}
-
 __device__ __forceinline__ void voxel_coords(long long v, const Src& s, int& n, int& z, int& y, int& x) {
     x = (int)(v % s.W);
     long long t = v / s.W;
@@ -222,13 +208,68 @@ __device__ __forceinline__ void voxel_coords(long long v, const Src& s, int& n, 
 }
 
 // ---------------------------------------------------------------------------
+// gather machinery shared by the two GEMM kernels
+// ---------------------------------------------------------------------------
+
+// 16-byte asynchronous copy global -> shared; src_bytes 0 writes zeros
+// (the zero padding outside the volume) without reading src.
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, uint32_t src_bytes) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(src_bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int PENDING>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(PENDING) : "memory");
+}
+
+// A voxel of a tile: flattened index (-1 outside the range), boundary
+// flags (bit 0 z > 0, 1 z < D-1, 2 y > 0, 3 y < H-1, 4 x > 0, 5 x < W-1),
+// and for the half-resolution source its coarse voxel index and the
+// parities of its coordinates (bit 0 x, 1 y, 2 z).
+struct VoxRec {
+    int v, flags, cv, par;
+};
+
+__device__ __forceinline__ VoxRec make_vox(long long v, long long n_vox, const Src& s) {
+    VoxRec r{-1, 0, 0, 0};
+    if (v < n_vox) {
+        int n, z, y, x;
+        voxel_coords(v, s, n, z, y, x);
+        r.v = (int)v;
+        r.flags = (z > 0) | ((z < s.D - 1) << 1) | ((y > 0) << 2) | ((y < s.H - 1) << 3) | ((x > 0) << 4) |
+                  ((x < s.W - 1) << 5);
+        if (s.cb) {
+            r.cv = ((n * (s.D >> 1) + (z >> 1)) * (s.H >> 1) + (y >> 1)) * (s.W >> 1) + (x >> 1);
+            r.par = (x & 1) | ((y & 1) << 1) | ((z & 1) << 2);
+        }
+    }
+    return r;
+}
+
+// Boundary flags a voxel needs for its neighbour at tap to lie inside.
+__host__ __device__ constexpr int tap_req(int t) {
+    return (t / 9 == 0 ? 1 : 0) | (t / 9 == 2 ? 2 : 0) | ((t / 3) % 3 == 0 ? 4 : 0) | ((t / 3) % 3 == 2 ? 8 : 0) |
+           (t % 3 == 0 ? 16 : 0) | (t % 3 == 2 ? 32 : 0);
+}
+
+// Offset (in coarse voxels) of the coarse voxel holding the neighbour at
+// tap of a fine voxel with coordinate parities par: the coarse coordinate
+// moves by floor((parity + d) / 2) along each axis.
+__device__ __forceinline__ int coarse_offset(const Src& s, int par, int tap) {
+    const int dz = tap / 9 - 1, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
+    const int cz = (((par >> 2) & 1) + dz) >> 1, cy = (((par >> 1) & 1) + dy) >> 1, cx = ((par & 1) + dx) >> 1;
+    return (cz * (s.H >> 1) + cy) * (s.W >> 1) + cx;
+}
+
+// ---------------------------------------------------------------------------
 // forward / backward-data convolution
 // ---------------------------------------------------------------------------
 
+constexpr int KS = 64;                      // K elements (tap x channel) per convolution stage
+
 struct ConvP {
     Src src;
-    int kc;                      // input channels per pipeline stage (divides ca + cb)
-    const __nv_bfloat16* w;      // [27][N][cin]
+    const __nv_bfloat16* w;      // packed in tile order: packed_elems(N, cin)
     const float* bias;           // [N] or null
     int relu;
     long long n_vox;
@@ -244,91 +285,143 @@ __host__ __device__ constexpr uint32_t tmem_cols(int n) {
     return n <= 32 ? 32u : (n <= 64 ? 64u : (n <= 128 ? 128u : 256u));
 }
 
+constexpr int CONV_STAGES = 3;
+__host__ __device__ constexpr uint32_t conv_stage_bytes(int n) { return (uint32_t)(TILE_M + n) * KS * 2; }
+
+// Weights packed in shared-memory tile order: stage s (K elements
+// [64 s, 64 s + 64) of 27 x c, k = tap * c + ch), chunk c8 of 8 elements,
+// output row r: element ((s * 8 + c8) * n + r) * 8 + e, zero beyond 27 x c.
+__host__ __device__ constexpr long long packed_elems(int n, int c) {
+    return (long long)((27 * c + KS - 1) / KS) * n * KS;
+}
+
+// K runs over (tap, channel) in stages of KS elements; a stage's A tile is
+// the 128 output voxels' neighbours for those (tap, channel) pairs, its B
+// tile the matching packed weights.  CONV_STAGES stages are in flight:
+// cp.async fills stage s + 2 while the tensor core works on stage s.  Each
+// thread gathers for one output row (m = tid % 128) four chunks per stage
+// (c8 = tid / 128 + 2 j) and steps their (tap, channel) incrementally.
 template <int N>
 __global__ void __launch_bounds__(THREADS) conv_kernel(const ConvP P) {
+    constexpr int NS = CONV_STAGES;
+    constexpr uint32_t A_BYTES = TILE_M * KS * 2, STAGE = conv_stage_bytes(N);
     extern __shared__ __align__(128) uint8_t smem[];
-    __shared__ uint64_t bar[2];
+    __shared__ uint64_t bar[NS];
     __shared__ uint32_t s_tmem;
-    __shared__ int s_row[TILE_M][4];
+    __shared__ int s_off[27];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int cin = P.src.ca + P.src.cb;
-    const int kc = P.kc;                             // 16, 32, 48 or 64
-    const int nkc = cin / kc;
-    const uint32_t a_bytes = TILE_M * kc * 2, b_bytes = N * kc * 2, stage_bytes = a_bytes + b_bytes;
+    const Src& S = P.src;
+    const int cin = S.ca + S.cb;
+    const int n_stages = (27 * cin + KS - 1) / KS;
     const long long m0 = (long long)blockIdx.x * TILE_M;
 
-    if (tid < TILE_M) {
-        long long v = m0 + tid;
-        int n = -1, z = 0, y = 0, x = 0;
-        if (v < P.n_vox) voxel_coords(v, P.src, n, z, y, x);
-        s_row[tid][0] = n;
-        s_row[tid][1] = z;
-        s_row[tid][2] = y;
-        s_row[tid][3] = x;
+    if (tid < 27) {
+        const int dz = tid / 9 - 1, dy = (tid / 3) % 3 - 1, dx = tid % 3 - 1;
+        s_off[tid] = ((dz * S.H + dy) * S.W + dx) * S.ca;          // element offset in a
     }
     if (warp == 0) tmem_alloc(&s_tmem, tmem_cols(N));
     if (tid == 0) {
-        mbar_init(&bar[0], 1);
-        mbar_init(&bar[1], 1);
+        for (int i = 0; i < NS; ++i) mbar_init(&bar[i], 1);
         mbar_init_fence();
     }
+    // this thread's output row
+    const int m = tid & (TILE_M - 1), c8_0 = tid >> 7;
+    const VoxRec row = make_vox(m0 + m, P.n_vox, S);
+    uint32_t valid = 0;                              // taps whose neighbour lies inside the volume
+    if (row.v >= 0) {
+#pragma unroll
+        for (int t = 0; t < 27; ++t)
+            if ((row.flags & tap_req(t)) == tap_req(t)) valid |= 1u << t;
+    }
+    const __nv_bfloat16* a_row = S.a + (size_t)(row.v < 0 ? 0 : row.v) * S.ca;
+    const __nv_bfloat16* b_row = S.cb ? S.b + (size_t)row.cv * S.cb : S.b;
+    // (tap, ch) of this thread's 4 chunks in stage 0; a stage advances K by KS
+    int tap[4], ch[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const int k = (c8_0 + 2 * j) * 8;
+        tap[j] = k / cin;
+        ch[j] = k - tap[j] * cin;
+    }
+    const int step_tap = KS / cin, step_ch = KS - (KS / cin) * cin;
+    uint32_t dstA[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) dstA[j] = (c8_0 + 2 * j) * (TILE_M * 16) + (m >> 3) * 128 + (m & 7) * 16;
+
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = s_tmem;
+    const uint32_t sbase = smem_u32(smem);
     constexpr uint32_t IDESC = idesc_bf16(TILE_M, N, 0, 0);
 
-    const int iters = 27 * nkc;
+    // copies of stage s; called for s = 0, 1, 2, ... in order
+    auto issue = [&](int s) {
+        const uint32_t sa = sbase + (uint32_t)(s % NS) * STAGE, sb = sa + A_BYTES;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int t = tap[j], c = ch[j];
+            uint32_t bytes = 0;
+            const void* src = S.a;
+            if ((valid >> t) & 1u) {                 // t <= 27, and bit 27 is never set
+                bytes = 16;
+                src = c < S.ca ? (const void*)(a_row + s_off[t] + c)
+                               : (const void*)(b_row + (size_t)coarse_offset(S, row.par, t) * S.cb + (c - S.ca));
+            }
+            cp_async16(sa + dstA[j], src, bytes);
+            int nc = c + step_ch, nt = t + step_tap;
+            if (nc >= cin) {
+                nc -= cin;
+                ++nt;
+            }
+            tap[j] = nt;
+            ch[j] = nc;
+        }
+        const __nv_bfloat16* wb = P.w + (size_t)s * (N * KS);
+        for (int i = tid; i < N * (KS / 8); i += THREADS) cp_async16(sb + i * 16, wb + (size_t)i * 8, 16u);
+    };
+
     bool ok = true;
     int issued = 0;                                  // stages whose MMAs were committed
-    for (int it = 0; it < iters && ok; ++it) {
-        const int st = it & 1;
-        if (it >= 2) ok = mbar_wait(&bar[st], ((it - 2) >> 1) & 1);
+    for (int s = 0; s < NS - 1; ++s) {
+        if (s < n_stages) issue(s);
+        cp_async_commit();
+    }
+    for (int it = 0; it < n_stages; ++it) {
+        cp_async_wait<NS - 2>();                     // this thread's copies of stage it landed
+        fence_proxy_async();                         // ... and are visible to the tensor core
         if (!__syncthreads_and(ok)) { ok = false; break; }
-        const int tap = it / nkc, kk = (it - tap * nkc) * kc;
-        const int dz = tap / 9 - 1, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
-        uint8_t* sA = smem + st * stage_bytes;
-        uint8_t* sB = sA + a_bytes;
-        // A: row m, channel chunk c8 at c8 * (TILE_M * 16) + (m / 8) * 128 + (m % 8) * 16
-        const int a_chunks = TILE_M * (kc >> 3);
-        for (int i = tid; i < a_chunks; i += THREADS) {
-            const int m = i & (TILE_M - 1), c8 = i >> 7;
-            uint4 val = make_uint4(0u, 0u, 0u, 0u);
-            const int n = s_row[m][0];
-            if (n >= 0) val = load_in8(P.src, n, s_row[m][1] + dz, s_row[m][2] + dy, s_row[m][3] + dx, kk + c8 * 8);
-            *reinterpret_cast<uint4*>(sA + c8 * (TILE_M * 16) + (m >> 3) * 128 + (m & 7) * 16) = val;
-        }
-        // B: output channel r, chunk c8 at c8 * (N * 16) + (r / 8) * 128 + (r % 8) * 16
-        const int b_chunks = N * (kc >> 3);
-        for (int i = tid; i < b_chunks; i += THREADS) {
-            const int r = i % N, c8 = i / N;
-            uint4 val = __ldg(reinterpret_cast<const uint4*>(P.w + ((size_t)tap * N + r) * cin + kk + c8 * 8));
-            *reinterpret_cast<uint4*>(sB + c8 * (N * 16) + (r >> 3) * 128 + (r & 7) * 16) = val;
-        }
-        fence_proxy_async();
-        __syncthreads();
         if (tid == 0) {
             tc_fence_after();
-            const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB);
-            for (int k = 0; k < (kc >> 4); ++k) {
+            const uint32_t a0 = sbase + (uint32_t)(it % NS) * STAGE, b0 = a0 + A_BYTES;
+#pragma unroll
+            for (int k = 0; k < KS / 16; ++k) {
                 uint64_t ad = smem_desc(a0 + k * 2 * (TILE_M * 16), TILE_M * 16, 128);
                 uint64_t bd = smem_desc(b0 + k * 2 * (N * 16), N * 16, 128);
                 mma_bf16(tmem, ad, bd, IDESC, (it > 0 || k > 0) ? 1u : 0u);
             }
-            mma_commit(&bar[st]);
+            mma_commit(&bar[it % NS]);
         }
         issued = it + 1;
+        // stage it + NS - 1 reuses the buffer that the MMAs of stage it - 1 read
+        const int nxt = it + NS - 1;
+        if (nxt < n_stages) {
+            if (it >= 1) ok = mbar_wait(&bar[(it - 1) % NS], ((it - 1) / NS) & 1);
+            if (ok) issue(nxt);
+        }
+        cp_async_commit();
     }
+    cp_async_wait<0>();
     // the last commit covers every earlier MMA of this thread; it is waited
     // for on the error path too, before the tensor memory is freed
-    if (issued > 0 && !mbar_wait(&bar[(issued - 1) & 1], ((issued - 1) >> 1) & 1)) ok = false;
-    ok = __syncthreads_and(ok && issued == iters);
+    if (issued > 0 && !mbar_wait(&bar[(issued - 1) % NS], ((issued - 1) / NS) & 1)) ok = false;
+    ok = __syncthreads_and(ok && issued == n_stages);
     tc_fence_after();
 
     if (ok) {
         const int q = warp & 3, half = warp >> 2;
-        const int row = q * 32 + lane;
-        const long long v = m0 + row;
+        const int row_i = q * 32 + lane;
+        const long long v = m0 + row_i;
         for (int c0 = half * 8; c0 < N; c0 += 16) {
             float f[8];
             tmem_ld8(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)c0, f);
@@ -373,105 +466,135 @@ struct WgradP {
     float* dw;                   // [27][N][cin], accumulated
 };
 
+__host__ __device__ constexpr int wgrad_stages(int n) { return n <= 64 ? 4 : 3; }
+__host__ __device__ constexpr uint32_t wgrad_stage_bytes(int n) { return (uint32_t)(TILE_M + n) * KSTAGE * 2; }
+
+// M = 128 rows (tap, ci) of 27 x cin, N = output channels, K = the CTA's
+// voxel range in stages of KSTAGE voxels; both operands MN-major.  Each
+// thread gathers one row group (8 channels of one tap) for four voxels of
+// every stage.
 template <int N>
 __global__ void __launch_bounds__(THREADS) wgrad_kernel(const WgradP P) {
+    constexpr int NS = wgrad_stages(N);
+    constexpr uint32_t A_BYTES = TILE_M * KSTAGE * 2, STAGE = wgrad_stage_bytes(N);
     extern __shared__ __align__(128) uint8_t smem[];
-    __shared__ uint64_t bar[2];
+    __shared__ uint64_t bar[NS];
     __shared__ uint32_t s_tmem;
-    __shared__ int s_vox[2][KSTAGE][4];
+    __shared__ VoxRec s_vox[NS][KSTAGE];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int cin = P.src.ca + P.src.cb;
+    const Src& S = P.src;
+    const int cin = S.ca + S.cb;
     const int rows = 27 * cin;
     const int r0 = blockIdx.x * TILE_M;
     const long long v_begin = (long long)blockIdx.y * P.vox_per_cta;
     const long long v_end = v_begin + P.vox_per_cta < P.n_vox ? v_begin + P.vox_per_cta : P.n_vox;
-    constexpr uint32_t a_bytes = TILE_M * KSTAGE * 2, b_bytes = N * KSTAGE * 2, stage_bytes = a_bytes + b_bytes;
+    const int n_stages = v_end > v_begin ? (int)((v_end - v_begin + KSTAGE - 1) / KSTAGE) : 0;
 
     if (warp == 0) tmem_alloc(&s_tmem, tmem_cols(N));
     if (tid == 0) {
-        mbar_init(&bar[0], 1);
-        mbar_init(&bar[1], 1);
+        for (int i = 0; i < NS; ++i) mbar_init(&bar[i], 1);
         mbar_init_fence();
     }
+    // voxel records of the first NS - 1 stages
+    for (int s = 0; s < NS - 1 && s < n_stages; ++s)
+        if (tid < KSTAGE) s_vox[s][tid] = make_vox(v_begin + (long long)s * KSTAGE + tid, v_end, S);
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem = s_tmem;
+    const uint32_t sbase = smem_u32(smem);
     constexpr uint32_t IDESC = idesc_bf16(TILE_M, N, 1, 1);
 
-    const long long n_vox_cta = v_end > v_begin ? v_end - v_begin : 0;
-    const int iters = (int)((n_vox_cta + KSTAGE - 1) / KSTAGE);
+    // this thread's A row group (8 channels of one tap) is fixed
+    const int g = (tid >> 3) & (TILE_M / 8 - 1);
+    const int r = r0 + g * 8;
+    const bool row_in = r < rows;
+    const int tap = row_in ? r / cin : 0, ci = row_in ? r - tap * cin : 0;
+    const int req = tap_req(tap);
+    const int dz = tap / 9 - 1, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
+    const bool from_a = ci < S.ca;
+    const long long a_off = (long long)((dz * S.H + dy) * S.W + dx);   // neighbour offset in voxels
+    const int klo = tid & 7, khi0 = tid >> 7;
+
+    auto issue = [&](int s) {
+        const int buf = s % NS;
+        const uint32_t sa = sbase + (uint32_t)buf * STAGE, sb = sa + A_BYTES;
+        // A (MN-major): voxel k, row group g at (k / 8) * (TILE_M * 16) + g * 128 + (k % 8) * 16
+#pragma unroll
+        for (int j = 0; j < TILE_M / 8 * KSTAGE / THREADS; ++j) {
+            const int khi = khi0 + 2 * j, k = khi * 8 + klo;
+            const VoxRec vr = s_vox[buf][k];
+            uint32_t bytes = 0;
+            const void* src = S.a;
+            if (row_in && vr.v >= 0 && (vr.flags & req) == req) {
+                bytes = 16;
+                if (from_a) {
+                    src = S.a + ((long long)vr.v + a_off) * S.ca + ci;
+                } else {
+                    const int cz = (((vr.par >> 2) & 1) + dz) >> 1, cy = (((vr.par >> 1) & 1) + dy) >> 1,
+                              cx = ((vr.par & 1) + dx) >> 1;
+                    src = S.b + (size_t)(vr.cv + (cz * (S.H >> 1) + cy) * (S.W >> 1) + cx) * S.cb + (ci - S.ca);
+                }
+            }
+            cp_async16(sa + khi * (TILE_M * 16) + g * 128 + klo * 16, src, bytes);
+        }
+        // B (MN-major): voxel k, output-channel group gg at (k / 8) * (N * 16) + gg * 128 + (k % 8) * 16
+        for (int i = tid; i < N / 8 * KSTAGE; i += THREADS) {
+            const int kl = i & 7, gg = (i >> 3) % (N / 8), kh = i / N;
+            const int v = s_vox[buf][kh * 8 + kl].v;
+            cp_async16(sb + kh * (N * 16) + gg * 128 + kl * 16,
+                       v >= 0 ? (const void*)(P.dz + (size_t)v * N + gg * 8) : (const void*)P.dz, v >= 0 ? 16u : 0u);
+        }
+    };
+
     bool ok = true;
     int issued = 0;
-    for (int it = 0; it < iters && ok; ++it) {
-        const int st = it & 1;
-        const long long vk = v_begin + (long long)it * KSTAGE;
-        if (tid < KSTAGE) {
-            const long long v = vk + tid;
-            int n = -1, z = 0, y = 0, x = 0;
-            if (v < v_end) voxel_coords(v, P.src, n, z, y, x);
-            s_vox[st][tid][0] = n;
-            s_vox[st][tid][1] = z;
-            s_vox[st][tid][2] = y;
-            s_vox[st][tid][3] = x;
-        }
-        if (it >= 2) ok = mbar_wait(&bar[st], ((it - 2) >> 1) & 1);
-        if (!__syncthreads_and(ok)) { ok = false; break; }
-        uint8_t* sA = smem + st * stage_bytes;
-        uint8_t* sB = sA + a_bytes;
-        // A (MN-major): voxel k, row group g (8 rows = 8 input channels of one
-        // tap) at (k / 8) * (TILE_M * 16) + g * 128 + (k % 8) * 16
-        for (int i = tid; i < TILE_M / 8 * KSTAGE; i += THREADS) {
-            const int klo = i & 7, g = (i >> 3) & (TILE_M / 8 - 1), khi = i >> 7;
-            const int k = khi * 8 + klo;
-            const int r = r0 + g * 8;
-            const int n = s_vox[st][k][0];
-            uint4 val = make_uint4(0u, 0u, 0u, 0u);
-            if (r < rows && n >= 0) {
-                const int tap = r / cin, ci = r - tap * cin;
-                val = load_in8(P.src, n, s_vox[st][k][1] + tap / 9 - 1, s_vox[st][k][2] + (tap / 3) % 3 - 1,
-                               s_vox[st][k][3] + tap % 3 - 1, ci);
-            }
-            *reinterpret_cast<uint4*>(sA + khi * (TILE_M * 16) + g * 128 + klo * 16) = val;
-        }
-        // B (MN-major): voxel k, output-channel group g at (k / 8) * (N * 16) + g * 128 + (k % 8) * 16
-        for (int i = tid; i < N / 8 * KSTAGE; i += THREADS) {
-            const int klo = i & 7, g = (i >> 3) % (N / 8), khi = i / (N / 8 * 8);
-            const int k = khi * 8 + klo;
-            const long long v = vk + k;
-            uint4 val = make_uint4(0u, 0u, 0u, 0u);
-            if (v < v_end) val = __ldg(reinterpret_cast<const uint4*>(P.dz + (size_t)v * N + g * 8));
-            *reinterpret_cast<uint4*>(sB + khi * (N * 16) + g * 128 + klo * 16) = val;
-        }
+    for (int s = 0; s < NS - 1; ++s) {
+        if (s < n_stages) issue(s);
+        cp_async_commit();
+    }
+    for (int it = 0; it < n_stages; ++it) {
+        cp_async_wait<NS - 2>();
         fence_proxy_async();
-        __syncthreads();
+        // records of stage it + NS - 1: their buffer was last read when stage
+        // it - 1 was issued, before the previous barrier
+        const int nxt = it + NS - 1;
+        if (nxt < n_stages && tid < KSTAGE)
+            s_vox[nxt % NS][tid] = make_vox(v_begin + (long long)nxt * KSTAGE + tid, v_end, S);
+        if (!__syncthreads_and(ok)) { ok = false; break; }
         if (tid == 0) {
             tc_fence_after();
-            const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB);
+            const uint32_t a0 = sbase + (uint32_t)(it % NS) * STAGE, b0 = a0 + A_BYTES;
 #pragma unroll
             for (int k = 0; k < KSTAGE / 16; ++k) {
                 uint64_t ad = smem_desc(a0 + k * 2 * (TILE_M * 16), TILE_M * 16, 128);
                 uint64_t bd = smem_desc(b0 + k * 2 * (N * 16), N * 16, 128);
                 mma_bf16(tmem, ad, bd, IDESC, (it > 0 || k > 0) ? 1u : 0u);
             }
-            mma_commit(&bar[st]);
+            mma_commit(&bar[it % NS]);
         }
         issued = it + 1;
+        if (nxt < n_stages) {
+            if (it >= 1) ok = mbar_wait(&bar[(it - 1) % NS], ((it - 1) / NS) & 1);
+            if (ok) issue(nxt);
+        }
+        cp_async_commit();
     }
-    if (issued > 0 && !mbar_wait(&bar[(issued - 1) & 1], ((issued - 1) >> 1) & 1)) ok = false;
-    ok = __syncthreads_and(ok && issued == iters);
+    cp_async_wait<0>();
+    if (issued > 0 && !mbar_wait(&bar[(issued - 1) % NS], ((issued - 1) / NS) & 1)) ok = false;
+    ok = __syncthreads_and(ok && issued == n_stages);
     tc_fence_after();
 
-    if (ok && iters > 0) {
+    if (ok && n_stages > 0) {
         const int q = warp & 3, half = warp >> 2;
-        const int r = r0 + q * 32 + lane;
-        const int tap = r / cin, ci = r - tap * cin;
+        const int rr = r0 + q * 32 + lane;
+        const int tp = rr / cin, cc = rr - tp * cin;
         for (int c0 = half * 8; c0 < N; c0 += 16) {
             float f[8];
             tmem_ld8(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)c0, f);
-            if (r < rows) {
+            if (rr < rows) {
 #pragma unroll
-                for (int j = 0; j < 8; ++j) atomicAdd(P.dw + ((size_t)tap * N + c0 + j) * cin + ci, f[j]);
+                for (int j = 0; j < 8; ++j) atomicAdd(P.dw + ((size_t)tp * N + c0 + j) * cin + cc, f[j]);
             }
         }
     } else if (!ok && tid == 0) {
@@ -686,21 +809,30 @@ __global__ void adam_kernel(float* __restrict__ p, const float* __restrict__ g, 
     }
 }
 
-// BF16 weights of one layer from its FP32 master copy: w[tap][co][ci] for
-// the forward pass and wt[26 - tap][ci][co] (flipped, transposed) for the
-// backward-data pass.
-__global__ void pack_weights_kernel(const float* __restrict__ w32, int cout, int cin, __nv_bfloat16* __restrict__ w,
-                                    __nv_bfloat16* __restrict__ wt) {
-    const long long total = 27LL * cout * cin;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+// BF16 weights of one layer from its FP32 master copy w32[27][cout][cin],
+// packed in tile order (packed_elems): wp for the forward convolution
+// (n = cout, c = cin, W(tap, r, ch) = w32[tap][r][ch]) and wtp for the
+// backward-data convolution (n = cin, c = cout, W(tap, r, ch) =
+// w32[26 - tap][ch][r]: flipped taps, transposed channels).
+__global__ void pack_weights_kernel(const float* __restrict__ w32, int cout, int cin, __nv_bfloat16* __restrict__ wp,
+                                    __nv_bfloat16* __restrict__ wtp) {
+    const long long nf = packed_elems(cout, cin), nb = wtp ? packed_elems(cin, cout) : 0;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < nf + nb;
          i += (long long)gridDim.x * blockDim.x) {
-        const int ci = (int)(i % cin);
-        long long t = i / cin;
-        const int co = (int)(t % cout);
-        const int tap = (int)(t / cout);
-        const __nv_bfloat16 h = __float2bfloat16_rn(w32[i]);
-        w[i] = h;
-        if (wt) wt[((size_t)(26 - tap) * cin + ci) * cout + co] = h;
+        const bool fwd = i < nf;
+        const long long j = fwd ? i : i - nf;
+        const int n = fwd ? cout : cin, c = fwd ? cin : cout;
+        const int e = (int)(j & 7);
+        long long t = j >> 3;
+        const int r = (int)(t % n);
+        t /= n;
+        const int c8 = (int)(t & 7);
+        const long long st = t >> 3;
+        const long long k = st * KS + c8 * 8 + e;
+        const int tap = (int)(k / c), ch = (int)(k - (long long)tap * c);
+        float val = 0.0f;
+        if (tap < 27) val = fwd ? w32[((size_t)tap * cout + r) * cin + ch] : w32[((size_t)(26 - tap) * cout + ch) * cin + r];
+        (fwd ? wp : wtp)[j] = __float2bfloat16_rn(val);
     }
 }
 
@@ -807,12 +939,12 @@ int grid_for(long long work, int threads) {
 
 bool aligned16(const void* p) { return ((uintptr_t)p & 15u) == 0; }
 
-// Shared memory per CTA: the two stages, raised where needed so that the
-// CTAs resident on one SM never ask for more than its 512 tensor-memory
+// Shared memory per CTA: the pipeline stages, raised where needed so that
+// the CTAs resident on one SM never ask for more than its 512 tensor-memory
 // columns together (an allocation beyond that would wait for another CTA).
 template <typename K>
-int tc_launch_smem(K kernel, uint32_t stage_bytes, uint32_t cols, size_t& smem) {
-    smem = 2 * (size_t)stage_bytes;
+int tc_launch_smem(K kernel, size_t stages_bytes, uint32_t cols, size_t& smem) {
+    smem = stages_bytes;
     const int max_ctas = (int)(512u / cols);
     int dev = 0;
     CU_CHECK(cudaGetDevice(&dev));
@@ -820,8 +952,10 @@ int tc_launch_smem(K kernel, uint32_t stage_bytes, uint32_t cols, size_t& smem) 
     CU_CHECK(cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
     const size_t floor_smem = (size_t)per_sm / (size_t)(max_ctas + 1) + 1024;
     if (smem < floor_smem) smem = floor_smem;
-    if (smem > 200 * 1024) return set_error(CCU_E_INVALID, "stage too large for shared memory");
+    if (smem > 200 * 1024) return set_error(CCU_E_INVALID, "stages too large for shared memory");
     CU_CHECK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    CU_CHECK(cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                  (int)cudaSharedmemCarveoutMaxShared));
     int occ = 0;
     CU_CHECK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, THREADS, smem));
     if (occ * (int)cols > 512) return set_error(CCU_E_INVALID, "tensor-memory budget per SM exceeded");
@@ -829,17 +963,10 @@ int tc_launch_smem(K kernel, uint32_t stage_bytes, uint32_t cols, size_t& smem) 
     return CCU_OK;
 }
 
-int stage_channels(int cin) {
-    for (int k = KSTAGE; k >= 16; k -= 16)
-        if (cin % k == 0) return k;
-    return 16;
-}
-
 template <int N>
 int launch_conv(const ConvP& P, cudaStream_t st) {
-    const int kc = P.kc;
     size_t smem = 0;
-    int rc = tc_launch_smem(conv_kernel<N>, (uint32_t)(TILE_M + N) * kc * 2, tmem_cols(N), smem);
+    int rc = tc_launch_smem(conv_kernel<N>, (size_t)CONV_STAGES * conv_stage_bytes(N), tmem_cols(N), smem);
     if (rc != CCU_OK) return rc;
     const long long blocks = (P.n_vox + TILE_M - 1) / TILE_M;
     conv_kernel<N><<<(unsigned)blocks, THREADS, smem, st>>>(P);
@@ -850,7 +977,7 @@ int launch_conv(const ConvP& P, cudaStream_t st) {
 template <int N>
 int launch_wgrad(const WgradP& P, int slices, int cin, cudaStream_t st) {
     size_t smem = 0;
-    int rc = tc_launch_smem(wgrad_kernel<N>, (uint32_t)(TILE_M + N) * KSTAGE * 2, tmem_cols(N), smem);
+    int rc = tc_launch_smem(wgrad_kernel<N>, (size_t)wgrad_stages(N) * wgrad_stage_bytes(N), tmem_cols(N), smem);
     if (rc != CCU_OK) return rc;
     dim3 grid((unsigned)((27 * cin + TILE_M - 1) / TILE_M), (unsigned)slices);
     wgrad_kernel<N><<<grid, THREADS, smem, st>>>(P);
@@ -864,6 +991,8 @@ int check_src(const void* a, int ca, const void* b, int cb, int batch, int d, in
     if (!aligned16(a) || (b && !aligned16(b))) return set_error(CCU_E_INVALID, "tensors must be 16-byte aligned");
     if (batch <= 0 || d <= 0 || h <= 0 || w <= 0) return set_error(CCU_E_INVALID, "empty volume");
     if (cb > 0 && (d % 2 || h % 2 || w % 2)) return set_error(CCU_E_INVALID, "upsampled input needs even dimensions");
+    if ((long long)batch * d * h * w >= (1LL << 31) - (long long)2 * h * w - 2 * w - 2)
+        return set_error(CCU_E_INVALID, "volume too large for 32-bit voxel indices");
     return CCU_OK;
 }
 
@@ -896,7 +1025,6 @@ int ccu_conv3d(const void* a, int ca, const void* b, int cb, int batch, int d, i
         return set_error(CCU_E_INVALID, "tensors must be 16-byte aligned");
     ConvP P;
     P.src = Src{(const __nv_bfloat16*)a, (const __nv_bfloat16*)b, ca, cb, batch, d, h, w};
-    P.kc = stage_channels(ca + cb);
     P.w = (const __nv_bfloat16*)weight;
     P.bias = bias;
     P.relu = relu;
@@ -1009,10 +1137,17 @@ int ccu_adam(float* p, const float* g, float* m, float* v, long long n, float lr
     return CCU_OK;
 }
 
+long long ccu_packed_weight_elems(int n, int c) {
+    if (n <= 0 || c <= 0 || n % 16 || c % 16) return set_error(CCU_E_INVALID, "channels must be positive multiples of 16");
+    return packed_elems(n, c);
+}
+
 int ccu_pack_weights(const float* w32, int cout, int cin, void* w, void* wt, void* stream) {
-    if (!w32 || !w || cout <= 0 || cin <= 0) return set_error(CCU_E_INVALID, "bad weight arguments");
-    pack_weights_kernel<<<grid_for(27LL * cout * cin, 256), 256, 0, (cudaStream_t)stream>>>(
-        w32, cout, cin, (__nv_bfloat16*)w, (__nv_bfloat16*)wt);
+    if (!w32 || !w || cout <= 0 || cin <= 0 || cout % 16 || cin % 16)
+        return set_error(CCU_E_INVALID, "bad weight arguments");
+    const long long total = packed_elems(cout, cin) + (wt ? packed_elems(cin, cout) : 0);
+    pack_weights_kernel<<<grid_for(total, 256), 256, 0, (cudaStream_t)stream>>>(w32, cout, cin, (__nv_bfloat16*)w,
+                                                                                (__nv_bfloat16*)wt);
     CU_CHECK(cudaGetLastError());
     return CCU_OK;
 }

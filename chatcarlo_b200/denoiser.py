@@ -111,8 +111,11 @@ class UNet3D:
         self.m = torch.zeros_like(self.p)
         self.v = torch.zeros_like(self.p)
         self.step_n = 0
-        self.w = {L.name: torch.empty(27 * L.cout * L.cin, dtype=torch.bfloat16, device=self.dev) for L in LAYERS}
-        self.wt = {L.name: torch.empty_like(self.w[L.name]) for L in LAYERS}
+        lib = U.lib()
+        self.w = {L.name: torch.empty(lib.ccu_packed_weight_elems(L.cout, L.cin), dtype=torch.bfloat16,
+                                      device=self.dev) for L in LAYERS}
+        self.wt = {L.name: torch.empty(lib.ccu_packed_weight_elems(L.cin, L.cout), dtype=torch.bfloat16,
+                                       device=self.dev) for L in LAYERS}
         self.acc = torch.zeros(1, dtype=torch.float32, device=self.dev)      # loss
         self.shape = None
         self.launches = 0

@@ -33,11 +33,13 @@ int ccu_status(unsigned* status, int reset);
 /* 3x3x3 "same" convolution on the tensor cores (tcgen05, BF16 in, FP32
  * accumulation).  The input is a [B, d, h, w, ca] concatenated on channels
  * with b [B, d/2, h/2, w/2, cb] read nearest-upsampled (b NULL, cb 0 for a
- * plain input).  weight [27][cout][ca + cb] BF16 (tap = (dz+1)*9 + (dy+1)*3
- * + dx+1), bias [cout] FP32 or NULL, relu 0/1.  Output channels [0, split)
+ * plain input).  weight: BF16 weights of 27 taps x cout x (ca + cb)
+ * (tap = (dz+1)*9 + (dy+1)*3 + dx+1) in the packed order that
+ * ccu_pack_weights writes (ccu_packed_weight_elems(cout, ca + cb)
+ * elements); bias [cout] FP32 or NULL; relu 0/1.  Output channels [0, split)
  * go to out0 [.., split], multiplied by (mask0 > 0) when mask0 (same layout
  * as out0) is given; channels [split, cout) go to out1 [.., cout - split].
- * cout is one of 16, 32, 48, 64, 96, 128, 192. */
+ * cout is one of 16, 32, 48, 64, 96, 128, 192; B*d*h*w < 2^31. */
 int ccu_conv3d(const void* a, int ca, const void* b, int cb, int batch, int d, int h, int w, const void* weight,
                const float* bias, int cout, int relu, void* out0, int split, const void* mask0, void* out1,
                void* stream);
@@ -86,9 +88,14 @@ int ccu_input(const float* xlog, const float* density, const uint8_t* mat, int n
 int ccu_adam(float* p, const float* g, float* m, float* v, long long n, float lr, float b1, float b2, float eps,
              int step, float wd, void* stream);
 
-/* BF16 weights of a layer from its FP32 master copy w32[27][cout][cin]:
- * w (same layout) and, when wt is not NULL, wt[26 - tap][cin][cout] for
- * the backward-data convolution. */
+/* Elements of a packed weight array for n output and c input channels
+ * (both multiples of 16): 64 x n x ceil(27 c / 64); negative on error. */
+long long ccu_packed_weight_elems(int n, int c);
+
+/* BF16 weights of a layer from its FP32 master copy w32[27][cout][cin],
+ * packed for ccu_conv3d: w for the forward convolution (n = cout, c = cin)
+ * and, when wt is not NULL, wt for the backward-data convolution (n = cin,
+ * c = cout; taps flipped, channels transposed). */
 int ccu_pack_weights(const float* w32, int cout, int cin, void* w, void* wt, void* stream);
 
 /* cudaMemsetAsync(p, 0, bytes) on the stream (gradient buffers). */

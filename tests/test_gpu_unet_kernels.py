@@ -61,7 +61,9 @@ def test_conv3d_forward(U, ca, cb, cout, dims):
     B, D, H, W = dims
     a = _bf((B, D, H, W, ca), gen)
     b = _bf((B, D // 2, H // 2, W // 2, cb), gen) if cb else None
-    w = _bf((27, cout, ca + cb), gen, scale=0.1)
+    w32 = (torch.randn(27 * cout * (ca + cb), generator=gen) * 0.1).cuda()
+    w = torch.empty(U.lib().ccu_packed_weight_elems(cout, ca + cb), dtype=torch.bfloat16, device="cuda")
+    U.check(U.lib().ccu_pack_weights(_ptr(w32), cout, ca + cb, _ptr(w), None, None))
     bias = (torch.randn(cout, generator=gen) * 0.1).cuda()
     split = ca if cb and cout == ca + cb else cout
     out0 = torch.empty(B, D, H, W, split, dtype=torch.bfloat16, device="cuda")
@@ -74,7 +76,7 @@ def test_conv3d_forward(U, ca, cb, cout, dims):
     x = _to_ncdhw(a)
     if cb:
         x = torch.cat([x, _up(_to_ncdhw(b))], dim=1)
-    ref = torch.relu(torch.nn.functional.conv3d(x, _torch_w(w, cout, ca + cb), bias, padding=1))
+    ref = torch.relu(torch.nn.functional.conv3d(x, _torch_w(w32.to(torch.bfloat16), cout, ca + cb), bias, padding=1))
     ref = ref.permute(0, 2, 3, 4, 1)
     got = out0.float() if out1 is None else torch.cat([out0.float(), out1.float()], dim=-1)
     torch.testing.assert_close(got, ref, rtol=1.6e-2, atol=1e-2)
@@ -94,8 +96,8 @@ def test_conv3d_weight_and_data_gradients(U, ca, cb, cout, dims):
     b = torch.relu(_bf((B, D // 2, H // 2, W // 2, cb), gen).float()).to(torch.bfloat16) if cb else None
     dz = _bf((B, D, H, W, cout), gen)
     w32 = (torch.randn(27 * cout * cin, generator=gen) * 0.1).cuda()
-    wbf = torch.empty(27 * cout * cin, dtype=torch.bfloat16, device="cuda")
-    wt = torch.empty_like(wbf)
+    wbf = torch.empty(U.lib().ccu_packed_weight_elems(cout, cin), dtype=torch.bfloat16, device="cuda")
+    wt = torch.empty(U.lib().ccu_packed_weight_elems(cin, cout), dtype=torch.bfloat16, device="cuda")
     U.check(U.lib().ccu_pack_weights(_ptr(w32), cout, cin, _ptr(wbf), _ptr(wt), None))
     dw = torch.zeros(27 * cout * cin, dtype=torch.float32, device="cuda")
     U.check(U.lib().ccu_conv3d_wgrad(_ptr(a), ca, _ptr(b) if b is not None else None, cb, B, D, H, W, _ptr(dz),
@@ -112,7 +114,7 @@ def test_conv3d_weight_and_data_gradients(U, ca, cb, cout, dims):
     x = _to_ncdhw(a).requires_grad_(True)
     xb = _to_ncdhw(b).requires_grad_(True) if cb else None
     xin = torch.cat([x, _up(xb)], dim=1) if cb else x
-    wt_ref = _torch_w(wbf, cout, cin).requires_grad_(True)
+    wt_ref = _torch_w(w32.to(torch.bfloat16), cout, cin).requires_grad_(True)
     y = torch.nn.functional.conv3d(xin, wt_ref, None, padding=1)
     y.backward(_to_ncdhw(dz))
     dw_ref = wt_ref.grad.permute(2, 3, 4, 0, 1).reshape(-1)
