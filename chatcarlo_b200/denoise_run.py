@@ -217,6 +217,40 @@ def run(args) -> dict:
     }
 
 
+def timing(B: int, S: int, steps: int = 10, warmup: int = 3) -> dict:
+    """Device time of the forward pass and of a whole training step (forward,
+    backward, Adam) on B random volumes of side S, with CUDA events."""
+    import torch
+    rng = np.random.default_rng(0)
+    xlog = rng.normal(size=(B, S, S, S)).astype(np.float32)
+    mat = rng.integers(0, DN.N_MAT, size=(B, S, S, S)).astype(np.uint8)
+    dens = np.array([0.0012, 1.0, 1.85, 11.35], dtype=np.float32)[mat]
+    model = DN.UNet3D(seed=0)
+    ho = DN.param_layout()["head"][0]
+    model.p[ho:ho + DN.HEAD_CH] = 0.1
+    model.set_input(xlog, dens, mat, B, S)
+    tgt = torch.zeros(B * S ** 3, device=model.dev)
+    wgt = torch.ones_like(tgt)
+    for _ in range(warmup):
+        model.forward(); model.backward(tgt, wgt, 1.0 / tgt.numel()); model.step(1e-4)
+    torch.cuda.synchronize()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    ev[0].record()
+    for _ in range(steps):
+        model.forward()
+    ev[1].record()
+    for _ in range(steps):
+        model.forward(); model.backward(tgt, wgt, 1.0 / tgt.numel()); model.step(1e-4)
+    ev[2].record()
+    torch.cuda.synchronize()
+    model.check_status()
+    fwd = ev[0].elapsed_time(ev[1]) / steps
+    step = ev[1].elapsed_time(ev[2]) / steps
+    fl = DN.conv_flops(B, S)
+    return {"batch": B, "side": S, "forward_ms": fwd, "train_step_ms": step,
+            "forward_tflops": fl / fwd / 1e9, "train_tflops": 3 * fl / step / 1e9}
+
+
 def main(argv=None) -> None:
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--side", type=int, default=64)
@@ -232,8 +266,11 @@ def main(argv=None) -> None:
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--seed", type=int, default=7)
     ap.add_argument("--save", default=None, help="write the trained parameters (.npy)")
+    ap.add_argument("--timing", type=int, nargs=2, metavar=("B", "S"), default=None,
+                    help="only time the network's kernels on B random volumes of side S")
+    ap.add_argument("--timing-steps", type=int, default=10)
     args = ap.parse_args(argv)
-    res = run(args)
+    res = timing(*args.timing, steps=args.timing_steps) if args.timing else run(args)
     print(json.dumps(res))
 
 
