@@ -171,6 +171,8 @@ def main():
     ap.add_argument("--cpu-histories-per-process", type=int, default=120_000,
                     help="CPU sample per step: histories in each of the host-core processes")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-precision", action="store_true", help="skip the FP32-vs-FP64 tracking tally report")
+    ap.add_argument("--precision-histories", type=float, default=1e7)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -333,6 +335,19 @@ def main():
                        "d2h_bytes_per_step": ne * (3 + 3 + 1) * 8 + ne * (4 + 1 + 1) + 2 * nvox * 8,
                        "api": "chatcarlo_b200.transport.transport_photons (C ABI cc_transport_photons, pinned host arrays)"}
 
+    # precision: the same room run tracked in FP32 (the engine) and in FP64,
+    # every tally's difference against its own statistical error
+    precision = None
+    if rank == 0 and world == 1 and not args.no_precision:
+        from chatcarlo_b200.precision import tally_precision
+        from chatcarlo_b200.transport import Engine as _Engine
+        rep = tally_precision(raw, W.ROOM_GRID, int(args.precision_histories), seed + 999, batch_size=BATCH,
+                              engine32=eng, engine64=_Engine(eng.device, precision="fp64"))
+        precision = {"reference": "the same engine tracking in FP64, same seed and random numbers",
+                     "histories": rep["histories"],
+                     **{t: {k: rep[t][k] for k in ("rel_median", "rel_p99", "sigma_median", "sigma_p99",
+                                                   "sigma_max", "total_rel")} for t in ("kerma", "h10")}}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         per_core = args.cpu_histories_per_process
@@ -357,7 +372,8 @@ def main():
                              "voxel_visits_per_history": n_vox,
                              "avg_launch_ms": tr_ms / max(tr_launch, 1),
                              "histories_per_launch": hist_per_launch},
-                "cpu_baseline": cpu, "e2e": e2e, "e2e_photons": e2e_photons, "clocks": clocks,
+                "cpu_baseline": cpu, "e2e": e2e, "e2e_photons": e2e_photons, "precision": precision,
+                "clocks": clocks,
                 "gpu_launches": int(launches),
                 "reduce_ms": red_ms}
         print(json.dumps(line))

@@ -12,6 +12,9 @@ import os
 
 LIB_PATH = Path(os.environ.get("CHATCARLO_B200_LIB") or
                 Path(__file__).resolve().parent / "lib" / "libccb200.so")
+# the same engine built with FP64 tracking (the precision reference)
+FP64_LIB_PATH = Path(os.environ.get("CHATCARLO_B200_FP64_LIB") or
+                     Path(__file__).resolve().parent / "lib" / "libccb200_fp64.so")
 
 CC_OK = 0
 CC_E_INVALID = -1
@@ -96,7 +99,7 @@ class RunOut(C.Structure):
 
 P = C.c_void_p
 PD = C.POINTER(C.c_double)
-_lib = None
+_libs: dict = {}
 
 
 def _bind(lib):
@@ -139,29 +142,31 @@ def _bind(lib):
         f.argtypes = args
 
 
-def lib():
-    """The loaded engine library (loaded once)."""
-    global _lib
-    if _lib is None:
-        if not LIB_PATH.exists():
+def lib(path: Path | None = None):
+    """The loaded engine library (each path loaded once); the FP32-tracking
+    build unless another path is given."""
+    path = Path(path) if path is not None else LIB_PATH
+    handle = _libs.get(path)
+    if handle is None:
+        if not path.exists():
             raise NativeLibraryError(
-                f"{LIB_PATH} is missing; build it with `python -m chatcarlo_b200.build`")
+                f"{path} is missing; build it with `python -m chatcarlo_b200.build`")
         try:
-            handle = C.CDLL(str(LIB_PATH))
+            handle = C.CDLL(str(path))
         except OSError as e:
-            raise NativeLibraryError(f"cannot load {LIB_PATH}: {e}") from e
+            raise NativeLibraryError(f"cannot load {path}: {e}") from e
         _bind(handle)
-        _lib = handle
-    return _lib
+        _libs[path] = handle
+    return handle
 
 
 _PY_ERRORS = {CC_E_ENERGY_RANGE: ValueError, CC_E_RAYLEIGH_Q_RANGE: ValueError,
               CC_E_UNKNOWN_MATERIAL: ValueError, CC_E_BAD_SHAPE: ValueError, CC_E_INVALID: ValueError}
 
 
-def check(rc: int) -> None:
+def check(rc: int, handle=None) -> None:
     if rc != CC_OK:
-        msg = lib().cc_last_error().decode(errors="replace")
+        msg = (handle or lib()).cc_last_error().decode(errors="replace")
         exc = _PY_ERRORS.get(rc)
         if exc is not None:
             raise exc(f"[{rc}] {msg}")

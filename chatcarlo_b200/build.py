@@ -1,5 +1,7 @@
-"""Compile the engine into chatcarlo_b200/lib/libccb200.so and the learned
-denoiser's kernels into chatcarlo_b200/lib/libccunet.so (sm_100a).
+"""Compile the engine into chatcarlo_b200/lib/libccb200.so (FP32 tracking)
+and libccb200_fp64.so (the same source tracking in FP64, the precision
+reference), and the learned denoiser's kernels into
+chatcarlo_b200/lib/libccunet.so (sm_100a).
 
 ``python -m chatcarlo_b200.build`` rebuilds a library when one of its
 sources is newer than it.  The libraries link the CUDA runtime statically so
@@ -20,6 +22,7 @@ LIB_PATH = LIB_DIR / "libccb200.so"
 HEADER = PKG.parent / "include" / "chatcarlo_b200.h"
 SOURCES = [CSRC / "cc_engine.cu"]
 DEPS = SOURCES + [CSRC / "philox.cuh", HEADER]
+FP64_LIB_PATH = LIB_DIR / "libccb200_fp64.so"
 UNET_LIB_PATH = LIB_DIR / "libccunet.so"
 UNET_SOURCES = [CSRC / "cc_unet.cu"]
 UNET_DEPS = UNET_SOURCES + [PKG.parent / "include" / "chatcarlo_b200_unet.h"]
@@ -30,6 +33,10 @@ UNET_DEPS = UNET_SOURCES + [PKG.parent / "include" / "chatcarlo_b200_unet.h"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
               "--use_fast_math", "-Xcompiler", "-fPIC", "-shared", "-cudart", "static"]
 
+
+# the precision reference: the engine tracking in FP64 (more registers per
+# thread, so two blocks per SM)
+FP64_NVCC_FLAGS = NVCC_FLAGS + ["-DCC_TRACK_FP64", "-DCC_MIN_BLOCKS=2"]
 
 # the denoiser's kernels keep IEEE arithmetic (their gradients are checked
 # against an FP64 oracle)
@@ -49,7 +56,7 @@ def _stale(lib: Path, deps: list[Path]) -> bool:
 
 
 def needs_build() -> bool:
-    return _stale(LIB_PATH, DEPS) or _stale(UNET_LIB_PATH, UNET_DEPS)
+    return _stale(LIB_PATH, DEPS) or _stale(FP64_LIB_PATH, DEPS) or _stale(UNET_LIB_PATH, UNET_DEPS)
 
 
 def _compile(lib: Path, sources: list[Path], flags: list[str], verbose: bool) -> None:
@@ -71,6 +78,8 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     """Build both libraries where stale; returns the engine's path."""
     if force or _stale(LIB_PATH, DEPS):
         _compile(LIB_PATH, SOURCES, NVCC_FLAGS, verbose)
+    if force or _stale(FP64_LIB_PATH, DEPS):
+        _compile(FP64_LIB_PATH, SOURCES, FP64_NVCC_FLAGS, verbose)
     if force or _stale(UNET_LIB_PATH, UNET_DEPS):
         _compile(UNET_LIB_PATH, UNET_SOURCES, UNET_NVCC_FLAGS, verbose)
     return LIB_PATH
@@ -79,4 +88,5 @@ def build(force: bool = False, verbose: bool = False) -> Path:
 if __name__ == "__main__":
     build(force="--force" in sys.argv, verbose="-v" in sys.argv)
     print(LIB_PATH)
+    print(FP64_LIB_PATH)
     print(UNET_LIB_PATH)

@@ -56,13 +56,26 @@ constexpr float TWO_PI = 6.283185307179586f;
 // status bits
 constexpr unsigned ST_ENERGY = 1u, ST_RAYLEIGH_Q = 2u, ST_STEPS = 4u, ST_BOUNDS = 8u;
 
+// Tracking precision: positions, directions, distances and the geometry they
+// meet.  The engine tracks in FP32; a second build of this file with
+// -DCC_TRACK_FP64 tracks in FP64 with the same random numbers and the same
+// FP32 physics, so that each tally's cost of FP32 tracking can be measured
+// against it.
+#ifdef CC_TRACK_FP64
+typedef double real;
+#else
+typedef float real;
+#endif
+__device__ __forceinline__ float rsqrt_r(float x) { return rsqrtf(x); }
+__device__ __forceinline__ double rsqrt_r(double x) { return rsqrt(x); }
+
 struct DevPrim {
     int type, material, axis, pad;
-    float c[3];
-    float h[3];     // box half sizes, ellipsoid semi-axes
-    float r2;       // radius^2
-    float r;        // radius; ellipsoid: 1 / smallest semi-axis
-    float hh;       // cylinder half height
+    real c[3];
+    real h[3];      // box half sizes, ellipsoid semi-axes
+    real r2;        // radius^2
+    real r;         // radius; ellipsoid: 1 / smallest semi-axis
+    real hh;        // cylinder half height
 };
 
 struct DevMaterial {
@@ -97,14 +110,15 @@ struct KTables {
 struct KScene {
     DevPrim prims[MAX_PRIMS];
     int n_prims, background;
-    float wlo[3], whi[3];
-    float eps;        // surface band half-width and smallest root (cm): 8 ulps of the world's FP32 extent
+    real wlo[3], whi[3];
+    real eps;         // surface band half-width and smallest root (cm): 8 ulps of the world's FP32 extent
+                      // (FP32 tracking) or 1e-6 cm (FP64 tracking, transport.py:155)
 };
 
 struct KGrid {
     double* tally;          // [n_scratch][nvox] double2 (kerma, h10)
-    float o[3];
-    float h, inv_h;
+    real o[3];
+    real h, inv_h;
     int nx, ny, nz;
     long long nvox;
     int enabled;
@@ -148,10 +162,10 @@ struct KRun {
 // geometry
 // ---------------------------------------------------------------------------
 
-__device__ __forceinline__ float fmin3(float a, float b, float c) { return fminf(a, fminf(b, c)); }
-__device__ __forceinline__ float fmax3(float a, float b, float c) { return fmaxf(a, fmaxf(b, c)); }
+__device__ __forceinline__ real fmin3(real a, real b, real c) { return fmin(a, fmin(b, c)); }
+__device__ __forceinline__ real fmax3(real a, real b, real c) { return fmax(a, fmax(b, c)); }
 
-// Positions are FP32, so a photon that has just reached a surface sits
+// Positions are FP32 (or FP64), so a photon that has just reached a surface sits
 // within a few ulps (of the world's largest coordinate) of it on either
 // side.  Points inside that band, of half-width tol, are classified by
 // their direction: on a surface, a photon is inside the primitive when it
@@ -166,23 +180,23 @@ __device__ __forceinline__ float fmax3(float a, float b, float c) { return fmaxf
 // order ulp / |radial direction|, can be far above tol at grazing angles.
 
 // Inside the slab |o| <= h, deciding points on a face by the direction d.
-__device__ __forceinline__ bool slab_inside(float o, float d, float h, float tol) {
-    float a = fabsf(o);
+__device__ __forceinline__ bool slab_inside(real o, real d, real h, real tol) {
+    real a = fabs(o);
     if (a < h - tol) return true;
     if (a > h + tol) return false;
     return o * d <= 0.0f;
 }
 
 // Inside the ball |o| <= r (o with n components folded into o2 = |o|^2 and od = o.d).
-__device__ __forceinline__ bool ball_inside(float o2, float od, float r, float tol) {
-    float lo = fmaxf(r - tol, 0.0f), hi = r + tol;
+__device__ __forceinline__ bool ball_inside(real o2, real od, real r, real tol) {
+    real lo = fmax(r - tol, (real)0), hi = r + tol;
     if (o2 < lo * lo) return true;
     if (o2 > hi * hi) return false;
     return od <= 0.0f;
 }
 
-__device__ __forceinline__ bool contains(const DevPrim& g, const float p[3], const float d[3], float tol) {
-    float o0 = p[0] - g.c[0], o1 = p[1] - g.c[1], o2 = p[2] - g.c[2];
+__device__ __forceinline__ bool contains(const DevPrim& g, const real p[3], const real d[3], real tol) {
+    real o0 = p[0] - g.c[0], o1 = p[1] - g.c[1], o2 = p[2] - g.c[2];
     if (g.type == CC_SHAPE_BOX) {
         return slab_inside(o0, d[0], g.h[0], tol) && slab_inside(o1, d[1], g.h[1], tol) &&
                slab_inside(o2, d[2], g.h[2], tol);
@@ -191,19 +205,19 @@ __device__ __forceinline__ bool contains(const DevPrim& g, const float p[3], con
     } else if (g.type == CC_SHAPE_ELLIPSOID) {
         // the unit ball in coordinates scaled by the semi-axes; the band
         // scaled by the smallest semi-axis covers the tol band everywhere
-        float u0 = o0 / g.h[0], u1 = o1 / g.h[1], u2 = o2 / g.h[2];
+        real u0 = o0 / g.h[0], u1 = o1 / g.h[1], u2 = o2 / g.h[2];
         return ball_inside(u0 * u0 + u1 * u1 + u2 * u2,
                            u0 * d[0] / g.h[0] + u1 * d[1] / g.h[1] + u2 * d[2] / g.h[2], 1.0f, tol * g.r);
     } else {
         const int ax = g.axis;
         const int i0 = ax == 0 ? 1 : 0, i1 = ax == 2 ? 1 : 2;
-        float oa = p[i0] - g.c[i0], ob = p[i1] - g.c[i1], ow = p[ax] - g.c[ax];
+        real oa = p[i0] - g.c[i0], ob = p[i1] - g.c[i1], ow = p[ax] - g.c[ax];
         return ball_inside(oa * oa + ob * ob, oa * d[i0] + ob * d[i1], g.r, tol) &&
                slab_inside(ow, d[ax], g.hh, tol);
     }
 }
 
-__device__ __forceinline__ int locate(const KScene& s, const float p[3], const float d[3]) {
+__device__ __forceinline__ int locate(const KScene& s, const real p[3], const real d[3]) {
     int m = s.background;
     for (int i = 0; i < s.n_prims; ++i)
         if (contains(s.prims[i], p, d, s.eps)) m = s.prims[i].material;
@@ -214,84 +228,84 @@ __device__ __forceinline__ int locate(const KScene& s, const float p[3], const f
 // (o = p - c relative coordinate, tol the band of this face); a face the
 // point sits on contributes t = 0.  Returns false for a ray parallel to the
 // slab outside it.
-__device__ __forceinline__ bool slab_pair(float o, float d, float inv, float lo, float hi, float tol,
-                                          float& tmin, float& tmax) {
-    float dlo = lo - o, dhi = hi - o;
-    if (fabsf(dlo) <= tol) dlo = 0.0f;
-    if (fabsf(dhi) <= tol) dhi = 0.0f;
-    if (fabsf(d) < 1e-12f) return dlo <= 0.0f && dhi >= 0.0f;
-    float ta = dlo * inv, tb = dhi * inv;
-    tmin = fmaxf(tmin, fminf(ta, tb));
-    tmax = fminf(tmax, fmaxf(ta, tb));
+__device__ __forceinline__ bool slab_pair(real o, real d, real inv, real lo, real hi, real tol,
+                                          real& tmin, real& tmax) {
+    real dlo = lo - o, dhi = hi - o;
+    if (fabs(dlo) <= tol) dlo = 0.0f;
+    if (fabs(dhi) <= tol) dhi = 0.0f;
+    if (fabs(d) < 1e-12f) return dlo <= 0.0f && dhi >= 0.0f;
+    real ta = dlo * inv, tb = dhi * inv;
+    tmin = fmax(tmin, fmin(ta, tb));
+    tmax = fmin(tmax, fmax(ta, tb));
     return true;
 }
 
-__device__ __forceinline__ void take_root(float t, float eps, float& best) {
+__device__ __forceinline__ void take_root(real t, real eps, real& best) {
     if (t > eps && t < best) best = t;
 }
 
 // Smallest root t > eps of primitive g along the ray (geometry.py:20-99), or best.
-__device__ float prim_next(const DevPrim& g, const float p[3], const float d[3], const float inv[3], float eps,
-                           float best) {
-    float ox = p[0] - g.c[0], oy = p[1] - g.c[1], oz = p[2] - g.c[2];
+__device__ real prim_next(const DevPrim& g, const real p[3], const real d[3], const real inv[3], real eps,
+                           real best) {
+    real ox = p[0] - g.c[0], oy = p[1] - g.c[1], oz = p[2] - g.c[2];
     if (g.type == CC_SHAPE_BOX) {
-        float tmin = -INFINITY, tmax = INFINITY;
+        real tmin = -INFINITY, tmax = INFINITY;
         if (!slab_pair(ox, d[0], inv[0], -g.h[0], g.h[0], eps, tmin, tmax)) return best;
         if (!slab_pair(oy, d[1], inv[1], -g.h[1], g.h[1], eps, tmin, tmax)) return best;
         if (!slab_pair(oz, d[2], inv[2], -g.h[2], g.h[2], eps, tmin, tmax)) return best;
         if (tmin <= tmax) { take_root(tmin, eps, best); take_root(tmax, eps, best); }
         return best;
     } else if (g.type == CC_SHAPE_SPHERE) {
-        float b = ox * d[0] + oy * d[1] + oz * d[2];
-        float o2 = ox * ox + oy * oy + oz * oz;
-        float lo = fmaxf(g.r - eps, 0.0f), hi = g.r + eps;
+        real b = ox * d[0] + oy * d[1] + oz * d[2];
+        real o2 = ox * ox + oy * oy + oz * oz;
+        real lo = fmax(g.r - eps, (real)0), hi = g.r + eps;
         if (o2 >= lo * lo && o2 <= hi * hi) {          // on the surface
             if (b <= 0.0f) take_root(-2.0f * b, eps, best);
             return best;
         }
         // squared distance of the line from the centre, computed without cancellation
-        float qx = ox - b * d[0], qy = oy - b * d[1], qz = oz - b * d[2];
-        float disc = g.r2 - (qx * qx + qy * qy + qz * qz);
+        real qx = ox - b * d[0], qy = oy - b * d[1], qz = oz - b * d[2];
+        real disc = g.r2 - (qx * qx + qy * qy + qz * qz);
         if (disc < 0.0f) return best;
-        float sq = sqrtf(disc);
-        float c = o2 - g.r2;
-        float q = -(b + copysignf(sq, b));
-        float t1 = q, t2 = (q != 0.0f) ? c / q : 0.0f;
+        real sq = sqrt(disc);
+        real c = o2 - g.r2;
+        real q = -(b + copysign(sq, b));
+        real t1 = q, t2 = (q != 0.0f) ? c / q : 0.0f;
         take_root(t1, eps, best);
         take_root(t2, eps, best);
         return best;
     } else if (g.type == CC_SHAPE_ELLIPSOID) {
         // |u + t v|^2 = 1 with u = o / h, v = d / h (componentwise)
-        float ux = ox / g.h[0], uy = oy / g.h[1], uz = oz / g.h[2];
-        float vx = d[0] / g.h[0], vy = d[1] / g.h[1], vz = d[2] / g.h[2];
-        float a = vx * vx + vy * vy + vz * vz;
-        float b = ux * vx + uy * vy + uz * vz;
-        float u2 = ux * ux + uy * uy + uz * uz;
-        float tl = eps * g.r;
-        float lo = fmaxf(1.0f - tl, 0.0f), hi = 1.0f + tl;
+        real ux = ox / g.h[0], uy = oy / g.h[1], uz = oz / g.h[2];
+        real vx = d[0] / g.h[0], vy = d[1] / g.h[1], vz = d[2] / g.h[2];
+        real a = vx * vx + vy * vy + vz * vz;
+        real b = ux * vx + uy * vy + uz * vz;
+        real u2 = ux * ux + uy * uy + uz * uz;
+        real tl = eps * g.r;
+        real lo = fmax(1.0f - tl, (real)0), hi = 1.0f + tl;
         if (u2 >= lo * lo && u2 <= hi * hi) {            // on the surface
             if (b <= 0.0f) take_root(-2.0f * b / a, eps, best);
             return best;
         }
-        float inva = 1.0f / a;
-        float ex = ux - b * inva * vx, ey = uy - b * inva * vy, ez = uz - b * inva * vz;
-        float disc = (1.0f - (ex * ex + ey * ey + ez * ez)) * a;   // b^2 - a c without cancellation
+        real inva = 1.0f / a;
+        real ex = ux - b * inva * vx, ey = uy - b * inva * vy, ez = uz - b * inva * vz;
+        real disc = (1.0f - (ex * ex + ey * ey + ez * ez)) * a;   // b^2 - a c without cancellation
         if (disc < 0.0f) return best;
-        float q = -(b + copysignf(sqrtf(disc), b));
+        real q = -(b + copysign(sqrt(disc), b));
         take_root(q * inva, eps, best);
         take_root((q != 0.0f) ? (u2 - 1.0f) / q : 0.0f, eps, best);
         return best;
     } else {
         const int ax = g.axis;
         const int i0 = ax == 0 ? 1 : 0, i1 = ax == 2 ? 1 : 2;
-        float a0 = p[i0] - g.c[i0], a1 = p[i1] - g.c[i1], aw = p[ax] - g.c[ax];
-        float dx = d[i0], dy = d[i1], dw = d[ax];
-        float a = dx * dx + dy * dy;
-        float rho2 = a0 * a0 + a1 * a1;
-        float cc = rho2 - g.r2;
-        float tmin, tmax;
-        float b = a0 * dx + a1 * dy;
-        float lo = fmaxf(g.r - eps, 0.0f), hi = g.r + eps;
+        real a0 = p[i0] - g.c[i0], a1 = p[i1] - g.c[i1], aw = p[ax] - g.c[ax];
+        real dx = d[i0], dy = d[i1], dw = d[ax];
+        real a = dx * dx + dy * dy;
+        real rho2 = a0 * a0 + a1 * a1;
+        real cc = rho2 - g.r2;
+        real tmin, tmax;
+        real b = a0 * dx + a1 * dy;
+        real lo = fmax(g.r - eps, (real)0), hi = g.r + eps;
         if (rho2 >= lo * lo && rho2 <= hi * hi) {      // on the side surface
             if (b > 0.0f) return best;
             tmin = 0.0f;
@@ -300,14 +314,14 @@ __device__ float prim_next(const DevPrim& g, const float p[3], const float d[3],
             if (cc > 0.0f) return best;        // parallel to the axis, outside the radius
             tmin = -INFINITY; tmax = INFINITY;
         } else {
-            float inva = 1.0f / a;
-            float ex = a0 - b * inva * dx, ey = a1 - b * inva * dy;
-            float disc = (g.r2 - (ex * ex + ey * ey)) * a;   // b^2 - a c without cancellation
+            real inva = 1.0f / a;
+            real ex = a0 - b * inva * dx, ey = a1 - b * inva * dy;
+            real disc = (g.r2 - (ex * ex + ey * ey)) * a;   // b^2 - a c without cancellation
             if (disc < 0.0f) return best;
-            float sq = sqrtf(disc);
-            float q = -(b + copysignf(sq, b));
-            float r1 = q * inva, r2 = (q != 0.0f) ? cc / q : 0.0f;
-            tmin = fminf(r1, r2); tmax = fmaxf(r1, r2);
+            real sq = sqrt(disc);
+            real q = -(b + copysign(sq, b));
+            real r1 = q * inva, r2 = (q != 0.0f) ? cc / q : 0.0f;
+            tmin = fmin(r1, r2); tmax = fmax(r1, r2);
         }
         if (!slab_pair(aw, dw, inv[ax], -g.hh, g.hh, eps, tmin, tmax)) return best;
         if (tmin <= tmax) { take_root(tmin, eps, best); take_root(tmax, eps, best); }
@@ -316,15 +330,15 @@ __device__ float prim_next(const DevPrim& g, const float p[3], const float d[3],
 }
 
 // Distance to the world-box exit.
-__device__ __forceinline__ float world_exit(const KScene& s, const float p[3], const float d[3],
-                                            const float inv[3]) {
-    float t = INFINITY;
+__device__ __forceinline__ real world_exit(const KScene& s, const real p[3], const real d[3],
+                                            const real inv[3]) {
+    real t = INFINITY;
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-        if (d[k] > 1e-12f) t = fminf(t, (s.whi[k] - p[k]) * inv[k]);
-        else if (d[k] < -1e-12f) t = fminf(t, (s.wlo[k] - p[k]) * inv[k]);
+        if (d[k] > 1e-12f) t = fmin(t, (s.whi[k] - p[k]) * inv[k]);
+        else if (d[k] < -1e-12f) t = fmin(t, (s.wlo[k] - p[k]) * inv[k]);
     }
-    return fmaxf(t, 0.0f);
+    return fmax(t, (real)0);
 }
 
 // ---------------------------------------------------------------------------
@@ -466,31 +480,33 @@ __device__ __noinline__ bool sample_rayleigh(const float* rx, const float* ra, c
 }
 
 // New direction from cos(theta) and a uniform azimuth (physics.py:354-367).
-__device__ __noinline__ float3 scatter_dir(float dx, float dy, float dz, float cost, float phi) {
-    const float d[3] = {dx, dy, dz};
-    float sint = sqrtf(fmaxf(0.0f, 1.0f - cost * cost));
-    float upx, upy, upz;
-    if (fabsf(d[2]) < 0.999f) { upx = 0.f; upy = 0.f; upz = 1.f; } else { upx = 1.f; upy = 0.f; upz = 0.f; }
-    float ux = upy * d[2] - upz * d[1], uy = upz * d[0] - upx * d[2], uz = upx * d[1] - upy * d[0];
-    float inv = rsqrtf(ux * ux + uy * uy + uz * uz);
+struct real3 { real x, y, z; };
+
+__device__ __noinline__ real3 scatter_dir(real dx, real dy, real dz, float cost, float phi) {
+    const real d[3] = {dx, dy, dz};
+    real sint = sqrt(fmax((real)0, (real)1 - (real)cost * (real)cost));
+    real upx, upy, upz;
+    if (fabs(d[2]) < (real)0.999f) { upx = 0; upy = 0; upz = 1; } else { upx = 1; upy = 0; upz = 0; }
+    real ux = upy * d[2] - upz * d[1], uy = upz * d[0] - upx * d[2], uz = upx * d[1] - upy * d[0];
+    real inv = rsqrt_r(ux * ux + uy * uy + uz * uz);
     ux *= inv; uy *= inv; uz *= inv;
-    float vx = d[1] * uz - d[2] * uy, vy = d[2] * ux - d[0] * uz, vz = d[0] * uy - d[1] * ux;
+    real vx = d[1] * uz - d[2] * uy, vy = d[2] * ux - d[0] * uz, vz = d[0] * uy - d[1] * ux;
     float sp, cp;
     __sincosf(phi, &sp, &cp);
-    float a = sint * cp, b = sint * sp;
-    float nx = a * ux + b * vx + cost * d[0];
-    float ny = a * uy + b * vy + cost * d[1];
-    float nz = a * uz + b * vz + cost * d[2];
-    float n = rsqrtf(nx * nx + ny * ny + nz * nz);
-    return make_float3(nx * n, ny * n, nz * n);
+    real a = sint * cp, b = sint * sp;
+    real nx = a * ux + b * vx + cost * d[0];
+    real ny = a * uy + b * vy + cost * d[1];
+    real nz = a * uz + b * vz + cost * d[2];
+    real n = rsqrt_r(nx * nx + ny * ny + nz * nz);
+    return real3{nx * n, ny * n, nz * n};
 }
 
-__device__ __forceinline__ void scatter_direction(float d[3], float cost, float phi) {
-    float3 r = scatter_dir(d[0], d[1], d[2], cost, phi);
+__device__ __forceinline__ void scatter_direction(real d[3], float cost, float phi) {
+    real3 r = scatter_dir(d[0], d[1], d[2], cost, phi);
     d[0] = r.x; d[1] = r.y; d[2] = r.z;
 }
 
-__device__ void isotropic(float d[3], HistoryRng& rng) {
+__device__ void isotropic(real d[3], HistoryRng& rng) {
     float c = 2.0f * rng.uniform() - 1.0f;
     float s = sqrtf(fmaxf(0.0f, 1.0f - c * c));
     float sp, cp;
@@ -502,27 +518,27 @@ __device__ void isotropic(float d[3], HistoryRng& rng) {
 // track-length tally: exact voxel traversal (Amanatides & Woo)
 // ---------------------------------------------------------------------------
 
-__device__ __forceinline__ void score(double* tally, int v, float wk_len, float wh_len) {
+__device__ __forceinline__ void score(double* tally, int v, real wk_len, real wh_len) {
     atomicAdd(tally + 2 * v, (double)wk_len);
     atomicAdd(tally + 2 * v + 1, (double)wh_len);
 }
 
 // Clip the ray p + t d, t in [0, s], to the grid box.  Returns false when
 // no part of it lies inside.
-__device__ __forceinline__ bool clip_to_grid(const KGrid& G, const float p[3], const float d[3],
-                                             const float invd[3], float s, float& t0, float& t1) {
+__device__ __forceinline__ bool clip_to_grid(const KGrid& G, const real p[3], const real d[3],
+                                             const real invd[3], real s, real& t0, real& t1) {
     t0 = 0.0f;
     t1 = s;
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-        float lo = G.o[k];
-        float hi = G.o[k] + G.h * (float)(k == 0 ? G.nx : (k == 1 ? G.ny : G.nz));
-        if (fabsf(d[k]) < 1e-12f) {
+        real lo = G.o[k];
+        real hi = G.o[k] + G.h * (real)(k == 0 ? G.nx : (k == 1 ? G.ny : G.nz));
+        if (fabs(d[k]) < 1e-12f) {
             if (p[k] < lo || p[k] >= hi) return false;
         } else {
-            float ta = (lo - p[k]) * invd[k], tb = (hi - p[k]) * invd[k];
-            t0 = fmaxf(t0, fminf(ta, tb));
-            t1 = fminf(t1, fmaxf(ta, tb));
+            real ta = (lo - p[k]) * invd[k], tb = (hi - p[k]) * invd[k];
+            t0 = fmax(t0, fmin(ta, tb));
+            t1 = fmin(t1, fmax(ta, tb));
         }
     }
     return t1 > t0;
@@ -531,13 +547,13 @@ __device__ __forceinline__ bool clip_to_grid(const KGrid& G, const float p[3], c
 __device__ __forceinline__ int grid_dim(const KGrid& G, int k) { return k == 0 ? G.nx : (k == 1 ? G.ny : G.nz); }
 
 // Number of voxels the clipped range [t0, t1] crosses (for load balancing).
-__device__ __forceinline__ int visit_estimate(const KGrid& G, const float p[3], const float d[3], float t0, float t1) {
+__device__ __forceinline__ int visit_estimate(const KGrid& G, const real p[3], const real d[3], real t0, real t1) {
     int n = 1;
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
         int nk = grid_dim(G, k);
-        int a = max(0, min(nk - 1, (int)floorf((p[k] + d[k] * t0 - G.o[k]) * G.inv_h)));
-        int b = max(0, min(nk - 1, (int)floorf((p[k] + d[k] * t1 - G.o[k]) * G.inv_h)));
+        int a = max(0, min(nk - 1, (int)floor((p[k] + d[k] * t0 - G.o[k]) * G.inv_h)));
+        int b = max(0, min(nk - 1, (int)floor((p[k] + d[k] * t1 - G.o[k]) * G.inv_h)));
         n += abs(b - a);
     }
     return n;
@@ -545,27 +561,27 @@ __device__ __forceinline__ int visit_estimate(const KGrid& G, const float p[3], 
 
 // Exact voxel traversal (Amanatides & Woo) of p + t d over [t0, t1], which
 // lies inside the grid box; scores weight x overlap length per voxel.
-__device__ int walk_range(const KGrid& G, double* tally, const float p[3], const float d[3],
-                          float t0, float t1, float wk, float wh) {
+__device__ int walk_range(const KGrid& G, double* tally, const real p[3], const real d[3],
+                          real t0, real t1, float wk, float wh) {
     int iv[3], step[3];
-    float tmax[3], tdel[3];
+    real tmax[3], tdel[3];
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
         // voxel of the entry point; a point that rounds onto the far side of
         // a face gets a zero-length first cell and steps back in
         int nk = grid_dim(G, k);
-        float x = (p[k] + d[k] * t0 - G.o[k]) * G.inv_h;
-        int i = max(0, min(nk - 1, (int)floorf(x)));
+        real x = (p[k] + d[k] * t0 - G.o[k]) * G.inv_h;
+        int i = max(0, min(nk - 1, (int)floor(x)));
         iv[k] = i;
         if (d[k] > 1e-12f) {
-            float inv = 1.0f / d[k];
+            real inv = 1.0f / d[k];
             step[k] = 1;
-            tmax[k] = (G.o[k] + (float)(i + 1) * G.h - p[k]) * inv;
+            tmax[k] = (G.o[k] + (real)(i + 1) * G.h - p[k]) * inv;
             tdel[k] = G.h * inv;
         } else if (d[k] < -1e-12f) {
-            float inv = 1.0f / d[k];
+            real inv = 1.0f / d[k];
             step[k] = -1;
-            tmax[k] = (G.o[k] + (float)i * G.h - p[k]) * inv;
+            tmax[k] = (G.o[k] + (real)i * G.h - p[k]) * inv;
             tdel[k] = -G.h * inv;
         } else {
             step[k] = 0;
@@ -573,7 +589,7 @@ __device__ int walk_range(const KGrid& G, double* tally, const float p[3], const
             tdel[k] = INFINITY;
         }
     }
-    float t = t0;
+    real t = t0;
     int guard = G.nx + G.ny + G.nz + 4;
     int visits = 0;
     // flat index (C order, tally.py:292) updated incrementally; grids are < 2^31 voxels
@@ -581,8 +597,8 @@ __device__ int walk_range(const KGrid& G, double* tally, const float p[3], const
     int v = (iv[0] * G.ny + iv[1]) * G.nz + iv[2];
     while (t < t1 && guard-- > 0) {
         int ax = (tmax[0] < tmax[1]) ? (tmax[0] < tmax[2] ? 0 : 2) : (tmax[1] < tmax[2] ? 1 : 2);
-        float tn = fminf(tmax[ax], t1);
-        float len = tn - t;
+        real tn = fmin(tmax[ax], t1);
+        real len = tn - t;
         if (len > 0.0f) {
             score(tally, v, wk * len, wh * len);
             ++visits;
@@ -599,8 +615,8 @@ __device__ int walk_range(const KGrid& G, double* tally, const float p[3], const
 
 // Track segments of one warp, shared so that the warp can split long ones.
 struct SegRec {
-    float p[3], d[3];
-    float t0, t1;
+    real p[3], d[3];
+    real t0, t1;
     float wk, wh;
     int batch, m;
 };
@@ -617,7 +633,7 @@ __device__ void rotate(float v[3], int axis, float ca, float sa) {
     else { v[0] = a0 * ca - a1 * sa; v[1] = a0 * sa + a1 * ca; }
 }
 
-__device__ void sample_source(const KSource& S, HistoryRng& rng, float p[3], float d[3], float& E) {
+__device__ void sample_source(const KSource& S, HistoryRng& rng, real p[3], real d[3], float& E) {
     float pos[3] = {S.pos[0], S.pos[1], S.pos[2]};
     float dir[3] = {S.dir[0], S.dir[1], S.dir[2]};
     float u[3] = {S.u[0], S.u[1], S.u[2]};
@@ -728,7 +744,8 @@ transport_kernel(const KTables T, const KScene S, const KGrid G, const KSource S
     long long pool_next = 0, pool_end = 0;
     bool live = false;
     long long h = 0;
-    float p[3], d[3], E = 0.f, tau = 0.f;
+    real p[3], d[3];
+    float E = 0.f, tau = 0.f;
     int nsc = 0, mat = -1, batch = 0;
     long long steps = 0;
     HistoryRng rng;
@@ -759,8 +776,8 @@ transport_kernel(const KTables T, const KScene S, const KGrid G, const KSource S
                     sample_source(SRC, rng, p, d, E);
                 } else {
                     for (int k = 0; k < 3; ++k) {
-                        p[k] = (float)R.pos[3 * h + k];
-                        d[k] = (float)R.dir[3 * h + k];
+                        p[k] = (real)R.pos[3 * h + k];
+                        d[k] = (real)R.dir[3 * h + k];
                     }
                     E = (float)R.energy[h];
                 }
@@ -777,8 +794,8 @@ transport_kernel(const KTables T, const KScene S, const KGrid G, const KSource S
         // ---- phase 1b: material, mu, next boundary ----
         bool go = live;
         bool interact = false, escape = false;
-        float s = 0.f, tau_b = 0.f, loge = 0.f;
-        float t0 = 0.f, t1 = 0.f, wk = 0.f, wh = 0.f;
+        real s = 0, t0 = 0, t1 = 0;
+        float tau_b = 0.f, loge = 0.f, wk = 0.f, wh = 0.f;
         int tal_n = 0;
         Lookup L;
         L.idx = 0;
@@ -799,15 +816,15 @@ transport_kernel(const KTables T, const KScene S, const KGrid G, const KSource S
             loge = __logf(E);
             L = energy_index(T, M, loge);
             float mu = mu_total(T, M, L);
-            const float invd[3] = {1.0f / d[0], 1.0f / d[1], 1.0f / d[2]};
-            float tb = INFINITY;
+            const real invd[3] = {(real)1 / d[0], (real)1 / d[1], (real)1 / d[2]};
+            real tb = INFINITY;
             for (int i = 0; i < S.n_prims; ++i) tb = prim_next(S.prims[i], p, d, invd, S.eps, tb);
-            float tw = world_exit(S, p, d, invd);
+            real tw = world_exit(S, p, d, invd);
             escape = tw <= tb;
-            tb = fminf(tb, tw);
-            tau_b = mu * tb;
+            tb = fmin(tb, tw);
+            tau_b = (float)(mu * tb);
             interact = tau < tau_b;
-            s = interact ? tau / fmaxf(mu, 1e-30f) : tb;
+            s = interact ? (real)tau / (real)fmaxf(mu, 1e-30f) : tb;
             if (TALLY && clip_to_grid(G, p, d, invd, s, t0, t1)) {
                 tally_weights(T, M, L, E, wk, wh);
                 tal_n = visit_estimate(G, p, d, t0, t1);
@@ -837,9 +854,9 @@ transport_kernel(const KTables T, const KScene S, const KGrid G, const KSource S
                     }
                     const SegRec& q = s_seg[warp][lo];
                     int k = u - s_pre[warp][lo];
-                    float dt = (q.t1 - q.t0) / (float)q.m;
-                    float ta = q.t0 + dt * (float)k;
-                    float tz = (k == q.m - 1) ? q.t1 : ta + dt;
+                    real dt = (q.t1 - q.t0) / (real)q.m;
+                    real ta = q.t0 + dt * (real)k;
+                    real tz = (k == q.m - 1) ? q.t1 : ta + dt;
                     int nv = walk_range(G, G.tally + (size_t)q.batch * 2 * G.nvox, q.p, q.d, ta, tz, q.wk, q.wh);
                     c_vox += max(nv - (k > 0 ? 1 : 0), 0);   // a cut voxel is one visit
                 }
@@ -969,8 +986,8 @@ struct KBatch {
 static_assert(sizeof(KSource) % 8 == 0 && sizeof(KGrid) % 8 == 0, "device tables hold 8-byte fields");
 
 struct SegRecB {
-    float p[3], d[3];
-    float t0, t1;
+    real p[3], d[3];
+    real t0, t1;
     float wk, wh;
     int scene, slot, m;
 };
@@ -1030,7 +1047,8 @@ batch_kernel(const KTables T, const KBatch B, const KRun R) {
     bool live = false;
     int sc = 0, slot = 0;
     long long li = 0;
-    float p[3], d[3], E = 0.f, tau = 0.f;
+    real p[3], d[3];
+    float E = 0.f, tau = 0.f;
     int nsc = 0, mat = -1;
     long long steps = 0;
     HistoryRng rng;
@@ -1074,8 +1092,8 @@ batch_kernel(const KTables T, const KBatch B, const KRun R) {
         const KScene& S = B.scenes[sc];
         bool go = live;
         bool interact = false, escape = false;
-        float s = 0.f, tau_b = 0.f, loge = 0.f;
-        float t0 = 0.f, t1 = 0.f, wk = 0.f, wh = 0.f;
+        real s = 0, t0 = 0, t1 = 0;
+        float tau_b = 0.f, loge = 0.f, wk = 0.f, wh = 0.f;
         int tal_n = 0;
         Lookup L;
         L.idx = 0;
@@ -1096,16 +1114,16 @@ batch_kernel(const KTables T, const KBatch B, const KRun R) {
             loge = __logf(E);
             L = energy_index(T, M, loge);
             float mu = mu_total(T, M, L);
-            const float invd[3] = {1.0f / d[0], 1.0f / d[1], 1.0f / d[2]};
-            float tb = INFINITY;
+            const real invd[3] = {(real)1 / d[0], (real)1 / d[1], (real)1 / d[2]};
+            real tb = INFINITY;
             const int np = S.n_prims;
             for (int i = 0; i < np; ++i) tb = prim_next(S.prims[i], p, d, invd, S.eps, tb);
-            float tw = world_exit(S, p, d, invd);
+            real tw = world_exit(S, p, d, invd);
             escape = tw <= tb;
-            tb = fminf(tb, tw);
-            tau_b = mu * tb;
+            tb = fmin(tb, tw);
+            tau_b = (float)(mu * tb);
             interact = tau < tau_b;
-            s = interact ? tau / fmaxf(mu, 1e-30f) : tb;
+            s = interact ? (real)tau / (real)fmaxf(mu, 1e-30f) : tb;
             if (TALLY && clip_to_grid(B.grids[sc], p, d, invd, s, t0, t1)) {
                 tally_weights(T, M, L, E, wk, wh);
                 tal_n = visit_estimate(B.grids[sc], p, d, t0, t1);
@@ -1135,9 +1153,9 @@ batch_kernel(const KTables T, const KBatch B, const KRun R) {
                     }
                     const SegRecB& q = s_seg[warp][lo];
                     int k = u - s_pre[warp][lo];
-                    float dt = (q.t1 - q.t0) / (float)q.m;
-                    float ta = q.t0 + dt * (float)k;
-                    float tz = (k == q.m - 1) ? q.t1 : ta + dt;
+                    real dt = (q.t1 - q.t0) / (real)q.m;
+                    real ta = q.t0 + dt * (real)k;
+                    real tz = (k == q.m - 1) ? q.t1 : ta + dt;
                     const KGrid& G = B.grids[q.scene];
                     int nv = walk_range(G, G.tally + (size_t)q.slot * 2 * G.nvox, q.p, q.d, ta, tz, q.wk, q.wh);
                     c_vox += max(nv - (k > 0 ? 1 : 0), 0);   // a cut voxel is one visit
@@ -1269,7 +1287,8 @@ __global__ void sample_source_kernel(const KSource SRC, long long n, long long f
     if (i >= n) return;
     HistoryRng rng;
     rng.init(seed, (unsigned long long)(first + i), 0u);
-    float p[3], d[3], E;
+    real p[3], d[3];
+    float E;
     sample_source(SRC, rng, p, d, E);
     for (int k = 0; k < 3; ++k) { pos[3 * i + k] = p[k]; dir[3 * i + k] = d[k]; }
     en[i] = E;
@@ -1580,13 +1599,17 @@ int cc_scene_create(cc_ctx* ctx, const cc_primitive* prims, int32_t n_prims, int
     k.background = background;
     double extent = 1.0;
     for (int a = 0; a < 3; ++a) {
-        k.wlo[a] = (float)world_lo[a];
-        k.whi[a] = (float)world_hi[a];
+        k.wlo[a] = (real)world_lo[a];
+        k.whi[a] = (real)world_hi[a];
         extent = std::max(extent, std::max(fabs(world_lo[a]), fabs(world_hi[a])));
     }
     // 8 ulps of the largest world coordinate, and at least the 1e-6 cm of
     // transport.py:155 / geometry.py:214
+#ifdef CC_TRACK_FP64
+    k.eps = (real)1e-6;
+#else
     k.eps = (float)std::max(1e-6, 8.0 * extent * 5.960464477539063e-08);
+#endif
     for (int i = 0; i < n_prims; ++i) {
         const cc_primitive& p = prims[i];
         DevPrim& g = k.prims[i];
@@ -1600,12 +1623,12 @@ int cc_scene_create(cc_ctx* ctx, const cc_primitive* prims, int32_t n_prims, int
         g.type = p.type;
         g.material = p.material;
         g.axis = p.axis;
-        for (int a = 0; a < 3; ++a) { g.c[a] = (float)p.center[a]; g.h[a] = (float)(0.5 * p.size[a]); }
-        g.r2 = (float)(p.radius * p.radius);
-        g.r = (float)p.radius;
-        g.hh = (float)(0.5 * p.height);
+        for (int a = 0; a < 3; ++a) { g.c[a] = (real)p.center[a]; g.h[a] = (real)(0.5 * p.size[a]); }
+        g.r2 = (real)(p.radius * p.radius);
+        g.r = (real)p.radius;
+        g.hh = (real)(0.5 * p.height);
         if (p.type == CC_SHAPE_ELLIPSOID)
-            g.r = (float)(2.0 / std::min(p.size[0], std::min(p.size[1], p.size[2])));
+            g.r = (real)(2.0 / std::min(p.size[0], std::min(p.size[1], p.size[2])));
     }
     *out = s;
     return CC_OK;
@@ -1715,9 +1738,9 @@ int cc_grid_create(cc_ctx* ctx, const double origin[3], int32_t nx, int32_t ny, 
     g->ctx = ctx;
     g->flags = flags;
     KGrid& k = g->k;
-    for (int a = 0; a < 3; ++a) k.o[a] = (float)origin[a];
-    k.h = (float)voxel_cm;
-    k.inv_h = (float)(1.0 / voxel_cm);
+    for (int a = 0; a < 3; ++a) k.o[a] = (real)origin[a];
+    k.h = (real)voxel_cm;
+    k.inv_h = (real)(1.0 / voxel_cm);
     k.nx = nx; k.ny = ny; k.nz = nz;
     k.nvox = (long long)nx * ny * nz;
     k.enabled = 1;

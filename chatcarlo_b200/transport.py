@@ -65,8 +65,9 @@ class DeviceGrid:
         self.handle = C.c_void_p()
         origin = np.ascontiguousarray(grid.origin_cm, dtype=float)
         nx, ny, nz = self.shape
-        N.check(N.lib().cc_grid_create(engine.ctx, N.dptr(origin), nx, ny, nz, float(grid.voxel_size_cm),
-                                       N.CC_GRID_STATS if stats else 0, C.byref(self.handle)))
+        self.lib = engine.lib
+        N.check(self.lib.cc_grid_create(engine.ctx, N.dptr(origin), nx, ny, nz, float(grid.voxel_size_cm),
+                                        N.CC_GRID_STATS if stats else 0, C.byref(self.handle)), self.lib)
         self.stats = stats
 
     def download(self, grid: VoxelGrid, accumulate: bool = False) -> None:
@@ -77,11 +78,11 @@ class DeviceGrid:
         nh = np.empty(self.shape, dtype=np.int32) if self.stats else None
         nb = C.c_int64()
         nhist = C.c_int64()
-        N.check(N.lib().cc_grid_download(
+        N.check(self.lib.cc_grid_download(
             self.handle, N.dptr(k), N.dptr(h), N.dptr(k2) if k2 is not None else None,
             N.dptr(h2) if h2 is not None else None,
             nh.ctypes.data_as(C.POINTER(C.c_int32)) if nh is not None else None,
-            C.byref(nb), C.byref(nhist)))
+            C.byref(nb), C.byref(nhist)), self.lib)
         if accumulate:
             grid.kerma_keV += k
             grid.h10_track_pSv_cm3 += h
@@ -96,19 +97,24 @@ class DeviceGrid:
             grid.n_histories = int(nhist.value)
 
     def reset(self):
-        N.check(N.lib().cc_grid_reset(self.handle))
+        N.check(self.lib.cc_grid_reset(self.handle), self.lib)
 
     def close(self):
         if self.handle:
-            N.lib().cc_grid_destroy(self.handle)
+            self.lib.cc_grid_destroy(self.handle)
             self.handle = C.c_void_p()
 
 
 class Engine:
     """A device context plus cached device tables per material set."""
 
-    def __init__(self, device: int = 0):
-        self.lib = N.lib()
+    def __init__(self, device: int = 0, precision: str = "fp32"):
+        """precision: "fp32" (the engine) or "fp64" (the same engine tracking
+        positions, directions and distances in FP64: the precision reference)."""
+        if precision not in ("fp32", "fp64"):
+            raise ValueError("precision must be 'fp32' or 'fp64'")
+        self.precision = precision
+        self.lib = N.lib(N.FP64_LIB_PATH if precision == "fp64" else None)
         self.ctx = C.c_void_p()
         N.check(self.lib.cc_ctx_create(int(device), C.byref(self.ctx)))
         self.device = device

@@ -21,8 +21,9 @@ def test_header_and_binding_agree():
     assert declared_functions() == sorted(N.EXPORTED)
 
 
-def test_library_exports_every_declared_symbol():
-    lib = C.CDLL(str(N.LIB_PATH))
+@pytest.mark.parametrize("path", [N.LIB_PATH, N.FP64_LIB_PATH])
+def test_library_exports_every_declared_symbol(path):
+    lib = C.CDLL(str(path))
     missing = [f for f in declared_functions() if not hasattr(lib, f)]
     assert not missing, missing
 
