@@ -281,8 +281,9 @@ def run_transport(scene, n_histories: int = 100_000, seed: int | None = None,
     """
     raw = scene.raw if hasattr(scene, "raw") else scene
     src = raw["source"]
-    if src.get("mas") is not None or src.get("ctdi_vol_mGy") is not None:
-        raise RuntimeError("absolute calibration (mas / ctdi_vol_mGy) needs SpekPy, which is not available")
+    if src.get("mas") is not None and src.get("ctdi_vol_mGy") is None:
+        raise RuntimeError("mAs calibration needs SpekPy's fluence, which is not available "
+                           "(ctdi_vol_mGy calibration is)")
     eng = engine or default_engine()
     geometry = Geometry(raw["geometry"])
     if dose_grid and grid is None:
@@ -316,6 +317,11 @@ def run_transport(scene, n_histories: int = 100_000, seed: int | None = None,
                         n_batches, int(n_histories))
         sem = {k: v / 1000.0 for k, v in mom.standard_errors().items()}
         rel = mom.relative_errors()
+    # absolute calibration from CTDIvol, once, with the run's seed (transport.py:442-451)
+    n_photons_real = None
+    if src.get("ctdi_vol_mGy") is not None:
+        from .ctdi import effective_histories_from_ctdi
+        n_photons_real = effective_histories_from_ctdi(src, seed=seed, engine=eng)
     nh = max(int(n_histories), 1)
     return TransportResult(
         n_histories=int(n_histories),
@@ -324,7 +330,7 @@ def run_transport(scene, n_histories: int = 100_000, seed: int | None = None,
         fraction_escaped=out.n_escaped / nh,
         mean_scatter_events=out.scatter_sum / nh,
         grid=grid,
-        n_photons_real=None,
+        n_photons_real=n_photons_real,
         n_fluorescence=int(out.n_fluorescence),
         n_batches=n_batches if track_uncertainty else (grid.n_batches if grid is not None else 0),
         energy_deposited_sem_MeV=sem,

@@ -839,3 +839,47 @@ def run_transport(raw, n_histories=100_000, seed=None, batch_size=200_000, grid_
                     g.n_batches += h.n_batches
                     g.n_histories += h.n_histories
     return total
+
+
+# ---------------------------------------------------------------------------
+# CTDIvol calibration (chatcarlo/ctdi.py)
+# ---------------------------------------------------------------------------
+
+def ctdi_per_history_Gy(src, phantom="body", n_histories=200_000, seed=None):
+    """ctdi.py:53-100: the PMMA CTDI phantom on the isocentre, a 1 cm grid
+    with 2 cm margins, host-sampled batches of 200,000 through
+    transport_photons, dose at the chamber positions."""
+    from chatcarlo_b200 import tables as tb
+    rot = src["rotation"]
+    diameter = {"body": 32.0, "head": 16.0}[phantom]
+    radius = diameter / 2.0
+    g = {"name": f"ctdi_phantom_{phantom}", "shape": "cylinder", "material": "pmma",
+         "axis": rot.get("axis", "z"), "radius_cm": radius, "height_cm": 15.0,
+         "center": [float(x) for x in rot["isocenter"]]}
+    geometry = OracleGeometry([g])
+    iso = np.asarray(rot["isocenter"], dtype=float)
+    ax = AXES[rot.get("axis", "z")]
+    plane = [k for k in range(3) if k != ax]
+    lo, hi = iso - radius - 2.0, iso + radius + 2.0
+    lo[ax] = iso[ax] - 7.5 - 2.0
+    hi[ax] = iso[ax] + 7.5 + 2.0
+    grid = OracleGrid.from_bbox(lo, hi, 1.0)
+    rng = np.random.default_rng(seed)
+    remaining = n_histories
+    while remaining > 0:
+        n = min(200_000, remaining)
+        remaining -= n
+        pos, dirv, energy = sample_source_photons(src, n, rng)
+        transport_photons(pos, dirv, energy, geometry, rng, grid=grid)
+    axes = [grid.origin_cm[k] + (np.arange(grid.shape[k]) + 0.5) * grid.voxel_size_cm for k in range(3)]
+    c = np.stack(np.meshgrid(*axes, indexing="ij"), axis=-1)
+    mats = geometry.material_at(c.reshape(-1, 3))
+    dens = np.array([tb.density(m) for m in mats]).reshape(grid.shape)
+    mass_kg = dens * grid.voxel_size_cm ** 3 * 1e-3
+    energy_j = grid.kerma_keV * 1e-3 * 1.602176634e-13
+    dose = np.divide(energy_j, mass_kg, out=np.zeros_like(energy_j), where=mass_kg > 0) / n_histories
+    r = np.sqrt((c[..., plane[0]] - iso[plane[0]]) ** 2 + (c[..., plane[1]] - iso[plane[1]]) ** 2)
+    z_ok = np.abs(c[..., ax] - iso[ax]) <= 5.0
+    d_center = float(dose[z_ok & (r < 2.0)].mean())
+    d_periph = float(dose[z_ok & (r >= radius - 2.0) & (r <= radius - 1.0)].mean())
+    return d_center / 3.0 + 2.0 * d_periph / 3.0, d_center, d_periph

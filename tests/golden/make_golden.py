@@ -238,8 +238,24 @@ def case_source():
     return out
 
 
+CT_SOURCE = {"position": [0.0, -60.0, 0.0], "direction": [0.0, 1.0, 0.0],
+             "field": {"shape": "rect", "size_cm": [50.0, 4.0], "sid_cm": 60.0},
+             "rotation": {"isocenter": [0.0, 0.0, 0.0], "axis": "z", "scan_length_cm": 10.0},
+             "spectrum": [{"energy_keV": 40.0, "weight": 1.0}, {"energy_keV": 60.0, "weight": 2.0},
+                          {"energy_keV": 80.0, "weight": 1.0}],
+             "ctdi_vol_mGy": 12.0}
+
+
+def case_ctdi():
+    from chatcarlo import ctdi as rctdi
+    import json
+    ctdiw, dc, dp = rctdi.ctdi_per_history_Gy(CT_SOURCE, phantom="head", n_histories=4000, seed=9)
+    return {"ctdi": np.array([ctdiw, dc, dp]), "source_json": np.array(json.dumps(CT_SOURCE))}
+
+
 CASES = {"geometry": case_geometry, "materials": case_materials, "samplers": case_samplers,
-         "tally": case_tally, "transport": case_transport, "run": case_run, "source": case_source}
+         "tally": case_tally, "transport": case_transport, "run": case_run, "source": case_source,
+         "ctdi": case_ctdi}
 
 
 def main(names=None):

@@ -203,3 +203,13 @@ def test_source_sampling_matches_reference(golden):
         np.testing.assert_array_equal(p, g[f"{k}_pos"], err_msg=k)
         np.testing.assert_array_equal(d, g[f"{k}_dir"], err_msg=k)
         np.testing.assert_array_equal(e, g[f"{k}_e"], err_msg=k)
+
+
+def test_ctdi_calibration_matches_reference(golden):
+    """ctdi.py:53-100 through the oracle: CTDIw, D_center, D_periphery of the
+    head phantom, 4000 histories, seed 9 -- identical to the reference."""
+    import json
+    g = golden("ctdi")
+    src = json.loads(str(g["source_json"]))
+    got = O.ctdi_per_history_Gy(src, phantom="head", n_histories=4000, seed=9)
+    np.testing.assert_array_equal(np.array(got), g["ctdi"])
