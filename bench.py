@@ -37,6 +37,17 @@ WORKLOAD = ("room-scale plain MC: 400x400x300 cm air room, water torso 35x25x20 
             "r1.5x20 cm, 0.05 cm lead 30x30 cm at 150 cm, 20 cm concrete wall; 80 kVp W spectrum 2.5 mm Al "
             "(Kramers model, 1 keV bins); rect field 35x43 cm at SID 180 cm; kerma + H*(10) on 5 cm voxels "
             "80x80x60 with batch statistics")
+WORKLOAD_CT = ("CT dosimetry plain MC: PMMA phantom 32 cm x 15 cm with five 1.3 cm air holes, 120 kVp W "
+               "spectrum 6.8 mm Al (Kramers model, 1 keV bins), fan 50x4 cm at SID 60 cm, continuous rotation "
+               "with 30 cm helical scan; kerma + H*(10) on 1 mm voxels 320x320x150 with batch statistics")
+
+
+def workload(name: str):
+    """(scene dict, grid spec, description) of a bench workload."""
+    from chatcarlo_b200 import workloads as W
+    if name == "ct":
+        return W.ct(), W.CT_GRID, WORKLOAD_CT
+    return W.room(), W.ROOM_GRID, WORKLOAD
 
 
 def peaks():
@@ -108,36 +119,38 @@ class ClockSampler:
 # reference arm: the CPU oracle on all host cores
 # ---------------------------------------------------------------------------
 
-def _ref_worker(n, seed):
+def _ref_worker(n, seed, name="room"):
     import cc_oracle as O
     from chatcarlo_b200 import workloads as W
-    raw = W.room()
-    agg = O.run_transport(raw, n_histories=n, seed=seed, batch_size=BATCH, grid_spec=W.ROOM_GRID,
+    raw, spec, _ = workload(name)
+    agg = O.run_transport(raw, n_histories=n, seed=seed, batch_size=BATCH, grid_spec=spec,
                           n_workers=1, track_uncertainty=True)
     g = agg["grid"]
     return n, g.kerma_keV, g.h10_track_pSv_cm3
 
 
-def _ref_warm(_):
-    _ref_worker(200, 0)      # builds the element tables in this process
+def _ref_warm(name):
+    _ref_worker(200, 0, name)      # builds the element tables in this process
     return os.getpid()
 
 
-def run_cpu_reference(steps: int, warmup: int, per_core: int, cores: int | None = None):
+def run_cpu_reference(steps: int, warmup: int, per_core: int, cores: int | None = None, name: str = "room"):
     """Times the oracle's run_transport on the workload with one process per
     host core (spawned), per_core histories per process per step."""
     import concurrent.futures
     import multiprocessing as mp
     sys.path.insert(0, str(ROOT / "oracle"))
     cores = cores or os.cpu_count() or 1
+    if name == "ct":
+        cores = min(cores, 8)        # each process holds the 15.4M-voxel grid with its statistics (~1 GB)
     ctx = mp.get_context("spawn")
     times, total = [], 0
     with concurrent.futures.ProcessPoolExecutor(max_workers=cores, mp_context=ctx,
                                                 initializer=_ref_init, initargs=(str(ROOT),)) as pool:
-        list(pool.map(_ref_warm, range(cores)))
+        list(pool.map(_ref_warm, [name] * cores))
         for s in range(warmup + steps):
             t0 = time.perf_counter()
-            futs = [pool.submit(_ref_worker, per_core, 1000 * s + i) for i in range(cores)]
+            futs = [pool.submit(_ref_worker, per_core, 1000 * s + i, name) for i in range(cores)]
             kerma = None
             n = 0
             for f in futs:
@@ -168,13 +181,18 @@ def main():
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--histories-per-step", type=float, default=1e7)
     ap.add_argument("--e2e-histories", type=float, default=4e6)
-    ap.add_argument("--cpu-histories-per-process", type=int, default=120_000,
-                    help="CPU sample per step: histories in each of the host-core processes")
+    ap.add_argument("--cpu-histories-per-process", type=int, default=None,
+                    help="CPU sample per step: histories in each of the host-core processes "
+                         "(default 120,000 for room, 1,000 for ct)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-precision", action="store_true", help="skip the FP32-vs-FP64 tracking tally report")
     ap.add_argument("--precision-histories", type=float, default=1e7)
+    ap.add_argument("--workload", choices=["room", "ct"], default="room",
+                    help="room-scale (the headline configuration) or CT dosimetry")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.cpu_histories_per_process is None:
+        args.cpu_histories_per_process = 1_000 if args.workload == "ct" else 120_000
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -184,12 +202,12 @@ def main():
         if rank != 0:
             return 0
         per_core = args.cpu_histories_per_process // 2
-        value, cores, times = run_cpu_reference(args.steps, args.warmup, per_core)
+        value, cores, times = run_cpu_reference(args.steps, args.warmup, per_core, name=args.workload)
         line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "histories/s",
                 "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
                 "ms_per_step": 1000.0 * float(np.mean(times)), "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                "config": {"workload": WORKLOAD, "histories_per_step": per_core * cores,
+                "config": {"workload": workload(args.workload)[2], "histories_per_step": per_core * cores,
                            "batch_size": BATCH, "l2": "n/a (CPU)"},
                 "cpu_baseline": {"value": value, "unit": "histories/s", "cores": cores, "kind": "port",
                                  "sample": f"{per_core} histories per process x {cores} processes per step"},
@@ -214,13 +232,13 @@ def main():
     device = local if world > 1 else 0
     torch.cuda.set_device(device)
     eng = Engine(device)
-    raw = W.room()
+    raw, gspec, desc = workload(args.workload)
     geom = Geometry(raw["geometry"])
     ts, th = eng.tables(geom.materials(), need_muen=True)
     sh = eng.scene(geom, ts)
     spec = SourceSpec(raw["source"])
     srch = eng.source(spec)
-    grid = W.make_grid(W.ROOM_GRID, track_uncertainty=True)
+    grid = W.make_grid(gspec, track_uncertainty=True)
     dg = DeviceGrid(eng, grid, stats=True)
     S = int(args.histories_per_step)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
@@ -282,7 +300,7 @@ def main():
     launches = sum(o.gpu_launches for o in outs)
     peak, peak_kind = peaks()
     achieved = b_hist * n_h / (tr_ms / 1e3) / 1e9
-    traffic_per_hist = profile_traffic()
+    traffic_per_hist = profile_traffic() if args.workload == "room" else None
     hist_per_launch = n_h / max(tr_launch, 1)
 
     # e2e: the public run_transport call a user makes, once per step: scene,
@@ -292,7 +310,7 @@ def main():
     e2e_photons = None
     if rank == 0:
         from chatcarlo_b200.transport import run_transport
-        eg = W.make_grid(W.ROOM_GRID, track_uncertainty=True)
+        eg = W.make_grid(gspec, track_uncertainty=True)
         e_ms = []
         for i in range(args.warmup + min(args.steps, 5)):
             flush.zero_()
@@ -316,7 +334,7 @@ def main():
         p0, d0, e0 = pin((ne, 3)), pin((ne, 3)), pin((ne,))
         N.check(eng.lib.cc_sample_source(eng.ctx, srch, ne, seed + 7, 1 << 50, N.dptr(p0), N.dptr(d0), N.dptr(e0)))
         p, d, e = pin((ne, 3)), pin((ne, 3)), pin((ne,))
-        egrid = W.make_grid(W.ROOM_GRID, track_uncertainty=False)
+        egrid = W.make_grid(gspec, track_uncertainty=False)
         e_ms = []
         for i in range(args.warmup + min(args.steps, 5)):
             np.copyto(p, p0)
@@ -341,7 +359,7 @@ def main():
     if rank == 0 and world == 1 and not args.no_precision:
         from chatcarlo_b200.precision import tally_precision
         from chatcarlo_b200.transport import Engine as _Engine
-        rep = tally_precision(raw, W.ROOM_GRID, int(args.precision_histories), seed + 999, batch_size=BATCH,
+        rep = tally_precision(raw, gspec, int(args.precision_histories), seed + 999, batch_size=BATCH,
                               engine32=eng, engine64=_Engine(eng.device, precision="fp64"))
         precision = {"reference": "the same engine tracking in FP64, same seed and random numbers",
                      "histories": rep["histories"],
@@ -351,17 +369,17 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         per_core = args.cpu_histories_per_process
-        v, cores, times = run_cpu_reference(1, 0, per_core)
+        v, cores, times = run_cpu_reference(1, 0, per_core, name=args.workload)
         cpu = {"value": v, "unit": "histories/s", "cores": cores, "kind": "port",
-               "sample": f"room workload, {per_core} histories in each of {cores} spawned processes "
+               "sample": f"{args.workload} workload, {per_core} histories in each of {cores} spawned processes "
                          f"({per_core * cores} histories, {times[0]:.1f} s wall incl. pool start)"}
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": "histories/s", "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": {"workload": WORKLOAD, "histories_per_step_per_gpu": S, "batch_size": BATCH,
-                           "grid": list(grid.shape), "voxel_cm": 5.0, "tally_dtype": "f64",
+                "config": {"workload": desc, "histories_per_step_per_gpu": S, "batch_size": BATCH,
+                           "grid": list(grid.shape), "voxel_cm": gspec["voxel_cm"], "tally_dtype": "f64",
                            "l2": "flushed between steps (256 MiB write)",
                            "parallelism": f"history shards x{world}"},
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",

@@ -10,6 +10,8 @@
   model ChatCarlo falls back to without SpekPy (spectrum.py:55-62), rect
   field 35x43 cm at SID 180 cm.  Kerma and H*(10) on 5 cm voxels over the
   whole room (80x80x60).
+* ``ct``: the CT dosimetry configuration (PMMA phantom with five holes,
+  helical 120 kVp fan beam, kerma on 320x320x150 voxels of 1 mm).
 
 Positions are fixed here (the configuration leaves them open) and the same
 dicts feed the engine and the CPU oracle.
@@ -74,6 +76,30 @@ def room() -> dict:
 
 
 ROOM_GRID = {"origin": (-200.0, -200.0, 0.0), "shape": (80, 80, 60), "voxel_cm": 5.0}
+
+
+def ct() -> dict:
+    """CT dosimetry: PMMA body CTDI-type phantom (32 cm diameter, 15 cm long,
+    axis z on the isocentre) with five 1.3 cm air holes (centre, and 1 cm
+    under the surface at 0/90/180/270 degrees; listed after the cylinder so
+    they win); 120 kVp tungsten spectrum with 6.8 mm Al (the Kramers model
+    of spectrum.py:55-62, 1 keV bins); focus 60 cm from the isocentre, fan
+    50x4 cm at SID 60 cm, continuous rotation about z with a 30 cm helical
+    scan length."""
+    holes = [(0.0, 0.0), (15.0, 0.0), (0.0, 15.0), (-15.0, 0.0), (0.0, -15.0)]
+    geoms = [{"name": "pmma_body", "shape": "cylinder", "material": "pmma", "axis": "z",
+              "center": [0.0, 0.0, 0.0], "radius_cm": 16.0, "height_cm": 15.0}]
+    geoms += [{"name": f"hole{i}", "shape": "cylinder", "material": "air", "axis": "z",
+               "center": [x, y, 0.0], "radius_cm": 0.65, "height_cm": 15.0} for i, (x, y) in enumerate(holes)]
+    e, w = kramers_spectrum(120.0, 6.8, n_bins=None)
+    return {"source": {"position": [0.0, -60.0, 0.0], "direction": [0.0, 1.0, 0.0],
+                       "field": {"shape": "rect", "size_cm": [50.0, 4.0], "sid_cm": 60.0},
+                       "rotation": {"isocenter": [0.0, 0.0, 0.0], "axis": "z", "scan_length_cm": 30.0},
+                       "spectrum": [{"energy_keV": float(a), "weight": float(b)} for a, b in zip(e, w)]},
+            "geometry": geoms, "physics": {"fluorescence": True}}
+
+
+CT_GRID = {"origin": (-16.0, -16.0, -7.5), "shape": (320, 320, 150), "voxel_cm": 0.1}
 
 
 def make_grid(spec: dict, track_uncertainty: bool = True):
