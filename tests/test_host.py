@@ -256,3 +256,13 @@ def test_denoiser_phantoms_validate_and_map_materials():
         assert mat.shape == (16, 16, 16) and mat.max() < 4
         assert np.any(mat == 1)                       # the water body
         np.testing.assert_allclose(dens[mat == 1], 1.0)
+
+
+def test_histories_for_error_interpolates_in_log_log():
+    from chatcarlo_b200.denoise_run import histories_for_error
+    h = [1e5, 4e5, 1.6e6]
+    e = [0.08, 0.04, 0.02]                       # exactly 1/sqrt(n)
+    assert histories_for_error(h, e, 0.02) == pytest.approx(1.6e6)
+    assert histories_for_error(h, e, 0.0283) == pytest.approx(8e5, rel=1e-2)
+    assert histories_for_error(h, e, 0.01) is None
+    assert histories_for_error(h, [0.01, 0.009, 0.008], 0.02) == 1e5
