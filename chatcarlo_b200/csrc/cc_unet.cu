@@ -281,6 +281,28 @@ struct ConvP {
     __nv_bfloat16* out1;
 };
 
+// Bias, ReLU, mask and BF16 store of output channels [c0, c0 + 8) of voxel v.
+__device__ __forceinline__ void conv_store(const ConvP& P, long long v, int c0, int n_out, float f[8]) {
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        if (P.bias) f[j] += __ldg(P.bias + c0 + j);
+        if (P.relu) f[j] = fmaxf(f[j], 0.0f);
+    }
+    if (c0 < P.split) {
+        const size_t o = (size_t)v * P.split + c0;
+        if (P.mask0) {
+            float mk[8];
+            unpack_bf16x8(__ldg(reinterpret_cast<const uint4*>(P.mask0 + o)), mk);
+#pragma unroll
+            for (int j = 0; j < 8; ++j) f[j] = mk[j] > 0.0f ? f[j] : 0.0f;
+        }
+        *reinterpret_cast<uint4*>(P.out0 + o) = pack_bf16x8(f);
+    } else {
+        const size_t o = (size_t)v * (n_out - P.split) + (c0 - P.split);
+        *reinterpret_cast<uint4*>(P.out1 + o) = pack_bf16x8(f);
+    }
+}
+
 __host__ __device__ constexpr uint32_t tmem_cols(int n) {
     return n <= 32 ? 32u : (n <= 64 ? 64u : (n <= 128 ? 128u : 256u));
 }
@@ -425,26 +447,112 @@ __global__ void __launch_bounds__(THREADS) conv_kernel(const ConvP P) {
         for (int c0 = half * 8; c0 < N; c0 += 16) {
             float f[8];
             tmem_ld8(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)c0, f);
-            if (v < P.n_vox) {
-#pragma unroll
-                for (int j = 0; j < 8; ++j) {
-                    if (P.bias) f[j] += __ldg(P.bias + c0 + j);
-                    if (P.relu) f[j] = fmaxf(f[j], 0.0f);
-                }
-                if (c0 < P.split) {
-                    size_t o = (size_t)v * P.split + c0;
-                    if (P.mask0) {
-                        float mk[8];
-                        unpack_bf16x8(__ldg(reinterpret_cast<const uint4*>(P.mask0 + o)), mk);
-#pragma unroll
-                        for (int j = 0; j < 8; ++j) f[j] = mk[j] > 0.0f ? f[j] : 0.0f;
-                    }
-                    *reinterpret_cast<uint4*>(P.out0 + o) = pack_bf16x8(f);
-                } else {
-                    size_t o = (size_t)v * (N - P.split) + (c0 - P.split);
-                    *reinterpret_cast<uint4*>(P.out1 + o) = pack_bf16x8(f);
-                }
+            if (v < P.n_vox) conv_store(P, v, c0, N, f);
+        }
+    } else if (tid == 0) {
+        atomicOr(&g_status, 1u);
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) tmem_dealloc(tmem, tmem_cols(N));
+}
+
+// ---------------------------------------------------------------------------
+// forward / backward-data convolution from a shared-memory halo
+// ---------------------------------------------------------------------------
+
+// For a tile of 16 (y) x 8 (x) output voxels at one z, the input halo of
+// 3 x 18 x 10 voxels is loaded into shared memory once, 8-channel chunk
+// planes of 540 voxels x 16 bytes.  Each tap's A operand is then the same
+// halo under a shifted descriptor start: the 8 rows of a core matrix are 8
+// consecutive x voxels (16 bytes apart, 128 contiguous bytes), the 16 row
+// groups are the tile's y rows (SBO = one halo row, 160 bytes), the two
+// 8-channel halves of a K = 16 step are two chunk planes (LBO = 8640
+// bytes) -- a valid K-major no-swizzle operand for every tap, so the 27
+// taps' MMAs need no gather.  The packed weights are chunk-major over
+// K = 27 x cin, so tap t's chunk pair (2j, 2j + 1) is the B operand at
+// chunk t * cin / 8 + 2j.  Used where the halo and all weights fit in
+// shared memory (cin, N <= 48) and the tile divides the volume (H % 16,
+// W % 8).
+constexpr int HALO_Y = 18, HALO_X = 10, HALO_V = 3 * HALO_Y * HALO_X;
+
+__host__ __device__ constexpr uint32_t halo_smem_bytes(int n, int cin) {
+    return (uint32_t)(cin / 8) * HALO_V * 16 + (uint32_t)((27 * cin + KS - 1) / KS) * 8 * n * 16;
+}
+
+template <int N>
+__global__ void __launch_bounds__(THREADS) conv_halo_kernel(const ConvP P) {
+    extern __shared__ __align__(128) uint8_t smem[];
+    __shared__ uint64_t bar;
+    __shared__ uint32_t s_tmem;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const Src& S = P.src;
+    const int cin = S.ca + S.cb, c8n = cin / 8;
+    const int tiles_x = S.W / 8, tiles_y = S.H / 16;
+    int t = blockIdx.x;
+    const int x0 = (t % tiles_x) * 8;
+    t /= tiles_x;
+    const int y0 = (t % tiles_y) * 16;
+    t /= tiles_y;
+    const int z = t % S.D, n = t / S.D;
+    const uint32_t halo_bytes = (uint32_t)c8n * HALO_V * 16;
+    const int w_chunks = ((27 * cin + KS - 1) / KS) * 8 * N;
+
+    if (warp == 0) tmem_alloc(&s_tmem, tmem_cols(N));
+    if (tid == 0) {
+        mbar_init(&bar, 1);
+        mbar_init_fence();
+    }
+    const uint32_t sbase = smem_u32(smem), swt = sbase + halo_bytes;
+    // halo: chunk c8, voxel hv = (hz * 18 + hy) * 10 + hx
+    for (int i = tid; i < c8n * HALO_V; i += THREADS) {
+        const int c8 = i / HALO_V, hv = i - c8 * HALO_V;
+        const int hz = hv / (HALO_Y * HALO_X), hy = (hv / HALO_X) % HALO_Y, hx = hv % HALO_X;
+        const int zz = z + hz - 1, yy = y0 + hy - 1, xx = x0 + hx - 1;
+        const int ch = c8 * 8;
+        uint32_t bytes = 0;
+        const void* src = S.a;
+        if ((unsigned)zz < (unsigned)S.D && (unsigned)yy < (unsigned)S.H && (unsigned)xx < (unsigned)S.W) {
+            bytes = 16;
+            if (ch < S.ca) {
+                src = S.a + ((((size_t)n * S.D + zz) * S.H + yy) * S.W + xx) * S.ca + ch;
+            } else {
+                const size_t cv = (((size_t)n * (S.D >> 1) + (zz >> 1)) * (S.H >> 1) + (yy >> 1)) * (S.W >> 1) + (xx >> 1);
+                src = S.b + cv * S.cb + (ch - S.ca);
             }
+        }
+        cp_async16(sbase + (uint32_t)i * 16, src, bytes);
+    }
+    for (int i = tid; i < w_chunks; i += THREADS) cp_async16(swt + (uint32_t)i * 16, P.w + (size_t)i * 8, 16u);
+    cp_async_commit();
+    cp_async_wait<0>();
+    fence_proxy_async();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = s_tmem;
+    constexpr uint32_t IDESC = idesc_bf16(TILE_M, N, 0, 0);
+    if (tid == 0) {
+        for (int tap = 0; tap < 27; ++tap) {
+            const uint32_t off = (uint32_t)(((tap / 9) * HALO_Y + (tap / 3) % 3) * HALO_X + tap % 3) * 16;
+            for (int j = 0; j < c8n / 2; ++j) {
+                uint64_t ad = smem_desc(sbase + (uint32_t)(2 * j) * HALO_V * 16 + off, HALO_V * 16, HALO_X * 16);
+                uint64_t bd = smem_desc(swt + (uint32_t)(tap * c8n + 2 * j) * N * 16, N * 16, 128);
+                mma_bf16(tmem, ad, bd, IDESC, (tap > 0 || j > 0) ? 1u : 0u);
+            }
+        }
+        mma_commit(&bar);
+    }
+    const bool ok = __syncthreads_and(mbar_wait(&bar, 0));
+    tc_fence_after();
+    if (ok) {
+        const int q = warp & 3, half = warp >> 2;
+        const int m = q * 32 + lane;
+        const long long v = (((long long)n * S.D + z) * S.H + y0 + (m >> 3)) * S.W + x0 + (m & 7);
+        for (int c0 = half * 8; c0 < N; c0 += 16) {
+            float f[8];
+            tmem_ld8(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)c0, f);
+            conv_store(P, v, c0, N, f);
         }
     } else if (tid == 0) {
         atomicOr(&g_status, 1u);
@@ -974,6 +1082,26 @@ int launch_conv(const ConvP& P, cudaStream_t st) {
     return CCU_OK;
 }
 
+int g_conv_path = 0;      // 0: halo kernel where it applies, 1: always the gathering kernel
+
+bool halo_applies(const ConvP& P, int n_out) {
+    const int cin = P.src.ca + P.src.cb;
+    return g_conv_path == 0 && P.src.H % 16 == 0 && P.src.W % 8 == 0 && cin <= 48 && n_out <= 48 &&
+           halo_smem_bytes(n_out, cin) <= 160 * 1024;
+}
+
+template <int N>
+int launch_conv_halo(const ConvP& P, cudaStream_t st) {
+    const int cin = P.src.ca + P.src.cb;
+    size_t smem = 0;
+    int rc = tc_launch_smem(conv_halo_kernel<N>, halo_smem_bytes(N, cin), tmem_cols(N), smem);
+    if (rc != CCU_OK) return rc;
+    const long long blocks = (long long)P.src.B * P.src.D * (P.src.H / 16) * (P.src.W / 8);
+    conv_halo_kernel<N><<<(unsigned)blocks, THREADS, smem, st>>>(P);
+    CU_CHECK(cudaGetLastError());
+    return CCU_OK;
+}
+
 template <int N>
 int launch_wgrad(const WgradP& P, int slices, int cin, cudaStream_t st) {
     size_t smem = 0;
@@ -1034,6 +1162,14 @@ int ccu_conv3d(const void* a, int ca, const void* b, int cb, int batch, int d, i
     P.split = split;
     P.out1 = (__nv_bfloat16*)out1;
     cudaStream_t st = (cudaStream_t)stream;
+    if (halo_applies(P, cout)) {
+        switch (cout) {
+            case 16: return launch_conv_halo<16>(P, st);
+            case 32: return launch_conv_halo<32>(P, st);
+            case 48: return launch_conv_halo<48>(P, st);
+            default: break;
+        }
+    }
     switch (cout) {
         case 16: return launch_conv<16>(P, st);
         case 32: return launch_conv<32>(P, st);
@@ -1149,6 +1285,12 @@ int ccu_pack_weights(const float* w32, int cout, int cin, void* w, void* wt, voi
     pack_weights_kernel<<<grid_for(total, 256), 256, 0, (cudaStream_t)stream>>>(w32, cout, cin, (__nv_bfloat16*)w,
                                                                                 (__nv_bfloat16*)wt);
     CU_CHECK(cudaGetLastError());
+    return CCU_OK;
+}
+
+int ccu_set_conv_path(int path) {
+    if (path < 0 || path > 1) return set_error(CCU_E_INVALID, "path must be 0 (automatic) or 1 (gathering kernel)");
+    g_conv_path = path;
     return CCU_OK;
 }
 

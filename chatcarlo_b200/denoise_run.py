@@ -142,7 +142,7 @@ def train(model: DN.UNet3D, data: Dataset, steps: int, batch: int, lr: float, se
     return losses, time.perf_counter() - t0
 
 
-def denoise(model: DN.UNet3D, data: Dataset, batch: int = 4) -> tuple[np.ndarray, float]:
+def denoise(model: DN.UNet3D, data: Dataset, batch: int = 8) -> tuple[np.ndarray, float]:
     """Denoised kerma maps of every sample and the device time (ms)."""
     import torch
     S = data.S

@@ -98,6 +98,12 @@ long long ccu_packed_weight_elems(int n, int c);
  * c = cout; taps flipped, channels transposed). */
 int ccu_pack_weights(const float* w32, int cout, int cin, void* w, void* wt, void* stream);
 
+/* Which convolution kernel ccu_conv3d uses: 0 (default) the shared-memory
+ * halo kernel where it applies (input and output channels <= 48, h % 16 ==
+ * 0, w % 8 == 0) and the gathering kernel elsewhere; 1 always the gathering
+ * kernel (for comparisons).  Process-wide. */
+int ccu_set_conv_path(int path);
+
 /* cudaMemsetAsync(p, 0, bytes) on the stream (gradient buffers). */
 int ccu_zero(void* p, long long bytes, void* stream);
 

@@ -55,7 +55,10 @@ def _up(x):
 
 @pytest.mark.parametrize("ca,cb,cout,dims", [(16, 0, 16, (2, 6, 8, 10)), (16, 32, 48, (1, 8, 8, 8)),
                                              (64, 128, 64, (1, 4, 6, 8)), (32, 64, 96, (1, 6, 4, 4)),
-                                             (128, 0, 128, (1, 5, 3, 7)), (16, 0, 192, (1, 4, 4, 4))])
+                                             (128, 0, 128, (1, 5, 3, 7)), (16, 0, 192, (1, 4, 4, 4)),
+                                             # shapes of the shared-memory halo kernel (H % 16, W % 8)
+                                             (16, 0, 16, (2, 3, 16, 8)), (16, 32, 48, (1, 4, 32, 16)),
+                                             (32, 0, 32, (1, 2, 16, 24)), (16, 32, 16, (2, 2, 16, 16))])
 def test_conv3d_forward(U, ca, cb, cout, dims):
     gen = torch.Generator().manual_seed(ca * 1000 + cb * 10 + cout)
     B, D, H, W = dims
@@ -84,7 +87,9 @@ def test_conv3d_forward(U, ca, cb, cout, dims):
 
 @pytest.mark.parametrize("ca,cb,cout,dims", [(16, 0, 16, (2, 6, 8, 10)), (16, 32, 16, (1, 8, 8, 8)),
                                              (64, 128, 64, (1, 4, 6, 8)), (64, 0, 128, (1, 5, 3, 7)),
-                                             (32, 0, 32, (3, 4, 4, 4))])
+                                             (32, 0, 32, (3, 4, 4, 4)),
+                                             # data gradients through the halo kernel
+                                             (16, 0, 16, (1, 4, 16, 8)), (16, 32, 16, (2, 2, 16, 16))])
 def test_conv3d_weight_and_data_gradients(U, ca, cb, cout, dims):
     """Weight gradient (tcgen05, MN-major operands) and the data gradient
     (the forward kernel on flipped, transposed weights with the ReLU mask
@@ -152,3 +157,28 @@ def test_pool_upsample_bias_helpers(U):
     red = gfull.float().reshape(B, D // 2, 2, H // 2, 2, W // 2, 2, c).sum(dim=(2, 4, 6))
     torch.testing.assert_close(dzc.float(), red * (coarse.float() > 0), rtol=1.6e-2, atol=2e-2)
     torch.testing.assert_close(db, gfull.float().sum(dim=(0, 1, 2, 3)), rtol=1e-4, atol=1e-2)
+
+
+def test_halo_and_gathering_kernels_agree(U):
+    """The two forward kernels on the same inputs (the halo one applies to
+    this shape; path 1 forces the gathering one)."""
+    gen = torch.Generator().manual_seed(77)
+    B, D, H, W, ca, cb, cout = 2, 4, 32, 16, 16, 32, 48
+    a = _bf((B, D, H, W, ca), gen)
+    b = _bf((B, D // 2, H // 2, W // 2, cb), gen)
+    w32 = (torch.randn(27 * cout * (ca + cb), generator=gen) * 0.1).cuda()
+    w = torch.empty(U.lib().ccu_packed_weight_elems(cout, ca + cb), dtype=torch.bfloat16, device="cuda")
+    U.check(U.lib().ccu_pack_weights(_ptr(w32), cout, ca + cb, _ptr(w), None, None))
+    outs = []
+    try:
+        for path in (0, 1):
+            U.check(U.lib().ccu_set_conv_path(path))
+            o = torch.empty(B, D, H, W, cout, dtype=torch.bfloat16, device="cuda")
+            U.check(U.lib().ccu_conv3d(_ptr(a), ca, _ptr(b), cb, B, D, H, W, _ptr(w), None, cout, 0, _ptr(o), cout,
+                                       None, None, None))
+            outs.append(o.float())
+    finally:
+        U.check(U.lib().ccu_set_conv_path(0))
+    torch.cuda.synchronize()
+    assert U.status() == 0
+    torch.testing.assert_close(outs[0], outs[1], rtol=1.6e-2, atol=1e-2)
