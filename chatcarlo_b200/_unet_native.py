@@ -36,7 +36,7 @@ _SIGS = {
     "ccu_pool_backward": ([P, P, I, I, I, I, I, P, P], I),
     "ccu_up_reduce": ([P, P, I, I, I, I, I, P, P], I),
     "ccu_head": ([P, P, P, P, P, C.c_float, LL, P, P, P, P, P], I),
-    "ccu_input": ([P, P, P, I, LL, P, P], I),
+    "ccu_input": ([P, P, P, I, P, LL, P, P], I),
     "ccu_adam": ([P, P, P, P, LL, C.c_float, C.c_float, C.c_float, C.c_float, I, C.c_float, P], I),
     "ccu_packed_weight_elems": ([I, I], LL),
     "ccu_pack_weights": ([P, I, I, P, P, P], I),

@@ -886,9 +886,11 @@ __global__ void head_kernel(const __nv_bfloat16* __restrict__ d0, const float* _
 }
 
 // Network input: 16 channels per voxel -- normalised log kerma, density,
-// material one-hot (n_mat <= 8), zero padding.
+// material one-hot (n_mat <= 13), zeros, and in channel 15 the input map's
+// relative standard error when given.
 __global__ void input_kernel(const float* __restrict__ xlog, const float* __restrict__ density,
-                             const uint8_t* __restrict__ mat, int n_mat, long long n_vox, __nv_bfloat16* __restrict__ x) {
+                             const uint8_t* __restrict__ mat, int n_mat, const float* __restrict__ unc, long long n_vox,
+                             __nv_bfloat16* __restrict__ x) {
     for (long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x; v < n_vox;
          v += (long long)gridDim.x * blockDim.x) {
         float f[16];
@@ -897,7 +899,8 @@ __global__ void input_kernel(const float* __restrict__ xlog, const float* __rest
         f[0] = xlog[v];
         f[1] = density[v];
         const int m = mat[v];
-        if (m < n_mat && m < 14) f[2 + m] = 1.0f;
+        if (m < n_mat && m < 13) f[2 + m] = 1.0f;
+        if (unc) f[15] = unc[v];
         *reinterpret_cast<uint4*>(x + (size_t)v * 16) = pack_bf16x8(f);
         *reinterpret_cast<uint4*>(x + (size_t)v * 16 + 8) = pack_bf16x8(f + 8);
     }
@@ -1255,10 +1258,10 @@ int ccu_head(const void* d0, const float* xlog, const float* target, const float
     return CCU_OK;
 }
 
-int ccu_input(const float* xlog, const float* density, const uint8_t* mat, int n_mat, long long n_vox, void* x,
-              void* stream) {
-    if (!xlog || !density || !mat || !x || n_mat > 14) return set_error(CCU_E_INVALID, "bad input arguments");
-    input_kernel<<<grid_for(n_vox, 256), 256, 0, (cudaStream_t)stream>>>(xlog, density, mat, n_mat, n_vox,
+int ccu_input(const float* xlog, const float* density, const uint8_t* mat, int n_mat, const float* unc,
+              long long n_vox, void* x, void* stream) {
+    if (!xlog || !density || !mat || !x || n_mat > 13) return set_error(CCU_E_INVALID, "bad input arguments");
+    input_kernel<<<grid_for(n_vox, 256), 256, 0, (cudaStream_t)stream>>>(xlog, density, mat, n_mat, unc, n_vox,
                                                                          (__nv_bfloat16*)x);
     CU_CHECK(cudaGetLastError());
     return CCU_OK;

@@ -87,8 +87,10 @@ class Dataset:
     [n, S, S, S] or a list of them (input maps at several history counts,
     one of which a training sample draws at random)."""
 
-    def __init__(self, k_in, k_tgt, mat, dens):
+    def __init__(self, k_in, k_tgt, mat, dens, rel=None):
         levels = k_in if isinstance(k_in, (list, tuple)) else [k_in]
+        rels = rel if isinstance(rel, (list, tuple)) else ([rel] if rel is not None else None)
+        self.unc = None if rels is None else [DN.uncertainty_channel(r) for r in rels]
         self.n = levels[0].shape[0]
         self.S = levels[0].shape[1]
         self.mat = mat
@@ -104,16 +106,22 @@ class Dataset:
     def batch(self, idx, rng=None):
         """Arrays of a minibatch: a random input level and a random flip of
         each axis per sample when rng is given."""
-        xs, ts, ds, ms, ws = [], [], [], [], []
+        xs, ts, ds, ms, ws, us = [], [], [], [], [], []
         for i in idx:
             j = int(rng.integers(len(self.xs))) if rng is not None else 0
             arrs = [self.xs[j][i], self.t[j][i], self.dens[i], self.mat[i], self.w[i]]
+            if self.unc is not None:
+                arrs.append(self.unc[j][i])
             if rng is not None:
                 for ax in range(3):
                     if rng.random() < 0.5:
                         arrs = [np.flip(a, axis=ax) for a in arrs]
             xs.append(arrs[0]); ts.append(arrs[1]); ds.append(arrs[2]); ms.append(arrs[3]); ws.append(arrs[4])
-        return [np.ascontiguousarray(np.stack(a)) for a in (xs, ts, ds, ms, ws)]
+            if self.unc is not None:
+                us.append(arrs[5])
+        out = [np.ascontiguousarray(np.stack(a)) for a in (xs, ts, ds, ms, ws)]
+        out.append(np.ascontiguousarray(np.stack(us)) if self.unc is not None else None)
+        return out
 
 
 def train(model: DN.UNet3D, data: Dataset, steps: int, batch: int, lr: float, seed: int = 0, log_every: int = 50):
@@ -126,8 +134,8 @@ def train(model: DN.UNet3D, data: Dataset, steps: int, batch: int, lr: float, se
     t0 = time.perf_counter()
     for step in range(steps):
         idx = rng.choice(data.n, size=batch, replace=data.n < batch)
-        x, t, d, m, w = data.batch(idx, rng)
-        model.set_input(x, d, m, batch, S)
+        x, t, d, m, w, u = data.batch(idx, rng)
+        model.set_input(x, d, m, batch, S, unc=u)
         tgt.copy_(torch.from_numpy(t.reshape(-1)))
         wgt.copy_(torch.from_numpy(w.reshape(-1)))
         model.forward()
@@ -151,7 +159,8 @@ def denoise(model: DN.UNet3D, data: Dataset, batch: int = 8) -> tuple[np.ndarray
     for b0 in range(0, data.n, batch):
         idx = list(range(b0, min(b0 + batch, data.n)))
         bsz = len(idx)
-        model.set_input(data.x[idx], data.dens[idx], data.mat[idx], bsz, S)
+        model.set_input(data.x[idx], data.dens[idx], data.mat[idx], bsz, S,
+                        unc=data.unc[0][idx] if data.unc is not None else None)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record()
         y = model.predict()
@@ -178,14 +187,16 @@ def run(args) -> dict:
     tr_mat = np.stack([m for m, _ in tr_maps]); tr_den = np.stack([d for _, d in tr_maps])
     te_mat = np.stack([m for m, _ in te_maps]); te_den = np.stack([d for _, d in te_maps])
 
-    k_in, ms_in = [], 0.0
+    k_in, r_in, ms_in = [], [], 0.0
+    slots = 16 if args.uncertainty else 1
     for j, n in enumerate(args.n_in):
-        k, _, ms = mc_maps(tr_sc, tr_gr, n, 1000 + 100 * j, eng)
+        k, r, ms = mc_maps(tr_sc, tr_gr, n, 1000 + 100 * j, eng, stats_slots=slots)
         k_in.append(k)
+        r_in.append(r)
         ms_in += ms
     k_tg, _, ms_tg = mc_maps(tr_sc, tr_gr, args.n_target, 2000, eng)
-    train_set = Dataset(k_in, k_tg, tr_mat, tr_den)
-    del k_in, k_tg
+    train_set = Dataset(k_in, k_tg, tr_mat, tr_den, rel=r_in if args.uncertainty else None)
+    del k_in, k_tg, r_in
     k_ref, rel_ref, ms_ref = mc_maps(te_sc, te_gr, args.n_ref, 3000, eng, stats_slots=16)
     model = DN.UNet3D(seed=args.seed)
     losses, t_train = train(model, train_set, args.steps, args.batch, args.lr, seed=args.seed)
@@ -198,7 +209,7 @@ def run(args) -> dict:
     levels = []
     for n in args.levels:
         k_n, rel_n, ms_n = mc_maps(te_sc, te_gr, n, 4000 + n % 997, eng, stats_slots=16)
-        test = Dataset(k_n, None, te_mat, te_den)
+        test = Dataset(k_n, None, te_mat, te_den, rel=rel_n if args.uncertainty else None)
         k_dn, ms_dn = denoise(model, test)
         plain_meas = median_rel_error(k_n, k_ref, inside)
         dn_meas = median_rel_error(k_dn, k_ref, inside)
@@ -220,6 +231,7 @@ def run(args) -> dict:
         "workload": f"denoiser: {args.train} training + {args.test} held-out phantoms, {S}^3 voxels of "
                     f"{args.voxel_cm} cm, ellipsoid water/bone/lead/air, 60-120 kVp cone beam",
         "histories": {"input": args.n_in, "target": args.n_target, "reference": args.n_ref},
+        "uncertainty_channel": bool(args.uncertainty),
         "mc_histories_per_s_batched": rate,
         "train": {"steps": args.steps, "batch": args.batch, "lr": args.lr, "seconds": t_train,
                   "tflops_per_s": flops_step * args.steps / t_train / 1e12, "losses": losses,
@@ -283,6 +295,8 @@ def main(argv=None) -> None:
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--seed", type=int, default=7)
     ap.add_argument("--save", default=None, help="write the trained parameters (.npy)")
+    ap.add_argument("--no-uncertainty", dest="uncertainty", action="store_false",
+                    help="do not give the network the input map's relative standard error")
     ap.add_argument("--timing", type=int, nargs=2, metavar=("B", "S"), default=None,
                     help="only time the network's kernels on B random volumes of side S")
     ap.add_argument("--timing-steps", type=int, default=10)

@@ -180,8 +180,11 @@ class UNet3D:
 
     # -- forward ----------------------------------------------------------
     def set_input(self, xlog: np.ndarray | None, density: np.ndarray | None, mat: np.ndarray | None,
-                  B: int, S: int, device_xlog=None, device_density=None, device_mat=None) -> None:
-        """Input volumes [B, S, S, S] (host arrays, or device tensors)."""
+                  B: int, S: int, device_xlog=None, device_density=None, device_mat=None,
+                  unc: np.ndarray | None = None) -> None:
+        """Input volumes [B, S, S, S] (host arrays, or device tensors); unc,
+        when given, is the input map's relative standard error (see
+        ``uncertainty_channel``)."""
         torch = self.torch
         self._alloc(B, S)
         n0 = B * S ** 3
@@ -191,10 +194,14 @@ class UNet3D:
             np.ascontiguousarray(density, dtype=np.float32).reshape(-1) * DENSITY_SCALE).to(self.dev, non_blocking=True)
         ma = device_mat if device_mat is not None else torch.from_numpy(
             np.ascontiguousarray(mat, dtype=np.uint8).reshape(-1)).to(self.dev, non_blocking=True)
+        un = None
+        if unc is not None:
+            un = torch.from_numpy(np.ascontiguousarray(unc, dtype=np.float32).reshape(-1)).to(self.dev,
+                                                                                           non_blocking=True)
         self.xlog.copy_(xl)
-        self._call(U.lib().ccu_input, self._ptr(self.xlog), self._ptr(de), self._ptr(ma), N_MAT, n0,
-                   self._ptr(self.a["x0"]), self._stream())
-        self._keep = (de, ma)
+        self._call(U.lib().ccu_input, self._ptr(self.xlog), self._ptr(de), self._ptr(ma), N_MAT,
+                   self._ptr(un) if un is not None else None, n0, self._ptr(self.a["x0"]), self._stream())
+        self._keep = (de, ma, un)
 
     def forward(self) -> None:
         a, lib, st = self.a, U.lib(), self._stream()
@@ -315,6 +322,17 @@ def kerma_scale(k_in: np.ndarray, inside: np.ndarray) -> float:
 
 def to_log(k: np.ndarray, s: float) -> np.ndarray:
     return np.log(np.maximum(k, 0.0) / s + EPS).astype(np.float32)
+
+
+UNC_MAX = 1.5
+
+
+def uncertainty_channel(rel: np.ndarray) -> np.ndarray:
+    """The relative standard error of an input map as a network channel:
+    clipped to [0, UNC_MAX], voxels without an estimate (no score, or fewer
+    than two batches) at UNC_MAX."""
+    r = np.nan_to_num(np.asarray(rel, dtype=np.float64), nan=UNC_MAX, posinf=UNC_MAX)
+    return np.clip(r, 0.0, UNC_MAX).astype(np.float32)
 
 
 def from_log(x: np.ndarray, s: float) -> np.ndarray:

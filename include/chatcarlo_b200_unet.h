@@ -78,10 +78,12 @@ int ccu_up_reduce(const void* g_full, const void* coarse_act, int batch, int d, 
 int ccu_head(const void* d0, const float* xlog, const float* target, const float* weight, const float* head,
              float inv_wsum, long long n_vox, float* out, void* dz, float* dhead, float* loss, void* stream);
 
-/* Network input [n_vox, 16] BF16: normalised log kerma, density, material
- * one-hot (mat < n_mat <= 14), zeros. */
-int ccu_input(const float* xlog, const float* density, const uint8_t* mat, int n_mat, long long n_vox, void* x,
-              void* stream);
+/* Network input [n_vox, 16] BF16: normalised log kerma, density,
+ * material one-hot (mat < n_mat <= 13), zeros, and in channel 15 unc[v]
+ * (the input map's relative standard error, clipped by the caller) when
+ * unc is not NULL. */
+int ccu_input(const float* xlog, const float* density, const uint8_t* mat, int n_mat, const float* unc,
+              long long n_vox, void* x, void* stream);
 
 /* One Adam step (bias-corrected, decoupled weight decay wd) on n FP32
  * parameters; step counts from 1. */

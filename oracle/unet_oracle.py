@@ -85,13 +85,15 @@ def up_sum(g):
     return g.reshape(B, D // 2, 2, H // 2, 2, W // 2, 2, C).sum(axis=(2, 4, 6))
 
 
-def make_input(xlog, density, mat):
+def make_input(xlog, density, mat, unc=None):
     """[B, S, S, S] maps -> [B, S, S, S, 16] network input (before rounding)."""
     x = np.zeros(xlog.shape + (IN_CH,))
     x[..., 0] = xlog
     x[..., 1] = density * DENSITY_SCALE
     for m in range(N_MAT):
         x[..., 2 + m] = (mat == m)
+    if unc is not None:
+        x[..., 15] = unc
     return x
 
 

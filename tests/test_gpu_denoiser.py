@@ -149,16 +149,17 @@ def test_trained_denoiser_beats_plain_monte_carlo_at_equal_histories():
     te_sc, te_gr = PH.phantoms(6, 12, S, 0.5)
     tr = [PH.voxel_maps(s, g) for s, g in zip(tr_sc, tr_gr)]
     te = [PH.voxel_maps(s, g) for s, g in zip(te_sc, te_gr)]
-    k_in = [R.mc_maps(tr_sc, tr_gr, n, 1 + n % 7, eng)[0] for n in (100_000, 400_000)]
+    runs = [R.mc_maps(tr_sc, tr_gr, n, 1 + n % 7, eng, stats_slots=16) for n in (100_000, 400_000)]
     k_tg, _, _ = R.mc_maps(tr_sc, tr_gr, 10_000_000, 2, eng)
-    data = R.Dataset(k_in, k_tg, np.stack([m for m, _ in tr]), np.stack([d for _, d in tr]))
+    data = R.Dataset([r[0] for r in runs], k_tg, np.stack([m for m, _ in tr]), np.stack([d for _, d in tr]),
+                     rel=[r[1] for r in runs])
     model = DN.UNet3D(seed=1)
     losses, _ = R.train(model, data, steps=400, batch=4, lr=2e-3, seed=1)
     assert losses[-1][1] < 0.5 * losses[0][1], losses
     te_mat = np.stack([m for m, _ in te])
     k_ref, _, _ = R.mc_maps(te_sc, te_gr, 100_000_000, 3, eng)
-    k_lo, _, _ = R.mc_maps(te_sc, te_gr, 100_000, 4, eng)
-    k_dn, _ = R.denoise(model, R.Dataset(k_lo, None, te_mat, np.stack([d for _, d in te])))
+    k_lo, r_lo, _ = R.mc_maps(te_sc, te_gr, 100_000, 4, eng, stats_slots=16)
+    k_dn, _ = R.denoise(model, R.Dataset(k_lo, None, te_mat, np.stack([d for _, d in te]), rel=r_lo))
     inside = R.inside_mask(te_mat)
     e_plain = R.median_rel_error(k_lo, k_ref, inside)
     e_dn = R.median_rel_error(k_dn, k_ref, inside)
