@@ -170,6 +170,77 @@ def _ref_init(root):
 
 
 # ---------------------------------------------------------------------------
+# learned denoiser leg
+# ---------------------------------------------------------------------------
+
+def denoiser_metric(eng, n_phantoms: int, levels=(500_000, 1_000_000, 2_000_000), n_ref: int = 400_000_000,
+                    seed: int = 1001) -> dict:
+    """Time to a 2 % median voxel-kerma error per phantom: plain batched
+    Monte Carlo (its error from its own batch statistics, 1/sqrt(n)) against
+    batched Monte Carlo at fewer histories plus the shipped denoiser (its
+    error against an n_ref-history reference, the reference's own noise
+    removed in quadrature), on phantoms the network was not trained on."""
+    import torch
+    from chatcarlo_b200 import denoise_run as R
+    from chatcarlo_b200 import denoiser as DN
+    from chatcarlo_b200 import phantoms as PH
+    params, meta = DN.load_params()
+    model = DN.UNet3D(params=params)
+    sc, gr = PH.phantoms(n_phantoms, seed, 64, 0.5)
+    maps = [PH.voxel_maps(a, b) for a, b in zip(sc, gr)]
+    mat = np.stack([m for m, _ in maps])
+    den = np.stack([d for _, d in maps])
+    inside = R.inside_mask(mat)
+    k_ref, rel_ref, ms_ref = R.mc_maps(sc, gr, n_ref, seed + 1, eng, stats_slots=16)
+    rate = n_ref * n_phantoms / (ms_ref * 1e-3)
+    ref_noise = float(np.median(0.6745 * np.nan_to_num(rel_ref[inside & (k_ref > 0)], nan=0.0)))
+    rows = []
+    for n in levels:
+        k_n, rel_n, _ = R.mc_maps(sc, gr, n, seed + 2 + n % 991, eng, stats_slots=16)
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record()
+        k_dn = DN.denoise_kerma(k_n, rel_n, mat, den, model=model)
+        ev1.record()
+        ev1.synchronize()
+        dn = R.median_rel_error(k_dn, k_ref, inside)
+        plain = float(np.median(0.6745 * np.nan_to_num(rel_n[inside & (k_ref > 0)], nan=1.0)))
+        rows.append({"histories": n, "plain": plain, "plain_measured": R.median_rel_error(k_n, k_ref, inside),
+                     "denoised": float(np.sqrt(max(dn * dn - ref_noise ** 2, 0.0))), "denoised_measured": dn})
+    t_inf = DN_inference_s(model, n_phantoms)
+    c = float(np.median([r["plain"] * np.sqrt(r["histories"]) for r in rows]))
+    n_plain = (c / 0.02) ** 2
+    n_dn = R.histories_for_error([r["histories"] for r in rows], [r["denoised"] for r in rows], 0.02)
+    t_plain = n_plain / rate
+    t_dn = n_dn / rate + t_inf if n_dn is not None else None
+    return {"metric": "time to 2% median voxel-kerma error per phantom (s)", "unit": "s",
+            "plain_mc": t_plain, "denoised_batched": t_dn, "speedup": (t_plain / t_dn) if t_dn else None,
+            "plain_histories": n_plain, "denoised_histories": n_dn, "inference_s_per_phantom": t_inf,
+            "batched_mc_histories_per_s": rate, "reference_histories": n_ref, "reference_noise": ref_noise,
+            "levels": rows, "phantoms": f"{n_phantoms} held-out 64^3 ellipsoid phantoms (seed {seed})",
+            "network": meta.get("trained_by")}
+
+
+def DN_inference_s(model, n_phantoms: int) -> float:
+    """Device time per phantom of the network's forward pass at batch 8."""
+    import torch
+    S, B = 64, min(8, n_phantoms)
+    rng = np.random.default_rng(0)
+    x = rng.normal(size=(B, S, S, S)).astype(np.float32)
+    m = rng.integers(0, 4, size=(B, S, S, S)).astype(np.uint8)
+    d = np.ones((B, S, S, S), np.float32)
+    model.set_input(x, d, m, B, S, unc=np.full((B, S, S, S), 0.1, np.float32))
+    model.predict()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    for _ in range(5):
+        model.predict()
+    ev1.record()
+    ev1.synchronize()
+    return ev0.elapsed_time(ev1) / 5 / B * 1e-3
+
+
+# ---------------------------------------------------------------------------
 # engine arm
 # ---------------------------------------------------------------------------
 
@@ -187,6 +258,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-precision", action="store_true", help="skip the FP32-vs-FP64 tracking tally report")
     ap.add_argument("--precision-histories", type=float, default=1e7)
+    ap.add_argument("--no-denoiser", action="store_true", help="skip the denoised time-to-2 %% measurement")
+    ap.add_argument("--denoiser-phantoms", type=int, default=8)
     ap.add_argument("--workload", choices=["room", "ct"], default="room",
                     help="room-scale (the headline configuration) or CT dosimetry")
     args = ap.parse_args()
@@ -366,6 +439,12 @@ def main():
                      **{t: {k: rep[t][k] for k in ("rel_median", "rel_p99", "sigma_median", "sigma_p99",
                                                    "sigma_max", "total_rel")} for t in ("kerma", "h10")}}
 
+    # learned denoiser: time to a 2 % median voxel-kerma error, denoised +
+    # batched Monte Carlo vs plain batched Monte Carlo, on held-out phantoms
+    denoise = None
+    if rank == 0 and world == 1 and not args.no_denoiser:
+        denoise = denoiser_metric(eng, args.denoiser_phantoms)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         per_core = args.cpu_histories_per_process
@@ -391,6 +470,7 @@ def main():
                              "avg_launch_ms": tr_ms / max(tr_launch, 1),
                              "histories_per_launch": hist_per_launch},
                 "cpu_baseline": cpu, "e2e": e2e, "e2e_photons": e2e_photons, "precision": precision,
+                "denoiser": denoise,
                 "clocks": clocks,
                 "gpu_launches": int(launches),
                 "reduce_ms": red_ms}

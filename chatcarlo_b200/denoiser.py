@@ -337,3 +337,76 @@ def uncertainty_channel(rel: np.ndarray) -> np.ndarray:
 
 def from_log(x: np.ndarray, s: float) -> np.ndarray:
     return (s * (np.exp(x.astype(np.float64)) - EPS)).clip(min=0.0)
+
+
+# ---------------------------------------------------------------------------
+# parameter files
+# ---------------------------------------------------------------------------
+
+PRETRAINED = __import__("pathlib").Path(__file__).resolve().parent / "data" / "denoiser_unet64.npz"
+
+
+def _bf16_bits(x: np.ndarray) -> np.ndarray:
+    u = np.ascontiguousarray(x, dtype=np.float32).view(np.uint32).astype(np.uint64)
+    return ((u + 0x7FFF + ((u >> 16) & 1)) >> 16).astype(np.uint16)
+
+
+def save_params(path, params: np.ndarray, meta: dict | None = None) -> None:
+    """Convolution weights as BF16 (the precision the kernels use), biases
+    and head FP32, and a JSON description."""
+    import json
+    p = np.asarray(params, dtype=np.float32)
+    lay = param_layout()
+    wmask = np.zeros(p.size, dtype=bool)
+    for L in LAYERS:
+        o, n, _, _ = lay[L.name]
+        wmask[o:o + n] = True
+    np.savez_compressed(path, weights_bf16=_bf16_bits(p[wmask]), rest=p[~wmask],
+                        meta=np.array(json.dumps(meta or {})), n_params=np.array(p.size))
+
+
+def load_params(path=None) -> tuple[np.ndarray, dict]:
+    """(flat FP32 parameters, description) from save_params; the shipped
+    pretrained network by default."""
+    import json
+    z = np.load(path or PRETRAINED)
+    n = int(z["n_params"])
+    if n != n_params():
+        raise ValueError(f"{path}: {n} parameters, this network has {n_params()}")
+    lay = param_layout()
+    wmask = np.zeros(n, dtype=bool)
+    for L in LAYERS:
+        o, m, _, _ = lay[L.name]
+        wmask[o:o + m] = True
+    p = np.empty(n, dtype=np.float32)
+    p[wmask] = (z["weights_bf16"].astype(np.uint32) << 16).view(np.float32)
+    p[~wmask] = z["rest"]
+    return p, json.loads(str(z["meta"]))
+
+
+def denoise_kerma(k_in: np.ndarray, rel: np.ndarray, mat: np.ndarray, density: np.ndarray,
+                  model: "UNet3D | None" = None, batch: int = 8) -> np.ndarray:
+    """Denoised kerma maps from plain Monte Carlo maps.
+
+    k_in: [n, S, S, S] kerma (any unit, per history or total), rel: its
+    per-voxel relative standard error (batch statistics), mat: material
+    index (air 0, water 1, bone 2, lead 3), density [g/cm^3]; S a multiple
+    of 8.  The shipped network (``PRETRAINED``) unless a model is given.
+    Returns the denoised maps in the unit of k_in."""
+    import torch
+    model = model or UNet3D(params=load_params()[0])
+    k_in = np.asarray(k_in, dtype=np.float64)
+    n, S = k_in.shape[0], k_in.shape[1]
+    out = np.empty_like(k_in)
+    for b0 in range(0, n, batch):
+        idx = list(range(b0, min(b0 + batch, n)))
+        inside = [mat[i] != 0 for i in idx]
+        scales = [kerma_scale(k_in[i], inside[j]) for j, i in enumerate(idx)]
+        x = np.stack([to_log(k_in[i], scales[j]) for j, i in enumerate(idx)])
+        model.set_input(x, density[idx], mat[idx], len(idx), S, unc=uncertainty_channel(rel[idx]))
+        y = model.predict().cpu().numpy().reshape(len(idx), S, S, S)
+        for j, i in enumerate(idx):
+            out[i] = from_log(y[j], scales[j])
+    torch.cuda.synchronize()
+    model.check_status()
+    return out

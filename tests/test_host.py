@@ -266,3 +266,15 @@ def test_histories_for_error_interpolates_in_log_log():
     assert histories_for_error(h, e, 0.0283) == pytest.approx(8e5, rel=1e-2)
     assert histories_for_error(h, e, 0.01) is None
     assert histories_for_error(h, [0.01, 0.009, 0.008], 0.02) == 1e5
+
+
+def test_shipped_denoiser_parameters_load():
+    from chatcarlo_b200 import denoiser as DN
+    p, meta = DN.load_params()
+    assert p.shape == (DN.n_params(),) and np.all(np.isfinite(p))
+    assert meta["uncertainty_channel"] is True and meta["held_out"]["time_to_2pct_s"]["speedup"] > 1
+    import tempfile, os
+    with tempfile.TemporaryDirectory() as d:
+        DN.save_params(os.path.join(d, "p.npz"), p, meta)
+        q, m2 = DN.load_params(os.path.join(d, "p.npz"))
+    np.testing.assert_array_equal(p, q)
