@@ -880,9 +880,14 @@ transport_kernel(const KTables T, const KScene S, const KGrid G, const KSource S
             float tot = ph + co + ra;
             float r = rng.uniform() * tot;
             ++nsc;
-            if (r < ph) {
+            const int kind = r < ph ? 0 : (r < ph + co ? 1 : 2);
+            // The element draw, the new direction and the new free path are
+            // common to the three interactions; they run outside the branches
+            // so that every interacting lane of the warp executes them together.
+            const int slot = pick_element(T, M, L, kind, rng.uniform());
+            float cost = 1.0f, e_new = E, dep = 0.0f;
+            if (kind == 0) {
                 // photoelectric, K fluorescence (physics.py:155-212, transport.py:174-198)
-                int slot = pick_element(T, M, L, 0, rng.uniform());
                 const DevElement& el = T.elems[slot];
                 float e_line = 0.0f;
                 bool emit = false;
@@ -896,36 +901,31 @@ transport_kernel(const KTables T, const KScene S, const KGrid G, const KSource S
                         if (el.line_e[li] >= FLUOR_CUTOFF) { emit = true; e_line = el.line_e[li]; }
                     }
                 }
-                atomicAdd(&s_edep[batch * T.n_mat + mat], (double)(emit ? E - e_line : E));
+                dep = emit ? E - e_line : E;
                 if (emit) {
                     ++c_fl;
-                    E = e_line;
-                    isotropic(d, rng);
-                    tau = -__logf(rng.uniform());
+                    e_new = e_line;
                 } else {
                     absd = true;
                     done = true;
                 }
-            } else if (r < ph + co) {
-                int slot = pick_element(T, M, L, 1, rng.uniform());
-                float eps, cost;
+            } else if (kind == 1) {
+                float eps;
                 sample_compton(T.sq + (size_t)slot * TABLE_N, E, rng, eps, cost);
-                float e_new = E * eps;
-                atomicAdd(&s_edep[batch * T.n_mat + mat], (double)(E - e_new));
-                scatter_direction(d, cost, TWO_PI * rng.uniform());
+                e_new = E * eps;
+                dep = E - e_new;
+            } else if (!sample_rayleigh(T.rx + (size_t)slot * TABLE_N, T.ra + (size_t)slot * TABLE_N,
+                                        T.ray_bucket + (size_t)slot * (RAY_BUCKETS + 1), T.elems[slot].ray_scale,
+                                        E, rng, cost)) {
+                atomicOr(R.status, ST_RAYLEIGH_Q);
+                live = false;
+                continue;
+            }
+            if (kind < 2) atomicAdd(&s_edep[batch * T.n_mat + mat], (double)dep);
+            if (!done) {
+                if (kind == 0) isotropic(d, rng);                     // the fluorescence photon
+                else scatter_direction(d, cost, TWO_PI * rng.uniform());
                 E = e_new;
-                tau = -__logf(rng.uniform());
-            } else {
-                int slot = pick_element(T, M, L, 2, rng.uniform());
-                float cost;
-                if (!sample_rayleigh(T.rx + (size_t)slot * TABLE_N, T.ra + (size_t)slot * TABLE_N,
-                                     T.ray_bucket + (size_t)slot * (RAY_BUCKETS + 1), T.elems[slot].ray_scale,
-                                     E, rng, cost)) {
-                    atomicOr(R.status, ST_RAYLEIGH_Q);
-                    live = false;
-                    continue;
-                }
-                scatter_direction(d, cost, TWO_PI * rng.uniform());
                 tau = -__logf(rng.uniform());
             }
             mat = -1;                      // new direction: re-locate (material_at every round)
@@ -1178,8 +1178,13 @@ batch_kernel(const KTables T, const KBatch B, const KRun R) {
                 parts(T, M, L, ph, co, ra);
                 float r = rng.uniform() * (ph + co + ra);
                 ++nsc;
-                if (r < ph) {
-                    int eslot = pick_element(T, M, L, 0, rng.uniform());
+                const int kind = r < ph ? 0 : (r < ph + co ? 1 : 2);
+                // element draw, new direction and new free path outside the
+                // branches: every interacting lane runs them together
+                const int eslot = pick_element(T, M, L, kind, rng.uniform());
+                float cost = 1.0f, e_new = E;
+                bool ok = true;
+                if (kind == 0) {
                     const DevElement& el = T.elems[eslot];
                     float e_line = 0.0f;
                     bool emit = false;
@@ -1195,32 +1200,27 @@ batch_kernel(const KTables T, const KBatch B, const KRun R) {
                     }
                     if (emit) {
                         atomicAdd(B.scene_cnt + 4 * (size_t)sc + 3, 1ull);   // rare: K lines of heavy elements
-                        E = e_line;
-                        isotropic(d, rng);
-                        tau = -__logf(rng.uniform());
+                        e_new = e_line;
                     } else {
                         absd = true;
                         ended = true;
                     }
-                } else if (r < ph + co) {
-                    int eslot = pick_element(T, M, L, 1, rng.uniform());
-                    float eps, cost;
+                } else if (kind == 1) {
+                    float eps;
                     sample_compton(T.sq + (size_t)eslot * TABLE_N, E, rng, eps, cost);
-                    scatter_direction(d, cost, TWO_PI * rng.uniform());
-                    E *= eps;
+                    e_new = E * eps;
+                } else if (!sample_rayleigh(T.rx + (size_t)eslot * TABLE_N, T.ra + (size_t)eslot * TABLE_N,
+                                            T.ray_bucket + (size_t)eslot * (RAY_BUCKETS + 1),
+                                            T.elems[eslot].ray_scale, E, rng, cost)) {
+                    atomicOr(R.status, ST_RAYLEIGH_Q);
+                    ended = true;
+                    ok = false;
+                }
+                if (ok && !ended) {
+                    if (kind == 0) isotropic(d, rng);                   // the fluorescence photon
+                    else scatter_direction(d, cost, TWO_PI * rng.uniform());
+                    E = e_new;
                     tau = -__logf(rng.uniform());
-                } else {
-                    int eslot = pick_element(T, M, L, 2, rng.uniform());
-                    float cost;
-                    if (!sample_rayleigh(T.rx + (size_t)eslot * TABLE_N, T.ra + (size_t)eslot * TABLE_N,
-                                         T.ray_bucket + (size_t)eslot * (RAY_BUCKETS + 1), T.elems[eslot].ray_scale,
-                                         E, rng, cost)) {
-                        atomicOr(R.status, ST_RAYLEIGH_Q);
-                        ended = true;
-                    } else {
-                        scatter_direction(d, cost, TWO_PI * rng.uniform());
-                        tau = -__logf(rng.uniform());
-                    }
                 }
                 mat = -1;
             }
