@@ -258,6 +258,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-precision", action="store_true", help="skip the FP32-vs-FP64 tracking tally report")
     ap.add_argument("--precision-histories", type=float, default=1e7)
+    ap.add_argument("--no-fp32-cells", action="store_true",
+                    help="skip the side measurement with FP32 tally scratch cells")
     ap.add_argument("--no-denoiser", action="store_true", help="skip the denoised time-to-2 %% measurement")
     ap.add_argument("--denoiser-phantoms", type=int, default=8)
     ap.add_argument("--workload", choices=["room", "ct"], default="room",
@@ -439,6 +441,47 @@ def main():
                      **{t: {k: rep[t][k] for k in ("rel_median", "rel_p99", "sigma_median", "sigma_p99",
                                                    "sigma_max", "total_rel")} for t in ("kerma", "h10")}}
 
+    # side measurement: the same steps with FP32 tally scratch cells (an
+    # opt-in of the context), and what they cost each tally against the
+    # default FP64 cells on the same histories (tracking identical, so the
+    # difference is the FP32 summation alone)
+    fp32_cells = None
+    if rank == 0 and world == 1 and not args.no_fp32_cells:
+        from chatcarlo_b200.precision import _stats
+        n_side = min(args.steps, 5)
+        eng.set_tally_fp32(True)
+        try:
+            N.check(eng.lib.cc_grid_reset(dg.handle))
+            for i in range(args.warmup):
+                step(i)
+            N.check(eng.lib.cc_grid_reset(dg.handle))
+            f_ms = []
+            for i in range(n_side):
+                flush.zero_()
+                torch.cuda.synchronize()
+                ev0.record()
+                step(args.warmup + i)
+                ev1.record()
+                torch.cuda.synchronize()
+                f_ms.append(ev0.elapsed_time(ev1))
+            grids = []
+            for on in (False, True):
+                eng.set_tally_fp32(on)
+                N.check(eng.lib.cc_grid_reset(dg.handle))
+                step(0)
+                g = W.make_grid(gspec, track_uncertainty=True)
+                dg.download(g)
+                grids.append(g)
+        finally:
+            eng.set_tally_fp32(False)
+        g64, g32 = grids
+        fp32_cells = {"value": S * n_side / (float(np.sum(f_ms)) / 1e3), "unit": "histories/s", "steps": n_side,
+                      "vs_fp64_cells": {"histories": S,
+                                        "kerma": _stats(g32.kerma_keV, g64.kerma_keV, g64.kerma_sum2,
+                                                        g64.n_batches, g64.n_histories),
+                                        "h10": _stats(g32.h10_track_pSv_cm3, g64.h10_track_pSv_cm3,
+                                                      g64.h10_sum2, g64.n_batches, g64.n_histories)}}
+
     # learned denoiser: time to a 2 % median voxel-kerma error, denoised +
     # batched Monte Carlo vs plain batched Monte Carlo, on held-out phantoms
     denoise = None
@@ -470,7 +513,7 @@ def main():
                              "avg_launch_ms": tr_ms / max(tr_launch, 1),
                              "histories_per_launch": hist_per_launch},
                 "cpu_baseline": cpu, "e2e": e2e, "e2e_photons": e2e_photons, "precision": precision,
-                "denoiser": denoise,
+                "denoiser": denoise, "tally_fp32_cells": fp32_cells,
                 "clocks": clocks,
                 "gpu_launches": int(launches),
                 "reduce_ms": red_ms}

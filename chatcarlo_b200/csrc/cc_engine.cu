@@ -116,7 +116,8 @@ struct KScene {
 };
 
 struct KGrid {
-    double* tally;          // [n_scratch][nvox] double2 (kerma, h10)
+    double* tally;          // [n_slots][nvox] 16-byte scratch cells (kerma, h10) of one batch each
+    int tally32;            // cells hold float2 (one vector reduction per visit) instead of double2
     real o[3];
     real h, inv_h;
     int nx, ny, nz;
@@ -195,6 +196,12 @@ __device__ __forceinline__ bool ball_inside(real o2, real od, real r, real tol) 
     return od <= 0.0f;
 }
 
+// Component k of a 3-vector held in registers.  Indexing a register array
+// with a runtime k would place the array in local memory for the whole
+// kernel, so every runtime axis goes through this select.
+template <typename V>
+__device__ __forceinline__ V comp(const V v[3], int k) { return k == 0 ? v[0] : (k == 1 ? v[1] : v[2]); }
+
 __device__ __forceinline__ bool contains(const DevPrim& g, const real p[3], const real d[3], real tol) {
     real o0 = p[0] - g.c[0], o1 = p[1] - g.c[1], o2 = p[2] - g.c[2];
     if (g.type == CC_SHAPE_BOX) {
@@ -211,9 +218,9 @@ __device__ __forceinline__ bool contains(const DevPrim& g, const real p[3], cons
     } else {
         const int ax = g.axis;
         const int i0 = ax == 0 ? 1 : 0, i1 = ax == 2 ? 1 : 2;
-        real oa = p[i0] - g.c[i0], ob = p[i1] - g.c[i1], ow = p[ax] - g.c[ax];
-        return ball_inside(oa * oa + ob * ob, oa * d[i0] + ob * d[i1], g.r, tol) &&
-               slab_inside(ow, d[ax], g.hh, tol);
+        real oa = comp(p, i0) - comp(g.c, i0), ob = comp(p, i1) - comp(g.c, i1), ow = comp(p, ax) - comp(g.c, ax);
+        return ball_inside(oa * oa + ob * ob, oa * comp(d, i0) + ob * comp(d, i1), g.r, tol) &&
+               slab_inside(ow, comp(d, ax), g.hh, tol);
     }
 }
 
@@ -245,7 +252,7 @@ __device__ __forceinline__ void take_root(real t, real eps, real& best) {
 }
 
 // Smallest root t > eps of primitive g along the ray (geometry.py:20-99), or best.
-__device__ real prim_next(const DevPrim& g, const real p[3], const real d[3], const real inv[3], real eps,
+__device__ __forceinline__ real prim_next(const DevPrim& g, const real p[3], const real d[3], const real inv[3], real eps,
                            real best) {
     real ox = p[0] - g.c[0], oy = p[1] - g.c[1], oz = p[2] - g.c[2];
     if (g.type == CC_SHAPE_BOX) {
@@ -298,8 +305,8 @@ __device__ real prim_next(const DevPrim& g, const real p[3], const real d[3], co
     } else {
         const int ax = g.axis;
         const int i0 = ax == 0 ? 1 : 0, i1 = ax == 2 ? 1 : 2;
-        real a0 = p[i0] - g.c[i0], a1 = p[i1] - g.c[i1], aw = p[ax] - g.c[ax];
-        real dx = d[i0], dy = d[i1], dw = d[ax];
+        real a0 = comp(p, i0) - comp(g.c, i0), a1 = comp(p, i1) - comp(g.c, i1), aw = comp(p, ax) - comp(g.c, ax);
+        real dx = comp(d, i0), dy = comp(d, i1), dw = comp(d, ax);
         real a = dx * dx + dy * dy;
         real rho2 = a0 * a0 + a1 * a1;
         real cc = rho2 - g.r2;
@@ -323,7 +330,7 @@ __device__ real prim_next(const DevPrim& g, const real p[3], const real d[3], co
             real r1 = q * inva, r2 = (q != 0.0f) ? cc / q : 0.0f;
             tmin = fmin(r1, r2); tmax = fmax(r1, r2);
         }
-        if (!slab_pair(aw, dw, inv[ax], -g.hh, g.hh, eps, tmin, tmax)) return best;
+        if (!slab_pair(aw, dw, comp(inv, ax), -g.hh, g.hh, eps, tmin, tmax)) return best;
         if (tmin <= tmax) { take_root(tmin, eps, best); take_root(tmax, eps, best); }
         return best;
     }
@@ -426,7 +433,7 @@ __device__ __forceinline__ float s_over_z(const float* s, float q) {
 }
 
 // Bound Compton: Kahn-type KN proposal with S(Z,q)/Z rejection (physics.py:41-56, 95-135).
-__device__ void sample_compton(const float* sz, float E, HistoryRng& rng, float& eps_out, float& cos_out) {
+__device__ __forceinline__ void sample_compton(const float* sz, float E, HistoryRng& rng, float& eps_out, float& cos_out) {
     float alpha = E / MEC2;
     float emin = 1.0f / (1.0f + 2.0f * alpha);
     float env = 1.0f / emin + emin;
@@ -447,7 +454,7 @@ __device__ void sample_compton(const float* sz, float E, HistoryRng& rng, float&
 // Rayleigh: inverse of A(x) then (1+cos^2)/2 rejection (physics.py:281-351).
 // The row of a target A comes from a uniform-in-A bucket index, then a
 // short binary search inside the bucket.
-__device__ __noinline__ bool sample_rayleigh(const float* rx, const float* ra, const int* bucket, float scale,
+__device__ __forceinline__ bool sample_rayleigh(const float* rx, const float* ra, const int* bucket, float scale,
                                              float E, HistoryRng& rng, float& cos_out) {
     float xmax = (E / HC) * (E / HC);
     if (xmax > __ldg(rx + TABLE_N - 1)) return false;
@@ -506,7 +513,7 @@ __device__ __forceinline__ void scatter_direction(real d[3], float cost, float p
     d[0] = r.x; d[1] = r.y; d[2] = r.z;
 }
 
-__device__ void isotropic(real d[3], HistoryRng& rng) {
+__device__ __forceinline__ void isotropic(real d[3], HistoryRng& rng) {
     float c = 2.0f * rng.uniform() - 1.0f;
     float s = sqrtf(fmaxf(0.0f, 1.0f - c * c));
     float sp, cp;
@@ -518,9 +525,20 @@ __device__ void isotropic(real d[3], HistoryRng& rng) {
 // track-length tally: exact voxel traversal (Amanatides & Woo)
 // ---------------------------------------------------------------------------
 
-__device__ __forceinline__ void score(double* tally, int v, real wk_len, real wh_len) {
-    atomicAdd(tally + 2 * v, (double)wk_len);
-    atomicAdd(tally + 2 * v + 1, (double)wh_len);
+// One voxel visit: kerma and H*(10) into the batch's scratch, FP64 cells
+// (two FP64 reductions).  With FP32 cells switched on for the context, a
+// slot that sums at most FP32_SLOT_HISTORIES histories holds FP32 partial
+// sums instead, both scored by one 8-byte vector reduction.  Every slot is
+// folded into the FP64 totals after its launch.
+__device__ __forceinline__ void score(double* tally, int tally32, int v, real wk_len, real wh_len) {
+    if (tally32) {
+        asm volatile("red.global.add.v2.f32 [%0], {%1, %2};" ::"l"(reinterpret_cast<float*>(tally + 2 * v)),
+                     "f"((float)wk_len), "f"((float)wh_len)
+                     : "memory");
+    } else {
+        atomicAdd(tally + 2 * v, (double)wk_len);
+        atomicAdd(tally + 2 * v + 1, (double)wh_len);
+    }
 }
 
 // Clip the ray p + t d, t in [0, s], to the grid box.  Returns false when
@@ -559,56 +577,71 @@ __device__ __forceinline__ int visit_estimate(const KGrid& G, const real p[3], c
     return n;
 }
 
-// Exact voxel traversal (Amanatides & Woo) of p + t d over [t0, t1], which
-// lies inside the grid box; scores weight x overlap length per voxel.
-__device__ int walk_range(const KGrid& G, double* tally, const real p[3], const real d[3],
-                          real t0, real t1, float wk, float wh) {
-    int iv[3], step[3];
-    real tmax[3], tdel[3];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        // voxel of the entry point; a point that rounds onto the far side of
-        // a face gets a zero-length first cell and steps back in
-        int nk = grid_dim(G, k);
-        real x = (p[k] + d[k] * t0 - G.o[k]) * G.inv_h;
-        int i = max(0, min(nk - 1, (int)floor(x)));
-        iv[k] = i;
-        if (d[k] > 1e-12f) {
-            real inv = 1.0f / d[k];
-            step[k] = 1;
-            tmax[k] = (G.o[k] + (real)(i + 1) * G.h - p[k]) * inv;
-            tdel[k] = G.h * inv;
-        } else if (d[k] < -1e-12f) {
-            real inv = 1.0f / d[k];
-            step[k] = -1;
-            tmax[k] = (G.o[k] + (real)i * G.h - p[k]) * inv;
-            tdel[k] = -G.h * inv;
-        } else {
-            step[k] = 0;
-            tmax[k] = INFINITY;
-            tdel[k] = INFINITY;
-        }
+// One axis of the traversal: the entry voxel i, the step s (-1, 0, 1), the
+// ray parameter tm of the next face crossing and the spacing td of those
+// crossings.  A point that rounds onto the far side of a face gets a
+// zero-length first cell and steps back in.
+__device__ __forceinline__ void walk_axis(real o, real h, real inv_h, int n, real p, real d, real t0, int& i,
+                                          int& s, real& tm, real& td) {
+    real x = (p + d * t0 - o) * inv_h;
+    i = max(0, min(n - 1, (int)floor(x)));
+    if (d > 1e-12f) {
+        real inv = 1.0f / d;
+        s = 1;
+        tm = (o + (real)(i + 1) * h - p) * inv;
+        td = h * inv;
+    } else if (d < -1e-12f) {
+        real inv = 1.0f / d;
+        s = -1;
+        tm = (o + (real)i * h - p) * inv;
+        td = -h * inv;
+    } else {
+        s = 0;
+        tm = INFINITY;
+        td = INFINITY;
     }
+}
+
+// Exact voxel traversal (Amanatides & Woo) of p + t d over [t0, t1], which
+// lies inside the grid box; scores weight x overlap length per voxel.  The
+// per-axis state is held in scalars and the crossing axis picked by
+// selects: a register array indexed by the crossing axis would live in
+// local memory.
+__device__ __forceinline__ int walk_range(const KGrid& G, double* tally, const real p[3], const real d[3],
+                                          real t0, real t1, float wk, float wh) {
+    int ix, iy, iz, sx, sy, sz;
+    real mx, my, mz, dx, dy, dz;
+    walk_axis(G.o[0], G.h, G.inv_h, G.nx, p[0], d[0], t0, ix, sx, mx, dx);
+    walk_axis(G.o[1], G.h, G.inv_h, G.ny, p[1], d[1], t0, iy, sy, my, dy);
+    walk_axis(G.o[2], G.h, G.inv_h, G.nz, p[2], d[2], t0, iz, sz, mz, dz);
     real t = t0;
     int guard = G.nx + G.ny + G.nz + 4;
     int visits = 0;
     // flat index (C order, tally.py:292) updated incrementally; grids are < 2^31 voxels
-    const int stride[3] = {G.ny * G.nz, G.nz, 1};
-    int v = (iv[0] * G.ny + iv[1]) * G.nz + iv[2];
+    const int vx = sx * G.ny * G.nz, vy = sy * G.nz, vz = sz;
+    int v = (ix * G.ny + iy) * G.nz + iz;
     while (t < t1 && guard-- > 0) {
-        int ax = (tmax[0] < tmax[1]) ? (tmax[0] < tmax[2] ? 0 : 2) : (tmax[1] < tmax[2] ? 1 : 2);
-        real tn = fmin(tmax[ax], t1);
+        // the axis whose face comes first; ties go to the later axis, except
+        // that x beats z only when strictly first
+        const bool ax0 = (mx < my) && (mx < mz);
+        const bool ax1 = !(mx < my) && (my < mz);
+        const bool ax2 = !ax0 && !ax1;
+        real tn = fmin(ax0 ? mx : (ax1 ? my : mz), t1);
         real len = tn - t;
         if (len > 0.0f) {
-            score(tally, v, wk * len, wh * len);
+            score(tally, G.tally32, v, wk * len, wh * len);
             ++visits;
         }
         t = tn;
         if (t >= t1) break;
-        iv[ax] += step[ax];
-        if (iv[ax] < 0 || iv[ax] >= grid_dim(G, ax)) break;
-        v += step[ax] * stride[ax];
-        tmax[ax] += tdel[ax];
+        ix += ax0 ? sx : 0;
+        iy += ax1 ? sy : 0;
+        iz += ax2 ? sz : 0;
+        if ((unsigned)ix >= (unsigned)G.nx || (unsigned)iy >= (unsigned)G.ny || (unsigned)iz >= (unsigned)G.nz) break;
+        v += ax0 ? vx : (ax1 ? vy : vz);
+        if (ax0) mx += dx;
+        if (ax1) my += dy;
+        if (ax2) mz += dz;
     }
     return visits;
 }
@@ -625,7 +658,7 @@ struct SegRec {
 // source (source.py:67-210)
 // ---------------------------------------------------------------------------
 
-__device__ void rotate(float v[3], int axis, float ca, float sa) {
+__device__ __forceinline__ void rotate(float v[3], int axis, float ca, float sa) {
     // Rodrigues rotation about a coordinate axis
     float a0 = v[0], a1 = v[1], a2 = v[2];
     if (axis == 0) { v[1] = a1 * ca - a2 * sa; v[2] = a1 * sa + a2 * ca; }
@@ -633,7 +666,7 @@ __device__ void rotate(float v[3], int axis, float ca, float sa) {
     else { v[0] = a0 * ca - a1 * sa; v[1] = a0 * sa + a1 * ca; }
 }
 
-__device__ void sample_source(const KSource& S, HistoryRng& rng, real p[3], real d[3], float& E) {
+__device__ __forceinline__ void sample_source(const KSource& S, HistoryRng& rng, real p[3], real d[3], float& E) {
     float pos[3] = {S.pos[0], S.pos[1], S.pos[2]};
     float dir[3] = {S.dir[0], S.dir[1], S.dir[2]};
     float u[3] = {S.u[0], S.u[1], S.u[2]};
@@ -656,7 +689,9 @@ __device__ void sample_source(const KSource& S, HistoryRng& rng, real p[3], real
         pos[0] = S.iso[0] + rel[0]; pos[1] = S.iso[1] + rel[1]; pos[2] = S.iso[2] + rel[2];
         if (S.scan > 0.0f) {
             float shift = S.scan * (rng.uniform() - 0.5f);
-            pos[S.rot_axis] += shift;
+            pos[0] += S.rot_axis == 0 ? shift : 0.0f;
+            pos[1] += S.rot_axis == 1 ? shift : 0.0f;
+            pos[2] += S.rot_axis == 2 ? shift : 0.0f;
         }
     }
     if (S.field == CC_FIELD_CONE) {
@@ -698,6 +733,10 @@ constexpr int HIST_CHUNK = 256;     // histories a warp takes from the global co
 #endif
 constexpr int BLOCK = 256;
 constexpr int WARPS_PER_BLOCK = BLOCK / 32;
+// A thread's 32-bit counters go to the block's 64-bit ones once any reaches
+// 2^30: one history adds far less than the remaining 2^31 (its steps are
+// capped by the step limit, its voxel visits by the grid's size per step).
+constexpr unsigned COUNTER_FLUSH = 1u << 30;
 constexpr unsigned FULL = 0xffffffffu;
 
 __device__ __forceinline__ int warp_inclusive_scan(int v, int lane) {
@@ -738,7 +777,9 @@ transport_kernel(const KTables T, const KScene S, const KGrid G, const KSource S
 
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
-    unsigned long long c_abs = 0, c_esc = 0, c_sc = 0, c_fl = 0, c_steps = 0, c_vox = 0;
+    // per-thread counters in 32 bits (registers are the kernel's limit); a
+    // thread hands them to the block's 64-bit counters before they near 2^31
+    unsigned c_abs = 0, c_esc = 0, c_sc = 0, c_fl = 0, c_steps = 0, c_vox = 0;
 
     // warp-local pool [pool_next, pool_end)
     long long pool_next = 0, pool_end = 0;
@@ -747,7 +788,7 @@ transport_kernel(const KTables T, const KScene S, const KGrid G, const KSource S
     real p[3], d[3];
     float E = 0.f, tau = 0.f;
     int nsc = 0, mat = -1, batch = 0;
-    long long steps = 0;
+    int steps = 0;
     HistoryRng rng;
 
     while (true) {
@@ -861,6 +902,10 @@ transport_kernel(const KTables T, const KScene S, const KGrid G, const KSource S
                     c_vox += max(nv - (k > 0 ? 1 : 0), 0);   // a cut voxel is one visit
                 }
                 __syncwarp();
+                if (c_vox >= COUNTER_FLUSH) {
+                    atomicAdd(&s_cnt[5], (unsigned long long)c_vox);
+                    c_vox = 0;
+                }
             }
         }
         if (!go) continue;
@@ -935,10 +980,19 @@ transport_kernel(const KTables T, const KScene S, const KGrid G, const KSource S
             done = true;
         }
         if (done) {
-            c_steps += steps;
+            c_steps += (unsigned)steps;
             c_sc += nsc;
             if (esc) ++c_esc;
             if (absd) ++c_abs;
+            if ((c_steps | c_vox | c_sc) >= COUNTER_FLUSH) {
+                atomicAdd(&s_cnt[0], (unsigned long long)c_abs);
+                atomicAdd(&s_cnt[1], (unsigned long long)c_esc);
+                atomicAdd(&s_cnt[2], (unsigned long long)c_sc);
+                atomicAdd(&s_cnt[3], (unsigned long long)c_fl);
+                atomicAdd(&s_cnt[4], (unsigned long long)c_steps);
+                atomicAdd(&s_cnt[5], (unsigned long long)c_vox);
+                c_abs = c_esc = c_sc = c_fl = c_steps = c_vox = 0;
+            }
             if (!FROM_SOURCE) {
                 for (int k = 0; k < 3; ++k) {
                     R.pos[3 * h + k] = (double)p[k] + (esc ? (double)d[k] * 1e-6 : 0.0);
@@ -953,12 +1007,12 @@ transport_kernel(const KTables T, const KScene S, const KGrid G, const KSource S
         }
     }
     // ---- reductions ----
-    atomicAdd(&s_cnt[0], c_abs);
-    atomicAdd(&s_cnt[1], c_esc);
-    atomicAdd(&s_cnt[2], c_sc);
-    atomicAdd(&s_cnt[3], c_fl);
-    atomicAdd(&s_cnt[4], c_steps);
-    atomicAdd(&s_cnt[5], c_vox);
+    atomicAdd(&s_cnt[0], (unsigned long long)c_abs);
+    atomicAdd(&s_cnt[1], (unsigned long long)c_esc);
+    atomicAdd(&s_cnt[2], (unsigned long long)c_sc);
+    atomicAdd(&s_cnt[3], (unsigned long long)c_fl);
+    atomicAdd(&s_cnt[4], (unsigned long long)c_steps);
+    atomicAdd(&s_cnt[5], (unsigned long long)c_vox);
     __syncthreads();
     for (int i = threadIdx.x; i < n_acc; i += blockDim.x)
         if (s_edep[i] != 0.0) atomicAdd(R.edep + i, s_edep[i]);
@@ -1040,7 +1094,7 @@ batch_kernel(const KTables T, const KBatch B, const KRun R) {
     const int warp = threadIdx.x >> 5;
     const unsigned long long seed = __ldg(B.run);
     const int fluorescence = (int)__ldg(B.run + 1);
-    unsigned long long c_steps = 0, c_vox = 0;
+    unsigned c_steps = 0, c_vox = 0;            // 32-bit, handed on before they near 2^31
 
     long long pool_next = 0, pool_end = 0;
     int pool_scene = 0;
@@ -1050,7 +1104,7 @@ batch_kernel(const KTables T, const KBatch B, const KRun R) {
     real p[3], d[3];
     float E = 0.f, tau = 0.f;
     int nsc = 0, mat = -1;
-    long long steps = 0;
+    int steps = 0;
     HistoryRng rng;
 
     while (true) {
@@ -1161,6 +1215,10 @@ batch_kernel(const KTables T, const KBatch B, const KRun R) {
                     c_vox += max(nv - (k > 0 ? 1 : 0), 0);   // a cut voxel is one visit
                 }
                 __syncwarp();
+                if (c_vox >= COUNTER_FLUSH) {
+                    atomicAdd(&s_cnt[1], (unsigned long long)c_vox);
+                    c_vox = 0;
+                }
             }
         }
 
@@ -1231,25 +1289,40 @@ batch_kernel(const KTables T, const KBatch B, const KRun R) {
         }
         add_scene_counts(B, ended, sc, absd ? 1u : 0u, esc ? 1u : 0u, ended ? (unsigned)nsc : 0u, 0u, lane);
         if (ended) {
-            c_steps += steps;
+            c_steps += (unsigned)steps;
             live = false;
+            if ((c_steps | c_vox) >= COUNTER_FLUSH) {
+                atomicAdd(&s_cnt[0], (unsigned long long)c_steps);
+                atomicAdd(&s_cnt[1], (unsigned long long)c_vox);
+                c_steps = c_vox = 0;
+            }
         }
     }
-    atomicAdd(&s_cnt[0], c_steps);
-    atomicAdd(&s_cnt[1], c_vox);
+    atomicAdd(&s_cnt[0], (unsigned long long)c_steps);
+    atomicAdd(&s_cnt[1], (unsigned long long)c_vox);
     __syncthreads();
     if (threadIdx.x < 2) atomicAdd(R.counters + 4 + threadIdx.x, s_cnt[threadIdx.x]);
 }
 
 // Batch statistics fold (tally.py:59-94): T += S, Q += S^2/n_b,
 // n_hit += (S_k != 0 or S_h != 0), S = 0.
+// (A scratch cell is read as FP32 pairs when cell32; the cell is zeroed
+// whole either way.)
+__device__ __forceinline__ double2 cell_read(const double2* scratch, long long i, int cell32) {
+    if (cell32) {
+        const float2 f = reinterpret_cast<const float2*>(scratch)[2 * i];
+        return make_double2((double)f.x, (double)f.y);
+    }
+    return scratch[i];
+}
+
 __global__ void fold_kernel(double2* __restrict__ total, double2* __restrict__ q,
                             int* __restrict__ nhit, double2* __restrict__ scratch,
-                            long long nvox, double inv_nb) {
+                            long long nvox, double inv_nb, int cell32) {
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     long long stride = (long long)gridDim.x * blockDim.x;
     for (; i < nvox; i += stride) {
-        double2 s = scratch[i];
+        double2 s = cell_read(scratch, i, cell32);
         if (s.x != 0.0 || s.y != 0.0) {
             double2 t = total[i];
             t.x += s.x; t.y += s.y;
@@ -1259,6 +1332,23 @@ __global__ void fold_kernel(double2* __restrict__ total, double2* __restrict__ q
             qq.y += s.y * s.y * inv_nb;
             q[i] = qq;
             nhit[i] += 1;
+            scratch[i] = make_double2(0.0, 0.0);
+        }
+    }
+}
+
+// Batch scratch into the totals without statistics: T += S, S = 0.
+__global__ void fold_plain_kernel(double2* __restrict__ total, double2* __restrict__ scratch, long long nvox,
+                                  int cell32) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    long long stride = (long long)gridDim.x * blockDim.x;
+    for (; i < nvox; i += stride) {
+        double2 s = cell_read(scratch, i, cell32);
+        if (s.x != 0.0 || s.y != 0.0) {
+            double2 t = total[i];
+            t.x += s.x;
+            t.y += s.y;
+            total[i] = t;
             scratch[i] = make_double2(0.0, 0.0);
         }
     }
@@ -1330,6 +1420,7 @@ struct cc_ctx {
     int block = 256;
     int blocks_per_sm = 0;                       // 0 = occupancy based
     long long max_steps = 100000;
+    int tally_fp32 = 0;                          // 1: FP32 scratch cells for slots of <= FP32_SLOT_HISTORIES
 };
 
 struct cc_tables {
@@ -1436,8 +1527,15 @@ int cc_ctx_set_launch(cc_ctx* c, int block_size, int blocks_per_sm) {
 }
 
 int cc_ctx_set_step_limit(cc_ctx* c, int64_t max_steps) {
-    if (!c || max_steps <= 0) return set_error(CC_E_INVALID, "invalid step limit");
+    if (!c || max_steps <= 0 || max_steps > (1LL << 30))
+        return set_error(CC_E_INVALID, "step limit must be in [1, 2^30]");
     c->max_steps = max_steps;
+    return CC_OK;
+}
+
+int cc_ctx_set_tally_fp32(cc_ctx* c, int32_t on) {
+    if (!c) return set_error(CC_E_INVALID, "NULL context");
+    c->tally_fp32 = on ? 1 : 0;
     return CC_OK;
 }
 
@@ -1751,7 +1849,9 @@ int cc_grid_create(cc_ctx* ctx, const double origin[3], int32_t nx, int32_t ny, 
             cc_grid_destroy(g);
             return set_error(CC_E_NOMEM, "device allocation of the statistics grids failed");
         }
-        int rc = grid_alloc_scratch(g, 1);
+    }
+    {
+        int rc = grid_alloc_scratch(g, 1);           // every grid scores into batch scratch
         if (rc != CC_OK) { cc_grid_destroy(g); return rc; }
     }
     int rc = cc_grid_reset(g);
@@ -1787,7 +1887,38 @@ int cc_grid_reset(cc_grid* g) {
     return CC_OK;
 }
 
-static int fold_batches(cc_grid* g, int n_slots, const long long* counts) {
+// Histories a scratch slot may sum in FP32 cells (an opt-in of the context).
+// Scores of unequal size round at random, ~sqrt(N) * 6e-8 relative after N
+// of them; equal scores (a monoenergetic pencil beam's uncollided photons
+// crossing the same voxels) round the same way each time, and at 2e5 such
+// histories per slot the busiest voxels were seen 7e-4 apart between two
+// summation orders.  Larger slots use FP64 cells; the FP64 build always does.
+constexpr long long FP32_SLOT_HISTORIES = 1000000;
+
+static int cell32_for(const cc_ctx* c, long long histories_per_slot) {
+#ifdef CC_TRACK_FP64
+    (void)c;
+    (void)histories_per_slot;
+    return 0;
+#else
+    return (c->tally_fp32 && histories_per_slot <= FP32_SLOT_HISTORIES) ? 1 : 0;
+#endif
+}
+
+// Scratch slots [0, n_slots) into the totals without batch statistics.
+static int fold_plain(cc_grid* g, int n_slots, int cell32) {
+    cc_ctx* c = g->ctx;
+    int threads = 256;
+    int blocks = std::max(1, std::min((int)((g->k.nvox + threads - 1) / threads), c->sm_count * 8));
+    for (int s = 0; s < n_slots; ++s) {
+        fold_plain_kernel<<<blocks, threads, 0, c->stream>>>(
+            (double2*)g->d_total, (double2*)(g->d_scratch + (size_t)s * 2 * g->k.nvox), g->k.nvox, cell32);
+        CC_CUDA(cudaGetLastError());
+    }
+    return CC_OK;
+}
+
+static int fold_batches(cc_grid* g, int n_slots, const long long* counts, int cell32) {
     cc_ctx* c = g->ctx;
     int threads = 256;
     int blocks = std::max(1, std::min((int)((g->k.nvox + threads - 1) / threads), c->sm_count * 8));
@@ -1795,7 +1926,7 @@ static int fold_batches(cc_grid* g, int n_slots, const long long* counts) {
         if (counts[s] <= 0) continue;
         fold_kernel<<<blocks, threads, 0, c->stream>>>(
             (double2*)g->d_total, (double2*)g->d_q, g->d_nhit,
-            (double2*)(g->d_scratch + (size_t)s * 2 * g->k.nvox), g->k.nvox, 1.0 / (double)counts[s]);
+            (double2*)(g->d_scratch + (size_t)s * 2 * g->k.nvox), g->k.nvox, 1.0 / (double)counts[s], cell32);
         CC_CUDA(cudaGetLastError());
         g->n_batches += 1;
         g->n_histories += counts[s];
@@ -1807,7 +1938,7 @@ int cc_grid_end_batch(cc_grid* g, int64_t n_hist) {
     if (!g) return set_error(CC_E_INVALID, "grid is NULL");
     if (!(g->flags & CC_GRID_STATS) || n_hist <= 0) return CC_OK;
     long long cnt = n_hist;
-    int rc = fold_batches(g, 1, &cnt);
+    int rc = fold_batches(g, 1, &cnt, 0);              // the pending batch is in FP64 cells
     if (rc != CC_OK) return rc;
     CC_CUDA(cudaStreamSynchronize(g->ctx->stream));
     return CC_OK;
@@ -1885,7 +2016,7 @@ static int grid_blocks_for(cc_ctx* c, size_t smem, bool fs, bool tl) {
 static int run_launch(cc_ctx* c, const cc_scene* scene, const cc_tables* tables, const KSource* src,
                       cc_grid* grid, double* tally_base, int n_slots, long long batch_size,
                       KRun R, std::vector<double>& edep_slots, unsigned long long* counters_out,
-                      float* kernel_ms) {
+                      float* kernel_ms, int cell32 = 0) {
     const KTables& T = tables->k;
     R.n_scratch = n_slots;
     R.batch_size = batch_size;
@@ -1903,7 +2034,7 @@ static int run_launch(cc_ctx* c, const cc_scene* scene, const cc_tables* tables,
     KGrid G;
     memset(&G, 0, sizeof(G));
     bool tl = grid != nullptr;
-    if (tl) { G = grid->k; G.tally = tally_base; }
+    if (tl) { G = grid->k; G.tally = tally_base; G.tally32 = cell32; }
     KSource S;
     memset(&S, 0, sizeof(S));
     bool fs = src != nullptr;
@@ -1945,12 +2076,20 @@ static int transport_common(cc_ctx* c, const cc_scene* scene, const cc_tables* t
     R.seed = seed;
     R.pos = d_pos; R.dir = d_dir; R.energy = d_en;
     R.n_scatter = d_nsc; R.absorbed = d_abs; R.escaped = d_esc;
-    double* tally = nullptr;
-    if (grid) tally = (grid->flags & CC_GRID_STATS) ? grid->d_scratch : grid->d_total;
+    // a statistics grid's slot 0 is its pending batch (FP64 cells, folded by
+    // cc_grid_end_batch); any other grid's slot 0 is folded after the call
+    double* tally = grid ? grid->d_scratch : nullptr;
+    const bool pending = grid && (grid->flags & CC_GRID_STATS);
+    const int cell32 = (grid && !pending) ? cell32_for(c, n) : 0;
     std::vector<double> slots;
     unsigned long long cnt[6] = {0, 0, 0, 0, 0, 0};
-    int rc = run_launch(c, scene, tables, nullptr, grid, tally, 1, std::max<long long>(n, 1), R, slots, cnt, nullptr);
+    int rc = run_launch(c, scene, tables, nullptr, grid, tally, 1, std::max<long long>(n, 1), R, slots, cnt, nullptr,
+                        cell32);
     if (rc != CC_OK) return rc;
+    if (grid && !pending) {
+        rc = fold_plain(grid, 1, cell32);
+        if (rc != CC_OK) return rc;
+    }
     if (edep) for (int m = 0; m < tables->n_mat; ++m) edep[m] += slots[m];
     if (n_fluor) *n_fluor = (int64_t)cnt[3];
     return CC_OK;
@@ -2028,7 +2167,11 @@ int cc_run(cc_ctx* c, const cc_scene* scene, const cc_tables* tables, const cc_s
     long long per_launch_target = 1LL << 22;
     int slots = (int)std::min<long long>(MAX_SCRATCH, std::max<long long>(1, per_launch_target / batch_size));
     slots = std::min(slots, std::max(1, (int)((48 * 1024) / (sizeof(double) * n_mat))));
-    if (stats) {
+    // a grid scores every batch into its own scratch slot (the batch
+    // statistics need that, and FP32 cells must not sum more than a batch)
+    const bool slotted = grid != nullptr;
+    const int cell32 = slotted ? cell32_for(c, batch_size) : 0;
+    if (grid) {
         size_t per = (size_t)grid->k.nvox * 2 * sizeof(double);
         size_t budget = (size_t)8 << 30;
         slots = (int)std::max<size_t>(1, std::min<size_t>(slots, budget / per));
@@ -2051,14 +2194,13 @@ int cc_run(cc_ctx* c, const cc_scene* scene, const cc_tables* tables, const cc_s
         R.first = first_history + done;
         R.fluorescence = fluorescence;
         R.seed = seed;
-        double* tally = nullptr;
-        if (grid) tally = stats ? grid->d_scratch : grid->d_total;
+        double* tally = grid ? grid->d_scratch : nullptr;
         std::vector<double> slot_edep;
         unsigned long long cnt[6];
         CC_CUDA(cudaEventRecord(c->ev0, c->stream));
         float kms = 0.f;
-        int rc = run_launch(c, scene, tables, &src->k, grid, tally, stats ? ns : 1,
-                            stats ? batch_size : std::max<long long>(n_launch, 1), R, slot_edep, cnt, &kms);
+        int rc = run_launch(c, scene, tables, &src->k, grid, tally, slotted ? ns : 1,
+                            slotted ? batch_size : std::max<long long>(n_launch, 1), R, slot_edep, cnt, &kms, cell32);
         if (rc != CC_OK) return rc;
         ++launches;
         ++transport_launches;
@@ -2067,7 +2209,7 @@ int cc_run(cc_ctx* c, const cc_scene* scene, const cc_tables* tables, const cc_s
         for (int b = 0; b < ns; ++b) {
             long long nb = std::min<long long>(batch_size, n_launch - (long long)b * batch_size);
             for (int m = 0; m < n_mat; ++m) {
-                double v = stats ? slot_edep[(size_t)b * n_mat + m] : (b == 0 ? slot_edep[m] : 0.0);
+                double v = slotted ? slot_edep[(size_t)b * n_mat + m] : (b == 0 ? slot_edep[m] : 0.0);
                 if (edep) edep[m] += v;
                 if (edep_sum2 && stats) edep_sum2[m] += v * v / (double)nb;
             }
@@ -2075,7 +2217,11 @@ int cc_run(cc_ctx* c, const cc_scene* scene, const cc_tables* tables, const cc_s
         if (stats) {
             std::vector<long long> counts(ns);
             for (int b = 0; b < ns; ++b) counts[b] = std::min<long long>(batch_size, n_launch - (long long)b * batch_size);
-            rc = fold_batches(grid, ns, counts.data());
+            rc = fold_batches(grid, ns, counts.data(), cell32);
+            if (rc != CC_OK) return rc;
+            launches += ns;
+        } else if (grid) {
+            rc = fold_plain(grid, ns, cell32);
             if (rc != CC_OK) return rc;
             launches += ns;
         }
@@ -2290,7 +2436,8 @@ int cc_batch_create(cc_ctx* c, const cc_tables* tables, int32_t n_scenes, const 
             if (slots > 1 && !(g->flags & CC_GRID_STATS)) { batch_free(b); return set_error(CC_E_INVALID, "batch statistics need CC_GRID_STATS grids"); }
             if (slots > 1) { int rc = grid_alloc_scratch(g, slots); if (rc != CC_OK) { batch_free(b); return rc; } }
             hg[i] = g->k;
-            hg[i].tally = slots > 1 ? g->d_scratch : g->d_total;
+            hg[i].tally = g->d_scratch;
+            hg[i].tally32 = cell32_for(c, (n_histories[i] + slots - 1) / slots);
             b->grids.push_back(g);
         }
         b->nhist[i] = n_histories[i];
@@ -2369,17 +2516,21 @@ int cc_batch_create(cc_ctx* c, const cc_tables* tables, int32_t n_scenes, const 
         e = cudaGetLastError();
         b->launches = 1;
     }
-    if (e == cudaSuccess && b->tally && slots > 1) {
+    if (e == cudaSuccess && b->tally) {
         int threads = 256;
         for (int i = 0; i < n_scenes && e == cudaSuccess; ++i) {
             cc_grid* g = grids[i];
+            const int cell32 = hg[i].tally32;
             int nb = std::max(1, std::min((int)((g->k.nvox + threads - 1) / threads), c->sm_count * 8));
             for (int sl = 0; sl < slots; ++sl) {
                 long long cnt = b->slot_counts[i][sl];
                 if (cnt <= 0) continue;
-                fold_kernel<<<nb, threads, 0, st>>>((double2*)g->d_total, (double2*)g->d_q, g->d_nhit,
-                                                     (double2*)(g->d_scratch + (size_t)sl * 2 * g->k.nvox),
-                                                     g->k.nvox, 1.0 / (double)cnt);
+                double2* scr = (double2*)(g->d_scratch + (size_t)sl * 2 * g->k.nvox);
+                if (slots > 1)
+                    fold_kernel<<<nb, threads, 0, st>>>((double2*)g->d_total, (double2*)g->d_q, g->d_nhit, scr,
+                                                         g->k.nvox, 1.0 / (double)cnt, cell32);
+                else
+                    fold_plain_kernel<<<nb, threads, 0, st>>>((double2*)g->d_total, scr, g->k.nvox, cell32);
                 ++b->launches;
             }
             e = cudaGetLastError();

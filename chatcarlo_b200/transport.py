@@ -126,6 +126,12 @@ class Engine:
     def set_launch(self, block_size: int = 256, blocks_per_sm: int = 0) -> None:
         N.check(self.lib.cc_ctx_set_launch(self.ctx, block_size, blocks_per_sm))
 
+    def set_tally_fp32(self, on: bool = True) -> None:
+        """FP32 tally scratch cells for batches of <= 1e6 histories (one
+        vector reduction per voxel visit; sums depend on the order of the
+        FP32 additions) instead of the default FP64 cells."""
+        N.check(self.lib.cc_ctx_set_tally_fp32(self.ctx, int(bool(on))), self.lib)
+
     def set_step_limit(self, max_steps: int = 100_000) -> None:
         """Transport steps a single photon may take before the run fails with CC_E_TIMEOUT."""
         N.check(self.lib.cc_ctx_set_step_limit(self.ctx, int(max_steps)))

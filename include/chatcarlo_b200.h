@@ -161,6 +161,16 @@ int cc_ctx_destroy(cc_ctx* ctx);
 int cc_ctx_set_launch(cc_ctx* ctx, int block_size, int blocks_per_sm);
 int cc_ctx_set_step_limit(cc_ctx* ctx, int64_t max_steps_per_photon);
 
+/* Tally scratch cells (no reference counterpart; the reference sums in
+ * NumPy FP64).  Every batch scores into its own scratch slot, folded into
+ * the FP64 totals after its launch.  By default (on = 0) the cells are FP64:
+ * a seed reproduces its tallies up to the order of FP64 additions.  on = 1
+ * makes a slot that sums at most 1e6 histories hold FP32 cells, so one
+ * vector reduction scores kerma and H*(10) of a voxel visit: faster, with
+ * sums that depend on the order of the FP32 additions (up to ~1e-3 relative
+ * in the busiest voxels of a monoenergetic pencil beam). */
+int cc_ctx_set_tally_fp32(cc_ctx* ctx, int32_t on);
+
 /* -- tables, scene, source, grid -------------------------------------------- */
 int cc_tables_create(cc_ctx* ctx, const cc_table_desc* desc, cc_tables** out);
 int cc_tables_destroy(cc_tables* t);

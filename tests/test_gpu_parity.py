@@ -200,22 +200,34 @@ def test_collision_and_track_length_estimators_agree(engine):
 
 def test_reproducible_and_launch_shape_independent(engine):
     """Same seed -> identical per-photon results, whatever the launch shape,
-    and the same kerma up to the order of the FP64 additions."""
+    and the same kerma up to the order of the FP64 additions.  The last run
+    sums in FP32 scratch cells: a monoenergetic pencil beam is their worst
+    case (equal scores round alike), so the busiest voxels may move by a few
+    1e-4 relative while the median voxel stays at FP32 rounding."""
     d = np.array([1.0, 0.05, 0.02])
     d /= np.linalg.norm(d)
     out, kerma = [], []
-    for block, per_sm in ((256, 0), (128, 3), (64, 1), (256, 0)):
+    for block, per_sm in ((256, 0), (128, 3), (64, 1), (256, 0), (256, 0)):
         engine.set_launch(block, per_sm)
+        engine.set_tally_fp32(len(out) == 4)
         g = W.make_grid({"origin": (-60.0, -50.0, -45.0), "shape": (60, 50, 45), "voxel_cm": 2.0},
                         track_uncertainty=False)
         p, dv, e, r = _gpu_tp(engine, MIXED, [-55.0, 1.0, 2.0], d, 80.0, 200_000, seed=99, grid=g)
         out.append((p, dv, e, r.n_scatter, r.absorbed, r.escaped))
         kerma.append(g.kerma_keV.copy())
     engine.set_launch(256, 0)
-    for other, k in zip(out[1:], kerma[1:]):
+    engine.set_tally_fp32(False)
+    for other, k in zip(out[1:], kerma[1:4]):
         for a, b in zip(out[0], other):
             np.testing.assert_array_equal(a, b)
         np.testing.assert_allclose(k, kerma[0], rtol=1e-9, atol=1e-12)
+    for a, b in zip(out[0], out[4]):
+        np.testing.assert_array_equal(a, b)
+    k32, k64 = kerma[4], kerma[0]
+    np.testing.assert_allclose(k32, k64, rtol=5e-3, atol=1e-6 * float(np.max(k64)))
+    sel = k64 > 0
+    assert float(np.median(np.abs(k32[sel] - k64[sel]) / k64[sel])) < 1e-5
+    assert abs(k32.sum() - k64.sum()) / k64.sum() < 2e-4
 
 
 def test_source_sampling_matches_oracle(engine):
