@@ -159,6 +159,9 @@ const char* cc_last_error(void);
 int cc_ctx_create(int device, cc_ctx** out);
 int cc_ctx_destroy(cc_ctx* ctx);
 int cc_ctx_set_launch(cc_ctx* ctx, int block_size, int blocks_per_sm);
+/* Transport steps a photon may take before the call fails with
+ * CC_E_TIMEOUT (a guard against runaway histories; default 100000);
+ * accepted range [1, 2^30]. */
 int cc_ctx_set_step_limit(cc_ctx* ctx, int64_t max_steps_per_photon);
 
 /* Tally scratch cells (no reference counterpart; the reference sums in
