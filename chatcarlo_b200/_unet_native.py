@@ -16,7 +16,7 @@ LIB_PATH = Path(os.environ.get("CHATCARLO_B200_UNET_LIB") or
 
 EXPORTED = [
     "ccu_version", "ccu_last_error", "ccu_status", "ccu_conv3d", "ccu_conv3d_wgrad", "ccu_bias_grad",
-    "ccu_avgpool", "ccu_pool_backward", "ccu_up_reduce", "ccu_head", "ccu_input", "ccu_adam",
+    "ccu_avgpool", "ccu_pool_backward", "ccu_up_reduce", "ccu_head", "ccu_input", "ccu_adam", "ccu_adam_clipped",
     "ccu_packed_weight_elems", "ccu_pack_weights", "ccu_set_conv_path", "ccu_zero", "ccu_gemm_test",
 ]
 
@@ -38,6 +38,8 @@ _SIGS = {
     "ccu_head": ([P, P, P, P, P, C.c_float, LL, P, P, P, P, P], I),
     "ccu_input": ([P, P, P, I, P, LL, P, P], I),
     "ccu_adam": ([P, P, P, P, LL, C.c_float, C.c_float, C.c_float, C.c_float, I, C.c_float, P], I),
+    "ccu_adam_clipped": ([P, P, P, P, LL, C.c_float, C.c_float, C.c_float, C.c_float, I, C.c_float, P, C.c_float,
+                          P], I),
     "ccu_packed_weight_elems": ([I, I], LL),
     "ccu_pack_weights": ([P, I, I, P, P, P], I),
     "ccu_set_conv_path": ([I], I),

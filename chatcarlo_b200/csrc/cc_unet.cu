@@ -27,6 +27,7 @@
 // Every mbarrier wait is bounded by the global timer; a wait that runs out
 // sets a status bit that the host reads, and the CTA still frees its tensor
 // memory before it returns.
+#include <algorithm>
 #include <cuda_runtime.h>
 #include <cuda_bf16.h>
 #include <stdint.h>
@@ -909,15 +910,50 @@ __global__ void input_kernel(const float* __restrict__ xlog, const float* __rest
 // Adam with decoupled weight decay on a flat FP32 parameter vector.
 __global__ void adam_kernel(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m,
                             float* __restrict__ v, long long n, float lr, float b1, float b2, float eps, float c1,
-                            float c2, float wd) {
+                            float c2, float wd, const double* __restrict__ clip) {
+    const float scale = clip ? (float)clip[2] : 1.0f;
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-        const float gi = g[i];
+        const float gi = g[i] * scale;
         const float mi = b1 * m[i] + (1.0f - b1) * gi;
         const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
         m[i] = mi;
         v[i] = vi;
         p[i] -= lr * ((mi * c1) / (sqrtf(vi * c2) + eps) + wd * p[i]);
     }
+}
+
+// Sum of squares of g[0, n) added to *out (block partials in FP64).
+__global__ void sumsq_kernel(const float* __restrict__ g, long long n, double* __restrict__ out) {
+    double s = 0.0;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const double x = g[i];
+        s += x * x;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    __shared__ double part[32];
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        s = (threadIdx.x < (blockDim.x >> 5)) ? part[threadIdx.x] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (threadIdx.x == 0) atomicAdd(out, s);
+    }
+}
+
+// Adaptive global-norm clipping, state [sumsq, ema, scale]: the gradient's
+// norm is capped at ratio x the running mean of the capped norms (the first
+// step sets that mean), so that one outlying minibatch cannot inflate
+// Adam's second moments or throw the weights far.
+__global__ void clip_scale_kernel(double* state, float ratio) {
+    const double norm = sqrt(state[0]);
+    double ema = state[1];
+    if (!(ema > 0.0)) ema = norm;
+    const double cap = ratio * ema;
+    const double kept = norm > cap ? cap : norm;
+    state[2] = norm > 0.0 ? kept / norm : 1.0;
+    state[1] = 0.95 * ema + 0.05 * kept;
 }
 
 // BF16 weights of one layer from its FP32 master copy w32[27][cout][cin],
@@ -1271,7 +1307,22 @@ int ccu_adam(float* p, const float* g, float* m, float* v, long long n, float lr
              int step, float wd, void* stream) {
     if (!p || !g || !m || !v || step < 1) return set_error(CCU_E_INVALID, "bad optimizer arguments");
     const float c1 = 1.0f / (1.0f - powf(b1, (float)step)), c2 = 1.0f / (1.0f - powf(b2, (float)step));
-    adam_kernel<<<grid_for(n, 256), 256, 0, (cudaStream_t)stream>>>(p, g, m, v, n, lr, b1, b2, eps, c1, c2, wd);
+    adam_kernel<<<grid_for(n, 256), 256, 0, (cudaStream_t)stream>>>(p, g, m, v, n, lr, b1, b2, eps, c1, c2, wd,
+                                                                     nullptr);
+    CU_CHECK(cudaGetLastError());
+    return CCU_OK;
+}
+
+int ccu_adam_clipped(float* p, const float* g, float* m, float* v, long long n, float lr, float b1, float b2,
+                     float eps, int step, float wd, double* clip_state, float clip_ratio, void* stream) {
+    if (!p || !g || !m || !v || step < 1 || !clip_state || !(clip_ratio >= 1.0f))
+        return set_error(CCU_E_INVALID, "bad optimizer arguments");
+    cudaStream_t st = (cudaStream_t)stream;
+    const float c1 = 1.0f / (1.0f - powf(b1, (float)step)), c2 = 1.0f / (1.0f - powf(b2, (float)step));
+    CU_CHECK(cudaMemsetAsync(clip_state, 0, sizeof(double), st));
+    sumsq_kernel<<<(unsigned)std::min<long long>(grid_for(n, 256), 2 * 148), 256, 0, st>>>(g, n, clip_state);
+    clip_scale_kernel<<<1, 1, 0, st>>>(clip_state, clip_ratio);
+    adam_kernel<<<grid_for(n, 256), 256, 0, st>>>(p, g, m, v, n, lr, b1, b2, eps, c1, c2, wd, clip_state);
     CU_CHECK(cudaGetLastError());
     return CCU_OK;
 }

@@ -124,9 +124,15 @@ class Dataset:
         return out
 
 
-def train(model: DN.UNet3D, data: Dataset, steps: int, batch: int, lr: float, seed: int = 0, log_every: int = 50):
+def train(model: DN.UNet3D, data: Dataset, steps: int, batch: int, lr: float, seed: int = 0, log_every: int = 50,
+          clip_ratio: float | None = None):
+    """Adam with cosine learning-rate decay on random minibatches (random
+    input level and axis flips); clip_ratio switches the model's adaptive
+    gradient clipping (None keeps the model's setting)."""
     import torch
     rng = np.random.default_rng(seed)
+    if clip_ratio is not None:
+        model.clip_ratio = float(clip_ratio)
     S = data.S
     tgt = torch.empty(batch * S ** 3, dtype=torch.float32, device=model.dev)
     wgt = torch.empty_like(tgt)

@@ -111,6 +111,10 @@ class UNet3D:
         self.m = torch.zeros_like(self.p)
         self.v = torch.zeros_like(self.p)
         self.step_n = 0
+        # adaptive gradient clipping: 0 = off, else the cap on the gradient
+        # norm as a multiple of its running mean (ccu_adam_clipped)
+        self.clip_ratio = 3.0
+        self.clip_state = torch.zeros(3, dtype=torch.float64, device=self.dev)
         lib = U.lib()
         self.w = {L.name: torch.empty(lib.ccu_packed_weight_elems(L.cout, L.cin), dtype=torch.bfloat16,
                                       device=self.dev) for L in LAYERS}
@@ -300,8 +304,13 @@ class UNet3D:
 
     def step(self, lr: float, b1: float = 0.9, b2: float = 0.999, eps: float = 1e-8, wd: float = 0.0) -> None:
         self.step_n += 1
-        self._call(U.lib().ccu_adam, self._ptr(self.p), self._ptr(self.g), self._ptr(self.m), self._ptr(self.v),
-                   self.p.numel(), lr, b1, b2, eps, self.step_n, wd, self._stream())
+        if self.clip_ratio > 0:
+            self._call(U.lib().ccu_adam_clipped, self._ptr(self.p), self._ptr(self.g), self._ptr(self.m),
+                       self._ptr(self.v), self.p.numel(), lr, b1, b2, eps, self.step_n, wd, self._ptr(self.clip_state),
+                       self.clip_ratio, self._stream())
+        else:
+            self._call(U.lib().ccu_adam, self._ptr(self.p), self._ptr(self.g), self._ptr(self.m), self._ptr(self.v),
+                       self.p.numel(), lr, b1, b2, eps, self.step_n, wd, self._stream())
         self.pack()
 
     def check_status(self) -> None:

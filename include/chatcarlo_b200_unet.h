@@ -90,6 +90,13 @@ int ccu_input(const float* xlog, const float* density, const uint8_t* mat, int n
 int ccu_adam(float* p, const float* g, float* m, float* v, long long n, float lr, float b1, float b2, float eps,
              int step, float wd, void* stream);
 
+/* ccu_adam on the gradient scaled by adaptive global-norm clipping: its
+ * norm is capped at clip_ratio (>= 1) x the running mean of the capped
+ * norms.  clip_state holds 3 doubles [sum of squares, running mean, last
+ * scale]; zero them before the first step of a training run. */
+int ccu_adam_clipped(float* p, const float* g, float* m, float* v, long long n, float lr, float b1, float b2,
+                     float eps, int step, float wd, double* clip_state, float clip_ratio, void* stream);
+
 /* Elements of a packed weight array for n output and c input channels
  * (both multiples of 16): 64 x n x ceil(27 c / 64); negative on error. */
 long long ccu_packed_weight_elems(int n, int c);

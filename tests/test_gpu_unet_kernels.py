@@ -182,3 +182,39 @@ def test_halo_and_gathering_kernels_agree(U):
     torch.cuda.synchronize()
     assert U.status() == 0
     torch.testing.assert_close(outs[0], outs[1], rtol=1.6e-2, atol=1e-2)
+
+
+def test_adam_with_adaptive_clipping(U):
+    """ccu_adam_clipped against a NumPy restatement: the first gradient sets
+    the running norm, a ten times larger one is cut to 3x that mean, and
+    the moments and parameters follow Adam on the scaled gradient."""
+    rng = np.random.default_rng(9)
+    n = 50_000
+    p0 = rng.normal(size=n).astype(np.float32)
+    grads = [rng.normal(size=n).astype(np.float32), 10 * rng.normal(size=n).astype(np.float32),
+             rng.normal(size=n).astype(np.float32)]
+    p, m, v = (torch.from_numpy(a.copy()).cuda() for a in (p0, np.zeros(n, np.float32), np.zeros(n, np.float32)))
+    state = torch.zeros(3, dtype=torch.float64, device="cuda")
+    lr, b1, b2, eps, ratio = 1e-2, 0.9, 0.999, 1e-8, 3.0
+    rp, rm, rv = p0.astype(np.float64), np.zeros(n), np.zeros(n)
+    ema = 0.0
+    for step, g in enumerate(grads, start=1):
+        gd = torch.from_numpy(g).cuda()
+        U.check(U.lib().ccu_adam_clipped(_ptr(p), _ptr(gd), _ptr(m), _ptr(v), n, lr, b1, b2, eps, step, 0.0,
+                                         _ptr(state), ratio, None))
+        norm = float(np.sqrt(np.sum(g.astype(np.float64) ** 2)))
+        ema = ema if ema > 0 else norm
+        kept = min(norm, ratio * ema)
+        scale = kept / norm
+        ema = 0.95 * ema + 0.05 * kept
+        gs = g * scale
+        rm = b1 * rm + (1 - b1) * gs
+        rv = b2 * rv + (1 - b2) * gs * gs
+        rp -= lr * (rm / (1 - b1 ** step)) / (np.sqrt(rv / (1 - b2 ** step)) + eps)
+        torch.cuda.synchronize()
+        assert float(state[2]) == pytest.approx(scale, rel=1e-9)
+        assert float(state[1]) == pytest.approx(ema, rel=1e-9)
+    assert float(state[2]) == pytest.approx(1.0)
+    np.testing.assert_allclose(p.cpu().numpy(), rp, rtol=1e-5, atol=1e-6)
+    np.testing.assert_allclose(m.cpu().numpy(), rm, rtol=1e-4, atol=1e-7)
+    np.testing.assert_allclose(v.cpu().numpy(), rv, rtol=1e-4, atol=1e-9)
