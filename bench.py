@@ -385,7 +385,7 @@ def main():
     e2e_photons = None
     if rank == 0:
         from chatcarlo_b200.transport import run_transport
-        eg = W.make_grid(gspec, track_uncertainty=True)
+        eg = W.make_grid(gspec, track_uncertainty=True, pinned=True)
         e_ms = []
         for i in range(args.warmup + min(args.steps, 5)):
             flush.zero_()

@@ -3,7 +3,8 @@
 Flags and outputs follow chatcarlo/__main__.py:131-253,327-349: the same
 summary lines (in English) and, with --dose-grid --dose-out, an .npz with the
 keys dose_per_history_Gy, h10_per_history_pSv, kerma_keV, h10_track_pSv_cm3,
-origin_cm, voxel_size_cm, shape.
+origin_cm, voxel_size_cm, shape (plus dose_Gy and h10_pSv for a CTDIvol-
+calibrated source).  The dose and H*(10) maps are computed on the device.
 """
 from __future__ import annotations
 
@@ -13,18 +14,7 @@ import sys
 import numpy as np
 
 
-def dose_map_Gy(grid, geometry) -> np.ndarray:
-    """Kerma to dose with the material density at each voxel centre
-    (chatcarlo/diagnostics.py:16-26)."""
-    from .tables import density
-    mat = geometry.material_at(grid.voxel_centers())
-    dens = {m: density(m) for m in set(mat.tolist())}
-    rho = np.array([dens[m] for m in mat]).reshape(grid.shape)
-    return grid.dose_map_Gy(rho)
-
-
 def cmd_run(args) -> int:
-    from .geometry import Geometry
     from .scene import load_scene
     from .transport import run_transport
     scene = load_scene(args.scene)
@@ -36,7 +26,8 @@ def cmd_run(args) -> int:
         print(f"[warning] {w}")
     res = run_transport(scene, n_histories=int(args.n_histories), seed=args.seed,
                         batch_size=int(args.batch_size), dose_grid=args.dose_grid,
-                        grid_resolution_cm=args.resolution, track_uncertainty=not args.no_uncertainty)
+                        grid_resolution_cm=args.resolution, track_uncertainty=not args.no_uncertainty,
+                        maps=args.dose_grid)
     print(f"histories: {res.n_histories:,}")
     print(f"absorbed (photoelectric) fraction: {res.fraction_absorbed:.4f}")
     print(f"escaped fraction: {res.fraction_escaped:.4f}")
@@ -48,18 +39,27 @@ def cmd_run(args) -> int:
         print(f"  {name}: {e:.6g}" + (f"  (R={rel:.3g})" if rel is not None else ""))
     print(f"device time: {res.device_ms:.1f} ms ({res.n_histories / max(res.device_ms, 1e-9) * 1e3:.4g} histories/s)")
     if args.dose_grid:
-        geometry = Geometry(scene.raw["geometry"])
+        # per-history dose (density at each voxel centre) and H*(10) maps,
+        # computed on the device (chatcarlo/__main__.py:200-209)
         g = res.grid
-        dose = dose_map_Gy(g, geometry) / res.n_histories
-        h10 = g.h10_map_pSv() / res.n_histories
+        dose = res.maps["dose_per_history_Gy"]
+        h10 = res.maps["h10_per_history_pSv"]
+        scale = res.n_photons_real
         print(f"dose grid: shape={g.shape}, resolution={g.voxel_size_cm}cm")
         print(f"  max absorbed dose [Gy/history]: {dose.max():.6g}")
         print(f"  total kerma: {g.total_kerma_MeV():.6g} MeV")
         print(f"  max H*(10) [pSv/history]: {h10.max():.6g}")
+        if scale is not None:
+            print(f"  max absorbed dose [Gy] (CTDIvol calibrated): {dose.max() * scale:.6g}")
+            print(f"  max H*(10) [pSv] (CTDIvol calibrated): {h10.max() * scale:.6g}")
         if args.dose_out:
-            np.savez(args.dose_out, dose_per_history_Gy=dose, h10_per_history_pSv=h10,
-                     kerma_keV=g.kerma_keV, h10_track_pSv_cm3=g.h10_track_pSv_cm3,
-                     origin_cm=g.origin_cm, voxel_size_cm=g.voxel_size_cm, shape=np.array(g.shape))
+            keys = dict(dose_per_history_Gy=dose, h10_per_history_pSv=h10,
+                        kerma_keV=g.kerma_keV, h10_track_pSv_cm3=g.h10_track_pSv_cm3,
+                        origin_cm=g.origin_cm, voxel_size_cm=g.voxel_size_cm, shape=np.array(g.shape))
+            if scale is not None:
+                keys["dose_Gy"] = dose * scale
+                keys["h10_pSv"] = h10 * scale
+            np.savez(args.dose_out, **keys)
             print(f"wrote {args.dose_out}")
     return 0
 

@@ -36,7 +36,7 @@ EXPORTED = [
     "cc_version", "cc_last_error", "cc_ctx_create", "cc_ctx_destroy", "cc_ctx_set_launch",
     "cc_ctx_set_step_limit", "cc_ctx_set_tally_fp32", "cc_tables_create", "cc_tables_destroy", "cc_scene_create",
     "cc_scene_destroy", "cc_source_create", "cc_source_destroy", "cc_grid_create",
-    "cc_grid_destroy", "cc_grid_reset", "cc_grid_download", "cc_grid_end_batch",
+    "cc_grid_destroy", "cc_grid_reset", "cc_grid_download", "cc_grid_end_batch", "cc_grid_maps", "cc_grid_upload",
     "cc_transport_photons", "cc_transport_photons_device", "cc_run", "cc_sample_source",
     "cc_transport_photons_device_noalloc", "cc_batch_create", "cc_batch_run", "cc_batch_destroy",
 ]
@@ -122,6 +122,8 @@ def _bind(lib):
         "cc_grid_reset": (C.c_int, [P]),
         "cc_grid_download": (C.c_int, [P, PD, PD, PD, PD, C.POINTER(C.c_int32), C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
         "cc_grid_end_batch": (C.c_int, [P, C.c_int64]),
+        "cc_grid_upload": (C.c_int, [P, PD, PD, PD, PD, C.POINTER(C.c_int32), C.c_int64, C.c_int64]),
+        "cc_grid_maps": (C.c_int, [P, C.POINTER(Primitive), C.c_int32, PD, C.c_double, C.c_double, C.c_double, C.c_int32, P, P, P, P]),
         "cc_transport_photons": (C.c_int, [P, P, P, P, C.c_int64, PD, PD, PD, C.c_uint64, C.c_uint64, C.c_int32,
                                            C.POINTER(C.c_int32), C.POINTER(C.c_uint8), C.POINTER(C.c_uint8), PD,
                                            C.POINTER(C.c_int64)]),

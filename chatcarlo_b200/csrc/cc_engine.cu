@@ -19,6 +19,7 @@
 // FP64.  Batches of histories score into separate scratch grids that a
 // fold kernel turns into the batch statistics of VoxelGrid.end_batch
 // (tally.py:59-94).
+#include <math_constants.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <stdio.h>
@@ -1371,6 +1372,102 @@ __global__ void unpack_kernel(const double2* __restrict__ total, const double2* 
     }
 }
 
+// ---------------------------------------------------------------------------
+// output maps (chatcarlo/diagnostics.py:16-26, tally.py:109-132, 135-175)
+// ---------------------------------------------------------------------------
+
+// One primitive in FP64 for the point test at voxel centres
+// (geometry.py:102-118 closed containment; an ellipsoid as (p-c)/semi).
+struct MapPrim {
+    int type, axis;
+    double c[3], s[3];      // centre; box / ellipsoid full edge or axis lengths
+    double r, height;       // sphere, cylinder
+    double density;         // of the primitive's material, g/cm^3
+};
+
+struct KMaps {
+    double o[3], h;         // grid origin and voxel edge (cm)
+    int nx, ny, nz;
+    double volume;          // voxel volume, computed by the caller as h ** 3
+    double divisor;         // every map is divided by it last (1, or the history count)
+    double bg_density;
+    double n_hist, n_batches_minus_1;
+    int rel_defined;        // M >= 2 and N > 0
+    int n_prims;
+};
+
+// Products and sums rounded one by one (no contraction into FMAs), in the
+// order NumPy evaluates the same expressions, so the maps equal the host's.
+__device__ __forceinline__ double sq_rn(double x) { return __dmul_rn(x, x); }
+
+__device__ __forceinline__ bool map_contains(const MapPrim& g, const double p[3]) {
+    if (g.type == CC_SHAPE_BOX) {
+        bool in = true;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const double half = __dmul_rn(g.s[k], 0.5);          // s / 2 (exact)
+            in = in && p[k] >= __dsub_rn(g.c[k], half) && p[k] <= __dadd_rn(g.c[k], half);
+        }
+        return in;
+    }
+    if (g.type == CC_SHAPE_SPHERE) {
+        double d2 = __dadd_rn(__dadd_rn(sq_rn(__dsub_rn(p[0], g.c[0])), sq_rn(__dsub_rn(p[1], g.c[1]))),
+                              sq_rn(__dsub_rn(p[2], g.c[2])));
+        return d2 <= sq_rn(g.r);
+    }
+    if (g.type == CC_SHAPE_ELLIPSOID) {
+        double u[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) u[k] = __ddiv_rn(__dsub_rn(p[k], g.c[k]), __dmul_rn(g.s[k], 0.5));
+        return __dadd_rn(__dadd_rn(sq_rn(u[0]), sq_rn(u[1])), sq_rn(u[2])) <= 1.0;
+    }
+    const int a = g.axis;
+    const int o0 = a == 0 ? 1 : 0, o1 = a == 2 ? 1 : 2;
+    const double r2 = __dadd_rn(sq_rn(__dsub_rn(comp(p, o0), comp(g.c, o0))), sq_rn(__dsub_rn(comp(p, o1), comp(g.c, o1))));
+    return r2 <= sq_rn(g.r) && fabs(__dsub_rn(comp(p, a), comp(g.c, a))) <= __dmul_rn(g.height, 0.5);
+}
+
+__global__ void maps_kernel(const double2* __restrict__ total, const double2* __restrict__ pending,
+                            const double2* __restrict__ q, const MapPrim* __restrict__ prims, const KMaps M,
+                            double* __restrict__ dose, double* __restrict__ h10, double* __restrict__ krel,
+                            double* __restrict__ hrel) {
+    const long long nvox = (long long)M.nx * M.ny * M.nz;
+    for (long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x; v < nvox;
+         v += (long long)gridDim.x * blockDim.x) {
+        double2 t = total[v];
+        if (pending) { const double2 y = pending[v]; t.x += y.x; t.y += y.y; }
+        if (dose) {
+            const int iz = (int)(v % M.nz), iy = (int)((v / M.nz) % M.ny), ix = (int)(v / ((long long)M.ny * M.nz));
+            const double p[3] = {__dadd_rn(M.o[0], __dmul_rn((double)ix + 0.5, M.h)),
+                                 __dadd_rn(M.o[1], __dmul_rn((double)iy + 0.5, M.h)),
+                                 __dadd_rn(M.o[2], __dmul_rn((double)iz + 0.5, M.h))};
+            double rho = M.bg_density;                         // the last primitive holding the centre wins
+            for (int i = 0; i < M.n_prims; ++i)
+                if (map_contains(prims[i], p)) rho = prims[i].density;
+            const double mass = __dmul_rn(__dmul_rn(rho, M.volume), 1e-3);
+            const double energy = __dmul_rn(__dmul_rn(t.x, 1e-3), 1.602176634e-13);
+            dose[v] = __ddiv_rn(mass > 0.0 ? __ddiv_rn(energy, mass) : 0.0, M.divisor);
+        }
+        if (h10) h10[v] = __ddiv_rn(__ddiv_rn(t.y, M.volume), M.divisor);
+        if (krel || hrel) {
+            const double2 s2 = q[v];
+            const double T[2] = {t.x, t.y}, Q[2] = {s2.x, s2.y};
+            double r[2];
+#pragma unroll
+            for (int j = 0; j < 2; ++j) {
+                if (!M.rel_defined) { r[j] = CUDART_NAN; continue; }
+                double var = __ddiv_rn(__dsub_rn(Q[j], __ddiv_rn(sq_rn(T[j]), M.n_hist)), M.n_batches_minus_1);
+                var = var < 0.0 ? 0.0 : var;                      // np.clip(var, 0, None); NaN stays NaN
+                const double sem = __dsqrt_rn(__ddiv_rn(var, M.n_hist));
+                const double mean = __ddiv_rn(T[j], M.n_hist);
+                r[j] = mean != 0.0 ? __ddiv_rn(sem, mean) : CUDART_NAN;
+            }
+            if (krel) krel[v] = r[0];
+            if (hrel) hrel[v] = r[1];
+        }
+    }
+}
+
 __global__ void sample_source_kernel(const KSource SRC, long long n, long long first,
                                      unsigned long long seed, double* pos, double* dir, double* en) {
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1451,6 +1548,9 @@ struct cc_grid {
     double* d_scratch = nullptr;    // [n_scratch][nvox] double2; slot 0 is the pending batch
     int n_scratch = 0;
     char* d_out = nullptr;          // download staging: kerma, h10, kerma_sum2, h10_sum2 (f64), n_hit (i32)
+    double* d_maps = nullptr;       // cc_grid_maps staging: 4 maps (f64), allocated on first use
+    double origin64[3] = {0, 0, 0}; // the caller's FP64 origin and voxel edge (the kernels track in FP32)
+    double voxel64 = 0;
     char* h_out = nullptr;          // pinned host copy of d_out
     long long n_batches = 0;
     long long n_histories = 0;
@@ -1836,7 +1936,8 @@ int cc_grid_create(cc_ctx* ctx, const double origin[3], int32_t nx, int32_t ny, 
     g->ctx = ctx;
     g->flags = flags;
     KGrid& k = g->k;
-    for (int a = 0; a < 3; ++a) k.o[a] = (real)origin[a];
+    for (int a = 0; a < 3; ++a) { k.o[a] = (real)origin[a]; g->origin64[a] = origin[a]; }
+    g->voxel64 = voxel_cm;
     k.h = (real)voxel_cm;
     k.inv_h = (real)(1.0 / voxel_cm);
     k.nx = nx; k.ny = ny; k.nz = nz;
@@ -1868,6 +1969,7 @@ int cc_grid_destroy(cc_grid* g) {
     cudaFree(g->d_nhit);
     cudaFree(g->d_scratch);
     cudaFree(g->d_out);
+    cudaFree(g->d_maps);
     cudaFreeHost(g->h_out);
     delete g;
     return CC_OK;
@@ -1934,6 +2036,91 @@ static int fold_batches(cc_grid* g, int n_slots, const long long* counts, int ce
     return CC_OK;
 }
 
+int cc_grid_upload(cc_grid* g, const double* kerma, const double* h10, const double* k2, const double* h2,
+                   const int32_t* nhit, int64_t n_batches, int64_t n_histories) {
+    if (!g || !kerma || !h10) return set_error(CC_E_INVALID, "grid, kerma and h10 are required");
+    const bool stats = g->d_q != nullptr;
+    if (stats && (!k2 || !h2 || !nhit)) return set_error(CC_E_INVALID, "a statistics grid needs its sums of squares and hit counts");
+    if (n_batches < 0 || n_histories < 0) return set_error(CC_E_INVALID, "negative batch or history count");
+    cc_ctx* c = g->ctx;
+    CC_CUDA(cudaSetDevice(c->device));
+    const long long nv = g->k.nvox;
+    std::vector<double> buf((size_t)2 * nv);
+    for (long long i = 0; i < nv; ++i) { buf[2 * i] = kerma[i]; buf[2 * i + 1] = h10[i]; }
+    CC_CUDA(cudaMemcpy(g->d_total, buf.data(), buf.size() * sizeof(double), cudaMemcpyHostToDevice));
+    if (stats) {
+        for (long long i = 0; i < nv; ++i) { buf[2 * i] = k2[i]; buf[2 * i + 1] = h2[i]; }
+        CC_CUDA(cudaMemcpy(g->d_q, buf.data(), buf.size() * sizeof(double), cudaMemcpyHostToDevice));
+        CC_CUDA(cudaMemcpy(g->d_nhit, nhit, (size_t)nv * sizeof(int), cudaMemcpyHostToDevice));
+    }
+    if (g->d_scratch) CC_CUDA(cudaMemset(g->d_scratch, 0, (size_t)g->n_scratch * nv * 2 * sizeof(double)));
+    g->n_batches = n_batches;
+    g->n_histories = n_histories;
+    return CC_OK;
+}
+
+int cc_grid_maps(cc_grid* g, const cc_primitive* prims, int32_t n_prims, const double* prim_density,
+                 double background_density, double voxel_volume_cm3, double divisor, int32_t on_device,
+                 double* dose_Gy, double* h10_pSv, double* kerma_rel, double* h10_rel) {
+    if (!g) return set_error(CC_E_INVALID, "grid is NULL");
+    if (n_prims < 0 || (n_prims > 0 && (!prims || !prim_density)))
+        return set_error(CC_E_INVALID, "primitives and their densities are required");
+    if (!(voxel_volume_cm3 > 0) || !(divisor > 0)) return set_error(CC_E_INVALID, "volume and divisor must be > 0");
+    if ((kerma_rel || h10_rel) && !g->d_q) return set_error(CC_E_INVALID, "relative errors need a CC_GRID_STATS grid");
+    cc_ctx* c = g->ctx;
+    CC_CUDA(cudaSetDevice(c->device));
+    std::vector<MapPrim> mp((size_t)n_prims);
+    for (int i = 0; i < n_prims; ++i) {
+        const cc_primitive& p = prims[i];
+        if (p.type < 0 || p.type > 3) return set_error(CC_E_BAD_SHAPE, "unknown primitive type " + std::to_string(p.type));
+        if (p.type == CC_SHAPE_CYLINDER && (p.axis < 0 || p.axis > 2)) return set_error(CC_E_INVALID, "cylinder axis must be 0, 1 or 2");
+        MapPrim& m = mp[i];
+        m.type = p.type;
+        m.axis = p.axis;
+        for (int a = 0; a < 3; ++a) { m.c[a] = p.center[a]; m.s[a] = p.size[a]; }
+        m.r = p.radius;
+        m.height = p.height;
+        m.density = prim_density[i];
+    }
+    KMaps M;
+    memset(&M, 0, sizeof(M));
+    for (int a = 0; a < 3; ++a) M.o[a] = g->origin64[a];
+    M.h = g->voxel64;
+    M.nx = g->k.nx; M.ny = g->k.ny; M.nz = g->k.nz;
+    M.volume = voxel_volume_cm3;
+    M.divisor = divisor;
+    M.bg_density = background_density;
+    M.n_hist = (double)g->n_histories;
+    M.n_batches_minus_1 = (double)(g->n_batches - 1);
+    M.rel_defined = (g->n_batches >= 2 && g->n_histories > 0) ? 1 : 0;
+    M.n_prims = n_prims;
+    const long long nv = g->k.nvox;
+    double* out[4] = {dose_Gy, h10_pSv, kerma_rel, h10_rel};
+    double* dev[4] = {dose_Gy, h10_pSv, kerma_rel, h10_rel};
+    if (!on_device) {
+        if (!g->d_maps) CC_CUDA(cudaMalloc(&g->d_maps, (size_t)4 * nv * sizeof(double)));
+        for (int j = 0; j < 4; ++j) dev[j] = out[j] ? g->d_maps + (size_t)j * nv : nullptr;
+    }
+    MapPrim* d_prims = nullptr;
+    if (n_prims > 0) {
+        CC_CUDA(cudaMalloc(&d_prims, mp.size() * sizeof(MapPrim)));
+        cudaError_t e = cudaMemcpyAsync(d_prims, mp.data(), mp.size() * sizeof(MapPrim), cudaMemcpyHostToDevice, c->stream);
+        if (e != cudaSuccess) { cudaFree(d_prims); return set_error(CC_E_DEVICE, cudaGetErrorString(e)); }
+    }
+    const int threads = 256;
+    const int blocks = std::max(1, std::min((int)((nv + threads - 1) / threads), c->sm_count * 8));
+    // totals as cc_grid_download gives them: folded batches plus the pending one
+    maps_kernel<<<blocks, threads, 0, c->stream>>>((const double2*)g->d_total, (const double2*)g->d_scratch,
+                                                   (const double2*)g->d_q, d_prims, M, dev[0], dev[1], dev[2], dev[3]);
+    cudaError_t e = cudaGetLastError();
+    for (int j = 0; j < 4 && e == cudaSuccess && !on_device; ++j)
+        if (out[j]) e = cudaMemcpyAsync(out[j], dev[j], (size_t)nv * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    cudaFree(d_prims);
+    if (e != cudaSuccess) return set_error(CC_E_DEVICE, std::string("grid maps: ") + cudaGetErrorString(e));
+    return CC_OK;
+}
+
 int cc_grid_end_batch(cc_grid* g, int64_t n_hist) {
     if (!g) return set_error(CC_E_INVALID, "grid is NULL");
     if (!(g->flags & CC_GRID_STATS) || n_hist <= 0) return CC_OK;
@@ -1952,15 +2139,8 @@ int cc_grid_download(cc_grid* g, double* kerma, double* h10, double* k2, double*
     const long long nv = g->k.nvox;
     const bool stats = g->d_q != nullptr;
     const size_t bytes = (size_t)nv * ((stats ? 4 : 2) * sizeof(double) + (stats ? sizeof(int) : 0));
-    if (!g->d_out) {
-        // staging allocated on the first download and kept with the grid
-        CC_CUDA(cudaMalloc(&g->d_out, bytes));
-        if (cudaHostAlloc((void**)&g->h_out, bytes, cudaHostAllocDefault) != cudaSuccess) {
-            cudaFree(g->d_out);
-            g->d_out = nullptr;
-            return set_error(CC_E_NOMEM, "pinned host staging for the grid download failed");
-        }
-    }
+    // device staging allocated on the first download and kept with the grid
+    if (!g->d_out) CC_CUDA(cudaMalloc(&g->d_out, bytes));
     double* ok = (double*)g->d_out;
     double* oh = ok + nv;
     double* ok2 = stats ? oh + nv : nullptr;
@@ -1971,17 +2151,37 @@ int cc_grid_download(cc_grid* g, double* kerma, double* h10, double* k2, double*
     unpack_kernel<<<blocks, threads, 0, c->stream>>>((const double2*)g->d_total, (const double2*)g->d_scratch,
                                                      (const double2*)g->d_q, g->d_nhit, ok, oh, ok2, oh2, on, nv);
     CC_CUDA(cudaGetLastError());
-    CC_CUDA(cudaMemcpyAsync(g->h_out, g->d_out, bytes, cudaMemcpyDeviceToHost, c->stream));
-    CC_CUDA(cudaStreamSynchronize(c->stream));
-    const double* hk = (const double*)g->h_out;
+    // each output goes straight into the caller's array when that is
+    // page-locked host memory, else through the grid's pinned staging
     const size_t b8 = (size_t)nv * sizeof(double);
-    if (kerma) memcpy(kerma, hk, b8);
-    if (h10) memcpy(h10, hk + nv, b8);
-    if (stats) {
-        if (k2) memcpy(k2, hk + 2 * nv, b8);
-        if (h2) memcpy(h2, hk + 3 * nv, b8);
-        if (nhit) memcpy(nhit, hk + 4 * nv, (size_t)nv * sizeof(int));
+    struct Out { void* dst; const char* src; size_t bytes; bool pinned; };
+    Out outs[5] = {{kerma, (const char*)ok, b8, false}, {h10, (const char*)oh, b8, false},
+                   {stats ? k2 : nullptr, (const char*)ok2, b8, false}, {stats ? h2 : nullptr, (const char*)oh2, b8, false},
+                   {stats ? nhit : nullptr, (const char*)on, (size_t)nv * sizeof(int), false}};
+    bool staged = false;
+    for (Out& o : outs) {
+        if (!o.dst) continue;
+        cudaPointerAttributes at;
+        o.pinned = cudaPointerGetAttributes(&at, o.dst) == cudaSuccess && at.type == cudaMemoryTypeHost;
+        cudaGetLastError();
+        // pinned host staging, allocated when an output first needs it
+        if (!o.pinned && !g->h_out && cudaHostAlloc((void**)&g->h_out, bytes, cudaHostAllocDefault) != cudaSuccess) {
+            g->h_out = nullptr;
+            cudaStreamSynchronize(c->stream);     // copies already queued finish before the error returns
+            return set_error(CC_E_NOMEM, "pinned host staging for the grid download failed");
+        }
+        const size_t off = (size_t)(o.src - g->d_out);
+        if (o.pinned) {
+            CC_CUDA(cudaMemcpyAsync(o.dst, o.src, o.bytes, cudaMemcpyDeviceToHost, c->stream));
+        } else {
+            CC_CUDA(cudaMemcpyAsync(g->h_out + off, o.src, o.bytes, cudaMemcpyDeviceToHost, c->stream));
+            staged = true;
+        }
     }
+    CC_CUDA(cudaStreamSynchronize(c->stream));
+    if (staged)
+        for (const Out& o : outs)
+            if (o.dst && !o.pinned) memcpy(o.dst, g->h_out + (size_t)(o.src - g->d_out), o.bytes);
     if (n_batches) *n_batches = g->n_batches;
     if (n_histories) *n_histories = g->n_histories;
     return CC_OK;

@@ -17,12 +17,27 @@ MEV_TO_JOULE = 1.602176634e-13
 G_TO_KG = 1e-3
 
 
+def host_zeros(shape, dtype=np.float64, pinned: bool = False) -> np.ndarray:
+    """Zeroed host array; page-locked (so device copies land in it directly)
+    when pinned and a CUDA device is present."""
+    if pinned:
+        try:
+            import torch
+            if torch.cuda.is_available():
+                tdt = {np.dtype(np.float64): torch.float64, np.dtype(np.int32): torch.int32}[np.dtype(dtype)]
+                return torch.zeros(tuple(shape), dtype=tdt, pin_memory=True).numpy()
+        except ImportError:
+            pass
+    return np.zeros(shape, dtype)
+
+
 @dataclass
 class VoxelGrid:
     origin_cm: np.ndarray
     shape: tuple
     voxel_size_cm: float
     track_uncertainty: bool = False
+    pinned: bool = False            # page-locked arrays: the device writes results straight into them
     kerma_keV: np.ndarray = field(init=False)
     h10_track_pSv_cm3: np.ndarray = field(init=False)
     kerma_sum2: np.ndarray = field(init=False, default=None)
@@ -34,19 +49,20 @@ class VoxelGrid:
     def __post_init__(self):
         self.origin_cm = np.asarray(self.origin_cm, dtype=float)
         self.shape = tuple(int(s) for s in self.shape)
-        self.kerma_keV = np.zeros(self.shape)
-        self.h10_track_pSv_cm3 = np.zeros(self.shape)
+        self.kerma_keV = host_zeros(self.shape, pinned=self.pinned)
+        self.h10_track_pSv_cm3 = host_zeros(self.shape, pinned=self.pinned)
         if self.track_uncertainty:
-            self.kerma_sum2 = np.zeros(self.shape)
-            self.h10_sum2 = np.zeros(self.shape)
-            self.n_batches_hit = np.zeros(self.shape, dtype=np.int32)
+            self.kerma_sum2 = host_zeros(self.shape, pinned=self.pinned)
+            self.h10_sum2 = host_zeros(self.shape, pinned=self.pinned)
+            self.n_batches_hit = host_zeros(self.shape, np.int32, pinned=self.pinned)
 
     @classmethod
-    def from_bbox(cls, bbox_min, bbox_max, resolution_cm: float, track_uncertainty: bool = False):
+    def from_bbox(cls, bbox_min, bbox_max, resolution_cm: float, track_uncertainty: bool = False,
+                  pinned: bool = False):
         extent = np.asarray(bbox_max, dtype=float) - np.asarray(bbox_min, dtype=float)
         shape = tuple(max(1, int(np.ceil(x / resolution_cm))) for x in extent)
         return cls(origin_cm=np.asarray(bbox_min, dtype=float), shape=shape,
-                   voxel_size_cm=resolution_cm, track_uncertainty=track_uncertainty)
+                   voxel_size_cm=resolution_cm, track_uncertainty=track_uncertainty, pinned=pinned)
 
     def kerma_relative_error(self) -> np.ndarray:
         return relative_error(self.kerma_keV, self.kerma_sum2, self.n_batches, self.n_histories)

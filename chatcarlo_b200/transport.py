@@ -54,6 +54,8 @@ class TransportResult:
     transport_launches: int = 0
     n_steps: int = 0
     n_voxel_visits: int = 0
+    # output maps computed on the device when run_transport(maps=True)
+    maps: dict | None = None
 
 
 class DeviceGrid:
@@ -69,13 +71,64 @@ class DeviceGrid:
         N.check(self.lib.cc_grid_create(engine.ctx, N.dptr(origin), nx, ny, nz, float(grid.voxel_size_cm),
                                         N.CC_GRID_STATS if stats else 0, C.byref(self.handle)), self.lib)
         self.stats = stats
+        self.voxel_cm = float(grid.voxel_size_cm)
+
+    def maps(self, geometry: Geometry, divisor: float = 1.0, dose: bool = True, h10: bool = True,
+             rel: bool = False, out: dict | None = None) -> dict:
+        """Output maps on the device (cc_grid_maps): ``dose_Gy`` (kerma to dose
+        with the density at each voxel centre, chatcarlo/diagnostics.py:16-26),
+        ``h10_pSv`` (tally.py:130-132) and, with ``rel``, ``kerma_rel`` /
+        ``h10_rel`` (tally.py:96-100), each divided by ``divisor``; equal to
+        the host computation bit for bit.  ``out`` may give the arrays
+        (host numpy arrays, or torch CUDA tensors to keep the maps on the
+        device)."""
+        from .tables import density
+        names = ["dose_Gy", "h10_pSv", "kerma_rel", "h10_rel"]
+        want = [dose, h10, rel, rel]
+        out = dict(out or {})
+        on_device = None
+        ptrs = []
+        for name, w in zip(names, want):
+            if not w:
+                ptrs.append(None)
+                continue
+            a = out.get(name)
+            if a is None:
+                a = out[name] = np.empty(self.shape)
+            dev = hasattr(a, "is_cuda") and a.is_cuda
+            if on_device is None:
+                on_device = dev
+            if dev != on_device or tuple(a.shape) != self.shape:
+                raise ValueError("map outputs must all be host arrays or all device tensors of the grid's shape")
+            if dev:
+                ptrs.append(a.data_ptr())
+            else:
+                if a.dtype != np.float64 or not a.flags.c_contiguous:
+                    raise ValueError("host map outputs must be C-contiguous float64 arrays")
+                ptrs.append(a.ctypes.data)
+        prims = geometry.primitives({m: i for i, m in enumerate(geometry.materials())})
+        dens = np.array([density(g["material"]) for g in geometry.geoms], dtype=float)
+        N.check(self.lib.cc_grid_maps(self.handle, prims, len(geometry.geoms), N.dptr(dens),
+                                      float(density(geometry.background)), self.voxel_cm ** 3, float(divisor),
+                                      int(bool(on_device)), *ptrs), self.lib)
+        return {k: out[k] for k, w in zip(names, want) if w}
 
     def download(self, grid: VoxelGrid, accumulate: bool = False) -> None:
-        k = np.empty(self.shape)
-        h = np.empty(self.shape)
-        k2 = np.empty(self.shape) if self.stats else None
-        h2 = np.empty(self.shape) if self.stats else None
-        nh = np.empty(self.shape, dtype=np.int32) if self.stats else None
+        """Totals (and batch statistics) into the host grid's arrays: written
+        in place when they are C-contiguous arrays of this shape (by the
+        device itself when they are page-locked), else copied over."""
+        stats = self.stats and grid.track_uncertainty
+
+        def target(a, dtype=np.float64):
+            ok = (not accumulate and isinstance(a, np.ndarray) and a.dtype == dtype and a.shape == self.shape
+                  and a.flags.c_contiguous and a.flags.writeable)
+            return a if ok else np.empty(self.shape, dtype)
+
+        k = target(grid.kerma_keV)
+        h = target(grid.h10_track_pSv_cm3)
+        k2 = target(grid.kerma_sum2) if stats else None
+        h2 = target(grid.h10_sum2) if stats else None
+        nh = target(grid.n_batches_hit, np.int32) if stats else None
         nb = C.c_int64()
         nhist = C.c_int64()
         N.check(self.lib.cc_grid_download(
@@ -87,14 +140,33 @@ class DeviceGrid:
             grid.kerma_keV += k
             grid.h10_track_pSv_cm3 += h
         else:
-            grid.kerma_keV[...] = k
-            grid.h10_track_pSv_cm3[...] = h
-        if self.stats and grid.track_uncertainty:
-            grid.kerma_sum2[...] = k2
-            grid.h10_sum2[...] = h2
-            grid.n_batches_hit[...] = nh
+            if k is not grid.kerma_keV:
+                grid.kerma_keV[...] = k
+            if h is not grid.h10_track_pSv_cm3:
+                grid.h10_track_pSv_cm3[...] = h
+        if stats:
+            for src, name in ((k2, "kerma_sum2"), (h2, "h10_sum2"), (nh, "n_batches_hit")):
+                if src is not getattr(grid, name):
+                    getattr(grid, name)[...] = src
             grid.n_batches = int(nb.value)
             grid.n_histories = int(nhist.value)
+
+    def upload(self, grid: VoxelGrid) -> None:
+        """Load a host grid's totals (and batch statistics) into this device
+        grid (cc_grid_upload)."""
+        f64 = lambda a: np.ascontiguousarray(a, dtype=np.float64)  # noqa: E731
+        k, h = f64(grid.kerma_keV), f64(grid.h10_track_pSv_cm3)
+        if self.stats:
+            if not grid.track_uncertainty:
+                raise ValueError("a statistics device grid needs a host grid with track_uncertainty")
+            k2, h2 = f64(grid.kerma_sum2), f64(grid.h10_sum2)
+            nh = np.ascontiguousarray(grid.n_batches_hit, dtype=np.int32)
+            N.check(self.lib.cc_grid_upload(self.handle, N.dptr(k), N.dptr(h), N.dptr(k2), N.dptr(h2),
+                                            nh.ctypes.data_as(C.POINTER(C.c_int32)), int(grid.n_batches),
+                                            int(grid.n_histories)), self.lib)
+        else:
+            N.check(self.lib.cc_grid_upload(self.handle, N.dptr(k), N.dptr(h), None, None, None,
+                                            int(grid.n_batches), int(grid.n_histories)), self.lib)
 
     def reset(self):
         N.check(self.lib.cc_grid_reset(self.handle), self.lib)
@@ -278,12 +350,17 @@ def run_transport(scene, n_histories: int = 100_000, seed: int | None = None,
                   batch_size: int = 200_000, dose_grid: bool = False,
                   grid_resolution_cm: float = 5.0, n_workers: int = 1,
                   track_uncertainty: bool = True, engine: Engine | None = None,
-                  first_history: int = 0, grid: VoxelGrid | None = None) -> TransportResult:
+                  first_history: int = 0, grid: VoxelGrid | None = None,
+                  maps: bool = False) -> TransportResult:
     """run_transport (chatcarlo/transport.py:358-474) on the GPU.
 
     ``n_workers`` is accepted for signature compatibility; the histories run
     on one device.  The source is sampled on the device, histories are
-    grouped into batches of ``batch_size`` for the batch statistics.
+    grouped into batches of ``batch_size`` for the batch statistics.  With
+    ``maps`` and a dose grid, ``result.maps`` holds the per-history dose and
+    H*(10) maps of chatcarlo/__main__.py:200-209 (``dose_per_history_Gy``,
+    ``h10_per_history_pSv``) and, with ``track_uncertainty``, the relative
+    error maps (``kerma_rel``, ``h10_rel``), all computed on the device.
     """
     raw = scene.raw if hasattr(scene, "raw") else scene
     src = raw["source"]
@@ -294,7 +371,7 @@ def run_transport(scene, n_histories: int = 100_000, seed: int | None = None,
     geometry = Geometry(raw["geometry"])
     if dose_grid and grid is None:
         grid = VoxelGrid.from_bbox(geometry.bbox_min, geometry.bbox_max, grid_resolution_cm,
-                                   track_uncertainty=track_uncertainty)
+                                   track_uncertainty=track_uncertainty, pinned=True)
     if not dose_grid:
         grid = None
     fluorescence = raw.get("physics", {}).get("fluorescence", True)
@@ -306,12 +383,19 @@ def run_transport(scene, n_histories: int = 100_000, seed: int | None = None,
     edep = np.zeros(len(names))
     edep2 = np.zeros(len(names))
     out = N.RunOut()
+    out_maps = None
     try:
         N.check(eng.lib.cc_run(eng.ctx, sh, th, srch, dg.handle if dg else None, int(n_histories),
                                int(batch_size), _seed_from(None, seed), int(first_history),
                                int(bool(fluorescence)), N.dptr(edep), N.dptr(edep2), C.byref(out)))
         if dg is not None:
             dg.download(grid)
+            if maps:
+                m = dg.maps(geometry, divisor=float(max(int(n_histories), 1)), rel=track_uncertainty)
+                out_maps = {"dose_per_history_Gy": m["dose_Gy"], "h10_per_history_pSv": m["h10_pSv"]}
+                if track_uncertainty:
+                    out_maps["kerma_rel"] = m["kerma_rel"]
+                    out_maps["h10_rel"] = m["h10_rel"]
     finally:
         eng.lib.cc_scene_destroy(sh)
     n_batches = int(out.n_batches)
@@ -347,4 +431,5 @@ def run_transport(scene, n_histories: int = 100_000, seed: int | None = None,
         transport_launches=int(out.transport_launches),
         n_steps=int(out.n_steps),
         n_voxel_visits=int(out.n_voxel_visits),
+        maps=out_maps,
     )

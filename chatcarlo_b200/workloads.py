@@ -102,10 +102,10 @@ def ct() -> dict:
 CT_GRID = {"origin": (-16.0, -16.0, -7.5), "shape": (320, 320, 150), "voxel_cm": 0.1}
 
 
-def make_grid(spec: dict, track_uncertainty: bool = True):
+def make_grid(spec: dict, track_uncertainty: bool = True, pinned: bool = False):
     from .tally import VoxelGrid
     return VoxelGrid(origin_cm=np.asarray(spec["origin"], dtype=float), shape=spec["shape"],
-                     voxel_size_cm=spec["voxel_cm"], track_uncertainty=track_uncertainty)
+                     voxel_size_cm=spec["voxel_cm"], track_uncertainty=track_uncertainty, pinned=pinned)
 
 
 def pencil_beam_arrays(n: int, start, direction, energy_kev: float):

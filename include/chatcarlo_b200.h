@@ -187,10 +187,42 @@ int cc_grid_create(cc_ctx* ctx, const double origin[3], int32_t nx, int32_t ny, 
                    double voxel_cm, int32_t flags, cc_grid** out);
 int cc_grid_destroy(cc_grid* g);
 int cc_grid_reset(cc_grid* g);
-/* Any output pointer may be NULL.  Arrays are C-ordered (nx, ny, nz). */
+/* Any output pointer may be NULL.  Arrays are C-ordered (nx, ny, nz).  An
+ * output in page-locked host memory is written by the device directly;
+ * other outputs go through a pinned staging buffer kept with the grid. */
 int cc_grid_download(cc_grid* g, double* kerma_keV, double* h10_track_pSv_cm3,
                      double* kerma_sum2, double* h10_sum2, int32_t* n_batches_hit,
                      int64_t* n_batches, int64_t* n_histories);
+/* Loads a grid's state (totals; for a CC_GRID_STATS grid also the sums of
+ * squares, hit counts, batch and history counts) from host arrays, C-ordered
+ * (nx, ny, nz), and clears any pending batch: no reference counterpart as
+ * one call (the reference assigns VoxelGrid arrays or merges worker grids,
+ * transport.py:416-417); for resuming a run or post-processing saved
+ * tallies on the device. */
+int cc_grid_upload(cc_grid* g, const double* kerma_keV, const double* h10_track_pSv_cm3,
+                   const double* kerma_sum2, const double* h10_sum2, const int32_t* n_batches_hit,
+                   int64_t n_batches, int64_t n_histories);
+/* Output maps of a grid computed on the device, with the grid's totals as
+ * cc_grid_download gives them:
+ *   dose_Gy   <- chatcarlo/diagnostics.py:16-26 dose_map_Gy: kerma to dose
+ *                with the density of the material at each voxel centre
+ *                (tally.py:109-116 centres, geometry.py:102-118 closed point
+ *                tests, the last primitive holding a centre wins, else
+ *                background_density; tally.py:124-128)
+ *   h10_pSv   <- tally.py:130-132 h10_map_pSv
+ *   kerma_rel, h10_rel <- tally.py:96-100,135-175 relative errors (NaN where
+ *                the reference gives NaN; need a CC_GRID_STATS grid)
+ * prims / prim_density: the scene's primitives (as for cc_scene_create) and
+ * the density of each one's material; voxel_volume_cm3: the caller's
+ * voxel_cm ** 3; every map is divided by divisor last (1 for totals, the
+ * history count for the per-history maps of chatcarlo/__main__.py:208-209).
+ * FP64, evaluated in NumPy's order without contraction: the maps equal the
+ * reference's host computation bit for bit.  on_device = 1: the outputs are
+ * device pointers and nothing is copied to the host.  Any output may be
+ * NULL. */
+int cc_grid_maps(cc_grid* g, const cc_primitive* prims, int32_t n_prims, const double* prim_density,
+                 double background_density, double voxel_volume_cm3, double divisor, int32_t on_device,
+                 double* dose_Gy, double* h10_pSv, double* kerma_rel, double* h10_rel);
 /* VoxelGrid.end_batch (tally.py:59-94) for photons scored outside cc_run:
  * folds the batch accumulated since the previous fold. */
 int cc_grid_end_batch(cc_grid* g, int64_t n_histories_in_batch);

@@ -883,3 +883,44 @@ def ctdi_per_history_Gy(src, phantom="body", n_histories=200_000, seed=None):
     d_center = float(dose[z_ok & (r < 2.0)].mean())
     d_periph = float(dose[z_ok & (r >= radius - 2.0) & (r <= radius - 1.0)].mean())
     return d_center / 3.0 + 2.0 * d_periph / 3.0, d_center, d_periph
+
+
+# ---------------------------------------------------------------------------
+# output maps (chatcarlo/diagnostics.py:16-26, chatcarlo/tally.py:109-175)
+# ---------------------------------------------------------------------------
+
+def voxel_centers(origin, shape, voxel_cm):
+    """tally.py:109-116: voxel centres in C order, (nx*ny*nz, 3)."""
+    axes = [origin[k] + (np.arange(shape[k]) + 0.5) * voxel_cm for k in range(3)]
+    g = np.meshgrid(*axes, indexing="ij")
+    return np.stack([x.ravel() for x in g], axis=1)
+
+
+def dose_map_Gy(kerma_keV, origin, voxel_cm, geometry, density_of):
+    """diagnostics.py:16-26 with tally.py:118-128: the material at each voxel
+    centre gives the density that turns kerma into dose."""
+    shape = kerma_keV.shape
+    mat = geometry.material_at(voxel_centers(np.asarray(origin, dtype=float), shape, voxel_cm))
+    rho = np.array([density_of(m) for m in mat]).reshape(shape)
+    mass_kg = rho * voxel_cm ** 3 * 1e-3
+    energy_j = kerma_keV * 1e-3 * 1.602176634e-13
+    return np.divide(energy_j, mass_kg, out=np.zeros_like(energy_j), where=mass_kg > 0)
+
+
+def h10_map_pSv(h10_track, voxel_cm):
+    """tally.py:130-132."""
+    return h10_track / voxel_cm ** 3
+
+
+def relative_error(T, Q, n_batches, n_histories):
+    """tally.py:135-175: R = SEM / (T/N) from batch sums, NaN where T = 0 or
+    fewer than two batches."""
+    T = np.asarray(T, dtype=float)
+    Q = np.asarray(Q, dtype=float)
+    if n_batches < 2 or n_histories <= 0:
+        return np.full_like(T, np.nan)
+    var = np.clip((Q - T ** 2 / n_histories) / (n_batches - 1), 0.0, None)
+    sem = np.sqrt(var / n_histories)
+    mean = T / n_histories
+    with np.errstate(divide="ignore", invalid="ignore"):
+        return np.where(mean != 0, sem / mean, np.nan)

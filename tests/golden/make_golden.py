@@ -253,9 +253,45 @@ def case_ctdi():
     return {"ctdi": np.array([ctdiw, dc, dp]), "source_json": np.array(json.dumps(CT_SOURCE))}
 
 
+def case_maps():
+    """The CLI's output maps (__main__.py:198-209): dose per history from the
+    material at each voxel centre (diagnostics.py:16-26), H*(10) per
+    history, and the relative-error maps (tally.py:96-100), on a random grid
+    state.  Voxel centres sit on integer coordinates, so some lie exactly on
+    a box face, the sphere or a cylinder (the closed point tests)."""
+    from chatcarlo.diagnostics import dose_map_Gy
+    rng = np.random.default_rng(77)
+    origin, shape = np.array([-16.5, -4.5, -6.5]), (33, 16, 14)
+    grid = rtally.VoxelGrid(origin_cm=origin, shape=shape, voxel_size_cm=1.0, track_uncertainty=True)
+    k = rng.lognormal(0.0, 2.0, shape) * (rng.random(shape) < 0.9)
+    h = rng.lognormal(1.0, 1.5, shape) * (rng.random(shape) < 0.9)
+    grid.kerma_keV[...] = k
+    grid.h10_track_pSv_cm3[...] = h
+    grid.kerma_sum2[...] = k ** 2 / 1000.0 * rng.uniform(0.5, 3.0, shape)
+    grid.h10_sum2[...] = h ** 2 / 1000.0 * rng.uniform(0.5, 3.0, shape)
+    grid.n_batches_hit[...] = rng.integers(0, 8, shape)
+    grid.n_batches = 7
+    grid.n_histories = 12345
+    geometry = rgeom.Geometry(GEOMS)
+    n = grid.n_histories
+    out = {"kerma": k, "h10": h, "k2": grid.kerma_sum2.copy(), "h2": grid.h10_sum2.copy(),
+           "nhit": grid.n_batches_hit.copy(), "nb": np.array(7), "nh": np.array(n),
+           "dose": dose_map_Gy(grid, geometry) / n, "h10map": grid.h10_map_pSv() / n,
+           "krel": grid.kerma_relative_error(), "hrel": grid.h10_relative_error()}
+    grid.n_batches = 1                        # fewer than two batches: relative errors undefined
+    out["krel_m1"] = grid.kerma_relative_error()
+    out["origin"] = origin
+    out["shape"] = np.array(shape)
+    out["voxel_cm"] = np.array(1.0)
+    names = sorted({g["material"] for g in GEOMS} | {"air"})
+    out["density_names"] = np.array(names)
+    out["density_values"] = np.array([rmat.density(m) for m in names])
+    return out
+
+
 CASES = {"geometry": case_geometry, "materials": case_materials, "samplers": case_samplers,
          "tally": case_tally, "transport": case_transport, "run": case_run, "source": case_source,
-         "ctdi": case_ctdi}
+         "ctdi": case_ctdi, "maps": case_maps}
 
 
 def main(names=None):

@@ -213,3 +213,23 @@ def test_ctdi_calibration_matches_reference(golden):
     src = json.loads(str(g["source_json"]))
     got = O.ctdi_per_history_Gy(src, phantom="head", n_histories=4000, seed=9)
     np.testing.assert_array_equal(np.array(got), g["ctdi"])
+
+
+def test_output_maps_match_reference(golden):
+    """Dose and H*(10) per history and the relative-error maps of the CLI
+    (chatcarlo/__main__.py:198-209), bit for bit."""
+    g = golden("maps")
+    dens = dict(zip(g["density_names"].tolist(), g["density_values"].tolist()))
+    for m, v in dens.items():
+        assert tb.density(m) == v, m
+    nh, nb, vox = int(g["nh"]), int(g["nb"]), float(g["voxel_cm"])
+    dose = O.dose_map_Gy(g["kerma"], g["origin"], vox, O.OracleGeometry(GEOMS), dens.__getitem__) / nh
+    np.testing.assert_array_equal(dose, g["dose"])
+    np.testing.assert_array_equal(O.h10_map_pSv(g["h10"], vox) / nh, g["h10map"])
+    np.testing.assert_array_equal(O.relative_error(g["kerma"], g["k2"], nb, nh), g["krel"])
+    np.testing.assert_array_equal(O.relative_error(g["h10"], g["h2"], nb, nh), g["hrel"])
+    np.testing.assert_array_equal(O.relative_error(g["kerma"], g["k2"], 1, nh), g["krel_m1"])
+    # centres on a box face, the sphere and the cylinders are part of the case
+    c = O.voxel_centers(g["origin"], tuple(g["shape"]), vox)
+    assert np.any(np.abs(c[:, 0]) == 15.0)
+    assert np.any(np.sum((c - np.array([5.0, -3.0, 2.0])) ** 2, axis=1) == 36.0)
