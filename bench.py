@@ -58,9 +58,10 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def profile_traffic():
-    """DRAM bytes per history of the transport kernel from the committed ncu summary."""
-    p = ROOT / "profiles" / "transport_kernel_room.json"
+def profile_traffic(workload: str = "room"):
+    """DRAM bytes per history of the transport kernel from the committed ncu
+    summary of that workload."""
+    p = ROOT / "profiles" / f"transport_kernel_{workload}.json"
     if p.exists():
         d = json.loads(p.read_text())
         return d.get("dram_bytes_per_history")
@@ -375,7 +376,7 @@ def main():
     launches = sum(o.gpu_launches for o in outs)
     peak, peak_kind = peaks()
     achieved = b_hist * n_h / (tr_ms / 1e3) / 1e9
-    traffic_per_hist = profile_traffic() if args.workload == "room" else None
+    traffic_per_hist = profile_traffic(args.workload)
     hist_per_launch = n_h / max(tr_launch, 1)
 
     # e2e: the public run_transport call a user makes, once per step: scene,
