@@ -46,7 +46,6 @@ constexpr int TABLE_N = 2000;            // F, A, S tables (materials.py:376-496
 constexpr int N_BUCKETS = 4096;          // uniform log-E index per material
 constexpr int RAY_BUCKETS = 1024;        // uniform-in-A index of each Rayleigh A(x) table
 constexpr int MAX_SCRATCH = 64;          // batches per launch
-constexpr float LOG_E_MIN = 0.0f;        // ln(1 keV)
 constexpr float E_MIN_KEV = 1.0f;
 constexpr float E_MAX_KEV = 150.0f;
 constexpr float HC = 12.3984193f;        // keV Angstrom (physics.py:35)
@@ -1352,6 +1351,62 @@ __global__ void fold_kernel(double2* __restrict__ total, double2* __restrict__ q
     }
 }
 
+// The batches of one launch at once (slots 0..n-1 in order, each as
+// fold_kernel): the totals, sums of squares and hit counts of a voxel are
+// read and written once per launch instead of once per batch.  The
+// additions per voxel happen in the same order as slot-by-slot folds.
+struct FoldSlots {
+    double inv_nb[MAX_SCRATCH];     // 1 / histories of each batch; 0 skips the slot
+    int n;
+};
+
+__global__ void fold_slots_kernel(double2* __restrict__ total, double2* __restrict__ q, int* __restrict__ nhit,
+                                  double2* __restrict__ scratch, long long nvox, const FoldSlots F, int cell32) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    long long stride = (long long)gridDim.x * blockDim.x;
+    for (; i < nvox; i += stride) {
+        double2 t = make_double2(0.0, 0.0), qq = make_double2(0.0, 0.0);
+        int h = 0;
+        bool loaded = false;
+        for (int s = 0; s < F.n; ++s) {
+            if (F.inv_nb[s] == 0.0) continue;
+            double2* sc = scratch + (size_t)s * nvox;
+            const double2 v = cell_read(sc, i, cell32);
+            if (v.x != 0.0 || v.y != 0.0) {
+                if (!loaded) { t = total[i]; qq = q[i]; h = nhit[i]; loaded = true; }
+                t.x += v.x; t.y += v.y;
+                qq.x += v.x * v.x * F.inv_nb[s];
+                qq.y += v.y * v.y * F.inv_nb[s];
+                h += 1;
+                sc[i] = make_double2(0.0, 0.0);
+            }
+        }
+        if (loaded) { total[i] = t; q[i] = qq; nhit[i] = h; }
+    }
+}
+
+// Slots 0..n-1 into the totals without statistics, in order: T += S_s, S_s = 0.
+__global__ void fold_plain_slots_kernel(double2* __restrict__ total, double2* __restrict__ scratch, long long nvox,
+                                        int n_slots, int cell32) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    long long stride = (long long)gridDim.x * blockDim.x;
+    for (; i < nvox; i += stride) {
+        double2 t = make_double2(0.0, 0.0);
+        bool loaded = false;
+        for (int s = 0; s < n_slots; ++s) {
+            double2* sc = scratch + (size_t)s * nvox;
+            const double2 v = cell_read(sc, i, cell32);
+            if (v.x != 0.0 || v.y != 0.0) {
+                if (!loaded) { t = total[i]; loaded = true; }
+                t.x += v.x;
+                t.y += v.y;
+                sc[i] = make_double2(0.0, 0.0);
+            }
+        }
+        if (loaded) total[i] = t;
+    }
+}
+
 // Batch scratch into the totals without statistics: T += S, S = 0.
 __global__ void fold_plain_kernel(double2* __restrict__ total, double2* __restrict__ scratch, long long nvox,
                                   int cell32) {
@@ -1532,6 +1587,20 @@ struct cc_ctx {
     int blocks_per_sm = 0;                       // 0 = occupancy based
     long long max_steps = 100000;
     int tally_fp32 = 0;                          // 1: FP32 scratch cells for slots of <= FP32_SLOT_HISTORIES
+    // cc_run keeps up to LAUNCH_RING launches in flight; each one's
+    // reductions land in its own page-locked record
+    static constexpr int LAUNCH_RING = 3;
+    struct LaunchRec {
+        double* h_edep = nullptr;                // [MAX_SCRATCH * MAX_MATS]
+        unsigned long long* h_cnt = nullptr;     // [6]
+        unsigned* h_status = nullptr;
+        cudaEvent_t k0 = nullptr, k1 = nullptr;  // around the transport kernel
+        cudaEvent_t done = nullptr;              // after the copies into this record
+        int ns = 0;                              // batches of the launch
+        long long n = 0;                         // histories of the launch
+        bool busy = false;
+    } ring[LAUNCH_RING];
+    char* h_ring = nullptr;
 };
 
 struct cc_tables {
@@ -1621,6 +1690,12 @@ int cc_ctx_destroy(cc_ctx* c) {
     cudaFree(c->d_counters);
     cudaFree(c->d_edep);
     cudaFree(c->d_io);
+    for (auto& r : c->ring) {
+        if (r.k0) cudaEventDestroy(r.k0);
+        if (r.k1) cudaEventDestroy(r.k1);
+        if (r.done) cudaEventDestroy(r.done);
+    }
+    cudaFreeHost(c->h_ring);
     cudaEventDestroy(c->ev0);
     cudaEventDestroy(c->ev1);
     cudaEventDestroy(c->kev0);
@@ -2026,6 +2101,12 @@ static int fold_plain(cc_grid* g, int n_slots, int cell32) {
     cc_ctx* c = g->ctx;
     int threads = 256;
     int blocks = std::max(1, std::min((int)((g->k.nvox + threads - 1) / threads), c->sm_count * 8));
+    if (n_slots > 1) {
+        fold_plain_slots_kernel<<<blocks, threads, 0, c->stream>>>((double2*)g->d_total, (double2*)g->d_scratch,
+                                                                   g->k.nvox, n_slots, cell32);
+        CC_CUDA(cudaGetLastError());
+        return CC_OK;
+    }
     for (int s = 0; s < n_slots; ++s) {
         fold_plain_kernel<<<blocks, threads, 0, c->stream>>>(
             (double2*)g->d_total, (double2*)(g->d_scratch + (size_t)s * 2 * g->k.nvox), g->k.nvox, cell32);
@@ -2038,6 +2119,21 @@ static int fold_batches(cc_grid* g, int n_slots, const long long* counts, int ce
     cc_ctx* c = g->ctx;
     int threads = 256;
     int blocks = std::max(1, std::min((int)((g->k.nvox + threads - 1) / threads), c->sm_count * 8));
+    if (n_slots > 1 && n_slots <= MAX_SCRATCH) {
+        FoldSlots F;
+        memset(&F, 0, sizeof(F));
+        F.n = n_slots;
+        for (int s = 0; s < n_slots; ++s) {
+            if (counts[s] <= 0) continue;
+            F.inv_nb[s] = 1.0 / (double)counts[s];
+            g->n_batches += 1;
+            g->n_histories += counts[s];
+        }
+        fold_slots_kernel<<<blocks, threads, 0, c->stream>>>((double2*)g->d_total, (double2*)g->d_q, g->d_nhit,
+                                                             (double2*)g->d_scratch, g->k.nvox, F, cell32);
+        CC_CUDA(cudaGetLastError());
+        return CC_OK;
+    }
     for (int s = 0; s < n_slots; ++s) {
         if (counts[s] <= 0) continue;
         fold_kernel<<<blocks, threads, 0, c->stream>>>(
@@ -2226,11 +2322,33 @@ static int grid_blocks_for(cc_ctx* c, size_t smem, bool fs, bool tl) {
     return c->sm_count * per_sm;
 }
 
-// One launch of the transport kernel plus its reductions.
-static int run_launch(cc_ctx* c, const cc_scene* scene, const cc_tables* tables, const KSource* src,
-                      cc_grid* grid, double* tally_base, int n_slots, long long batch_size,
-                      KRun R, std::vector<double>& edep_slots, unsigned long long* counters_out,
-                      float* kernel_ms, int cell32 = 0) {
+// Page-locked records and events of the launch ring, created on first use.
+static int ensure_ring(cc_ctx* c) {
+    if (c->h_ring) return CC_OK;
+    const size_t per = (size_t)MAX_SCRATCH * MAX_MATS * sizeof(double) + 8 * sizeof(unsigned long long);
+    char* h = nullptr;
+    if (cudaHostAlloc((void**)&h, per * cc_ctx::LAUNCH_RING, cudaHostAllocDefault) != cudaSuccess)
+        return set_error(CC_E_NOMEM, "page-locked launch records");
+    for (int i = 0; i < cc_ctx::LAUNCH_RING; ++i) {
+        auto& r = c->ring[i];
+        r.h_edep = (double*)(h + per * i);
+        r.h_cnt = (unsigned long long*)(h + per * i + (size_t)MAX_SCRATCH * MAX_MATS * sizeof(double));
+        r.h_status = (unsigned*)(r.h_cnt + 6);
+        if (cudaEventCreate(&r.k0) != cudaSuccess || cudaEventCreate(&r.k1) != cudaSuccess ||
+            cudaEventCreateWithFlags(&r.done, cudaEventDisableTiming) != cudaSuccess) {
+            cudaFreeHost(h);
+            return set_error(CC_E_DEVICE, "launch ring events");
+        }
+    }
+    c->h_ring = h;
+    return CC_OK;
+}
+
+// One launch of the transport kernel plus the copies of its reductions into
+// a ring record, queued on the context's stream without waiting.
+static int enqueue_launch(cc_ctx* c, const cc_scene* scene, const cc_tables* tables, const KSource* src,
+                          cc_grid* grid, double* tally_base, int n_slots, long long batch_size, KRun R,
+                          int cell32, cc_ctx::LaunchRec& rec) {
     const KTables& T = tables->k;
     R.n_scratch = n_slots;
     R.batch_size = batch_size;
@@ -2256,27 +2374,53 @@ static int run_launch(cc_ctx* c, const cc_scene* scene, const cc_tables* tables,
     if (fs) S = *src;
     size_t smem = n_acc * sizeof(double);
     int blocks = grid_blocks_for(c, smem, fs, tl);
-    CC_CUDA(cudaEventRecord(c->kev0, st));
+    CC_CUDA(cudaEventRecord(rec.k0, st));
     cudaError_t e;
     if (fs && tl) e = launch_transport<true, true>(c, T, scene->k, G, S, R, smem, blocks);
     else if (fs) e = launch_transport<true, false>(c, T, scene->k, G, S, R, smem, blocks);
     else if (tl) e = launch_transport<false, true>(c, T, scene->k, G, S, R, smem, blocks);
     else e = launch_transport<false, false>(c, T, scene->k, G, S, R, smem, blocks);
     if (e != cudaSuccess) return set_error(CC_E_DEVICE, std::string("transport launch: ") + cudaGetErrorString(e));
-    CC_CUDA(cudaEventRecord(c->kev1, st));
-    edep_slots.assign(n_acc, 0.0);
-    unsigned st_h = 0;
-    e = cudaMemcpyAsync(edep_slots.data(), c->d_edep, n_acc * sizeof(double), cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(counters_out, c->d_counters, 6 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(&st_h, c->d_status, sizeof(unsigned), cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    CC_CUDA(cudaEventRecord(rec.k1, st));
+    e = cudaMemcpyAsync(rec.h_edep, c->d_edep, n_acc * sizeof(double), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(rec.h_cnt, c->d_counters, 6 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(rec.h_status, c->d_status, sizeof(unsigned), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaEventRecord(rec.done, st);
+    if (e != cudaSuccess) return set_error(CC_E_DEVICE, std::string("transport: ") + cudaGetErrorString(e));
+    rec.ns = n_slots;
+    rec.busy = true;
+    return CC_OK;
+}
+
+// Waits for a ring record's launch (its copies were queued after the kernel)
+// and returns its status as an error code.
+static int finish_launch(cc_ctx::LaunchRec& rec, float* kernel_ms) {
+    cudaError_t e = cudaEventSynchronize(rec.done);
+    rec.busy = false;
     if (e != cudaSuccess) return set_error(CC_E_DEVICE, std::string("transport: ") + cudaGetErrorString(e));
     if (kernel_ms) {
         float ms = 0.f;
-        cudaEventElapsedTime(&ms, c->kev0, c->kev1);
+        cudaEventElapsedTime(&ms, rec.k0, rec.k1);
         *kernel_ms = ms;
     }
-    return status_to_error(st_h);
+    return status_to_error(*rec.h_status);
+}
+
+// One synchronous launch: queued, then waited for.
+static int run_launch(cc_ctx* c, const cc_scene* scene, const cc_tables* tables, const KSource* src,
+                      cc_grid* grid, double* tally_base, int n_slots, long long batch_size,
+                      KRun R, std::vector<double>& edep_slots, unsigned long long* counters_out,
+                      float* kernel_ms, int cell32 = 0) {
+    int rc = ensure_ring(c);
+    if (rc != CC_OK) return rc;
+    cc_ctx::LaunchRec& rec = c->ring[0];
+    rc = enqueue_launch(c, scene, tables, src, grid, tally_base, n_slots, batch_size, R, cell32, rec);
+    if (rc != CC_OK) return rc;
+    rc = finish_launch(rec, kernel_ms);
+    const size_t n_acc = (size_t)n_slots * tables->k.n_mat;
+    edep_slots.assign(rec.h_edep, rec.h_edep + n_acc);
+    for (int k = 0; k < 6; ++k) counters_out[k] = rec.h_cnt[k];
+    return rc;
 }
 
 static int transport_common(cc_ctx* c, const cc_scene* scene, const cc_tables* tables, cc_grid* grid,
@@ -2399,6 +2543,41 @@ int cc_run(cc_ctx* c, const cc_scene* scene, const cc_tables* tables, const cc_s
     float ms_total = 0.0f;
     double ms_transport = 0.0;
     long long transport_launches = 0;
+    int rc = ensure_ring(c);
+    if (rc != CC_OK) return rc;
+    // Launches are queued up to LAUNCH_RING deep; a launch's reductions are
+    // read from its ring record when the record is needed again or at the
+    // end, so the host never leaves the GPU idle between launches.  Records
+    // are finished in launch order, so the per-batch sums below are added in
+    // the same order as with one launch at a time.
+    auto finish = [&](cc_ctx::LaunchRec& rec) -> int {
+        float kms = 0.f;
+        const int frc = finish_launch(rec, &kms);
+        ms_transport += kms;
+        // per-batch collision-estimator moments (ScalarMoments.add_batch, tally.py:204-213)
+        for (int b = 0; b < rec.ns; ++b) {
+            long long nb = std::min<long long>(batch_size, rec.n - (long long)b * batch_size);
+            for (int m = 0; m < n_mat; ++m) {
+                double v = rec.h_edep[(size_t)b * n_mat + m];
+                if (edep) edep[m] += v;
+                if (edep_sum2 && stats) edep_sum2[m] += v * v / (double)nb;
+            }
+        }
+        for (int k = 0; k < 6; ++k) tot[k] += rec.h_cnt[k];
+        return frc;
+    };
+    auto drain = [&](int from) -> int {
+        int first_err = CC_OK;
+        for (int i = 0; i < cc_ctx::LAUNCH_RING; ++i) {
+            cc_ctx::LaunchRec& r = c->ring[(from + i) % cc_ctx::LAUNCH_RING];
+            if (!r.busy) continue;
+            const int frc = finish(r);
+            if (first_err == CC_OK) first_err = frc;
+        }
+        return first_err;
+    };
+    CC_CUDA(cudaEventRecord(c->ev0, c->stream));
+    long long li = 0;
     while (done < n_hist) {
         int ns = slots;
         long long n_launch = std::min<long long>(n_hist - done, (long long)ns * batch_size);
@@ -2410,44 +2589,37 @@ int cc_run(cc_ctx* c, const cc_scene* scene, const cc_tables* tables, const cc_s
         R.fluorescence = fluorescence;
         R.seed = seed;
         double* tally = grid ? grid->d_scratch : nullptr;
-        std::vector<double> slot_edep;
-        unsigned long long cnt[6];
-        CC_CUDA(cudaEventRecord(c->ev0, c->stream));
-        float kms = 0.f;
-        int rc = run_launch(c, scene, tables, &src->k, grid, tally, slotted ? ns : 1,
-                            slotted ? batch_size : std::max<long long>(n_launch, 1), R, slot_edep, cnt, &kms, cell32);
-        if (rc != CC_OK) return rc;
+        const int ri = (int)(li % cc_ctx::LAUNCH_RING);
+        cc_ctx::LaunchRec& rec = c->ring[ri];
+        if (rec.busy) {
+            rc = finish(rec);
+            if (rc != CC_OK) { drain(ri + 1); return rc; }
+        }
+        rc = enqueue_launch(c, scene, tables, &src->k, grid, tally, slotted ? ns : 1,
+                            slotted ? batch_size : std::max<long long>(n_launch, 1), R, cell32, rec);
+        if (rc != CC_OK) { drain(ri + 1); cudaStreamSynchronize(c->stream); return rc; }
+        rec.n = n_launch;     // rec.ns: its batches (one slot for all histories without a grid)
+        ++li;
         ++launches;
         ++transport_launches;
-        ms_transport += kms;
-        // per-batch collision-estimator moments (ScalarMoments.add_batch, tally.py:204-213)
-        for (int b = 0; b < ns; ++b) {
-            long long nb = std::min<long long>(batch_size, n_launch - (long long)b * batch_size);
-            for (int m = 0; m < n_mat; ++m) {
-                double v = slotted ? slot_edep[(size_t)b * n_mat + m] : (b == 0 ? slot_edep[m] : 0.0);
-                if (edep) edep[m] += v;
-                if (edep_sum2 && stats) edep_sum2[m] += v * v / (double)nb;
-            }
-        }
         if (stats) {
             std::vector<long long> counts(ns);
             for (int b = 0; b < ns; ++b) counts[b] = std::min<long long>(batch_size, n_launch - (long long)b * batch_size);
             rc = fold_batches(grid, ns, counts.data(), cell32);
-            if (rc != CC_OK) return rc;
-            launches += ns;
+            if (rc != CC_OK) { drain(ri + 1); return rc; }
+            launches += ns > 1 ? 1 : ns;
         } else if (grid) {
             rc = fold_plain(grid, ns, cell32);
-            if (rc != CC_OK) return rc;
-            launches += ns;
+            if (rc != CC_OK) { drain(ri + 1); return rc; }
+            launches += ns > 1 ? 1 : ns;
         }
-        CC_CUDA(cudaEventRecord(c->ev1, c->stream));
-        CC_CUDA(cudaEventSynchronize(c->ev1));
-        float ms = 0.f;
-        cudaEventElapsedTime(&ms, c->ev0, c->ev1);
-        ms_total += ms;
-        for (int k = 0; k < 6; ++k) tot[k] += cnt[k];
         done += n_launch;
     }
+    CC_CUDA(cudaEventRecord(c->ev1, c->stream));
+    rc = drain((int)(li % cc_ctx::LAUNCH_RING));
+    CC_CUDA(cudaEventSynchronize(c->ev1));
+    cudaEventElapsedTime(&ms_total, c->ev0, c->ev1);
+    if (rc != CC_OK) return rc;
     if (out) {
         out->n_histories = n_hist;
         out->n_absorbed = (int64_t)tot[0];
@@ -2737,6 +2909,19 @@ int cc_batch_create(cc_ctx* c, const cc_tables* tables, int32_t n_scenes, const 
             cc_grid* g = grids[i];
             const int cell32 = hg[i].tally32;
             int nb = std::max(1, std::min((int)((g->k.nvox + threads - 1) / threads), c->sm_count * 8));
+            if (slots > 1) {
+                // all batch slots of the scene in one fold
+                FoldSlots F;
+                memset(&F, 0, sizeof(F));
+                F.n = slots;
+                for (int sl = 0; sl < slots; ++sl)
+                    if (b->slot_counts[i][sl] > 0) F.inv_nb[sl] = 1.0 / (double)b->slot_counts[i][sl];
+                fold_slots_kernel<<<nb, threads, 0, st>>>((double2*)g->d_total, (double2*)g->d_q, g->d_nhit,
+                                                          (double2*)g->d_scratch, g->k.nvox, F, cell32);
+                ++b->launches;
+                e = cudaGetLastError();
+                continue;
+            }
             for (int sl = 0; sl < slots; ++sl) {
                 long long cnt = b->slot_counts[i][sl];
                 if (cnt <= 0) continue;
