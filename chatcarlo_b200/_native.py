@@ -34,7 +34,7 @@ CC_FIELD_RECT, CC_FIELD_CONE, CC_FIELD_PARALLEL = 0, 1, 2
 # every symbol the header declares
 EXPORTED = [
     "cc_version", "cc_last_error", "cc_ctx_create", "cc_ctx_destroy", "cc_ctx_set_launch",
-    "cc_ctx_set_step_limit", "cc_ctx_set_tally_fp32", "cc_tables_create", "cc_tables_destroy", "cc_scene_create",
+    "cc_ctx_set_step_limit", "cc_ctx_set_tally_fp32", "cc_ctx_set_tally_queue", "cc_tables_create", "cc_tables_destroy", "cc_scene_create",
     "cc_scene_destroy", "cc_source_create", "cc_source_destroy", "cc_grid_create",
     "cc_grid_destroy", "cc_grid_reset", "cc_grid_download", "cc_grid_end_batch", "cc_grid_maps", "cc_grid_upload",
     "cc_transport_photons", "cc_transport_photons_device", "cc_run", "cc_sample_source",
@@ -111,6 +111,7 @@ def _bind(lib):
         "cc_ctx_set_launch": (C.c_int, [P, C.c_int, C.c_int]),
         "cc_ctx_set_step_limit": (C.c_int, [P, C.c_int64]),
         "cc_ctx_set_tally_fp32": (C.c_int, [P, C.c_int32]),
+        "cc_ctx_set_tally_queue": (C.c_int, [P, C.c_int32, C.c_int64]),
         "cc_tables_create": (C.c_int, [P, C.POINTER(TableDesc), C.POINTER(P)]),
         "cc_tables_destroy": (C.c_int, [P]),
         "cc_scene_create": (C.c_int, [P, C.POINTER(Primitive), C.c_int32, C.c_int32, PD, PD, C.POINTER(P)]),

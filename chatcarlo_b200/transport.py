@@ -204,6 +204,12 @@ class Engine:
         FP32 additions) instead of the default FP64 cells."""
         N.check(self.lib.cc_ctx_set_tally_fp32(self.ctx, int(bool(on))), self.lib)
 
+    def set_tally_queue(self, on: bool = True, capacity: int = 0) -> None:
+        """Deferred tally: segments queued in device memory and scored by a
+        second kernel (same scores; slower on B200, off by default).
+        ``capacity`` > 0 fixes the queue size in records."""
+        N.check(self.lib.cc_ctx_set_tally_queue(self.ctx, int(bool(on)), int(capacity)), self.lib)
+
     def set_step_limit(self, max_steps: int = 100_000) -> None:
         """Transport steps a single photon may take before the run fails with CC_E_TIMEOUT."""
         N.check(self.lib.cc_ctx_set_step_limit(self.ctx, int(max_steps)))

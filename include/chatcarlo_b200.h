@@ -174,6 +174,15 @@ int cc_ctx_set_step_limit(cc_ctx* ctx, int64_t max_steps_per_photon);
  * in the busiest voxels of a monoenergetic pencil beam). */
 int cc_ctx_set_tally_fp32(cc_ctx* ctx, int32_t on);
 
+/* Deferred tally (no reference counterpart): with on = 1 the transport
+ * kernel queues its in-grid track segments in device memory and a second
+ * kernel scores them; the scores are the same as the default in-kernel
+ * tally's up to the order of the additions.  Off by default: slower on B200,
+ * whose tally is bound by its atomics.  capacity > 0 fixes the queue's size in
+ * records (segments beyond it are scored in the transport kernel); 0 sizes it
+ * from the launch. */
+int cc_ctx_set_tally_queue(cc_ctx* ctx, int32_t on, int64_t capacity);
+
 /* -- tables, scene, source, grid -------------------------------------------- */
 int cc_tables_create(cc_ctx* ctx, const cc_table_desc* desc, cc_tables** out);
 int cc_tables_destroy(cc_tables* t);

@@ -230,6 +230,40 @@ def test_reproducible_and_launch_shape_independent(engine):
     assert abs(k32.sum() - k64.sum()) / k64.sum() < 2e-4
 
 
+def test_deferred_tally_scores_the_same_pieces(engine):
+    """The deferred tally (segments queued, scored by a second kernel) and
+    its overflow path (a 1,000-record queue: the rest scored in place) give
+    the in-kernel tally's kerma and H*(10) up to the order of the FP64
+    additions, through transport_photons and through run_transport with
+    batch statistics."""
+    from chatcarlo_b200.transport import run_transport
+    d = np.array([1.0, 0.05, 0.02])
+    d /= np.linalg.norm(d)
+    spec = {"origin": (-60.0, -50.0, -45.0), "shape": (60, 50, 45), "voxel_cm": 2.0}
+    tp, runs = [], []
+    try:
+        for on, cap in ((False, 0), (True, 0), (True, 1000)):
+            engine.set_tally_queue(on, cap)
+            g = W.make_grid(spec, track_uncertainty=False)
+            _, _, _, r = _gpu_tp(engine, MIXED, [-55.0, 1.0, 2.0], d, 80.0, 200_000, seed=99, grid=g)
+            tp.append((g.kerma_keV.copy(), g.h10_track_pSv_cm3.copy()))
+            gr = W.make_grid(W.ROOM_GRID, track_uncertainty=True)
+            res = run_transport(W.room(), n_histories=600_000, seed=4, batch_size=100_000, dose_grid=True, grid=gr,
+                                engine=engine)
+            runs.append((gr, res))
+    finally:
+        engine.set_tally_queue(False, 0)
+    for k, h in tp[1:]:
+        np.testing.assert_allclose(k, tp[0][0], rtol=1e-9, atol=1e-12)
+        np.testing.assert_allclose(h, tp[0][1], rtol=1e-9, atol=1e-12)
+    g0, r0 = runs[0]
+    for g, r in runs[1:]:
+        assert r.n_voxel_visits == r0.n_voxel_visits and r.n_steps == r0.n_steps
+        for a in ("kerma_keV", "h10_track_pSv_cm3", "kerma_sum2", "h10_sum2"):
+            np.testing.assert_allclose(getattr(g, a), getattr(g0, a), rtol=1e-9, atol=1e-12)
+        np.testing.assert_array_equal(g.n_batches_hit, g0.n_batches_hit)
+
+
 def test_source_sampling_matches_oracle(engine):
     """Device source sampling vs source.py distributions (rect with rotation
     and helical shift): means and spreads of positions/directions."""
