@@ -85,9 +85,11 @@ def median_rel_error(k: np.ndarray, k_ref: np.ndarray, mask: np.ndarray) -> floa
 class Dataset:
     """Normalised log maps of a set of phantoms.  ``k_in`` is one array
     [n, S, S, S] or a list of them (input maps at several history counts,
-    one of which a training sample draws at random)."""
+    one of which a training sample draws at random).  ``scale`` [levels, n]
+    overrides the per-sample kerma scales (crops of a larger volume take
+    that volume's)."""
 
-    def __init__(self, k_in, k_tgt, mat, dens, rel=None):
+    def __init__(self, k_in, k_tgt, mat, dens, rel=None, scale=None):
         levels = k_in if isinstance(k_in, (list, tuple)) else [k_in]
         rels = rel if isinstance(rel, (list, tuple)) else ([rel] if rel is not None else None)
         self.unc = None if rels is None else [DN.uncertainty_channel(r) for r in rels]
@@ -96,7 +98,8 @@ class Dataset:
         self.mat = mat
         self.dens = dens
         inside = inside_mask(mat)
-        self.scale = np.array([[DN.kerma_scale(k[i], inside[i]) for i in range(self.n)] for k in levels])
+        self.scale = (np.asarray(scale, dtype=float).reshape(len(levels), self.n) if scale is not None else
+                      np.array([[DN.kerma_scale(k[i], inside[i]) for i in range(self.n)] for k in levels]))
         self.xs = [np.stack([DN.to_log(k[i], self.scale[j, i]) for i in range(self.n)]) for j, k in enumerate(levels)]
         self.x = self.xs[0]
         self.t = None if k_tgt is None else [

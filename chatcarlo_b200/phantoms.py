@@ -60,17 +60,18 @@ def phantoms(n: int, seed: int, side: int = 64, voxel_cm: float = 0.5):
     return [s for s, _ in out], [g for _, g in out]
 
 
-def voxel_maps(scene: dict, grid: dict) -> tuple[np.ndarray, np.ndarray]:
-    """(material index uint8, density float32) at the voxel centres, shaped
-    (nx, ny, nz) like the kerma grid."""
+def voxel_maps(scene: dict, grid: dict, materials: list[str] | None = None) -> tuple[np.ndarray, np.ndarray]:
+    """(material index uint8 into ``materials``, default MATERIALS; density
+    float32) at the voxel centres, shaped (nx, ny, nz) like the kerma grid."""
+    mats = MATERIALS if materials is None else materials
     nx, ny, nz = grid["shape"]
     h = grid["voxel_cm"]
     o = np.asarray(grid["origin"], dtype=float)
     ix, iy, iz = np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij")
     pts = np.stack([o[0] + (ix + 0.5) * h, o[1] + (iy + 0.5) * h, o[2] + (iz + 0.5) * h], axis=-1).reshape(-1, 3)
-    idx = np.full(pts.shape[0], MATERIALS.index(Geometry(scene["geometry"]).background), dtype=np.uint8)
+    idx = np.full(pts.shape[0], mats.index(Geometry(scene["geometry"]).background), dtype=np.uint8)
     for g in scene["geometry"]:                      # later primitives win (geometry.py:205-212)
-        idx[contains(g, pts)] = MATERIALS.index(g["material"])
+        idx[contains(g, pts)] = mats.index(g["material"])
     idx = idx.reshape(nx, ny, nz)
-    dens = np.array([tb.density(m) for m in MATERIALS], dtype=np.float32)[idx]
+    dens = np.array([tb.density(m) for m in mats], dtype=np.float32)[idx]
     return idx, dens

@@ -278,3 +278,36 @@ def test_shipped_denoiser_parameters_load():
         DN.save_params(os.path.join(d, "p.npz"), p, meta)
         q, m2 = DN.load_params(os.path.join(d, "p.npz"))
     np.testing.assert_array_equal(p, q)
+
+
+@pytest.mark.parametrize("n", [64, 65, 150, 320, 111])
+def test_ct_denoiser_tiles_cover_each_voxel_once_from_inside_a_tile(n):
+    """Tiled inference of the CT denoiser: the tiles cover the axis, the
+    owned ranges partition it, and every owned range lies in its tile at
+    least 8 voxels from an inner tile edge."""
+    from chatcarlo_b200.ct_denoise import TILE, owned_bounds, tile_starts
+    s = tile_starts(n)
+    b = owned_bounds(s, n)
+    assert s[0] == 0 and s[-1] == n - TILE and all(0 < s[i + 1] - s[i] <= 48 for i in range(len(s) - 1))
+    assert b[0] == 0 and b[-1] == n and all(b[i] < b[i + 1] for i in range(len(b) - 1))
+    for i, st in enumerate(s):
+        assert st <= b[i] and b[i + 1] <= st + TILE
+        if i > 0:
+            assert b[i] - st >= 8
+        if i < len(s) - 1:
+            assert st + TILE - b[i + 1] >= 8
+
+
+def test_ct_phantoms_are_valid_scenes():
+    from chatcarlo_b200.ct_denoise import CT_MATERIALS, ct_phantom
+    from chatcarlo_b200.scene import validate_scene
+    rng = np.random.default_rng(3)
+    for _ in range(20):
+        sc = ct_phantom(rng)
+        rep = validate_scene(sc)
+        assert rep.ok, rep.errors
+        assert all(g["material"] in CT_MATERIALS for g in sc["geometry"])
+        body = sc["geometry"][0]
+        for g in sc["geometry"][1:]:
+            assert np.hypot(*g["center"][:2]) + g["radius_cm"] <= body["radius_cm"]
+            assert abs(g["center"][2]) + g["height_cm"] / 2 <= 7.5 + 1e-9
