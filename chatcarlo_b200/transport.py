@@ -326,9 +326,11 @@ def transport_photons(pos: np.ndarray, dirv: np.ndarray, energy: np.ndarray, geo
         p = np.ascontiguousarray(pos, dtype=np.float64)
         d = np.ascontiguousarray(dirv, dtype=np.float64)
         e = np.ascontiguousarray(energy, dtype=np.float64)
-        nsc = np.zeros(n, dtype=np.int32)
-        absd = np.zeros(n, dtype=np.uint8)
-        esc = np.zeros(n, dtype=np.uint8)
+        # the device writes every element: no zero fill; the flags land
+        # directly in bool arrays (one byte, 0 or 1)
+        nsc = np.empty(n, dtype=np.int32)
+        absd = np.empty(n, dtype=bool)
+        esc = np.empty(n, dtype=bool)
         edep = np.zeros(len(names))
         nfl = C.c_int64(0)
         dg = eng.device_grid(grid, stats=False) if grid is not None else None
@@ -348,7 +350,7 @@ def transport_photons(pos: np.ndarray, dirv: np.ndarray, energy: np.ndarray, geo
     if e is not energy:
         energy[...] = e
     dep = {name: float(edep[i]) for i, name in enumerate(names) if edep[i] != 0.0}
-    return BatchResult(n_scatter=nsc.astype(int), absorbed=absd.astype(bool), escaped=esc.astype(bool),
+    return BatchResult(n_scatter=nsc.astype(np.int64), absorbed=absd, escaped=esc,
                        final_energy=energy, energy_deposited=dep, n_fluorescence=int(nfl.value))
 
 
