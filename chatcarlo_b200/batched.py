@@ -157,3 +157,41 @@ def autotune(scenes, grid_specs, n_histories, slots=1, engine=None, scale=0.02,
     except OSError:
         pass
     return shape
+
+
+def main(argv=None) -> None:
+    """``python -m chatcarlo_b200.batched``: the batched configuration (256
+    random scenes, log-uniform 1e5-1e7 histories each, 64^3 tally grids) in
+    one launch, after the autotuner picked its shape; one JSON line."""
+    import argparse
+    from . import workloads as W
+    ap = argparse.ArgumentParser(description=main.__doc__.split("\n")[0])
+    ap.add_argument("--scenes", type=int, default=256)
+    ap.add_argument("--seed", type=int, default=2026)
+    ap.add_argument("--repeats", type=int, default=3)
+    args = ap.parse_args(argv)
+    eng = default_engine()
+    scenes, specs, counts = W.batched_scenes(n_scenes=args.scenes, seed=args.seed)
+    t0 = time.perf_counter()
+    shape = autotune(scenes, specs, counts, engine=eng, use_cache=False)
+    t_tune = time.perf_counter() - t0
+    br = BatchedRun(scenes, specs, counts, engine=eng, shape=shape)
+    try:
+        br.run(seed=1)
+        outs = []
+        for i in range(args.repeats):
+            br.reset()
+            outs.append(br.run(seed=2 + i)[1])
+    finally:
+        br.close()
+    ms = float(np.median([o.elapsed_ms for o in outs]))
+    total = int(sum(counts))
+    o = outs[-1]
+    print(json.dumps({"workload": f"{args.scenes} random scenes, 1e5-1e7 histories each, 64^3 grids",
+                      "histories": total, "launch_ms": ms, "histories_per_s": total / (ms * 1e-3),
+                      "segments_per_history": o.n_steps / total, "voxel_visits_per_history": o.n_voxel_visits / total,
+                      "shape": shape, "autotune_s": t_tune, "gpu_launches_per_replay": int(o.gpu_launches)}))
+
+
+if __name__ == "__main__":
+    main()
