@@ -551,7 +551,11 @@ def main():
                              "bytes_per_history": b_hist, "segments_per_history": n_seg,
                              "voxel_visits_per_history": n_vox,
                              "avg_launch_ms": tr_ms / max(tr_launch, 1),
-                             "histories_per_launch": hist_per_launch},
+                             "histories_per_launch": hist_per_launch,
+                             # the tally's atomic bound: two FP64 reductions (kerma, H*(10)) per voxel visit
+                             "atomics": {"per_history": 2.0 * n_vox,
+                                         "achieved_per_s": 2.0 * n_vox * n_h / (tr_ms / 1e3),
+                                         "cells": "fp64"}},
                 "cpu_baseline": cpu, "e2e": e2e, "e2e_photons": e2e_photons, "precision": precision,
                 "denoiser": denoise, "denoiser_ct": ct_denoise, "tally_fp32_cells": fp32_cells,
                 "clocks": clocks,
