@@ -1,4 +1,4 @@
-"""Train and judge the kerma denoiser on the engine's own Monte Carlo.
+"""Train and score the kerma denoiser on the engine's own Monte Carlo.
 
 ``python -m chatcarlo_b200.denoise_run`` runs the whole learned-denoiser
 workload on one GPU and prints one JSON line:

@@ -10,8 +10,8 @@ mean input kerma per history inside the phantom,
 
 and is trained on ln(k_target / s + EPS) with a squared error weighted
 towards the phantom's voxels.  Plain Monte Carlo stays the fallback and
-the judge: the denoised map is only ever scored against a high-history
-Monte Carlo map.
+the measure of its error: the denoised map is only ever scored against a
+high-history Monte Carlo map.
 
 Architecture: 4 levels with 16, 32, 64 and 128 channels; two 3x3x3 ReLU
 convolutions per level; 2x2x2 average pooling down; nearest upsampling up,

@@ -1,4 +1,4 @@
-"""History sharding over ranks and the one tally exchange (SURVEY 8e).
+"""History sharding over ranks and the one tally exchange.
 
 Histories are independent: rank r of W simulates its own contiguous range
 of history indices (disjoint Philox counters, so no two ranks share a

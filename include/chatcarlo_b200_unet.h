@@ -1,8 +1,8 @@
 /* C ABI of the learned kerma denoiser's kernels (libccunet.so).
  *
  * The reference has no learned part; these entry points implement the 3D
- * U-Net denoiser that the engine's own Monte Carlo trains and that plain
- * Monte Carlo judges.  Tensors are device pointers (16-byte aligned),
+ * U-Net denoiser that the engine's own Monte Carlo trains and against which
+ * plain Monte Carlo measures the error.  Tensors are device pointers (16-byte aligned),
  * channels-last BF16 [B, D, H, W, C] activations with C a multiple of 16,
  * FP32 master weights and gradients.  Every call is asynchronous on the
  * given CUDA stream (NULL = legacy default stream) and returns 0 or a

@@ -2,7 +2,7 @@
 
 The engine draws Philox streams, the oracle NumPy's PCG64, so results are
 compared as estimates with their statistical errors: differences are
-judged in units of the combined standard error (|z| < 4 per quantity, a
+measured in units of the combined standard error (|z| < 4 per quantity, a
 chi^2 per degree of freedom <= 1.2 for voxel maps).
 """
 import numpy as np
