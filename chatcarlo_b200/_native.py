@@ -126,7 +126,7 @@ def _bind(lib):
         "cc_grid_upload": (C.c_int, [P, PD, PD, PD, PD, C.POINTER(C.c_int32), C.c_int64, C.c_int64]),
         "cc_grid_maps": (C.c_int, [P, C.POINTER(Primitive), C.c_int32, PD, C.c_double, C.c_double, C.c_double, C.c_int32, P, P, P, P]),
         "cc_transport_photons": (C.c_int, [P, P, P, P, C.c_int64, PD, PD, PD, C.c_uint64, C.c_uint64, C.c_int32,
-                                           C.POINTER(C.c_int32), C.POINTER(C.c_uint8), C.POINTER(C.c_uint8), PD,
+                                           C.POINTER(C.c_int64), C.POINTER(C.c_uint8), C.POINTER(C.c_uint8), PD,
                                            C.POINTER(C.c_int64)]),
         "cc_transport_photons_device": (C.c_int, [P, P, P, P, C.c_int64, P, P, P, C.c_uint64, C.c_uint64, C.c_int32,
                                                   P, P, P, PD, C.POINTER(C.c_int64)]),

@@ -2608,9 +2608,15 @@ int cc_transport_photons_device(cc_ctx* c, const cc_scene* scene, const cc_table
                             fluorescence, d_nsc, d_abs, d_esc, edep, n_fluor);
 }
 
+// Interaction counts widened to int64 for the host (the reference's dtype).
+__global__ void widen_kernel(const int32_t* __restrict__ in, int64_t* __restrict__ out, long long n) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        out[i] = in[i];
+}
+
 int cc_transport_photons(cc_ctx* c, const cc_scene* scene, const cc_tables* tables, cc_grid* grid,
                          int64_t n, double* pos, double* dir, double* energy, uint64_t seed,
-                         uint64_t stream_offset, int32_t fluorescence, int32_t* n_scatter,
+                         uint64_t stream_offset, int32_t fluorescence, int64_t* n_scatter,
                          uint8_t* absorbed, uint8_t* escaped, double* edep, int64_t* n_fluor) {
     if (!c || !scene || !tables) return set_error(CC_E_INVALID, "NULL argument");
     if (n < 0) return set_error(CC_E_INVALID, "n < 0");
@@ -2619,7 +2625,7 @@ int cc_transport_photons(cc_ctx* c, const cc_scene* scene, const cc_tables* tabl
     CC_CUDA(cudaSetDevice(c->device));
     cudaStream_t st = c->stream;
     size_t b3 = (size_t)n * 3 * sizeof(double), b1 = (size_t)n * sizeof(double);
-    size_t total = 2 * b3 + b1 + (size_t)n * (sizeof(int32_t) + 2);
+    size_t total = 2 * b3 + b1 + (size_t)n * (sizeof(int64_t) + sizeof(int32_t) + 2);
     if (total > c->io_bytes) {
         cudaFree(c->d_io);
         c->d_io = nullptr;
@@ -2631,7 +2637,8 @@ int cc_transport_photons(cc_ctx* c, const cc_scene* scene, const cc_tables* tabl
     double* d_pos = (double*)buf;
     double* d_dir = (double*)(buf + b3);
     double* d_en = (double*)(buf + 2 * b3);
-    int32_t* d_nsc = (int32_t*)(buf + 2 * b3 + b1);
+    int64_t* d_nsc64 = (int64_t*)(buf + 2 * b3 + b1);
+    int32_t* d_nsc = (int32_t*)(d_nsc64 + n);
     uint8_t* d_abs = (uint8_t*)(d_nsc + n);
     uint8_t* d_esc = d_abs + n;
     cudaError_t e = cudaMemcpyAsync(d_pos, pos, b3, cudaMemcpyHostToDevice, st);
@@ -2645,7 +2652,12 @@ int cc_transport_photons(cc_ctx* c, const cc_scene* scene, const cc_tables* tabl
         e = cudaMemcpyAsync(pos, d_pos, b3, cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess) e = cudaMemcpyAsync(dir, d_dir, b3, cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess) e = cudaMemcpyAsync(energy, d_en, b1, cudaMemcpyDeviceToHost, st);
-        if (e == cudaSuccess && n_scatter) e = cudaMemcpyAsync(n_scatter, d_nsc, (size_t)n * sizeof(int32_t), cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess && n_scatter) {
+            const int blocks = (int)std::max<long long>(1, std::min<long long>((n + 255) / 256, (long long)c->sm_count * 8));
+            widen_kernel<<<blocks, 256, 0, st>>>(d_nsc, d_nsc64, n);
+            e = cudaGetLastError();
+            if (e == cudaSuccess) e = cudaMemcpyAsync(n_scatter, d_nsc64, (size_t)n * sizeof(int64_t), cudaMemcpyDeviceToHost, st);
+        }
         if (e == cudaSuccess && absorbed) e = cudaMemcpyAsync(absorbed, d_abs, (size_t)n, cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess && escaped) e = cudaMemcpyAsync(escaped, d_esc, (size_t)n, cudaMemcpyDeviceToHost, st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);

@@ -328,7 +328,7 @@ def transport_photons(pos: np.ndarray, dirv: np.ndarray, energy: np.ndarray, geo
         e = np.ascontiguousarray(energy, dtype=np.float64)
         # the device writes every element: no zero fill; the flags land
         # directly in bool arrays (one byte, 0 or 1)
-        nsc = np.empty(n, dtype=np.int32)
+        nsc = np.empty(n, dtype=np.int64)
         absd = np.empty(n, dtype=bool)
         esc = np.empty(n, dtype=bool)
         edep = np.zeros(len(names))
@@ -337,7 +337,7 @@ def transport_photons(pos: np.ndarray, dirv: np.ndarray, energy: np.ndarray, geo
         N.check(eng.lib.cc_transport_photons(
             eng.ctx, sh, th, dg.handle if dg else None, n, N.dptr(p), N.dptr(d), N.dptr(e),
             _seed_from(rng, seed), int(stream_offset), int(bool(fluorescence_enabled)),
-            nsc.ctypes.data_as(C.POINTER(C.c_int32)), absd.ctypes.data_as(C.POINTER(C.c_uint8)),
+            nsc.ctypes.data_as(C.POINTER(C.c_int64)), absd.ctypes.data_as(C.POINTER(C.c_uint8)),
             esc.ctypes.data_as(C.POINTER(C.c_uint8)), N.dptr(edep), C.byref(nfl)))
         if dg is not None:
             dg.download(grid, accumulate=True)
@@ -350,7 +350,7 @@ def transport_photons(pos: np.ndarray, dirv: np.ndarray, energy: np.ndarray, geo
     if e is not energy:
         energy[...] = e
     dep = {name: float(edep[i]) for i, name in enumerate(names) if edep[i] != 0.0}
-    return BatchResult(n_scatter=nsc.astype(np.int64), absorbed=absd, escaped=esc,
+    return BatchResult(n_scatter=nsc, absorbed=absd, escaped=esc,
                        final_energy=energy, energy_deposited=dep, n_fluorescence=int(nfl.value))
 
 

@@ -242,11 +242,12 @@ int cc_grid_end_batch(cc_grid* g, int64_t n_histories_in_batch);
  * final state like the NumPy path does.  grid may be NULL.  Per-photon
  * outputs may be NULL.  edep_by_material has n_materials entries (keV),
  * accumulated into (not overwritten).  The photons' random streams are
- * Philox4x32-10 keyed by seed, counter (history index + stream_offset). */
+ * Philox4x32-10 keyed by seed, counter (history index + stream_offset).
+ * n_scatter is int64 like the reference's BatchResult.n_scatter. */
 int cc_transport_photons(cc_ctx* ctx, const cc_scene* scene, const cc_tables* tables,
                          cc_grid* grid, int64_t n, double* pos, double* dir, double* energy,
                          uint64_t seed, uint64_t stream_offset, int32_t fluorescence,
-                         int32_t* n_scatter, uint8_t* absorbed, uint8_t* escaped,
+                         int64_t* n_scatter, uint8_t* absorbed, uint8_t* escaped,
                          double* edep_by_material, int64_t* n_fluorescence);
 
 /* Same on device-resident arrays (pointers into this device's memory). */

@@ -217,6 +217,8 @@ def test_reproducible_and_launch_shape_independent(engine):
         kerma.append(g.kerma_keV.copy())
     engine.set_launch(256, 0)
     engine.set_tally_fp32(False)
+    # BatchResult's types as in the reference (transport.py:86-93)
+    assert out[0][3].dtype == np.int64 and out[0][4].dtype == bool and out[0][5].dtype == bool
     for other, k in zip(out[1:], kerma[1:4]):
         for a, b in zip(out[0], other):
             np.testing.assert_array_equal(a, b)
