@@ -1698,6 +1698,9 @@ struct cc_ctx {
     double seg_per_history = 8.0;
     int tally_queue = 0;                         // cc_ctx_set_tally_queue
     long long tally_queue_cap = 0;               // fixed capacity (records), 0 = automatic
+    // copy streams and events of cc_transport_photons' chunked pipeline
+    cudaStream_t s_in = nullptr, s_out = nullptr;
+    cudaEvent_t ev_in[LAUNCH_RING] = {}, ev_k[LAUNCH_RING] = {};
 };
 
 struct cc_tables {
@@ -1799,6 +1802,12 @@ int cc_ctx_destroy(cc_ctx* c) {
     }
     cudaFreeHost(c->h_ring);
     cudaFree(c->d_seg);
+    for (int i = 0; i < cc_ctx::LAUNCH_RING; ++i) {
+        if (c->ev_in[i]) cudaEventDestroy(c->ev_in[i]);
+        if (c->ev_k[i]) cudaEventDestroy(c->ev_k[i]);
+    }
+    if (c->s_in) cudaStreamDestroy(c->s_in);
+    if (c->s_out) cudaStreamDestroy(c->s_out);
     cudaEventDestroy(c->ev0);
     cudaEventDestroy(c->ev1);
     cudaEventDestroy(c->kev0);
@@ -2614,6 +2623,104 @@ __global__ void widen_kernel(const int32_t* __restrict__ in, int64_t* __restrict
         out[i] = in[i];
 }
 
+// Photon counts from which cc_transport_photons overlaps its copies with
+// the transport: the photons go in LAUNCH_RING chunks, each uploaded on one
+// copy stream, transported, and downloaded on another while the next chunk
+// runs.  Histories stay keyed by their index, so the results are those of
+// one launch over all photons.
+constexpr long long PIPE_MIN_PHOTONS = 1LL << 21;
+
+static int ensure_copy_streams(cc_ctx* c) {
+    if (c->s_in) return CC_OK;
+    cudaError_t e = cudaStreamCreateWithFlags(&c->s_in, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->s_out, cudaStreamNonBlocking);
+    for (int i = 0; i < cc_ctx::LAUNCH_RING && e == cudaSuccess; ++i) {
+        e = cudaEventCreateWithFlags(&c->ev_in[i], cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_k[i], cudaEventDisableTiming);
+    }
+    if (e != cudaSuccess) return set_error(CC_E_DEVICE, std::string("copy streams: ") + cudaGetErrorString(e));
+    return CC_OK;
+}
+
+static int transport_photons_chunked(cc_ctx* c, const cc_scene* scene, const cc_tables* tables, cc_grid* grid,
+                                     int64_t n, double* pos, double* dir, double* energy, uint64_t seed,
+                                     uint64_t stream_offset, int32_t fluorescence, int64_t* n_scatter,
+                                     uint8_t* absorbed, uint8_t* escaped, double* edep, int64_t* n_fluor,
+                                     double* d_pos, double* d_dir, double* d_en, int64_t* d_nsc64, int32_t* d_nsc,
+                                     uint8_t* d_abs, uint8_t* d_esc) {
+    int rc = ensure_ring(c);
+    if (rc == CC_OK) rc = ensure_copy_streams(c);
+    if (rc != CC_OK) return rc;
+    const int K = cc_ctx::LAUNCH_RING;
+    const long long per = (n + K - 1) / K;
+    cudaStream_t st = c->stream;
+    // as transport_common: a statistics grid's slot 0 is its pending batch,
+    // any other grid's slot 0 is folded after the call
+    double* tally = grid ? grid->d_scratch : nullptr;
+    const bool pending = grid && (grid->flags & CC_GRID_STATS);
+    const int cell32 = (grid && !pending) ? cell32_for(c, n) : 0;
+    cudaError_t e = cudaSuccess;
+    for (int i = 0; i < K && e == cudaSuccess; ++i) {
+        const long long a = std::min<long long>(n, i * per), m = std::min<long long>(n, a + per) - a;
+        if (m <= 0) break;
+        e = cudaMemcpyAsync(d_pos + 3 * a, pos + 3 * a, (size_t)m * 3 * sizeof(double), cudaMemcpyHostToDevice, c->s_in);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(d_dir + 3 * a, dir + 3 * a, (size_t)m * 3 * sizeof(double), cudaMemcpyHostToDevice, c->s_in);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(d_en + a, energy + a, (size_t)m * sizeof(double), cudaMemcpyHostToDevice, c->s_in);
+        if (e == cudaSuccess) e = cudaEventRecord(c->ev_in[i], c->s_in);
+    }
+    int used = 0;
+    for (int i = 0; i < K && e == cudaSuccess && rc == CC_OK; ++i) {
+        const long long a = std::min<long long>(n, i * per), m = std::min<long long>(n, a + per) - a;
+        if (m <= 0) break;
+        e = cudaStreamWaitEvent(st, c->ev_in[i], 0);
+        if (e != cudaSuccess) break;
+        KRun R;
+        memset(&R, 0, sizeof(R));
+        R.n = m;
+        R.first = (long long)stream_offset + a;
+        R.fluorescence = fluorescence;
+        R.seed = seed;
+        R.pos = d_pos + 3 * a; R.dir = d_dir + 3 * a; R.energy = d_en + a;
+        R.n_scatter = n_scatter ? d_nsc + a : nullptr;
+        R.absorbed = absorbed ? d_abs + a : nullptr;
+        R.escaped = escaped ? d_esc + a : nullptr;
+        rc = enqueue_launch(c, scene, tables, nullptr, grid, tally, 1, m, R, cell32, c->ring[i]);
+        if (rc != CC_OK) break;
+        c->ring[i].n = m;
+        ++used;
+        if (n_scatter) {
+            const int blocks = (int)std::max<long long>(1, std::min<long long>((m + 255) / 256, (long long)c->sm_count * 8));
+            widen_kernel<<<blocks, 256, 0, st>>>(d_nsc + a, d_nsc64 + a, m);
+            e = cudaGetLastError();
+        }
+        if (e == cudaSuccess) e = cudaEventRecord(c->ev_k[i], st);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(c->s_out, c->ev_k[i], 0);
+        cudaStream_t so = c->s_out;
+        if (e == cudaSuccess) e = cudaMemcpyAsync(pos + 3 * a, d_pos + 3 * a, (size_t)m * 3 * sizeof(double), cudaMemcpyDeviceToHost, so);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(dir + 3 * a, d_dir + 3 * a, (size_t)m * 3 * sizeof(double), cudaMemcpyDeviceToHost, so);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(energy + a, d_en + a, (size_t)m * sizeof(double), cudaMemcpyDeviceToHost, so);
+        if (e == cudaSuccess && n_scatter) e = cudaMemcpyAsync(n_scatter + a, d_nsc64 + a, (size_t)m * sizeof(int64_t), cudaMemcpyDeviceToHost, so);
+        if (e == cudaSuccess && absorbed) e = cudaMemcpyAsync(absorbed + a, d_abs + a, (size_t)m, cudaMemcpyDeviceToHost, so);
+        if (e == cudaSuccess && escaped) e = cudaMemcpyAsync(escaped + a, d_esc + a, (size_t)m, cudaMemcpyDeviceToHost, so);
+    }
+    if (e == cudaSuccess && rc == CC_OK && grid && !pending) rc = fold_plain(grid, 1, cell32);
+    // the chunks' reductions, in launch order
+    unsigned long long fl = 0;
+    for (int i = 0; i < used; ++i) {
+        const int frc = finish_launch(c, c->ring[i], nullptr);
+        if (rc == CC_OK) rc = frc;
+        if (edep) for (int m = 0; m < tables->n_mat; ++m) edep[m] += c->ring[i].h_edep[m];
+        fl += c->ring[i].h_cnt[3];
+    }
+    cudaError_t e2 = cudaStreamSynchronize(c->s_out);
+    cudaError_t e3 = cudaStreamSynchronize(st);
+    cudaError_t e4 = cudaStreamSynchronize(c->s_in);
+    if (e == cudaSuccess) e = e2 != cudaSuccess ? e2 : (e3 != cudaSuccess ? e3 : e4);
+    if (e != cudaSuccess) return set_error(CC_E_DEVICE, std::string("chunked transport: ") + cudaGetErrorString(e));
+    if (rc == CC_OK && n_fluor) *n_fluor = (int64_t)fl;
+    return rc;
+}
+
 int cc_transport_photons(cc_ctx* c, const cc_scene* scene, const cc_tables* tables, cc_grid* grid,
                          int64_t n, double* pos, double* dir, double* energy, uint64_t seed,
                          uint64_t stream_offset, int32_t fluorescence, int64_t* n_scatter,
@@ -2641,6 +2748,10 @@ int cc_transport_photons(cc_ctx* c, const cc_scene* scene, const cc_tables* tabl
     int32_t* d_nsc = (int32_t*)(d_nsc64 + n);
     uint8_t* d_abs = (uint8_t*)(d_nsc + n);
     uint8_t* d_esc = d_abs + n;
+    if (n >= PIPE_MIN_PHOTONS)
+        return transport_photons_chunked(c, scene, tables, grid, n, pos, dir, energy, seed, stream_offset,
+                                         fluorescence, n_scatter, absorbed, escaped, edep, n_fluor, d_pos, d_dir,
+                                         d_en, d_nsc64, d_nsc, d_abs, d_esc);
     cudaError_t e = cudaMemcpyAsync(d_pos, pos, b3, cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(d_dir, dir, b3, cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(d_en, energy, b1, cudaMemcpyHostToDevice, st);

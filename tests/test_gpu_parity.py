@@ -378,3 +378,55 @@ def test_ellipsoid_transmission_and_oblique_rays(engine):
                          (rg.absorbed, ro.absorbed)):
         pg, po = np.mean(sel_g), np.mean(sel_o)
         assert abs(_z(pg, 400_000, po, 40_000)) < 4, (pg, po)
+
+
+def test_chunked_host_transport_equals_one_device_launch(engine):
+    """cc_transport_photons overlaps its copies with the transport from 2^21
+    photons on (three chunks on copy streams); per photon the results equal
+    one launch of cc_transport_photons_device over the same photons and
+    seed, and the kerma equals it up to the order of the FP64 additions."""
+    import ctypes as C
+    import torch
+    from chatcarlo_b200 import _native as N
+    from chatcarlo_b200.transport import DeviceGrid
+    n, seed = 2_500_000, 77
+    d = np.array([1.0, 0.05, 0.02])
+    d /= np.linalg.norm(d)
+    spec = {"origin": (-60.0, -50.0, -45.0), "shape": (60, 50, 45), "voxel_cm": 2.0}
+    g_host = W.make_grid(spec, track_uncertainty=False)
+    p, dv, e, r = _gpu_tp(engine, MIXED, [-55.0, 1.0, 2.0], d, 80.0, n, seed=seed, grid=g_host)
+    geom = Geometry(MIXED)
+    ts, th = engine.tables(geom.materials(), need_muen=True)
+    sh = engine.scene(geom, ts)
+    g_dev = W.make_grid(spec, track_uncertainty=False)
+    dg = DeviceGrid(engine, g_dev, stats=False)
+    try:
+        p0, d0, e0 = W.pencil_beam_arrays(n, [-55.0, 1.0, 2.0], d, 80.0)
+        tp, td, te = (torch.from_numpy(np.ascontiguousarray(a)).cuda() for a in (p0, d0, e0))
+        nsc = torch.zeros(n, dtype=torch.int32, device="cuda")
+        ab = torch.zeros(n, dtype=torch.uint8, device="cuda")
+        es = torch.zeros(n, dtype=torch.uint8, device="cuda")
+        edep = np.zeros(len(ts.names))
+        nfl = C.c_int64()
+        ptr = lambda t: C.c_void_p(t.data_ptr())  # noqa: E731
+        N.check(engine.lib.cc_transport_photons_device(engine.ctx, sh, th, dg.handle, n, ptr(tp), ptr(td), ptr(te),
+                                                       seed, 0, 1, ptr(nsc), ptr(ab), ptr(es), N.dptr(edep),
+                                                       C.byref(nfl)))
+        torch.cuda.synchronize()
+        dg.download(g_dev)
+        np.testing.assert_array_equal(p, tp.cpu().numpy())
+        np.testing.assert_array_equal(dv, td.cpu().numpy())
+        np.testing.assert_array_equal(e, te.cpu().numpy())
+        np.testing.assert_array_equal(r.n_scatter, nsc.cpu().numpy().astype(np.int64))
+        np.testing.assert_array_equal(r.absorbed, ab.cpu().numpy().astype(bool))
+        np.testing.assert_array_equal(r.escaped, es.cpu().numpy().astype(bool))
+        assert r.n_fluorescence == nfl.value
+        dep = {name: float(edep[i]) for i, name in enumerate(ts.names) if edep[i] != 0.0}
+        assert set(dep) == set(r.energy_deposited)
+        for k, v in dep.items():
+            assert r.energy_deposited[k] == pytest.approx(v, rel=1e-9)
+        np.testing.assert_allclose(g_host.kerma_keV, g_dev.kerma_keV, rtol=1e-9, atol=1e-12)
+        np.testing.assert_allclose(g_host.h10_track_pSv_cm3, g_dev.h10_track_pSv_cm3, rtol=1e-9, atol=1e-12)
+    finally:
+        dg.close()
+        engine.lib.cc_scene_destroy(sh)
