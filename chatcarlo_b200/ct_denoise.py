@@ -13,8 +13,9 @@ rotating fan beam.
    of those scans, every crop normalised by its scan's kerma scale;
 3. the CT configuration's own phantom (PMMA with five air holes, never
    seen in training): a high-history reference, plain runs at several
-   history counts, each denoised tile by tile (64^3 tiles, every voxel
-   taken from the tile it lies deepest in);
+   history counts, each denoised in one pass over the whole volume (or,
+   with --tiled, in 64^3 tiles, every voxel taken from the tile it lies
+   deepest in);
 4. the median relative voxel-kerma error inside the phantom of the plain
    and the denoised maps against the reference (its own noise removed in
    quadrature), and the time each needs to reach a 2 % median error.
@@ -85,14 +86,27 @@ def owned_bounds(starts: list[int], n: int, t: int = TILE) -> list[int]:
 
 
 def denoise_volume(model: DN.UNet3D, k: np.ndarray, rel: np.ndarray, mat: np.ndarray, dens: np.ndarray,
-                   batch: int = 8) -> tuple[np.ndarray, float]:
-    """Denoised kerma of a whole volume (each axis >= 64 voxels) tile by
-    tile, and the device time (ms)."""
+                   batch: int = 8, tiled: bool = False) -> tuple[np.ndarray, float]:
+    """Denoised kerma of a whole volume and the device time (ms): in one pass
+    over the volume (each axis padded to a multiple of 8 by repeating its
+    edge), or with ``tiled`` in overlapping 64^3 tiles (each axis >= 64)."""
     import torch
     inside = mat != 0
     scale = DN.kerma_scale(k, inside)
     x = DN.to_log(k, scale)
     unc = DN.uncertainty_channel(rel)
+    if not tiled:
+        pad = [(0, (-n) % 8) for n in k.shape]
+        xp, dp, mp, up = (np.pad(a, pad, mode="edge") for a in (x, dens, mat, unc))
+        model.set_input(xp[None], dp[None], mp[None], 1, xp.shape, unc=up[None])
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        y = model.predict()
+        e1.record()
+        e1.synchronize()
+        out = y.cpu().numpy().reshape(xp.shape)[:k.shape[0], :k.shape[1], :k.shape[2]]
+        model.check_status()
+        return DN.from_log(out, scale), e0.elapsed_time(e1)
     axes = [tile_starts(n) for n in k.shape]
     bounds = [owned_bounds(a, n) for a, n in zip(axes, k.shape)]
     tiles = [(i, j, l) for i in range(len(axes[0])) for j in range(len(axes[1])) for l in range(len(axes[2]))]
@@ -122,10 +136,10 @@ def denoise_volume(model: DN.UNet3D, k: np.ndarray, rel: np.ndarray, mat: np.nda
 
 def denoise_ct_kerma(k: np.ndarray, rel: np.ndarray, mat: np.ndarray, density: np.ndarray,
                      model: DN.UNet3D | None = None) -> np.ndarray:
-    """Denoised kerma of a CT-type volume (1 mm voxels, every axis >= 64
-    voxels) from a plain run and its batch statistics, with the CT network
-    that ships with the package unless a model is given.  mat indexes
-    CT_MATERIALS (air 0, pmma 1, water 2, bone 3)."""
+    """Denoised kerma of a CT-type volume (1 mm voxels, any shape) from a
+    plain run and its batch statistics, with the CT network that ships with
+    the package unless a model is given.  mat indexes CT_MATERIALS (air 0,
+    pmma 1, water 2, bone 3)."""
     model = model or DN.UNet3D(params=DN.load_params(CT_PRETRAINED)[0])
     return denoise_volume(model, np.asarray(k, dtype=np.float64), rel, mat, density)[0]
 
@@ -196,7 +210,7 @@ def _evaluate(args, eng, model, training, grid, t_all):
     levels = []
     for n in args.levels:
         k_n, rel_n, ms_n = scan(c5, n, 11 + n % 991, eng, grid)
-        k_dn, ms_dn = denoise_volume(model, k_n, rel_n, mat, dens)
+        k_dn, ms_dn = denoise_volume(model, k_n, rel_n, mat, dens, tiled=args.tiled)
         err = lambda k: float(np.median(np.abs(k[sel] - k_ref[sel]) / k_ref[sel]))  # noqa: E731
         dn_meas = err(k_dn)
         levels.append({"histories": n, "plain_measured": err(k_n),
@@ -240,6 +254,7 @@ def main(argv=None) -> None:
     ap.add_argument("--lr", type=float, default=2e-3)
     ap.add_argument("--seed", type=int, default=5)
     ap.add_argument("--save", default=None, help="write the trained parameters (.npy)")
+    ap.add_argument("--tiled", action="store_true", help="denoise in 64^3 tiles instead of one pass")
     ap.add_argument("--load", default=None,
                     help="evaluate a saved network (save_params file, e.g. the shipped denoiser_ct64.npz) "
                          "instead of training one")

@@ -146,34 +146,49 @@ class UNet3D:
     def params_numpy(self) -> np.ndarray:
         return self.p.detach().cpu().numpy()
 
-    def _alloc(self, B: int, S: int) -> None:
-        if self.shape == (B, S):
-            return
-        if S % 8:
-            raise ValueError("the volume side must be a multiple of 8 (three 2x2x2 poolings)")
-        torch = self.torch
-        bf = torch.bfloat16
+    @staticmethod
+    def _side3(S) -> tuple[int, int, int]:
+        """(D, H, W) of a volume given as one side or three."""
+        d = (int(S),) * 3 if np.isscalar(S) else tuple(int(x) for x in S)
+        if len(d) != 3 or any(x <= 0 or x % 8 for x in d):
+            raise ValueError("every volume side must be a positive multiple of 8 (three 2x2x2 poolings)")
+        return d
 
-        def t(level, c, dtype=bf):
-            return torch.empty(B * (S >> level) ** 3 * c, dtype=dtype, device=self.dev)
+    def _t(self, level: int, c: int, dtype=None):
+        B, D, H, W = self.shape
+        return self.torch.empty(B * (D >> level) * (H >> level) * (W >> level) * c,
+                                dtype=dtype or self.torch.bfloat16, device=self.dev)
+
+    def _alloc(self, B: int, S) -> None:
+        D, H, W = self._side3(S)
+        if self.shape == (B, D, H, W):
+            return
+        torch = self.torch
+        self.shape = (B, D, H, W)
+        t = self._t
         a = {"x0": t(0, IN_CH), "p0": t(1, 16), "p1": t(2, 32), "p2": t(3, 64)}
         for L in LAYERS:
             a[L.name] = t(L.level, L.cout)
+        self.a = a
+        self.gb = None                       # gradient buffers: allocated by the first backward pass
+        n0 = B * D * H * W
+        self.xlog = torch.empty(n0, dtype=torch.float32, device=self.dev)
+        self.out = torch.empty(n0, dtype=torch.float32, device=self.dev)
+
+    def _alloc_grads(self) -> None:
+        if self.gb is not None:
+            return
+        t = self._t
         g = {}
         for L in LAYERS:
             g["dz_" + L.name] = t(L.level, L.cout)
         g.update({"g_up1": t(0, 32), "g_up2": t(1, 64), "g_up3": t(2, 128),
                   "g_p0": t(1, 16), "g_p1": t(2, 32), "g_p2": t(3, 64)})
-        self.a, self.gb = a, g
-        n0 = B * S ** 3
-        self.xlog = torch.empty(n0, dtype=torch.float32, device=self.dev)
-        self.out = torch.empty(n0, dtype=torch.float32, device=self.dev)
-        self.shape = (B, S)
+        self.gb = g
 
     def _dims(self, level: int):
-        B, S = self.shape
-        s = S >> level
-        return B, s, s, s
+        B, D, H, W = self.shape
+        return B, D >> level, H >> level, W >> level
 
     def _conv(self, L: Conv, a, b, out) -> None:
         o, _, bo, _ = self.lay[L.name]
@@ -184,14 +199,15 @@ class UNet3D:
 
     # -- forward ----------------------------------------------------------
     def set_input(self, xlog: np.ndarray | None, density: np.ndarray | None, mat: np.ndarray | None,
-                  B: int, S: int, device_xlog=None, device_density=None, device_mat=None,
+                  B: int, S, device_xlog=None, device_density=None, device_mat=None,
                   unc: np.ndarray | None = None) -> None:
-        """Input volumes [B, S, S, S] (host arrays, or device tensors); unc,
+        """Input volumes [B, S, S, S], or [B, D, H, W] with S = (D, H, W)
+        (host arrays, or device tensors; every side a multiple of 8); unc,
         when given, is the input map's relative standard error (see
         ``uncertainty_channel``)."""
         torch = self.torch
         self._alloc(B, S)
-        n0 = B * S ** 3
+        n0 = int(np.prod(self.shape))
         xl = device_xlog if device_xlog is not None else torch.from_numpy(
             np.ascontiguousarray(xlog, dtype=np.float32).reshape(-1)).to(self.dev, non_blocking=True)
         de = device_density if device_density is not None else torch.from_numpy(
@@ -212,16 +228,16 @@ class UNet3D:
         L = {x.name: x for x in LAYERS}
         self._conv(L["e0a"], a["x0"], None, a["e0a"])
         self._conv(L["e0"], a["e0a"], None, a["e0"])
-        B, S0, _, _ = self._dims(0)
-        self._call(lib.ccu_avgpool, self._ptr(a["e0"]), B, S0, S0, S0, 16, self._ptr(a["p0"]), st)
+        B, *S0 = self._dims(0)
+        self._call(lib.ccu_avgpool, self._ptr(a["e0"]), B, *S0, 16, self._ptr(a["p0"]), st)
         self._conv(L["e1a"], a["p0"], None, a["e1a"])
         self._conv(L["e1"], a["e1a"], None, a["e1"])
-        _, S1, _, _ = self._dims(1)
-        self._call(lib.ccu_avgpool, self._ptr(a["e1"]), B, S1, S1, S1, 32, self._ptr(a["p1"]), st)
+        _, *S1 = self._dims(1)
+        self._call(lib.ccu_avgpool, self._ptr(a["e1"]), B, *S1, 32, self._ptr(a["p1"]), st)
         self._conv(L["e2a"], a["p1"], None, a["e2a"])
         self._conv(L["e2"], a["e2a"], None, a["e2"])
-        _, S2, _, _ = self._dims(2)
-        self._call(lib.ccu_avgpool, self._ptr(a["e2"]), B, S2, S2, S2, 64, self._ptr(a["p2"]), st)
+        _, *S2 = self._dims(2)
+        self._call(lib.ccu_avgpool, self._ptr(a["e2"]), B, *S2, 64, self._ptr(a["p2"]), st)
         self._conv(L["b3a"], a["p2"], None, a["b3a"])
         self._conv(L["b3"], a["b3a"], None, a["b3"])
         self._conv(L["d2a"], a["e2"], a["b3"], a["d2a"])
@@ -232,12 +248,12 @@ class UNet3D:
         self._conv(L["d0"], a["d0a"], None, a["d0"])
 
     def _head(self, target=None, weight=None, inv_wsum: float = 0.0, backward: bool = False) -> None:
-        B, S = self.shape
+        n0 = int(np.prod(self.shape))
         ho, _, _, _ = self.lay["head"]
         self._call(U.lib().ccu_head, self._ptr(self.a["d0"]), self._ptr(self.xlog),
                    self._ptr(target) if target is not None else None,
                    self._ptr(weight) if weight is not None else None, self._ptr(self.p, ho), inv_wsum,
-                   B * S ** 3, self._ptr(self.out), self._ptr(self.gb["dz_d0"]) if backward else None,
+                   n0, self._ptr(self.out), self._ptr(self.gb["dz_d0"]) if backward else None,
                    self._ptr(self.g, ho) if backward else None, self._ptr(self.acc) if target is not None else None,
                    self._stream())
 
@@ -264,37 +280,38 @@ class UNet3D:
                        self._ptr(out1) if out1 is not None else None, st)
 
     def backward(self, target, weight, inv_wsum: float) -> None:
+        self._alloc_grads()
         a, g, lib, st = self.a, self.gb, U.lib(), self._stream()
         L = {x.name: x for x in LAYERS}
         self._call(lib.ccu_zero, self._ptr(self.g), self.g.numel() * 4, st)
         self._call(lib.ccu_zero, self._ptr(self.acc), self.acc.numel() * 4, st)
         self._head(target, weight, inv_wsum, backward=True)
-        B, S0, _, _ = self._dims(0)
-        _, S1, _, _ = self._dims(1)
-        _, S2, _, _ = self._dims(2)
+        B, *S0 = self._dims(0)
+        _, *S1 = self._dims(1)
+        _, *S2 = self._dims(2)
         self._layer_back(L["d0"], a["d0a"], None, g["dz_d0"], g["dz_d0a"], a["d0a"])
         self._layer_back(L["d0a"], a["e0"], a["d1"], g["dz_d0a"], g["dz_e0"], a["e0"], g["g_up1"])
-        self._call(lib.ccu_up_reduce, self._ptr(g["g_up1"]), self._ptr(a["d1"]), B, S0, S0, S0, 32,
+        self._call(lib.ccu_up_reduce, self._ptr(g["g_up1"]), self._ptr(a["d1"]), B, *S0, 32,
                    self._ptr(g["dz_d1"]), st)
         self._layer_back(L["d1"], a["d1a"], None, g["dz_d1"], g["dz_d1a"], a["d1a"])
         self._layer_back(L["d1a"], a["e1"], a["d2"], g["dz_d1a"], g["dz_e1"], a["e1"], g["g_up2"])
-        self._call(lib.ccu_up_reduce, self._ptr(g["g_up2"]), self._ptr(a["d2"]), B, S1, S1, S1, 64,
+        self._call(lib.ccu_up_reduce, self._ptr(g["g_up2"]), self._ptr(a["d2"]), B, *S1, 64,
                    self._ptr(g["dz_d2"]), st)
         self._layer_back(L["d2"], a["d2a"], None, g["dz_d2"], g["dz_d2a"], a["d2a"])
         self._layer_back(L["d2a"], a["e2"], a["b3"], g["dz_d2a"], g["dz_e2"], a["e2"], g["g_up3"])
-        self._call(lib.ccu_up_reduce, self._ptr(g["g_up3"]), self._ptr(a["b3"]), B, S2, S2, S2, 128,
+        self._call(lib.ccu_up_reduce, self._ptr(g["g_up3"]), self._ptr(a["b3"]), B, *S2, 128,
                    self._ptr(g["dz_b3"]), st)
         self._layer_back(L["b3"], a["b3a"], None, g["dz_b3"], g["dz_b3a"], a["b3a"])
         self._layer_back(L["b3a"], a["p2"], None, g["dz_b3a"], g["g_p2"], None)
-        self._call(lib.ccu_pool_backward, self._ptr(g["g_p2"]), self._ptr(a["e2"]), B, S2, S2, S2, 64,
+        self._call(lib.ccu_pool_backward, self._ptr(g["g_p2"]), self._ptr(a["e2"]), B, *S2, 64,
                    self._ptr(g["dz_e2"]), st)
         self._layer_back(L["e2"], a["e2a"], None, g["dz_e2"], g["dz_e2a"], a["e2a"])
         self._layer_back(L["e2a"], a["p1"], None, g["dz_e2a"], g["g_p1"], None)
-        self._call(lib.ccu_pool_backward, self._ptr(g["g_p1"]), self._ptr(a["e1"]), B, S1, S1, S1, 32,
+        self._call(lib.ccu_pool_backward, self._ptr(g["g_p1"]), self._ptr(a["e1"]), B, *S1, 32,
                    self._ptr(g["dz_e1"]), st)
         self._layer_back(L["e1"], a["e1a"], None, g["dz_e1"], g["dz_e1a"], a["e1a"])
         self._layer_back(L["e1a"], a["p0"], None, g["dz_e1a"], g["g_p0"], None)
-        self._call(lib.ccu_pool_backward, self._ptr(g["g_p0"]), self._ptr(a["e0"]), B, S0, S0, S0, 16,
+        self._call(lib.ccu_pool_backward, self._ptr(g["g_p0"]), self._ptr(a["e0"]), B, *S0, 16,
                    self._ptr(g["dz_e0"]), st)
         self._layer_back(L["e0"], a["e0a"], None, g["dz_e0"], g["dz_e0a"], a["e0a"])
         self._layer_back(L["e0a"], a["x0"], None, g["dz_e0a"])

@@ -208,3 +208,28 @@ def test_shipped_ct_network_denoises_the_ct_configuration():
     err = lambda k: float(np.median(np.abs(k[sel] - k_ref[sel]) / k_ref[sel]))  # noqa: E731
     e_plain, e_dn = err(k_n), err(k_dn)
     assert e_dn < 0.25 * e_plain, (e_dn, e_plain)
+
+
+def test_whole_volume_pass_equals_the_oracle_on_a_non_cubic_volume():
+    """The network on a non-cubic volume (16 x 32 x 24 voxels, one pass): its
+    first layer's output against the denoiser's oracle, and a finite
+    prediction of the right shape."""
+    import unet_oracle as UO
+    from chatcarlo_b200 import denoiser as DN
+    params, _ = DN.load_params()
+    model = DN.UNet3D(params=params)
+    rng = np.random.default_rng(4)
+    shape = (16, 32, 24)
+    xl = rng.normal(size=(1, *shape)).astype(np.float32)
+    mt = rng.integers(0, 4, size=(1, *shape)).astype(np.uint8)
+    dn = np.array([0.0012, 1.0, 1.85, 11.35], dtype=np.float32)[mt]
+    un = np.full((1, *shape), 0.2, np.float32)
+    model.set_input(xl, dn, mt, 1, shape, unc=un)
+    out = model.predict().cpu().numpy().reshape(shape)
+    model.check_status()
+    o, nw, bo, bn = DN.param_layout()["e0a"]
+    x0 = UO.bf16(UO.make_input(xl.astype(np.float64), dn, mt, un))
+    y = UO.bf16(np.maximum(UO.conv3d(x0, UO.bf16(params[o:o + nw]).reshape(27, 16, 16)) + params[bo:bo + bn], 0))
+    got = model.a["e0a"].float().cpu().numpy().reshape(y.shape)
+    assert np.all(np.isfinite(out))
+    assert float(np.linalg.norm(got - y) / np.linalg.norm(y)) < 3e-3
