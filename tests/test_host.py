@@ -311,3 +311,14 @@ def test_ct_phantoms_are_valid_scenes():
         for g in sc["geometry"][1:]:
             assert np.hypot(*g["center"][:2]) + g["radius_cm"] <= body["radius_cm"]
             assert abs(g["center"][2]) + g["height_cm"] / 2 <= 7.5 + 1e-9
+
+
+def test_denoiser_volume_shapes():
+    """The network takes cubic (S) or non-cubic (D, H, W) volumes whose
+    sides are multiples of 8 (three 2x2x2 poolings)."""
+    from chatcarlo_b200.denoiser import UNet3D
+    assert UNet3D._side3(64) == (64, 64, 64)
+    assert UNet3D._side3((320, 320, 152)) == (320, 320, 152)
+    for bad in (12, (16, 30, 8), (16, 16), (0, 8, 8)):
+        with pytest.raises(ValueError):
+            UNet3D._side3(bad)
