@@ -387,9 +387,12 @@ def main():
             step_ms.append(ev0.elapsed_time(ev1))
         red_ms = 0.0
         if world > 1:
-            # the one exchange step: sum the tally grids over ranks
+            # the one exchange step: sum the tally grids and their batch
+            # statistics over ranks (totals, sums of squares and hit counts
+            # are additive, as when the reference merges its workers)
             dg.download(grid)
-            t = torch.from_numpy(np.stack([grid.kerma_keV, grid.h10_track_pSv_cm3])).cuda()
+            t = torch.from_numpy(np.stack([grid.kerma_keV, grid.h10_track_pSv_cm3, grid.kerma_sum2, grid.h10_sum2,
+                                           grid.n_batches_hit.astype(np.float64)])).cuda()
             ev0.record()
             dist.all_reduce(t)
             ev1.record()
