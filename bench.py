@@ -224,7 +224,8 @@ def denoiser_metric(eng, n_phantoms: int, levels=(500_000, 1_000_000, 2_000_000)
 def ct_denoiser_metric(eng, levels=(1_000_000, 3_000_000, 10_000_000), n_ref: int = 2_000_000_000) -> dict:
     """The same measurement on the CT configuration (1 mm voxels,
     320x320x150): its own phantom, never seen by the shipped CT network,
-    denoised tile by tile, against an n_ref-history reference."""
+    denoised as one whole volume in a single pass of the network, against an
+    n_ref-history reference."""
     from chatcarlo_b200 import ct_denoise as CD
     from chatcarlo_b200 import denoiser as DN
     from chatcarlo_b200 import phantoms as PH
@@ -256,7 +257,7 @@ def ct_denoiser_metric(eng, levels=(1_000_000, 3_000_000, 10_000_000), n_ref: in
             "plain_mc": t_plain, "denoised": t_dn, "speedup": (t_plain / t_dn) if t_dn else None,
             "plain_histories": n_plain, "denoised_histories": n_dn, "inference_s": float(np.median(t_inf)),
             "mc_histories_per_s": rate, "reference_histories": n_ref, "reference_noise": ref_noise,
-            "levels": rows, "volume": "320x320x150 voxels of 1 mm, 147 tiles of 64^3"}
+            "levels": rows, "volume": "320x320x150 voxels of 1 mm, one pass of the network over the whole volume"}
 
 
 def DN_inference_s(model, n_phantoms: int) -> float:

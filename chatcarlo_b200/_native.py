@@ -30,6 +30,7 @@ CC_E_NOMEM = -9
 CC_SHAPE_BOX, CC_SHAPE_SPHERE, CC_SHAPE_CYLINDER, CC_SHAPE_ELLIPSOID = 0, 1, 2, 3
 CC_GRID_STATS = 1
 CC_FIELD_RECT, CC_FIELD_CONE, CC_FIELD_PARALLEL = 0, 1, 2
+CC_INTERACT_PHOTO, CC_INTERACT_COMPTON, CC_INTERACT_RAYLEIGH = 0, 1, 2
 
 # every symbol the header declares
 EXPORTED = [
@@ -39,6 +40,8 @@ EXPORTED = [
     "cc_grid_destroy", "cc_grid_reset", "cc_grid_download", "cc_grid_end_batch", "cc_grid_maps", "cc_grid_upload",
     "cc_transport_photons", "cc_transport_photons_device", "cc_run", "cc_sample_source",
     "cc_transport_photons_device_noalloc", "cc_batch_create", "cc_batch_run", "cc_batch_destroy",
+    "cc_sample_interactions", "cc_philox4x32_10", "cc_grid_device_buffers", "cc_grid_set_counts",
+    "cc_measure_fp64_reductions",
 ]
 
 
@@ -139,6 +142,15 @@ def _bind(lib):
         "cc_batch_destroy": (C.c_int, [P]),
         "cc_transport_photons_device_noalloc": (C.c_int, [P, P, C.c_int64, P, P, P, C.c_uint64, C.c_uint64,
                                                           C.c_int32, P, P, P, PD, C.POINTER(C.c_int64), P]),
+        "cc_sample_interactions": (C.c_int, [P, P, C.c_int32, C.c_int64, C.POINTER(C.c_int32), PD, C.c_uint64,
+                                             C.c_int32, PD, PD, C.POINTER(C.c_int32)]),
+        "cc_philox4x32_10": (C.c_int, [P, C.c_int64, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32),
+                                       C.POINTER(C.c_uint32)]),
+        "cc_grid_device_buffers": (C.c_int, [P, C.POINTER(P), C.POINTER(P), C.POINTER(P), C.POINTER(C.c_int64),
+                                             C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+        "cc_grid_set_counts": (C.c_int, [P, C.c_int64, C.c_int64]),
+        "cc_measure_fp64_reductions": (C.c_int, [C.c_int, P, C.c_int64, C.c_int32, C.c_int32, C.c_int32,
+                                                 C.c_int32, C.c_int32, C.c_int32, C.c_int64, C.c_int32, PD]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

@@ -20,7 +20,7 @@ CSRC = PKG / "csrc"
 LIB_DIR = PKG / "lib"
 LIB_PATH = LIB_DIR / "libccb200.so"
 HEADER = PKG.parent / "include" / "chatcarlo_b200.h"
-SOURCES = [CSRC / "cc_engine.cu"]
+SOURCES = [CSRC / "cc_engine.cu", CSRC / "cc_atomics.cu"]
 DEPS = SOURCES + [CSRC / "philox.cuh", HEADER]
 FP64_LIB_PATH = LIB_DIR / "libccb200_fp64.so"
 UNET_LIB_PATH = LIB_DIR / "libccunet.so"

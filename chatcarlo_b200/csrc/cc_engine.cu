@@ -88,7 +88,7 @@ struct DevMaterial {
 
 struct DevElement {
     float k_edge, k_prob, omega;
-    int n_lines, emits, pad;
+    int n_lines, emits, z;
     float ray_scale;        // RAY_BUCKETS / A(x_end)
     float line_e[8];
     float line_cum[8];
@@ -489,6 +489,22 @@ __device__ __forceinline__ bool sample_rayleigh(const float* rx, const float* ra
     }
     cos_out = 1.0f;
     return true;
+}
+
+// Photoelectric absorption on a chosen element (physics.py:155-212): above
+// the K edge the K shell takes the photon with probability k_prob, it
+// relaxes radiatively with probability omega_K and emits one of the K lines
+// (cumulative line probabilities), which leaves only when at or above the
+// 5 keV cut-off.  Returns the emitted line's energy, 0 when none.
+__device__ __forceinline__ float sample_k_line(const DevElement& el, float E, int fluorescence, HistoryRng& rng) {
+    if (!(fluorescence && el.emits && E > el.k_edge)) return 0.0f;
+    const bool is_k = rng.uniform() < el.k_prob;
+    const bool is_rad = rng.uniform() < el.omega;
+    if (!(is_k && is_rad)) return 0.0f;
+    const float rl = rng.uniform();
+    int li = el.n_lines - 1;
+    for (int k = 0; k < el.n_lines; ++k) if (rl <= el.line_cum[k]) { li = k; break; }
+    return el.line_e[li] >= FLUOR_CUTOFF ? el.line_e[li] : 0.0f;
 }
 
 // New direction from cos(theta) and a uniform azimuth (physics.py:354-367).
@@ -1000,19 +1016,8 @@ transport_kernel(const KTables T, const KScene S, const KGrid G, const KSource S
             float cost = 1.0f, e_new = E, dep = 0.0f;
             if (kind == 0) {
                 // photoelectric, K fluorescence (physics.py:155-212, transport.py:174-198)
-                const DevElement& el = T.elems[slot];
-                float e_line = 0.0f;
-                bool emit = false;
-                if (R.fluorescence && el.emits && E > el.k_edge) {
-                    bool is_k = rng.uniform() < el.k_prob;
-                    bool is_rad = rng.uniform() < el.omega;
-                    if (is_k && is_rad) {
-                        float rl = rng.uniform();
-                        int li = el.n_lines - 1;
-                        for (int k = 0; k < el.n_lines; ++k) if (rl <= el.line_cum[k]) { li = k; break; }
-                        if (el.line_e[li] >= FLUOR_CUTOFF) { emit = true; e_line = el.line_e[li]; }
-                    }
-                }
+                const float e_line = sample_k_line(T.elems[slot], E, R.fluorescence, rng);
+                const bool emit = e_line > 0.0f;
                 dep = emit ? E - e_line : E;
                 if (emit) {
                     ++c_fl;
@@ -1345,20 +1350,8 @@ batch_kernel(const KTables T, const KBatch B, const KRun R) {
                 float cost = 1.0f, e_new = E;
                 bool ok = true;
                 if (kind == 0) {
-                    const DevElement& el = T.elems[eslot];
-                    float e_line = 0.0f;
-                    bool emit = false;
-                    if (fluorescence && el.emits && E > el.k_edge) {
-                        bool is_k = rng.uniform() < el.k_prob;
-                        bool is_rad = rng.uniform() < el.omega;
-                        if (is_k && is_rad) {
-                            float rl = rng.uniform();
-                            int lidx = el.n_lines - 1;
-                            for (int k = 0; k < el.n_lines; ++k) if (rl <= el.line_cum[k]) { lidx = k; break; }
-                            if (el.line_e[lidx] >= FLUOR_CUTOFF) { emit = true; e_line = el.line_e[lidx]; }
-                        }
-                    }
-                    if (emit) {
+                    const float e_line = sample_k_line(T.elems[eslot], E, fluorescence, rng);
+                    if (e_line > 0.0f) {
                         atomicAdd(B.scene_cnt + 4 * (size_t)sc + 3, 1ull);   // rare: K lines of heavy elements
                         e_new = e_line;
                     } else {
@@ -1636,6 +1629,62 @@ __global__ void sample_source_kernel(const KSource SRC, long long n, long long f
     sample_source(SRC, rng, p, d, E);
     for (int k = 0; k < 3; ++k) { pos[3 * i + k] = p[k]; dir[3 * i + k] = d[k]; }
     en[i] = E;
+}
+
+// One interaction per thread through the transport kernel's own device
+// functions: the element draw of the interaction kind, then the photoelectric
+// K-line draw, the bound-Compton sampler or the Rayleigh sampler.  Photon i
+// draws the Philox stream of history i under the seed.
+constexpr int INTERACT_PHOTO = 0, INTERACT_COMPTON = 1, INTERACT_RAYLEIGH = 2;
+
+__global__ void interaction_kernel(const KTables T, int kind, long long n, const int* __restrict__ mat,
+                                   const float* __restrict__ energy, unsigned long long seed, int fluorescence,
+                                   double* out_a, double* out_b, int* out_z, unsigned* status) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int m = mat[i];
+    const float E = energy[i];
+    out_a[i] = 0.0;
+    out_b[i] = 0.0;
+    out_z[i] = 0;
+    if (m < 0 || m >= T.n_mat) { atomicOr(status, ST_BOUNDS); return; }
+    if (!(E >= E_MIN_KEV && E <= E_MAX_KEV)) { atomicOr(status, ST_ENERGY); return; }
+    HistoryRng rng;
+    rng.init(seed, (unsigned long long)i, 0u);
+    const DevMaterial& M = T.mats[m];
+    const Lookup L = energy_index(T, M, __logf(E));
+    const int slot = pick_element(T, M, L, kind, rng.uniform());
+    out_z[i] = T.elems[slot].z;
+    if (kind == INTERACT_PHOTO) {
+        out_a[i] = sample_k_line(T.elems[slot], E, fluorescence, rng);
+    } else if (kind == INTERACT_COMPTON) {
+        float eps, cost;
+        sample_compton(T.sq + (size_t)slot * TABLE_N, E, rng, eps, cost);
+        out_a[i] = eps;
+        out_b[i] = cost;
+    } else {
+        float cost;
+        if (!sample_rayleigh(T.rx + (size_t)slot * TABLE_N, T.ra + (size_t)slot * TABLE_N,
+                             T.ray_bucket + (size_t)slot * (RAY_BUCKETS + 1), T.elems[slot].ray_scale, E, rng,
+                             cost)) {
+            atomicOr(status, ST_RAYLEIGH_Q);
+            return;
+        }
+        out_a[i] = cost;
+    }
+}
+
+// Raw Philox4x32-10 blocks (known-answer tests of the generator).
+__global__ void philox_kernel(long long n, const uint32_t* __restrict__ ctr, const uint32_t* __restrict__ key,
+                              uint32_t* __restrict__ out) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const u32x4 r = philox_block(ctr[4 * i], ctr[4 * i + 1], ctr[4 * i + 2], ctr[4 * i + 3], key[2 * i],
+                                 key[2 * i + 1]);
+    out[4 * i] = r.x;
+    out[4 * i + 1] = r.y;
+    out[4 * i + 2] = r.z;
+    out[4 * i + 3] = r.w;
 }
 
 }  // namespace cc
@@ -1933,6 +1982,7 @@ int cc_tables_create(cc_ctx* ctx, const cc_table_desc* desc, cc_tables** out) {
         de.omega = (float)ed.omega_k;
         de.n_lines = ed.n_lines;
         de.emits = ed.emits && ed.n_lines > 0;
+        de.z = ed.z;
         double cum = 0.0;
         for (int k = 0; k < ed.n_lines; ++k) {
             cum += ed.line_p[k];
@@ -2194,6 +2244,29 @@ int cc_grid_reset(cc_grid* g) {
     CC_CUDA(cudaStreamSynchronize(st));
     g->n_batches = 0;
     g->n_histories = 0;
+    return CC_OK;
+}
+
+int cc_grid_device_buffers(cc_grid* g, double** totals, double** sum2s, int32_t** n_batches_hit,
+                           int64_t* n_voxels, int64_t* n_batches, int64_t* n_histories) {
+    if (!g) return set_error(CC_E_INVALID, "grid is NULL");
+    // the grid's stream may still be writing the totals
+    CC_CUDA(cudaSetDevice(g->ctx->device));
+    CC_CUDA(cudaStreamSynchronize(g->ctx->stream));
+    if (totals) *totals = g->d_total;
+    if (sum2s) *sum2s = g->d_q;
+    if (n_batches_hit) *n_batches_hit = (int32_t*)g->d_nhit;
+    if (n_voxels) *n_voxels = g->k.nvox;
+    if (n_batches) *n_batches = g->n_batches;
+    if (n_histories) *n_histories = g->n_histories;
+    return CC_OK;
+}
+
+int cc_grid_set_counts(cc_grid* g, int64_t n_batches, int64_t n_histories) {
+    if (!g) return set_error(CC_E_INVALID, "grid is NULL");
+    if (n_batches < 0 || n_histories < 0) return set_error(CC_E_INVALID, "negative count");
+    g->n_batches = n_batches;
+    g->n_histories = n_histories;
     return CC_OK;
 }
 
@@ -2612,6 +2685,9 @@ int cc_transport_photons_device(cc_ctx* c, const cc_scene* scene, const cc_table
     if (n < 0) return set_error(CC_E_INVALID, "n < 0");
     if (n == 0) { if (n_fluor) *n_fluor = 0; return CC_OK; }
     if (!d_pos || !d_dir || !d_en) return set_error(CC_E_INVALID, "photon arrays are NULL");
+    if (scene->ctx->device != c->device || tables->ctx->device != c->device ||
+        (grid && grid->ctx->device != c->device))
+        return set_error(CC_E_INVALID, "scene, tables and grid must belong to the context's device");
     CC_CUDA(cudaSetDevice(c->device));
     return transport_common(c, scene, tables, grid, n, d_pos, d_dir, d_en, seed, stream_offset,
                             fluorescence, d_nsc, d_abs, d_esc, edep, n_fluor);
@@ -2921,6 +2997,71 @@ int cc_sample_source(cc_ctx* c, const cc_source* src, int64_t n, uint64_t seed, 
     return CC_OK;
 }
 
+int cc_sample_interactions(cc_ctx* c, const cc_tables* tables, int32_t kind, int64_t n, const int32_t* material,
+                           const double* energy, uint64_t seed, int32_t fluorescence, double* out_a,
+                           double* out_b, int32_t* out_z) {
+    if (!c || !tables || !material || !energy || !out_a || !out_b || !out_z)
+        return set_error(CC_E_INVALID, "NULL argument");
+    if (kind < INTERACT_PHOTO || kind > INTERACT_RAYLEIGH) return set_error(CC_E_INVALID, "unknown interaction kind");
+    if (n < 0) return set_error(CC_E_INVALID, "n < 0");
+    if (n == 0) return CC_OK;
+    if (tables->ctx->device != c->device) return set_error(CC_E_INVALID, "tables belong to another device");
+    CC_CUDA(cudaSetDevice(c->device));
+    std::vector<float> ef((size_t)n);
+    for (int64_t i = 0; i < n; ++i) ef[i] = (float)energy[i];
+    // [status 256 B][mat n x 4][energy n x 4][z n x 4][pad][a n x 8][b n x 8]
+    const size_t n4 = ((size_t)n * 4 + 255) / 256 * 256;
+    const size_t bytes = 256 + 3 * n4 + 2 * (size_t)n * 8;
+    char* buf = nullptr;
+    CC_CUDA(cudaMalloc(&buf, bytes));
+    unsigned* d_st = (unsigned*)buf;
+    int* d_mat = (int*)(buf + 256);
+    float* d_e = (float*)(buf + 256 + n4);
+    int* d_z = (int*)(buf + 256 + 2 * n4);
+    double* d_a = (double*)(buf + 256 + 3 * n4);
+    double* d_b = d_a + n;
+    unsigned st = 0;
+    cudaStream_t s = c->stream;
+    cudaError_t e = cudaMemsetAsync(d_st, 0, sizeof(unsigned), s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_mat, material, (size_t)n * 4, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_e, ef.data(), (size_t)n * 4, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) {
+        const int threads = 256;
+        interaction_kernel<<<(unsigned)((n + threads - 1) / threads), threads, 0, s>>>(
+            tables->k, kind, n, d_mat, d_e, seed, fluorescence, d_a, d_b, d_z, d_st);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out_a, d_a, (size_t)n * 8, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out_b, d_b, (size_t)n * 8, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out_z, d_z, (size_t)n * 4, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&st, d_st, sizeof(unsigned), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    cudaFree(buf);
+    if (e != cudaSuccess) return set_error(CC_E_DEVICE, std::string("sample_interactions: ") + cudaGetErrorString(e));
+    return status_to_error(st);
+}
+
+int cc_philox4x32_10(cc_ctx* c, int64_t n, const uint32_t* ctr, const uint32_t* key, uint32_t* out) {
+    if (!c || !ctr || !key || !out) return set_error(CC_E_INVALID, "NULL argument");
+    if (n < 0) return set_error(CC_E_INVALID, "n < 0");
+    if (n == 0) return CC_OK;
+    CC_CUDA(cudaSetDevice(c->device));
+    uint32_t* buf = nullptr;
+    CC_CUDA(cudaMalloc(&buf, (size_t)n * 10 * sizeof(uint32_t)));
+    cudaStream_t s = c->stream;
+    cudaError_t e = cudaMemcpyAsync(buf, ctr, (size_t)n * 16, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(buf + 4 * n, key, (size_t)n * 8, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) {
+        philox_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, buf, buf + 4 * n, buf + 6 * n);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, buf + 6 * n, (size_t)n * 16, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    cudaFree(buf);
+    if (e != cudaSuccess) return set_error(CC_E_DEVICE, std::string("philox: ") + cudaGetErrorString(e));
+    return CC_OK;
+}
+
 // ---------------------------------------------------------------------------
 // Allocation-free transport of device-resident photons.
 //
@@ -2957,6 +3098,7 @@ int cc_transport_photons_device_noalloc(const cc_scene* scene, const cc_tables* 
     if (n == 0) { if (n_fluor) *n_fluor = 0; return CC_OK; }
     if (!d_pos || !d_dir || !d_en) return set_error(CC_E_INVALID, "photon arrays are NULL");
     const int dev = tables->ctx->device;
+    if (scene->ctx->device != dev) return set_error(CC_E_INVALID, "scene and tables belong to different devices");
     if (dev < 0 || dev >= 64) return set_error(CC_E_INVALID, "device ordinal out of range");
     CC_CUDA(cudaSetDevice(dev));
     unsigned long long* scratch = nullptr;
@@ -3007,12 +3149,15 @@ int cc_transport_photons_device_noalloc(const cc_scene* scene, const cc_tables* 
     unsigned long long words[8 + MAX_MATS];
     CC_CUDA(cudaMemcpyAsync(words, scratch, sizeof(words), cudaMemcpyDeviceToHost, st));
     CC_CUDA(cudaStreamSynchronize(st));
+    // a failed call leaves the caller's accumulators as they were
+    const int rc = status_to_error((unsigned)words[7]);
+    if (rc != CC_OK) return rc;
     if (edep) {
         const double* dep = (const double*)(words + 8);
         for (int m = 0; m < tables->n_mat; ++m) edep[m] += dep[m];
     }
     if (n_fluor) *n_fluor = (int64_t)words[3];
-    return status_to_error((unsigned)words[7]);
+    return CC_OK;
 }
 
 // ---------------------------------------------------------------------------

@@ -56,6 +56,9 @@ class TransportResult:
     n_voxel_visits: int = 0
     # output maps computed on the device when run_transport(maps=True)
     maps: dict | None = None
+    # batch moments of the energy deposited per material (keV; ScalarMoments,
+    # tally.py:191-245): what merging runs over ranks needs
+    moments: ScalarMoments | None = None
 
 
 class DeviceGrid:
@@ -359,16 +362,25 @@ def run_transport(scene, n_histories: int = 100_000, seed: int | None = None,
                   grid_resolution_cm: float = 5.0, n_workers: int = 1,
                   track_uncertainty: bool = True, engine: Engine | None = None,
                   first_history: int = 0, grid: VoxelGrid | None = None,
-                  maps: bool = False) -> TransportResult:
+                  maps: bool = False, distributed: bool | None = None) -> TransportResult:
     """run_transport (chatcarlo/transport.py:358-474) on the GPU.
 
-    ``n_workers`` is accepted for signature compatibility; the histories run
-    on one device.  The source is sampled on the device, histories are
-    grouped into batches of ``batch_size`` for the batch statistics.  With
-    ``maps`` and a dose grid, ``result.maps`` holds the per-history dose and
-    H*(10) maps of chatcarlo/__main__.py:200-209 (``dose_per_history_Gy``,
+    ``n_workers`` is accepted for signature compatibility; the reference's
+    process workers (transport.py:397-437) are ranks here.  The source is
+    sampled on the device, histories are grouped into batches of
+    ``batch_size`` for the batch statistics.  With ``maps`` and a dose grid,
+    ``result.maps`` holds the per-history dose and H*(10) maps of
+    chatcarlo/__main__.py:200-209 (``dose_per_history_Gy``,
     ``h10_per_history_pSv``) and, with ``track_uncertainty``, the relative
     error maps (``kerma_rel``, ``h10_rel``), all computed on the device.
+
+    Under torchrun (a default process group of W > 1 ranks, one GPU each;
+    ``distributed=None`` detects it, ``False`` turns it off) rank r runs
+    histories ``shard_range(n_histories, r, W)`` of the run keyed by
+    ``seed``, so the ranks together run exactly the histories of a one-GPU
+    run; the device grids are summed in place by one NCCL all-reduce per
+    array, the counters and per-material moments by a few small ones, and
+    every rank returns the whole run's result.
     """
     raw = scene.raw if hasattr(scene, "raw") else scene
     src = raw["source"]
@@ -383,6 +395,15 @@ def run_transport(scene, n_histories: int = 100_000, seed: int | None = None,
     if not dose_grid:
         grid = None
     fluorescence = raw.get("physics", {}).get("fluorescence", True)
+    rank, world = 0, 1
+    if distributed is not False:
+        from .distributed import world_info
+        rank, world = world_info()
+    n_local, first_local = int(n_histories), int(first_history)
+    if world > 1:
+        from .distributed import shard_range
+        first, n_local = shard_range(n_histories, rank, world)
+        first_local += first
     names = geometry.materials()
     ts, th = eng.tables(names, need_muen=grid is not None)
     sh = eng.scene(geometry, ts)
@@ -393,10 +414,13 @@ def run_transport(scene, n_histories: int = 100_000, seed: int | None = None,
     out = N.RunOut()
     out_maps = None
     try:
-        N.check(eng.lib.cc_run(eng.ctx, sh, th, srch, dg.handle if dg else None, int(n_histories),
-                               int(batch_size), _seed_from(None, seed), int(first_history),
+        N.check(eng.lib.cc_run(eng.ctx, sh, th, srch, dg.handle if dg else None, n_local,
+                               int(batch_size), _seed_from(None, seed), first_local,
                                int(bool(fluorescence)), N.dptr(edep), N.dptr(edep2), C.byref(out)))
         if dg is not None:
+            if world > 1:
+                from .distributed import allreduce_device_grid
+                allreduce_device_grid(dg)
             dg.download(grid)
             if maps:
                 m = dg.maps(geometry, divisor=float(max(int(n_histories), 1)), rel=track_uncertainty)
@@ -409,10 +433,11 @@ def run_transport(scene, n_histories: int = 100_000, seed: int | None = None,
     n_batches = int(out.n_batches)
     dep = {name: float(edep[i]) for i, name in enumerate(names) if edep[i] != 0.0}
     sem, rel = {}, {}
+    mom = None
     if track_uncertainty:
         mom = ScalarMoments()
         mom.add_moments(dep, {name: float(edep2[i]) for i, name in enumerate(names) if edep[i] != 0.0},
-                        n_batches, int(n_histories))
+                        n_batches, n_local)
         sem = {k: v / 1000.0 for k, v in mom.standard_errors().items()}
         rel = mom.relative_errors()
     # absolute calibration from CTDIvol, once, with the run's seed (transport.py:442-451)
@@ -420,9 +445,9 @@ def run_transport(scene, n_histories: int = 100_000, seed: int | None = None,
     if src.get("ctdi_vol_mGy") is not None:
         from .ctdi import effective_histories_from_ctdi
         n_photons_real = effective_histories_from_ctdi(src, seed=seed, engine=eng)
-    nh = max(int(n_histories), 1)
-    return TransportResult(
-        n_histories=int(n_histories),
+    nh = max(n_local, 1)
+    res = TransportResult(
+        n_histories=n_local,
         energy_deposited_MeV={k: v / 1000.0 for k, v in dep.items()},
         fraction_absorbed=out.n_absorbed / nh,
         fraction_escaped=out.n_escaped / nh,
@@ -440,4 +465,10 @@ def run_transport(scene, n_histories: int = 100_000, seed: int | None = None,
         n_steps=int(out.n_steps),
         n_voxel_visits=int(out.n_voxel_visits),
         maps=out_maps,
+        moments=mom,
     )
+    if world > 1:
+        import torch
+        from .distributed import reduce_result
+        reduce_result(res, device=torch.device("cuda", eng.device), grid=False)
+    return res

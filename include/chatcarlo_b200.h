@@ -236,6 +236,22 @@ int cc_grid_maps(cc_grid* g, const cc_primitive* prims, int32_t n_prims, const d
  * folds the batch accumulated since the previous fold. */
 int cc_grid_end_batch(cc_grid* g, int64_t n_histories_in_batch);
 
+/* The grid's device-resident state, for summing grids of several ranks in
+ * place with a collective (the reference sums its process workers' grids
+ * on the host, transport.py:416-437; T, Q and the hit counts are additive).
+ * totals: [nvox][2] FP64 (kerma, H*(10) interleaved per voxel); sum2s: the
+ * same layout for the batch sums of squares (NULL without CC_GRID_STATS);
+ * n_batches_hit: [nvox] int32 (NULL without CC_GRID_STATS).  Waits for the
+ * grid's context stream first.  A batch still pending (photons scored by
+ * cc_transport_photons* on a statistics grid since the last
+ * cc_grid_end_batch) is not part of these arrays.  The pointers stay valid
+ * until cc_grid_destroy.  Any output may be NULL. */
+int cc_grid_device_buffers(cc_grid* g, double** totals, double** sum2s, int32_t** n_batches_hit,
+                           int64_t* n_voxels, int64_t* n_batches, int64_t* n_histories);
+/* Sets the batch and history counts (after the arrays were summed over
+ * ranks, the counts are the ranks' sums). */
+int cc_grid_set_counts(cc_grid* g, int64_t n_batches, int64_t n_histories);
+
 /* -- transport ----------------------------------------------------------------
  * cc_transport_photons: transport_photons() on caller-provided photons.
  * pos/dir ([n][3]) and energy ([n]) are host arrays, updated in place with the
@@ -309,6 +325,46 @@ int cc_batch_destroy(cc_batch* batch);
 /* Sample source photons only (tests of source.py parity). */
 int cc_sample_source(cc_ctx* ctx, const cc_source* src, int64_t n, uint64_t seed,
                      int64_t first_history, double* pos, double* dir, double* energy);
+
+/* Single interactions, for sampler-by-sampler tests of the device physics
+ * against the reference's samplers (physics.py:78-92,95-135,138-212,
+ * 223-351; the reference calls them on whole photon arrays inside
+ * transport_photons, transport.py:160-198).  Photon i of energy[i] keV in
+ * material[i] (an index into the table set) takes one interaction of
+ * `kind` through the transport kernel's own device code: the element draw
+ * of that kind (w_i sigma_i(E) weights), then
+ *   CC_INTERACT_PHOTO:    out_a = energy of the emitted K line, 0 when none
+ *                         (fluorescence = 0 switches emission off)
+ *   CC_INTERACT_COMPTON:  out_a = eps = E'/E, out_b = cos(theta)
+ *   CC_INTERACT_RAYLEIGH: out_a = cos(theta)
+ * out_z[i] = atomic number of the element drawn.  Photon i draws the
+ * Philox stream of history i under seed.  Host arrays of n entries;
+ * CC_E_ENERGY_RANGE / CC_E_RAYLEIGH_Q_RANGE as in transport. */
+#define CC_INTERACT_PHOTO    0
+#define CC_INTERACT_COMPTON  1
+#define CC_INTERACT_RAYLEIGH 2
+int cc_sample_interactions(cc_ctx* ctx, const cc_tables* tables, int32_t kind, int64_t n,
+                           const int32_t* material, const double* energy, uint64_t seed,
+                           int32_t fluorescence, double* out_a, double* out_b, int32_t* out_z);
+
+/* Raw blocks of the device's Philox4x32-10 generator (known-answer tests;
+ * the reference draws from NumPy's PCG64 instead, transport.py:120-121):
+ * out[i][0..3] = Philox4x32-10(counter ctr[i][0..3], key key[i][0..1]).
+ * Host arrays. */
+int cc_philox4x32_10(cc_ctx* ctx, int64_t n, const uint32_t* ctr, const uint32_t* key, uint32_t* out);
+
+/* Measured ceiling of the tally's FP64 reductions (no reference
+ * counterpart; the reference tallies with np.add.at on the host,
+ * tally.py:286-293).  Launches blocks x threads threads on device d_cells'
+ * device, each scoring `per` voxel visits of two red.global.add.f64 into
+ * one 16-byte cell of d_cells ([n_cells][2] doubles, zeroed by the caller):
+ * mode 0 spreads the cells uniformly over the region, mode 1 over its
+ * first `hot` cells, mode 2 walks `run` cells `stride` apart from a random
+ * start.  visits_per_s = visits of `repeats` launches / their device time
+ * (CUDA events, after one warm-up launch). */
+int cc_measure_fp64_reductions(int device, double* d_cells, int64_t n_cells, int32_t mode, int32_t blocks,
+                               int32_t threads, int32_t per, int32_t hot, int32_t run, int64_t stride,
+                               int32_t repeats, double* visits_per_s);
 
 #ifdef __cplusplus
 }

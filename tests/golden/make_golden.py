@@ -1,9 +1,9 @@
 """Generate the golden vectors that pin the CPU oracle to ChatCarlo itself.
 
-Run in an environment that has the reference checkout (default
-/root/reference, or $CHATCARLO_REFERENCE):
+Run in an environment that has the reference checkout, naming its path
+in $CHATCARLO_REFERENCE (required):
 
-    python tests/golden/make_golden.py
+    CHATCARLO_REFERENCE=<path to the chatcarlo checkout> python tests/golden/make_golden.py
 
 The reference's modules are imported unmodified, with the stand-in data
 module oracle/xraylib_standin first on sys.path in place of the absent
@@ -21,7 +21,9 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 REPO = HERE.parent.parent
-REF = Path(os.environ.get("CHATCARLO_REFERENCE", "/root/reference"))
+if not os.environ.get("CHATCARLO_REFERENCE"):
+    sys.exit("set CHATCARLO_REFERENCE to the path of the chatcarlo checkout")
+REF = Path(os.environ["CHATCARLO_REFERENCE"])
 
 sys.dont_write_bytecode = True
 sys.path.insert(0, str(REPO / "oracle" / "xraylib_standin"))

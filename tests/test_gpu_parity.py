@@ -430,3 +430,33 @@ def test_chunked_host_transport_equals_one_device_launch(engine):
     finally:
         dg.close()
         engine.lib.cc_scene_destroy(sh)
+
+
+def test_step_limit_ends_a_run_with_a_timeout_error(engine):
+    """The per-photon step limit (the device-side guard against runaway
+    histories) turns into CC_E_TIMEOUT on the host, and the context stays
+    usable: with the limit reset the same photons finish."""
+    from chatcarlo_b200 import _native as N
+    geoms = [{"name": "slab", "shape": "box", "material": "water", "center": [0, 0, 0],
+              "size_cm": [40.0, 40.0, 40.0]}]
+    engine.set_step_limit(3)
+    try:
+        with pytest.raises(N.CCError) as ei:
+            _gpu_tp(engine, geoms, [-25.0, 0, 0], [1, 0, 0], 60.0, 100_000, seed=2)
+        assert ei.value.code == N.CC_E_TIMEOUT
+    finally:
+        engine.set_step_limit(100_000)
+    _, _, _, r = _gpu_tp(engine, geoms, [-25.0, 0, 0], [1, 0, 0], 60.0, 100_000, seed=2)
+    assert np.all(r.escaped | r.absorbed)
+
+
+def test_energy_outside_the_tables_is_a_value_error(engine):
+    """A photon above 150 keV is the reference's ValueError
+    (materials.py:234-237), through transport_photons and the device
+    status word; the next call runs normally."""
+    geoms = [{"name": "slab", "shape": "box", "material": "water", "center": [0, 0, 0],
+              "size_cm": [10.0, 10.0, 10.0]}]
+    with pytest.raises(ValueError):
+        _gpu_tp(engine, geoms, [-15.0, 0, 0], [1, 0, 0], 200.0, 1000, seed=3)
+    _, _, _, r = _gpu_tp(engine, geoms, [-15.0, 0, 0], [1, 0, 0], 100.0, 1000, seed=3)
+    assert np.all(r.escaped | r.absorbed)

@@ -10,7 +10,7 @@ import pytest
 import cc_oracle as O
 from chatcarlo_b200 import devtables, tables as tb, workloads as W
 from chatcarlo_b200.scene import validate_scene
-from chatcarlo_b200.tally import VoxelGrid, relative_error, standard_error
+from chatcarlo_b200.tally import ScalarMoments, VoxelGrid, relative_error, standard_error
 
 
 def test_benchmark_scenes_validate():
@@ -162,12 +162,34 @@ def _rank_main(rank, world, port, q):
     g.h10_sum2 += 0.25
     g.n_batches_hit += 1
     g.n_batches, g.n_histories = 3, 300
-    res = TransportResult(n_histories=1000, energy_deposited_MeV={}, fraction_absorbed=0.25 * (rank + 1),
-                          fraction_escaped=0.5, mean_scatter_events=2.0, grid=g, n_fluorescence=7)
+    # per-material batch moments (keV): rank 0 deposits in water and lead,
+    # rank 1 in water and air, so each rank lacks a name the other has
+    mom = ScalarMoments()
+    for b in range(5):
+        vals = {"water": 100.0 * (rank + 1) + b}
+        vals["lead" if rank == 0 else "air"] = 7.0 + b
+        mom.add_batch(vals, 200)
+    dep = {k: v / 1000.0 for k, v in mom.sums.items()}
+    res = TransportResult(n_histories=1000, energy_deposited_MeV=dep, fraction_absorbed=0.25 * (rank + 1),
+                          fraction_escaped=0.5, mean_scatter_events=2.0, grid=g, n_fluorescence=7, n_batches=5,
+                          moments=mom)
     reduce_result(res)
     q.put((rank, float(g.kerma_keV.sum()), float(g.h10_track_pSv_cm3[0, 0, 0]), int(g.n_batches_hit.max()),
-           g.n_batches, g.n_histories, res.n_histories, res.fraction_absorbed, res.n_fluorescence))
+           g.n_batches, g.n_histories, res.n_histories, res.fraction_absorbed, res.n_fluorescence,
+           res.n_batches, res.energy_deposited_MeV, res.energy_deposited_sem_MeV, res.energy_deposited_rel_err))
     dist.destroy_process_group()
+
+
+def _merged_reference():
+    """The two ranks' batches merged the way the reference merges process
+    workers (ScalarMoments.merge_from, transport.py:420-437)."""
+    mom = ScalarMoments()
+    for rank in range(2):
+        for b in range(5):
+            vals = {"water": 100.0 * (rank + 1) + b}
+            vals["lead" if rank == 0 else "air"] = 7.0 + b
+            mom.add_batch(vals, 200)
+    return mom
 
 
 def test_tally_reduction_over_two_ranks():
@@ -182,11 +204,18 @@ def test_tally_reduction_over_two_ranks():
     for p in procs:
         p.join(timeout=60)
         assert p.exitcode == 0
-    for rank, ksum, h0, nhit, nb, nh, n, fa, nfl in out:
+    want = _merged_reference()
+    for rank, ksum, h0, nhit, nb, nh, n, fa, nfl, nbat, dep, sem, rel in out:
         assert ksum == pytest.approx(24 * 3.0)
         assert h0 == pytest.approx(30.0)
-        assert nhit == 2 and nb == 6 and nh == 600 and n == 2000 and nfl == 14
+        assert nhit == 2 and nb == 6 and nh == 600 and n == 2000 and nfl == 14 and nbat == 10
         assert fa == pytest.approx((250 + 500) / 2000)
+        assert set(dep) == {"water", "lead", "air"}
+        for k in dep:
+            assert dep[k] == pytest.approx(want.sums[k] / 1000.0)
+            assert sem[k] == pytest.approx(want.standard_errors()[k] / 1000.0)
+            assert rel[k] == pytest.approx(want.relative_errors()[k])
+        assert sem["water"] > 0
 
 
 def test_ellipsoid_extension_primitive():

@@ -233,3 +233,21 @@ def test_output_maps_match_reference(golden):
     c = O.voxel_centers(g["origin"], tuple(g["shape"]), vox)
     assert np.any(np.abs(c[:, 0]) == 15.0)
     assert np.any(np.sum((c - np.array([5.0, -3.0, 2.0])) ** 2, axis=1) == 36.0)
+
+
+def test_voxel_fixtures_are_consistent():
+    """The oracle's configuration-scale voxel fixtures
+    (tests/golden/make_voxel_fixtures.py): every stored voxel has a
+    positive mean and a relative error under the cut, the masks and arrays
+    agree, and the chunk totals add up to the run's history count."""
+    from conftest import GOLDEN
+    for name in ("plain", "room", "ct_slab"):
+        f = np.load(GOLDEN / f"voxels_{name}.npz")
+        nv = int(np.prod(f["shape"]))
+        assert int(f["chunk_n"].sum()) == int(f["n_histories"])
+        for tag in ("kerma", "h10"):
+            mask = np.unpackbits(f[f"{tag}_mask"])[:nv].astype(bool)
+            assert mask.sum() == f[f"{tag}_mean"].size == f[f"{tag}_rel"].size > 10_000
+            assert np.all(f[f"{tag}_mean"] > 0)
+            assert np.all(f[f"{tag}_rel"].astype(float) < float(f["rel_cut"]) + 1e-3)
+            assert np.all(np.flatnonzero(mask) % int(f["keep_every"]) == 0)
