@@ -82,6 +82,13 @@ class TableDesc(C.Structure):
                 ("materials", C.POINTER(MaterialDesc)), ("elements", C.POINTER(ElementDesc))]
 
 
+class HeelDesc(C.Structure):
+    _fields_ = [("h_u", C.c_double), ("h_v", C.c_double), ("span_cm", C.c_double), ("n_bins", C.c_int32),
+                ("pad", C.c_int32), ("centers", C.POINTER(C.c_double)), ("rel_fluence", C.POINTER(C.c_double)),
+                ("bin_sizes", C.POINTER(C.c_int32)), ("energies_kev", C.POINTER(C.c_double)),
+                ("weights", C.POINTER(C.c_double))]
+
+
 class SourceDesc(C.Structure):
     _fields_ = [("field", C.c_int32), ("rotation", C.c_int32), ("rot_axis", C.c_int32),
                 ("n_angles", C.c_int32), ("position", C.c_double * 3), ("direction", C.c_double * 3),
@@ -89,7 +96,8 @@ class SourceDesc(C.Structure):
                 ("size_u", C.c_double), ("size_v", C.c_double), ("cos_half_angle", C.c_double),
                 ("isocenter", C.c_double * 3), ("scan_length_cm", C.c_double),
                 ("n_energies", C.c_int32), ("pad", C.c_int32),
-                ("energies_kev", C.POINTER(C.c_double)), ("weights", C.POINTER(C.c_double))]
+                ("energies_kev", C.POINTER(C.c_double)), ("weights", C.POINTER(C.c_double)),
+                ("heel", C.POINTER(HeelDesc))]
 
 
 class RunOut(C.Structure):

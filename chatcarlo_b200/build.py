@@ -34,9 +34,10 @@ NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", 
               "--use_fast_math", "-Xcompiler", "-fPIC", "-shared", "-cudart", "static"]
 
 
-# the precision reference: the engine tracking in FP64 (more registers per
+# the precision reference: the engine tracking and sampling in FP64 with FP64
+# tables and IEEE arithmetic (no fast-math intrinsics; more registers per
 # thread, so two blocks per SM)
-FP64_NVCC_FLAGS = NVCC_FLAGS + ["-DCC_TRACK_FP64", "-DCC_MIN_BLOCKS=2"]
+FP64_NVCC_FLAGS = [f for f in NVCC_FLAGS if f != "--use_fast_math"] + ["-DCC_TRACK_FP64", "-DCC_MIN_BLOCKS=2"]
 
 # the denoiser's kernels keep IEEE arithmetic (their gradients are checked
 # against an FP64 oracle)

@@ -46,28 +46,59 @@ constexpr int TABLE_N = 2000;            // F, A, S tables (materials.py:376-496
 constexpr int N_BUCKETS = 4096;          // uniform log-E index per material
 constexpr int RAY_BUCKETS = 1024;        // uniform-in-A index of each Rayleigh A(x) table
 constexpr int MAX_SCRATCH = 64;          // batches per launch
-constexpr float E_MIN_KEV = 1.0f;
-constexpr float E_MAX_KEV = 150.0f;
-constexpr float HC = 12.3984193f;        // keV Angstrom (physics.py:35)
-constexpr float MEC2 = 511.0f;           // keV (physics.py:34)
-constexpr float FLUOR_CUTOFF = 5.0f;     // keV (physics.py:38)
-constexpr float TWO_PI = 6.283185307179586f;
-
 // status bits
 constexpr unsigned ST_ENERGY = 1u, ST_RAYLEIGH_Q = 2u, ST_STEPS = 4u, ST_BOUNDS = 8u;
 
-// Tracking precision: positions, directions, distances and the geometry they
-// meet.  The engine tracks in FP32; a second build of this file with
-// -DCC_TRACK_FP64 tracks in FP64 with the same random numbers and the same
-// FP32 physics, so that each tally's cost of FP32 tracking can be measured
-// against it.
+// Precision.  The engine tracks and samples in FP32: positions, directions,
+// distances, energies, optical depths, cross-section lookups and the
+// samplers' arithmetic (tallies and the collision estimator are FP64
+// either way).  A second build of this file with -DCC_TRACK_FP64 does all of
+// that in FP64, with FP64 tables and the same random numbers (each 32-bit
+// draw turned into an FP64 uniform), and without fast-math intrinsics: the
+// FP64 reference against which every tally's cost of FP32 is measured.
+// P(x) is a floating literal of the build's precision.
 #ifdef CC_TRACK_FP64
 typedef double real;
+typedef double phys;
+struct __align__(16) PNode { double x, y, z, w; };
+#define P(x) x
 #else
 typedef float real;
+typedef float phys;
+typedef float4 PNode;
+#define P(x) x##f
 #endif
 __device__ __forceinline__ float rsqrt_r(float x) { return rsqrtf(x); }
 __device__ __forceinline__ double rsqrt_r(double x) { return rsqrt(x); }
+__device__ __forceinline__ float p_log(float x) { return __logf(x); }
+__device__ __forceinline__ double p_log(double x) { return log(x); }
+__device__ __forceinline__ float p_exp(float x) { return __expf(x); }
+__device__ __forceinline__ double p_exp(double x) { return exp(x); }
+__device__ __forceinline__ void p_sincos(float x, float* s, float* c) { __sincosf(x, s, c); }
+__device__ __forceinline__ void p_sincos(double x, double* s, double* c) { sincos(x, s, c); }
+__device__ __forceinline__ PNode ldg_node(const PNode* p) {
+#ifdef CC_TRACK_FP64
+    const double2 a = __ldg(reinterpret_cast<const double2*>(p)), b = __ldg(reinterpret_cast<const double2*>(p) + 1);
+    return PNode{a.x, a.y, b.x, b.y};
+#else
+    return __ldg(p);
+#endif
+}
+// a uniform draw in (0, 1] of the build's precision from the next 32 bits
+__device__ __forceinline__ phys uni(HistoryRng& r) {
+#ifdef CC_TRACK_FP64
+    return r.uniform_d();
+#else
+    return r.uniform();
+#endif
+}
+
+constexpr phys E_MIN_KEV = P(1.0);
+constexpr phys E_MAX_KEV = P(150.0);
+constexpr phys HC = P(12.3984193);        // keV Angstrom (physics.py:35)
+constexpr phys MEC2 = P(511.0);           // keV (physics.py:34)
+constexpr phys FLUOR_CUTOFF = P(5.0);     // keV (physics.py:38)
+constexpr phys TWO_PI = P(6.283185307179586);
 
 struct DevPrim {
     int type, material, axis, pad;
@@ -79,30 +110,30 @@ struct DevPrim {
 };
 
 struct DevMaterial {
-    float density;
+    phys density;
     int n_nodes, n_el, node_off;
     int elem_off, bucket_off;
-    float bucket_scale;
+    phys bucket_scale;
     int el_slot[MAX_ELEMS_PER_MAT];
 };
 
 struct DevElement {
-    float k_edge, k_prob, omega;
+    phys k_edge, k_prob, omega;
     int n_lines, emits, z;
-    float ray_scale;        // RAY_BUCKETS / A(x_end)
-    float line_e[8];
-    float line_cum[8];
+    phys ray_scale;        // RAY_BUCKETS / A(x_end)
+    phys line_e[8];
+    phys line_cum[8];
 };
 
 struct KTables {
-    const float4* nodes;        // 2 per node: {ln E, ln photo, ln Compton, ln Rayleigh}, {ln total, ln mu_en, ln h10, 0}
-    const float* elem_cum;      // per material [3][n_el - 1][n_nodes] normalised cumulative element weights
+    const PNode* nodes;        // 2 per node: {ln E, ln photo, ln Compton, ln Rayleigh}, {ln total, ln mu_en, ln h10, 0}
+    const phys* elem_cum;      // per material [3][n_el - 1][n_nodes] normalised cumulative element weights
     const unsigned short* bucket;
     const DevMaterial* mats;
     const DevElement* elems;
-    const float* sq;       // [n_elem][TABLE_N] S/Z
-    const float* rx;       // [n_elem][TABLE_N]
-    const float* ra;       // [n_elem][TABLE_N]
+    const phys* sq;       // [n_elem][TABLE_N] S/Z
+    const phys* rx;       // [n_elem][TABLE_N]
+    const phys* ra;       // [n_elem][TABLE_N]
     const int* ray_bucket; // [n_elem][RAY_BUCKETS + 1] last row with A <= bucket start
     int n_mat, n_elem;
 };
@@ -127,14 +158,24 @@ struct KGrid {
 
 struct KSource {
     int field, rotation, rot_axis, n_angles;
-    float pos[3], dir[3], u[3], v[3];
-    float sid, su, sv, cos_half;
-    float iso[3];
-    float scan;
+    phys pos[3], dir[3], u[3], v[3];
+    phys sid, su, sv, cos_half;
+    phys iso[3];
+    phys scan;
     int n_e;
-    const float* e;          // energies
-    const float* alias_p;    // alias table
+    const phys* e;          // energies
+    const phys* alias_p;    // alias table
     const int* alias_i;
+    // heel effect (source.py:130-149,195-207): heel_n bins along the anode
+    // axis; rejection on the relative fluence, then the bin's alias table
+    int heel_n, heel_lo, heel_hi;   // bins; first and last bin with fluence
+    phys h_u, h_v, span, bin_w;
+    const phys* heel_c;      // [heel_n] bin centres
+    const phys* heel_f;      // [heel_n] relative fluence
+    const int* heel_off;      // [heel_n + 1] each bin's first entry in the tables below
+    const phys* heel_e;      // energies
+    const phys* heel_q;      // alias probabilities
+    const int* heel_a;        // alias entries (table indices)
 };
 
 struct KRun {
@@ -190,7 +231,7 @@ __device__ __forceinline__ bool slab_inside(real o, real d, real h, real tol) {
     real a = fabs(o);
     if (a < h - tol) return true;
     if (a > h + tol) return false;
-    return o * d <= 0.0f;
+    return o * d <= P(0.0);
 }
 
 // Inside the ball |o| <= r (o with n components folded into o2 = |o|^2 and od = o.d).
@@ -198,7 +239,7 @@ __device__ __forceinline__ bool ball_inside(real o2, real od, real r, real tol) 
     real lo = fmax(r - tol, (real)0), hi = r + tol;
     if (o2 < lo * lo) return true;
     if (o2 > hi * hi) return false;
-    return od <= 0.0f;
+    return od <= P(0.0);
 }
 
 // Component k of a 3-vector held in registers.  Indexing a register array
@@ -219,7 +260,7 @@ __device__ __forceinline__ bool contains(const DevPrim& g, const real p[3], cons
         // scaled by the smallest semi-axis covers the tol band everywhere
         real u0 = o0 / g.h[0], u1 = o1 / g.h[1], u2 = o2 / g.h[2];
         return ball_inside(u0 * u0 + u1 * u1 + u2 * u2,
-                           u0 * d[0] / g.h[0] + u1 * d[1] / g.h[1] + u2 * d[2] / g.h[2], 1.0f, tol * g.r);
+                           u0 * d[0] / g.h[0] + u1 * d[1] / g.h[1] + u2 * d[2] / g.h[2], P(1.0), tol * g.r);
     } else {
         const int ax = g.axis;
         const int i0 = ax == 0 ? 1 : 0, i1 = ax == 2 ? 1 : 2;
@@ -243,9 +284,9 @@ __device__ __forceinline__ int locate(const KScene& s, const real p[3], const re
 __device__ __forceinline__ bool slab_pair(real o, real d, real inv, real lo, real hi, real tol,
                                           real& tmin, real& tmax) {
     real dlo = lo - o, dhi = hi - o;
-    if (fabs(dlo) <= tol) dlo = 0.0f;
-    if (fabs(dhi) <= tol) dhi = 0.0f;
-    if (fabs(d) < 1e-12f) return dlo <= 0.0f && dhi >= 0.0f;
+    if (fabs(dlo) <= tol) dlo = P(0.0);
+    if (fabs(dhi) <= tol) dhi = P(0.0);
+    if (fabs(d) < P(1e-12)) return dlo <= P(0.0) && dhi >= P(0.0);
     real ta = dlo * inv, tb = dhi * inv;
     tmin = fmax(tmin, fmin(ta, tb));
     tmax = fmin(tmax, fmax(ta, tb));
@@ -272,17 +313,17 @@ __device__ __forceinline__ real prim_next(const DevPrim& g, const real p[3], con
         real o2 = ox * ox + oy * oy + oz * oz;
         real lo = fmax(g.r - eps, (real)0), hi = g.r + eps;
         if (o2 >= lo * lo && o2 <= hi * hi) {          // on the surface
-            if (b <= 0.0f) take_root(-2.0f * b, eps, best);
+            if (b <= P(0.0)) take_root(-P(2.0) * b, eps, best);
             return best;
         }
         // squared distance of the line from the centre, computed without cancellation
         real qx = ox - b * d[0], qy = oy - b * d[1], qz = oz - b * d[2];
         real disc = g.r2 - (qx * qx + qy * qy + qz * qz);
-        if (disc < 0.0f) return best;
+        if (disc < P(0.0)) return best;
         real sq = sqrt(disc);
         real c = o2 - g.r2;
         real q = -(b + copysign(sq, b));
-        real t1 = q, t2 = (q != 0.0f) ? c / q : 0.0f;
+        real t1 = q, t2 = (q != P(0.0)) ? c / q : P(0.0);
         take_root(t1, eps, best);
         take_root(t2, eps, best);
         return best;
@@ -294,18 +335,18 @@ __device__ __forceinline__ real prim_next(const DevPrim& g, const real p[3], con
         real b = ux * vx + uy * vy + uz * vz;
         real u2 = ux * ux + uy * uy + uz * uz;
         real tl = eps * g.r;
-        real lo = fmax(1.0f - tl, (real)0), hi = 1.0f + tl;
+        real lo = fmax(P(1.0) - tl, (real)0), hi = P(1.0) + tl;
         if (u2 >= lo * lo && u2 <= hi * hi) {            // on the surface
-            if (b <= 0.0f) take_root(-2.0f * b / a, eps, best);
+            if (b <= P(0.0)) take_root(-P(2.0) * b / a, eps, best);
             return best;
         }
-        real inva = 1.0f / a;
+        real inva = P(1.0) / a;
         real ex = ux - b * inva * vx, ey = uy - b * inva * vy, ez = uz - b * inva * vz;
-        real disc = (1.0f - (ex * ex + ey * ey + ez * ez)) * a;   // b^2 - a c without cancellation
-        if (disc < 0.0f) return best;
+        real disc = (P(1.0) - (ex * ex + ey * ey + ez * ez)) * a;   // b^2 - a c without cancellation
+        if (disc < P(0.0)) return best;
         real q = -(b + copysign(sqrt(disc), b));
         take_root(q * inva, eps, best);
-        take_root((q != 0.0f) ? (u2 - 1.0f) / q : 0.0f, eps, best);
+        take_root((q != P(0.0)) ? (u2 - P(1.0)) / q : P(0.0), eps, best);
         return best;
     } else {
         const int ax = g.axis;
@@ -319,20 +360,20 @@ __device__ __forceinline__ real prim_next(const DevPrim& g, const real p[3], con
         real b = a0 * dx + a1 * dy;
         real lo = fmax(g.r - eps, (real)0), hi = g.r + eps;
         if (rho2 >= lo * lo && rho2 <= hi * hi) {      // on the side surface
-            if (b > 0.0f) return best;
-            tmin = 0.0f;
-            tmax = a < 1e-12f ? INFINITY : -2.0f * b / a;
-        } else if (a < 1e-12f) {
-            if (cc > 0.0f) return best;        // parallel to the axis, outside the radius
+            if (b > P(0.0)) return best;
+            tmin = P(0.0);
+            tmax = a < P(1e-12) ? INFINITY : -P(2.0) * b / a;
+        } else if (a < P(1e-12)) {
+            if (cc > P(0.0)) return best;        // parallel to the axis, outside the radius
             tmin = -INFINITY; tmax = INFINITY;
         } else {
-            real inva = 1.0f / a;
+            real inva = P(1.0) / a;
             real ex = a0 - b * inva * dx, ey = a1 - b * inva * dy;
             real disc = (g.r2 - (ex * ex + ey * ey)) * a;   // b^2 - a c without cancellation
-            if (disc < 0.0f) return best;
+            if (disc < P(0.0)) return best;
             real sq = sqrt(disc);
             real q = -(b + copysign(sq, b));
-            real r1 = q * inva, r2 = (q != 0.0f) ? cc / q : 0.0f;
+            real r1 = q * inva, r2 = (q != P(0.0)) ? cc / q : P(0.0);
             tmin = fmin(r1, r2); tmax = fmax(r1, r2);
         }
         if (!slab_pair(aw, dw, comp(inv, ax), -g.hh, g.hh, eps, tmin, tmax)) return best;
@@ -347,8 +388,8 @@ __device__ __forceinline__ real world_exit(const KScene& s, const real p[3], con
     real t = INFINITY;
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-        if (d[k] > 1e-12f) t = fmin(t, (s.whi[k] - p[k]) * inv[k]);
-        else if (d[k] < -1e-12f) t = fmin(t, (s.wlo[k] - p[k]) * inv[k]);
+        if (d[k] > P(1e-12)) t = fmin(t, (s.whi[k] - p[k]) * inv[k]);
+        else if (d[k] < -P(1e-12)) t = fmin(t, (s.wlo[k] - p[k]) * inv[k]);
     }
     return fmax(t, (real)0);
 }
@@ -357,15 +398,15 @@ __device__ __forceinline__ real world_exit(const KScene& s, const real p[3], con
 // tables
 // ---------------------------------------------------------------------------
 
-struct Lookup { int idx; float frac; };
+struct Lookup { int idx; phys frac; };
 
-__device__ __forceinline__ Lookup energy_index(const KTables& T, const DevMaterial& m, float loge) {
+__device__ __forceinline__ Lookup energy_index(const KTables& T, const DevMaterial& m, phys loge) {
     int b = (int)(loge * m.bucket_scale);
     b = max(0, min(N_BUCKETS - 1, b));
     int i = __ldg(T.bucket + m.bucket_off + b);       // last node with log E <= bucket start
-    const float4* x = T.nodes + 2 * (size_t)m.node_off;
+    const PNode* x = T.nodes + 2 * (size_t)m.node_off;
     int last = m.n_nodes - 2;
-    float x0 = __ldg(&x[2 * i].x), x1 = __ldg(&x[2 * i + 2].x);
+    phys x0 = __ldg(&x[2 * i].x), x1 = __ldg(&x[2 * i + 2].x);
     while (i < last && x1 < loge) {
         ++i;
         x0 = x1;
@@ -377,32 +418,32 @@ __device__ __forceinline__ Lookup energy_index(const KTables& T, const DevMateri
     return L;
 }
 
-__device__ __forceinline__ float mu_total(const KTables& T, const DevMaterial& m, const Lookup& L) {
-    const float4* r = T.nodes + 2 * ((size_t)m.node_off + L.idx);
-    float a = __ldg(&r[1].x), b = __ldg(&r[3].x);
-    return m.density * __expf(a + L.frac * (b - a));
+__device__ __forceinline__ phys mu_total(const KTables& T, const DevMaterial& m, const Lookup& L) {
+    const PNode* r = T.nodes + 2 * ((size_t)m.node_off + L.idx);
+    phys a = __ldg(&r[1].x), b = __ldg(&r[3].x);
+    return m.density * p_exp(a + L.frac * (b - a));
 }
 
 __device__ __forceinline__ void parts(const KTables& T, const DevMaterial& m, const Lookup& L,
-                                      float& ph, float& co, float& ra) {
-    const float4* r = T.nodes + 2 * ((size_t)m.node_off + L.idx);
-    float4 a = __ldg(r), b = __ldg(r + 2);
-    ph = __expf(a.y + L.frac * (b.y - a.y));
-    co = __expf(a.z + L.frac * (b.z - a.z));
-    ra = __expf(a.w + L.frac * (b.w - a.w));
+                                      phys& ph, phys& co, phys& ra) {
+    const PNode* r = T.nodes + 2 * ((size_t)m.node_off + L.idx);
+    PNode a = ldg_node(r), b = ldg_node(r + 2);
+    ph = p_exp(a.y + L.frac * (b.y - a.y));
+    co = p_exp(a.z + L.frac * (b.z - a.z));
+    ra = p_exp(a.w + L.frac * (b.w - a.w));
 }
 
 // Element of the material that takes the interaction of kind k (0 photo,
 // 1 Compton, 2 Rayleigh), chosen with probability w_i sigma_i / sum
 // (physics.py:78-92, 138-152, 223-236).  Returns the element slot.
-__device__ __noinline__ int pick_element(const KTables& T, const DevMaterial& m, const Lookup& L, int k, float r) {
+__device__ __noinline__ int pick_element(const KTables& T, const DevMaterial& m, const Lookup& L, int k, phys r) {
     const int n_el = m.n_el;
     if (n_el == 1) return m.el_slot[0];
     // cumulative sums of w_i sigma_i / sum_j w_j sigma_j, tabulated per node in
     // FP64 on the host and interpolated linearly: first i with r <= cum_i
-    const float* c = T.elem_cum + m.elem_off + (size_t)k * (n_el - 1) * m.n_nodes + L.idx;
+    const phys* c = T.elem_cum + m.elem_off + (size_t)k * (n_el - 1) * m.n_nodes + L.idx;
     for (int i = 0; i < n_el - 1; ++i) {
-        float c0 = __ldg(c), c1 = __ldg(c + 1);
+        phys c0 = __ldg(c), c1 = __ldg(c + 1);
         if (r <= c0 + L.frac * (c1 - c0)) return m.el_slot[i];
         c += m.n_nodes;
     }
@@ -413,11 +454,11 @@ __device__ __noinline__ int pick_element(const KTables& T, const DevMaterial& m,
 // transport.py:59-64) and h*(10)/Phi (dose_coefficients.py:32-42), both
 // linear in ln E between the material's nodes.
 __device__ __forceinline__ void tally_weights(const KTables& T, const DevMaterial& m, const Lookup& L,
-                                              float E, float& wk, float& wh) {
-    const float4* r = T.nodes + 2 * ((size_t)m.node_off + L.idx);
-    float4 a = __ldg(r + 1), b = __ldg(r + 3);
-    wk = E * m.density * __expf(a.y + L.frac * (b.y - a.y));
-    wh = __expf(a.z + L.frac * (b.z - a.z));
+                                              phys E, phys& wk, phys& wh) {
+    const PNode* r = T.nodes + 2 * ((size_t)m.node_off + L.idx);
+    PNode a = ldg_node(r + 1), b = ldg_node(r + 3);
+    wk = E * m.density * p_exp(a.y + L.frac * (b.y - a.y));
+    wh = p_exp(a.z + L.frac * (b.z - a.z));
 }
 
 // ---------------------------------------------------------------------------
@@ -425,69 +466,69 @@ __device__ __forceinline__ void tally_weights(const KTables& T, const DevMateria
 // ---------------------------------------------------------------------------
 
 // S(Z,q)/Z on q = {0} U linspace(1e-3, 20, 1999) (materials.py:484-496), np.interp.
-__device__ __forceinline__ float s_over_z(const float* s, float q) {
-    const float q1 = 1e-3f;
-    const float dq = (20.0f - 1e-3f) / 1998.0f;
+__device__ __forceinline__ phys s_over_z(const phys* s, phys q) {
+    const phys q1 = P(1e-3);
+    const phys dq = (P(20.0) - P(1e-3)) / P(1998.0);
     if (q <= q1) return __ldg(s + 1) * (q / q1);
-    float u = (q - q1) / dq;
+    phys u = (q - q1) / dq;
     int j = (int)u;
     if (j >= TABLE_N - 2) return __ldg(s + TABLE_N - 1);
-    float f = u - (float)j;
-    float a = __ldg(s + 1 + j), b = __ldg(s + 2 + j);
+    phys f = u - (phys)j;
+    phys a = __ldg(s + 1 + j), b = __ldg(s + 2 + j);
     return a + f * (b - a);
 }
 
 // Bound Compton: Kahn-type KN proposal with S(Z,q)/Z rejection (physics.py:41-56, 95-135).
-__device__ __forceinline__ void sample_compton(const float* sz, float E, HistoryRng& rng, float& eps_out, float& cos_out) {
-    float alpha = E / MEC2;
-    float emin = 1.0f / (1.0f + 2.0f * alpha);
-    float env = 1.0f / emin + emin;
-    float qscale = E / HC;
+__device__ __forceinline__ void sample_compton(const phys* sz, phys E, HistoryRng& rng, phys& eps_out, phys& cos_out) {
+    phys alpha = E / MEC2;
+    phys emin = P(1.0) / (P(1.0) + P(2.0) * alpha);
+    phys env = P(1.0) / emin + emin;
+    phys qscale = E / HC;
     for (int trial = 0; trial < 100000; ++trial) {
-        float x1 = rng.uniform(), x2 = rng.uniform(), x3 = rng.uniform();
-        float eps = emin + x1 * (1.0f - emin);
-        float c = 1.0f - (1.0f / eps - 1.0f) / alpha;
-        float g = 1.0f / eps + eps - (1.0f - c * c);
+        phys x1 = uni(rng), x2 = uni(rng), x3 = uni(rng);
+        phys eps = emin + x1 * (P(1.0) - emin);
+        phys c = P(1.0) - (P(1.0) / eps - P(1.0)) / alpha;
+        phys g = P(1.0) / eps + eps - (P(1.0) - c * c);
         if (x2 * env > g) continue;
-        float cc = fminf(fmaxf(c, -1.0f), 1.0f);
-        float q = qscale * sqrtf(0.5f * (1.0f - cc));
+        phys cc = fmin(fmax(c, -P(1.0)), P(1.0));
+        phys q = qscale * sqrt(P(0.5) * (P(1.0) - cc));
         if (x3 <= s_over_z(sz, q)) { eps_out = eps; cos_out = c; return; }
     }
-    eps_out = 1.0f; cos_out = 1.0f;
+    eps_out = P(1.0); cos_out = P(1.0);
 }
 
 // Rayleigh: inverse of A(x) then (1+cos^2)/2 rejection (physics.py:281-351).
 // The row of a target A comes from a uniform-in-A bucket index, then a
 // short binary search inside the bucket.
-__device__ __forceinline__ bool sample_rayleigh(const float* rx, const float* ra, const int* bucket, float scale,
-                                             float E, HistoryRng& rng, float& cos_out) {
-    float xmax = (E / HC) * (E / HC);
+__device__ __forceinline__ bool sample_rayleigh(const phys* rx, const phys* ra, const int* bucket, phys scale,
+                                             phys E, HistoryRng& rng, phys& cos_out) {
+    phys xmax = (E / HC) * (E / HC);
     if (xmax > __ldg(rx + TABLE_N - 1)) return false;
     // A(x_max): x grid is q^2 with q uniform on [0, 20]
-    const float dq = 20.0f / (float)(TABLE_N - 1);
-    int j = (int)(sqrtf(xmax) / dq);
+    const phys dq = P(20.0) / (phys)(TABLE_N - 1);
+    int j = (int)(sqrt(xmax) / dq);
     j = min(max(j, 0), TABLE_N - 2);
     while (j > 0 && __ldg(rx + j) > xmax) --j;
     while (j < TABLE_N - 2 && __ldg(rx + j + 1) < xmax) ++j;
-    float xa = __ldg(rx + j), xb = __ldg(rx + j + 1);
-    float aa = __ldg(ra + j), ab = __ldg(ra + j + 1);
-    float a_cut = aa + (xmax - xa) / (xb - xa) * (ab - aa);
+    phys xa = __ldg(rx + j), xb = __ldg(rx + j + 1);
+    phys aa = __ldg(ra + j), ab = __ldg(ra + j + 1);
+    phys a_cut = aa + (xmax - xa) / (xb - xa) * (ab - aa);
     for (int trial = 0; trial < 100000; ++trial) {
-        float target = rng.uniform() * a_cut;
+        phys target = uni(rng) * a_cut;
         int bk = min((int)(target * scale), RAY_BUCKETS - 1);
         int lo = __ldg(bucket + bk), hi = min(__ldg(bucket + bk + 1) + 1, TABLE_N - 1);
         while (hi - lo > 1) {                    // ra[lo] <= target < ra[hi]
             int mid = (lo + hi) >> 1;
             if (__ldg(ra + mid) <= target) lo = mid; else hi = mid;
         }
-        float a0 = __ldg(ra + lo), a1 = __ldg(ra + lo + 1);
-        float x0 = __ldg(rx + lo), x1 = __ldg(rx + lo + 1);
-        float x = (a1 > a0) ? x0 + (target - a0) / (a1 - a0) * (x1 - x0) : x0;
-        x = fminf(x, xmax);
-        float c = fminf(fmaxf(1.0f - 2.0f * x / xmax, -1.0f), 1.0f);
-        if (rng.uniform() <= 0.5f * (1.0f + c * c)) { cos_out = c; return true; }
+        phys a0 = __ldg(ra + lo), a1 = __ldg(ra + lo + 1);
+        phys x0 = __ldg(rx + lo), x1 = __ldg(rx + lo + 1);
+        phys x = (a1 > a0) ? x0 + (target - a0) / (a1 - a0) * (x1 - x0) : x0;
+        x = fmin(x, xmax);
+        phys c = fmin(fmax(P(1.0) - P(2.0) * x / xmax, -P(1.0)), P(1.0));
+        if (uni(rng) <= P(0.5) * (P(1.0) + c * c)) { cos_out = c; return true; }
     }
-    cos_out = 1.0f;
+    cos_out = P(1.0);
     return true;
 }
 
@@ -496,31 +537,31 @@ __device__ __forceinline__ bool sample_rayleigh(const float* rx, const float* ra
 // relaxes radiatively with probability omega_K and emits one of the K lines
 // (cumulative line probabilities), which leaves only when at or above the
 // 5 keV cut-off.  Returns the emitted line's energy, 0 when none.
-__device__ __forceinline__ float sample_k_line(const DevElement& el, float E, int fluorescence, HistoryRng& rng) {
-    if (!(fluorescence && el.emits && E > el.k_edge)) return 0.0f;
-    const bool is_k = rng.uniform() < el.k_prob;
-    const bool is_rad = rng.uniform() < el.omega;
-    if (!(is_k && is_rad)) return 0.0f;
-    const float rl = rng.uniform();
+__device__ __forceinline__ phys sample_k_line(const DevElement& el, phys E, int fluorescence, HistoryRng& rng) {
+    if (!(fluorescence && el.emits && E > el.k_edge)) return P(0.0);
+    const bool is_k = uni(rng) < el.k_prob;
+    const bool is_rad = uni(rng) < el.omega;
+    if (!(is_k && is_rad)) return P(0.0);
+    const phys rl = uni(rng);
     int li = el.n_lines - 1;
     for (int k = 0; k < el.n_lines; ++k) if (rl <= el.line_cum[k]) { li = k; break; }
-    return el.line_e[li] >= FLUOR_CUTOFF ? el.line_e[li] : 0.0f;
+    return el.line_e[li] >= FLUOR_CUTOFF ? el.line_e[li] : P(0.0);
 }
 
 // New direction from cos(theta) and a uniform azimuth (physics.py:354-367).
 struct real3 { real x, y, z; };
 
-__device__ __noinline__ real3 scatter_dir(real dx, real dy, real dz, float cost, float phi) {
+__device__ __noinline__ real3 scatter_dir(real dx, real dy, real dz, phys cost, phys phi) {
     const real d[3] = {dx, dy, dz};
     real sint = sqrt(fmax((real)0, (real)1 - (real)cost * (real)cost));
     real upx, upy, upz;
-    if (fabs(d[2]) < (real)0.999f) { upx = 0; upy = 0; upz = 1; } else { upx = 1; upy = 0; upz = 0; }
+    if (fabs(d[2]) < (real)P(0.999)) { upx = 0; upy = 0; upz = 1; } else { upx = 1; upy = 0; upz = 0; }
     real ux = upy * d[2] - upz * d[1], uy = upz * d[0] - upx * d[2], uz = upx * d[1] - upy * d[0];
     real inv = rsqrt_r(ux * ux + uy * uy + uz * uz);
     ux *= inv; uy *= inv; uz *= inv;
     real vx = d[1] * uz - d[2] * uy, vy = d[2] * ux - d[0] * uz, vz = d[0] * uy - d[1] * ux;
-    float sp, cp;
-    __sincosf(phi, &sp, &cp);
+    phys sp, cp;
+    p_sincos(phi, &sp, &cp);
     real a = sint * cp, b = sint * sp;
     real nx = a * ux + b * vx + cost * d[0];
     real ny = a * uy + b * vy + cost * d[1];
@@ -529,16 +570,16 @@ __device__ __noinline__ real3 scatter_dir(real dx, real dy, real dz, float cost,
     return real3{nx * n, ny * n, nz * n};
 }
 
-__device__ __forceinline__ void scatter_direction(real d[3], float cost, float phi) {
+__device__ __forceinline__ void scatter_direction(real d[3], phys cost, phys phi) {
     real3 r = scatter_dir(d[0], d[1], d[2], cost, phi);
     d[0] = r.x; d[1] = r.y; d[2] = r.z;
 }
 
 __device__ __forceinline__ void isotropic(real d[3], HistoryRng& rng) {
-    float c = 2.0f * rng.uniform() - 1.0f;
-    float s = sqrtf(fmaxf(0.0f, 1.0f - c * c));
-    float sp, cp;
-    __sincosf(TWO_PI * rng.uniform(), &sp, &cp);
+    phys c = P(2.0) * uni(rng) - P(1.0);
+    phys s = sqrt(fmax(P(0.0), P(1.0) - c * c));
+    phys sp, cp;
+    p_sincos(TWO_PI * uni(rng), &sp, &cp);
     d[0] = s * cp; d[1] = s * sp; d[2] = c;
 }
 
@@ -566,13 +607,13 @@ __device__ __forceinline__ void score(double* tally, int tally32, int v, real wk
 // no part of it lies inside.
 __device__ __forceinline__ bool clip_to_grid(const KGrid& G, const real p[3], const real d[3],
                                              const real invd[3], real s, real& t0, real& t1) {
-    t0 = 0.0f;
+    t0 = P(0.0);
     t1 = s;
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
         real lo = G.o[k];
         real hi = G.o[k] + G.h * (real)(k == 0 ? G.nx : (k == 1 ? G.ny : G.nz));
-        if (fabs(d[k]) < 1e-12f) {
+        if (fabs(d[k]) < P(1e-12)) {
             if (p[k] < lo || p[k] >= hi) return false;
         } else {
             real ta = (lo - p[k]) * invd[k], tb = (hi - p[k]) * invd[k];
@@ -606,13 +647,13 @@ __device__ __forceinline__ void walk_axis(real o, real h, real inv_h, int n, rea
                                           int& s, real& tm, real& td) {
     real x = (p + d * t0 - o) * inv_h;
     i = max(0, min(n - 1, (int)floor(x)));
-    if (d > 1e-12f) {
-        real inv = 1.0f / d;
+    if (d > P(1e-12)) {
+        real inv = P(1.0) / d;
         s = 1;
         tm = (o + (real)(i + 1) * h - p) * inv;
         td = h * inv;
-    } else if (d < -1e-12f) {
-        real inv = 1.0f / d;
+    } else if (d < -P(1e-12)) {
+        real inv = P(1.0) / d;
         s = -1;
         tm = (o + (real)i * h - p) * inv;
         td = -h * inv;
@@ -629,7 +670,7 @@ __device__ __forceinline__ void walk_axis(real o, real h, real inv_h, int n, rea
 // selects: a register array indexed by the crossing axis would live in
 // local memory.
 __device__ __forceinline__ int walk_range(const KGrid& G, double* tally, const real p[3], const real d[3],
-                                          real t0, real t1, float wk, float wh) {
+                                          real t0, real t1, phys wk, phys wh) {
     int ix, iy, iz, sx, sy, sz;
     real mx, my, mz, dx, dy, dz;
     walk_axis(G.o[0], G.h, G.inv_h, G.nx, p[0], d[0], t0, ix, sx, mx, dx);
@@ -649,7 +690,7 @@ __device__ __forceinline__ int walk_range(const KGrid& G, double* tally, const r
         const bool ax2 = !ax0 && !ax1;
         real tn = fmin(ax0 ? mx : (ax1 ? my : mz), t1);
         real len = tn - t;
-        if (len > 0.0f) {
+        if (len > P(0.0)) {
             score(tally, G.tally32, v, wk * len, wh * len);
             ++visits;
         }
@@ -672,7 +713,7 @@ __device__ __forceinline__ int walk_range(const KGrid& G, double* tally, const r
 struct SegRec {
     real p[3], d[3];
     real t0, t1;
-    float wk, wh;
+    phys wk, wh;
     int batch, m;           // scratch slot; pieces of at most TALLY_PIECE visits
 };
 
@@ -680,62 +721,114 @@ struct SegRec {
 // source (source.py:67-210)
 // ---------------------------------------------------------------------------
 
-__device__ __forceinline__ void rotate(float v[3], int axis, float ca, float sa) {
+__device__ __forceinline__ void rotate(phys v[3], int axis, phys ca, phys sa) {
     // Rodrigues rotation about a coordinate axis
-    float a0 = v[0], a1 = v[1], a2 = v[2];
+    phys a0 = v[0], a1 = v[1], a2 = v[2];
     if (axis == 0) { v[1] = a1 * ca - a2 * sa; v[2] = a1 * sa + a2 * ca; }
     else if (axis == 1) { v[0] = a0 * ca + a2 * sa; v[2] = -a0 * sa + a2 * ca; }
     else { v[0] = a0 * ca - a1 * sa; v[1] = a0 * sa + a1 * ca; }
 }
 
-__device__ __forceinline__ void sample_source(const KSource& S, HistoryRng& rng, real p[3], real d[3], float& E) {
-    float pos[3] = {S.pos[0], S.pos[1], S.pos[2]};
-    float dir[3] = {S.dir[0], S.dir[1], S.dir[2]};
-    float u[3] = {S.u[0], S.u[1], S.u[2]};
-    float v[3] = {S.v[0], S.v[1], S.v[2]};
+// np.interp(s, centres, fluence): clamped to the end values outside.
+__device__ __forceinline__ phys heel_fluence(const KSource& S, phys s) {
+    const int n = S.heel_n;
+    if (s <= __ldg(S.heel_c)) return __ldg(S.heel_f);
+    if (s >= __ldg(S.heel_c + n - 1)) return __ldg(S.heel_f + n - 1);
+    int lo = 0, hi = n - 1;                  // c[lo] < s < c[hi]
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (__ldg(S.heel_c + mid) <= s) lo = mid; else hi = mid;
+    }
+    const phys c0 = __ldg(S.heel_c + lo), c1 = __ldg(S.heel_c + hi);
+    const phys f0 = __ldg(S.heel_f + lo), f1 = __ldg(S.heel_f + hi);
+    return f0 + (s - c0) / (c1 - c0) * (f1 - f0);
+}
+
+// Energy of a photon at heel coordinate s: the alias table of its bin,
+// clamped to the bins that have fluence (source.py:195-207).
+__device__ __forceinline__ phys heel_energy(const KSource& S, phys s, HistoryRng& rng) {
+    int b = (int)((s + S.span) / S.bin_w);
+    b = min(max(b, 0), S.heel_n - 1);
+    b = min(max(b, S.heel_lo), S.heel_hi);
+    const int off = __ldg(S.heel_off + b), nb = __ldg(S.heel_off + b + 1) - off;
+    const phys r = uni(rng) * (phys)nb;
+    const int i = min((int)r, nb - 1);
+    const int pick = (r - (phys)i <= __ldg(S.heel_q + off + i)) ? off + i : __ldg(S.heel_a + off + i);
+    return __ldg(S.heel_e + pick);
+}
+
+constexpr int HEEL_MAX_TRIALS = 100000;
+
+// HEEL: the source may carry the heel effect (a separate instantiation, so
+// that the kernels of sources without it keep their registers).
+template <bool HEEL>
+__device__ __forceinline__ void sample_source(const KSource& S, HistoryRng& rng, real p[3], real d[3], phys& E) {
+    phys pos[3] = {S.pos[0], S.pos[1], S.pos[2]};
+    phys dir[3] = {S.dir[0], S.dir[1], S.dir[2]};
+    phys u[3] = {S.u[0], S.u[1], S.u[2]};
+    phys v[3] = {S.v[0], S.v[1], S.v[2]};
     if (S.rotation) {
-        float ang;
+        phys ang;
         if (S.n_angles > 0) {
             uint32_t k = (uint32_t)(((uint64_t)rng.next_u32() * (uint64_t)S.n_angles) >> 32);
-            ang = TWO_PI * (float)k / (float)S.n_angles;
+            ang = TWO_PI * (phys)k / (phys)S.n_angles;
         } else {
-            ang = TWO_PI * (rng.uniform() - 0.5f) + 3.14159265358979f;
+            ang = TWO_PI * (uni(rng) - P(0.5)) + P(3.14159265358979);
         }
-        float sa, ca;
-        __sincosf(ang, &sa, &ca);
-        float rel[3] = {pos[0] - S.iso[0], pos[1] - S.iso[1], pos[2] - S.iso[2]};
+        phys sa, ca;
+        p_sincos(ang, &sa, &ca);
+        phys rel[3] = {pos[0] - S.iso[0], pos[1] - S.iso[1], pos[2] - S.iso[2]};
         rotate(rel, S.rot_axis, ca, sa);
         rotate(dir, S.rot_axis, ca, sa);
         rotate(u, S.rot_axis, ca, sa);
         rotate(v, S.rot_axis, ca, sa);
         pos[0] = S.iso[0] + rel[0]; pos[1] = S.iso[1] + rel[1]; pos[2] = S.iso[2] + rel[2];
-        if (S.scan > 0.0f) {
-            float shift = S.scan * (rng.uniform() - 0.5f);
-            pos[0] += S.rot_axis == 0 ? shift : 0.0f;
-            pos[1] += S.rot_axis == 1 ? shift : 0.0f;
-            pos[2] += S.rot_axis == 2 ? shift : 0.0f;
+        if (S.scan > P(0.0)) {
+            phys shift = S.scan * (uni(rng) - P(0.5));
+            pos[0] += S.rot_axis == 0 ? shift : P(0.0);
+            pos[1] += S.rot_axis == 1 ? shift : P(0.0);
+            pos[2] += S.rot_axis == 2 ? shift : P(0.0);
         }
     }
+    const bool heel = HEEL && S.heel_n > 0 && S.field != CC_FIELD_PARALLEL;
+    phys s_heel = P(0.0);
     if (S.field == CC_FIELD_CONE) {
-        float c = S.cos_half + (1.0f - S.cos_half) * (1.0f - rng.uniform());
-        float sp, cp;
-        __sincosf(TWO_PI * rng.uniform(), &sp, &cp);
-        float s = sqrtf(fmaxf(0.0f, 1.0f - c * c));
+        phys c, sp, cp;
+        for (int trial = 0; ; ++trial) {
+            c = S.cos_half + (P(1.0) - S.cos_half) * (P(1.0) - uni(rng));
+            p_sincos(TWO_PI * uni(rng), &sp, &cp);
+            if (!heel) break;
+            // the direction's offset along the heel axis on the SID plane
+            s_heel = S.sid * (sqrt(fmax(P(0.0), P(1.0) - c * c)) / c) * (cp * S.h_u + sp * S.h_v);
+            if (uni(rng) < heel_fluence(S, s_heel) || trial >= HEEL_MAX_TRIALS) break;
+        }
+        phys s = sqrt(fmax(P(0.0), P(1.0) - c * c));
         for (int k = 0; k < 3; ++k) { p[k] = pos[k]; d[k] = c * dir[k] + s * cp * u[k] + s * sp * v[k]; }
     } else if (S.field == CC_FIELD_PARALLEL) {
-        float a = S.su * (rng.uniform() - 0.5f), b = S.sv * (rng.uniform() - 0.5f);
+        phys a = S.su * (uni(rng) - P(0.5)), b = S.sv * (uni(rng) - P(0.5));
         for (int k = 0; k < 3; ++k) { p[k] = pos[k] + a * u[k] + b * v[k]; d[k] = dir[k]; }
     } else {
-        float a = S.su * (rng.uniform() - 0.5f), b = S.sv * (rng.uniform() - 0.5f);
-        float t[3];
+        phys a, b;
+        for (int trial = 0; ; ++trial) {
+            a = S.su * (uni(rng) - P(0.5));
+            b = S.sv * (uni(rng) - P(0.5));
+            if (!heel) break;
+            s_heel = a * S.h_u + b * S.h_v;
+            if (uni(rng) < heel_fluence(S, s_heel) || trial >= HEEL_MAX_TRIALS) break;
+        }
+        phys t[3];
         for (int k = 0; k < 3; ++k) t[k] = dir[k] * S.sid + a * u[k] + b * v[k];
-        float inv = rsqrtf(t[0] * t[0] + t[1] * t[1] + t[2] * t[2]);
+        phys inv = rsqrt(t[0] * t[0] + t[1] * t[1] + t[2] * t[2]);
         for (int k = 0; k < 3; ++k) { p[k] = pos[k]; d[k] = t[k] * inv; }
     }
+    if (heel) {
+        E = heel_energy(S, s_heel, rng);
+        return;
+    }
     // discrete spectrum by Walker's alias method
-    float r = rng.uniform() * (float)S.n_e;
+    phys r = uni(rng) * (phys)S.n_e;
     int i = min((int)r, S.n_e - 1);
-    float f = r - (float)i;
+    phys f = r - (phys)i;
     int pick = (f <= __ldg(S.alias_p + i)) ? i : __ldg(S.alias_i + i);
     E = __ldg(S.e + pick);
 }
@@ -836,7 +929,7 @@ __device__ __forceinline__ void score_warp_segments(const KGrid& G, const SegRec
 #define CC_MIN_BLOCKS 4
 #endif
 
-template <bool FROM_SOURCE, bool TALLY>
+template <bool FROM_SOURCE, bool TALLY, bool HEEL = false>
 __global__ void __launch_bounds__(BLOCK, CC_MIN_BLOCKS)
 transport_kernel(const KTables T, const KScene S, const KGrid G, const KSource SRC, const KRun R) {
     extern __shared__ double s_edep[];             // [n_scratch][n_mat]
@@ -862,7 +955,7 @@ transport_kernel(const KTables T, const KScene S, const KGrid G, const KSource S
     bool live = false;
     long long h = 0;
     real p[3], d[3];
-    float E = 0.f, tau = 0.f;
+    phys E = P(0.), tau = P(0.);
     int nsc = 0, mat = -1, batch = 0;
     int steps = 0;
     HistoryRng rng;
@@ -890,15 +983,15 @@ transport_kernel(const KTables T, const KScene S, const KGrid G, const KSource S
                 batch = (int)(h / R.batch_size);
                 if (batch >= R.n_scratch) batch = R.n_scratch - 1;
                 if (FROM_SOURCE) {
-                    sample_source(SRC, rng, p, d, E);
+                    sample_source<HEEL>(SRC, rng, p, d, E);
                 } else {
                     for (int k = 0; k < 3; ++k) {
                         p[k] = (real)R.pos[3 * h + k];
                         d[k] = (real)R.dir[3 * h + k];
                     }
-                    E = (float)R.energy[h];
+                    E = (phys)R.energy[h];
                 }
-                tau = -__logf(rng.uniform());
+                tau = -p_log(uni(rng));
                 nsc = 0;
                 mat = -1;
                 steps = 0;
@@ -912,11 +1005,11 @@ transport_kernel(const KTables T, const KScene S, const KGrid G, const KSource S
         bool go = live;
         bool interact = false, escape = false;
         real s = 0, t0 = 0, t1 = 0;
-        float tau_b = 0.f, loge = 0.f, wk = 0.f, wh = 0.f;
+        phys tau_b = P(0.), loge = P(0.), wk = P(0.), wh = P(0.);
         int tal_n = 0;
         Lookup L;
         L.idx = 0;
-        L.frac = 0.f;
+        L.frac = P(0.);
         if (go) {
             ++steps;
             if (mat < 0) mat = locate(S, p, d);
@@ -930,18 +1023,18 @@ transport_kernel(const KTables T, const KScene S, const KGrid G, const KSource S
         }
         if (go) {
             const DevMaterial& M = T.mats[mat];
-            loge = __logf(E);
+            loge = p_log(E);
             L = energy_index(T, M, loge);
-            float mu = mu_total(T, M, L);
+            phys mu = mu_total(T, M, L);
             const real invd[3] = {(real)1 / d[0], (real)1 / d[1], (real)1 / d[2]};
             real tb = INFINITY;
             for (int i = 0; i < S.n_prims; ++i) tb = prim_next(S.prims[i], p, d, invd, S.eps, tb);
             real tw = world_exit(S, p, d, invd);
             escape = tw <= tb;
             tb = fmin(tb, tw);
-            tau_b = (float)(mu * tb);
+            tau_b = (phys)(mu * tb);
             interact = tau < tau_b;
-            s = interact ? (real)tau / (real)fmaxf(mu, 1e-30f) : tb;
+            s = interact ? (real)tau / (real)fmax(mu, P(1e-30)) : tb;
             if (TALLY && clip_to_grid(G, p, d, invd, s, t0, t1)) {
                 tally_weights(T, M, L, E, wk, wh);
                 tal_n = visit_estimate(G, p, d, t0, t1);
@@ -1003,21 +1096,21 @@ transport_kernel(const KTables T, const KScene S, const KGrid G, const KSource S
             if (escape) { esc = true; done = true; }
             mat = -1;                      // re-locate after the crossing
         } else {
-            float ph, co, ra;
+            phys ph, co, ra;
             parts(T, M, L, ph, co, ra);
-            float tot = ph + co + ra;
-            float r = rng.uniform() * tot;
+            phys tot = ph + co + ra;
+            phys r = uni(rng) * tot;
             ++nsc;
             const int kind = r < ph ? 0 : (r < ph + co ? 1 : 2);
             // The element draw, the new direction and the new free path are
             // common to the three interactions; they run outside the branches
             // so that every interacting lane of the warp executes them together.
-            const int slot = pick_element(T, M, L, kind, rng.uniform());
-            float cost = 1.0f, e_new = E, dep = 0.0f;
+            const int slot = pick_element(T, M, L, kind, uni(rng));
+            phys cost = P(1.0), e_new = E, dep = P(0.0);
             if (kind == 0) {
                 // photoelectric, K fluorescence (physics.py:155-212, transport.py:174-198)
-                const float e_line = sample_k_line(T.elems[slot], E, R.fluorescence, rng);
-                const bool emit = e_line > 0.0f;
+                const phys e_line = sample_k_line(T.elems[slot], E, R.fluorescence, rng);
+                const bool emit = e_line > P(0.0);
                 dep = emit ? E - e_line : E;
                 if (emit) {
                     ++c_fl;
@@ -1027,7 +1120,7 @@ transport_kernel(const KTables T, const KScene S, const KGrid G, const KSource S
                     done = true;
                 }
             } else if (kind == 1) {
-                float eps;
+                phys eps;
                 sample_compton(T.sq + (size_t)slot * TABLE_N, E, rng, eps, cost);
                 e_new = E * eps;
                 dep = E - e_new;
@@ -1041,9 +1134,9 @@ transport_kernel(const KTables T, const KScene S, const KGrid G, const KSource S
             if (kind < 2) atomicAdd(&s_edep[batch * T.n_mat + mat], (double)dep);
             if (!done) {
                 if (kind == 0) isotropic(d, rng);                     // the fluorescence photon
-                else scatter_direction(d, cost, TWO_PI * rng.uniform());
+                else scatter_direction(d, cost, TWO_PI * uni(rng));
                 E = e_new;
-                tau = -__logf(rng.uniform());
+                tau = -p_log(uni(rng));
             }
             mat = -1;                      // new direction: re-locate (material_at every round)
         }
@@ -1149,7 +1242,7 @@ static_assert(sizeof(KSource) % 8 == 0 && sizeof(KGrid) % 8 == 0, "device tables
 struct SegRecB {
     real p[3], d[3];
     real t0, t1;
-    float wk, wh;
+    phys wk, wh;
     int scene, slot, m;
 };
 
@@ -1189,7 +1282,7 @@ __device__ __forceinline__ void add_scene_counts(const KBatch& B, bool ended, in
     }
 }
 
-template <bool TALLY>
+template <bool TALLY, bool HEEL = false>
 __global__ void __launch_bounds__(BLOCK, CC_MIN_BLOCKS)
 batch_kernel(const KTables T, const KBatch B, const KRun R) {
     __shared__ SegRecB s_seg[TALLY ? WARPS_PER_BLOCK : 1][32];
@@ -1209,7 +1302,7 @@ batch_kernel(const KTables T, const KBatch B, const KRun R) {
     int sc = 0, slot = 0;
     long long li = 0;
     real p[3], d[3];
-    float E = 0.f, tau = 0.f;
+    phys E = P(0.), tau = P(0.);
     int nsc = 0, mat = -1;
     int steps = 0;
     HistoryRng rng;
@@ -1238,8 +1331,8 @@ batch_kernel(const KTables T, const KBatch B, const KRun R) {
                 rng.init(seed, ((unsigned long long)sc << 40) + (unsigned long long)li, 0u);
                 long long nh = __ldg(B.n_hist + sc);
                 slot = (int)((li * B.slots) / nh);
-                sample_source(B.sources[sc], rng, p, d, E);
-                tau = -__logf(rng.uniform());
+                sample_source<HEEL>(B.sources[sc], rng, p, d, E);
+                tau = -p_log(uni(rng));
                 nsc = 0;
                 mat = -1;
                 steps = 0;
@@ -1254,11 +1347,11 @@ batch_kernel(const KTables T, const KBatch B, const KRun R) {
         bool go = live;
         bool interact = false, escape = false;
         real s = 0, t0 = 0, t1 = 0;
-        float tau_b = 0.f, loge = 0.f, wk = 0.f, wh = 0.f;
+        phys tau_b = P(0.), loge = P(0.), wk = P(0.), wh = P(0.);
         int tal_n = 0;
         Lookup L;
         L.idx = 0;
-        L.frac = 0.f;
+        L.frac = P(0.);
         if (go) {
             ++steps;
             if (mat < 0) mat = locate(S, p, d);
@@ -1272,9 +1365,9 @@ batch_kernel(const KTables T, const KBatch B, const KRun R) {
         }
         if (go) {
             const DevMaterial& M = T.mats[mat];
-            loge = __logf(E);
+            loge = p_log(E);
             L = energy_index(T, M, loge);
-            float mu = mu_total(T, M, L);
+            phys mu = mu_total(T, M, L);
             const real invd[3] = {(real)1 / d[0], (real)1 / d[1], (real)1 / d[2]};
             real tb = INFINITY;
             const int np = S.n_prims;
@@ -1282,9 +1375,9 @@ batch_kernel(const KTables T, const KBatch B, const KRun R) {
             real tw = world_exit(S, p, d, invd);
             escape = tw <= tb;
             tb = fmin(tb, tw);
-            tau_b = (float)(mu * tb);
+            tau_b = (phys)(mu * tb);
             interact = tau < tau_b;
-            s = interact ? (real)tau / (real)fmaxf(mu, 1e-30f) : tb;
+            s = interact ? (real)tau / (real)fmax(mu, P(1e-30)) : tb;
             if (TALLY && clip_to_grid(B.grids[sc], p, d, invd, s, t0, t1)) {
                 tally_weights(T, M, L, E, wk, wh);
                 tal_n = visit_estimate(B.grids[sc], p, d, t0, t1);
@@ -1339,19 +1432,19 @@ batch_kernel(const KTables T, const KBatch B, const KRun R) {
                 if (escape) { esc = true; ended = true; }
                 mat = -1;
             } else {
-                float ph, co, ra;
+                phys ph, co, ra;
                 parts(T, M, L, ph, co, ra);
-                float r = rng.uniform() * (ph + co + ra);
+                phys r = uni(rng) * (ph + co + ra);
                 ++nsc;
                 const int kind = r < ph ? 0 : (r < ph + co ? 1 : 2);
                 // element draw, new direction and new free path outside the
                 // branches: every interacting lane runs them together
-                const int eslot = pick_element(T, M, L, kind, rng.uniform());
-                float cost = 1.0f, e_new = E;
+                const int eslot = pick_element(T, M, L, kind, uni(rng));
+                phys cost = P(1.0), e_new = E;
                 bool ok = true;
                 if (kind == 0) {
-                    const float e_line = sample_k_line(T.elems[eslot], E, fluorescence, rng);
-                    if (e_line > 0.0f) {
+                    const phys e_line = sample_k_line(T.elems[eslot], E, fluorescence, rng);
+                    if (e_line > P(0.0)) {
                         atomicAdd(B.scene_cnt + 4 * (size_t)sc + 3, 1ull);   // rare: K lines of heavy elements
                         e_new = e_line;
                     } else {
@@ -1359,7 +1452,7 @@ batch_kernel(const KTables T, const KBatch B, const KRun R) {
                         ended = true;
                     }
                 } else if (kind == 1) {
-                    float eps;
+                    phys eps;
                     sample_compton(T.sq + (size_t)eslot * TABLE_N, E, rng, eps, cost);
                     e_new = E * eps;
                 } else if (!sample_rayleigh(T.rx + (size_t)eslot * TABLE_N, T.ra + (size_t)eslot * TABLE_N,
@@ -1371,9 +1464,9 @@ batch_kernel(const KTables T, const KBatch B, const KRun R) {
                 }
                 if (ok && !ended) {
                     if (kind == 0) isotropic(d, rng);                   // the fluorescence photon
-                    else scatter_direction(d, cost, TWO_PI * rng.uniform());
+                    else scatter_direction(d, cost, TWO_PI * uni(rng));
                     E = e_new;
-                    tau = -__logf(rng.uniform());
+                    tau = -p_log(uni(rng));
                 }
                 mat = -1;
             }
@@ -1625,8 +1718,8 @@ __global__ void sample_source_kernel(const KSource SRC, long long n, long long f
     HistoryRng rng;
     rng.init(seed, (unsigned long long)(first + i), 0u);
     real p[3], d[3];
-    float E;
-    sample_source(SRC, rng, p, d, E);
+    phys E;
+    sample_source<true>(SRC, rng, p, d, E);
     for (int k = 0; k < 3; ++k) { pos[3 * i + k] = p[k]; dir[3 * i + k] = d[k]; }
     en[i] = E;
 }
@@ -1638,12 +1731,12 @@ __global__ void sample_source_kernel(const KSource SRC, long long n, long long f
 constexpr int INTERACT_PHOTO = 0, INTERACT_COMPTON = 1, INTERACT_RAYLEIGH = 2;
 
 __global__ void interaction_kernel(const KTables T, int kind, long long n, const int* __restrict__ mat,
-                                   const float* __restrict__ energy, unsigned long long seed, int fluorescence,
+                                   const phys* __restrict__ energy, unsigned long long seed, int fluorescence,
                                    double* out_a, double* out_b, int* out_z, unsigned* status) {
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const int m = mat[i];
-    const float E = energy[i];
+    const phys E = energy[i];
     out_a[i] = 0.0;
     out_b[i] = 0.0;
     out_z[i] = 0;
@@ -1652,18 +1745,18 @@ __global__ void interaction_kernel(const KTables T, int kind, long long n, const
     HistoryRng rng;
     rng.init(seed, (unsigned long long)i, 0u);
     const DevMaterial& M = T.mats[m];
-    const Lookup L = energy_index(T, M, __logf(E));
-    const int slot = pick_element(T, M, L, kind, rng.uniform());
+    const Lookup L = energy_index(T, M, p_log(E));
+    const int slot = pick_element(T, M, L, kind, uni(rng));
     out_z[i] = T.elems[slot].z;
     if (kind == INTERACT_PHOTO) {
         out_a[i] = sample_k_line(T.elems[slot], E, fluorescence, rng);
     } else if (kind == INTERACT_COMPTON) {
-        float eps, cost;
+        phys eps, cost;
         sample_compton(T.sq + (size_t)slot * TABLE_N, E, rng, eps, cost);
         out_a[i] = eps;
         out_b[i] = cost;
     } else {
-        float cost;
+        phys cost;
         if (!sample_rayleigh(T.rx + (size_t)slot * TABLE_N, T.ra + (size_t)slot * TABLE_N,
                              T.ray_bucket + (size_t)slot * (RAY_BUCKETS + 1), T.elems[slot].ray_scale, E, rng,
                              cost)) {
@@ -1799,10 +1892,10 @@ static int dev_upload(std::vector<void*>& allocs, const std::vector<T>& v, const
     return CC_OK;
 }
 
-template <bool FS, bool TL>
+template <bool FS, bool TL, bool HEEL = false>
 static cudaError_t launch_transport(cc_ctx* c, const KTables& T, const KScene& S, const KGrid& G,
                                     const KSource& SRC, const KRun& R, size_t smem, int grid_blocks) {
-    transport_kernel<FS, TL><<<grid_blocks, c->block, smem, c->stream>>>(T, S, G, SRC, R);
+    transport_kernel<FS, TL, HEEL><<<grid_blocks, c->block, smem, c->stream>>>(T, S, G, SRC, R);
     return cudaGetLastError();
 }
 
@@ -1905,8 +1998,8 @@ int cc_tables_create(cc_ctx* ctx, const cc_table_desc* desc, cc_tables** out) {
     if (desc->n_elements < 1 || desc->n_elements > MAX_ELEMS)
         return set_error(CC_E_INVALID, "n_elements must be in [1, 48]");
     CC_CUDA(cudaSetDevice(ctx->device));
-    std::vector<float> loge, elem_cum;
-    std::vector<float4> nodes;
+    std::vector<phys> loge, elem_cum;
+    std::vector<PNode> nodes;
     std::vector<unsigned short> bucket;
     std::vector<DevMaterial> mats(desc->n_materials);
     for (int m = 0; m < desc->n_materials; ++m) {
@@ -1916,28 +2009,28 @@ int cc_tables_create(cc_ctx* ctx, const cc_table_desc* desc, cc_tables** out) {
             return set_error(CC_E_INVALID, "material " + std::to_string(m) + ": bad sizes");
         DevMaterial& dm = mats[m];
         memset(&dm, 0, sizeof(dm));
-        dm.density = (float)md_.density;
+        dm.density = (phys)md_.density;
         dm.n_nodes = md_.n_nodes;
         dm.n_el = md_.n_elements;
         dm.node_off = (int)loge.size();
         dm.elem_off = (int)elem_cum.size();
         dm.bucket_off = (int)bucket.size();
         double lmax = log(150.0);
-        dm.bucket_scale = (float)(N_BUCKETS / lmax);
+        dm.bucket_scale = (phys)(N_BUCKETS / lmax);
         for (int i = 0; i < md_.n_nodes; ++i) {
             if (i > 0 && !(md_.log_e[i] > md_.log_e[i - 1]))
                 return set_error(CC_E_INVALID, "material " + std::to_string(m) + ": log_e not increasing");
-            loge.push_back((float)md_.log_e[i]);
+            loge.push_back((phys)md_.log_e[i]);
             const double* q = md_.log_parts + 4 * (size_t)i;
             const double* t = md_.log_tally + 2 * (size_t)i;
-            nodes.push_back(make_float4((float)md_.log_e[i], (float)q[0], (float)q[1], (float)q[2]));
-            nodes.push_back(make_float4((float)q[3], (float)t[0], (float)t[1], 0.0f));
+            nodes.push_back(PNode{(phys)md_.log_e[i], (phys)q[0], (phys)q[1], (phys)q[2]});
+            nodes.push_back(PNode{(phys)q[3], (phys)t[0], (phys)t[1], (phys)0});
         }
-        // node index per bucket: last node whose float log E <= the bucket start
+        // node index per bucket: last node whose (table-precision) log E <= the bucket start
         int node = 0;
-        const float* lf = loge.data() + dm.node_off;
+        const phys* lf = loge.data() + dm.node_off;
         for (int b = 0; b < N_BUCKETS; ++b) {
-            float start = (float)b / dm.bucket_scale;
+            phys start = (phys)b / dm.bucket_scale;
             while (node + 1 < md_.n_nodes - 1 && lf[node + 1] <= start) ++node;
             bucket.push_back((unsigned short)node);
         }
@@ -1957,7 +2050,7 @@ int cc_tables_create(cc_ctx* ctx, const cc_table_desc* desc, cc_tables** out) {
                     double acc = 0.0;
                     for (int e = 0; e < ne - 1; ++e) {
                         acc += w[e];
-                        elem_cum[base + (size_t)e * nn + j] = (float)(tot > 0.0 ? acc / tot : 1.0);
+                        elem_cum[base + (size_t)e * nn + j] = (phys)(tot > 0.0 ? acc / tot : 1.0);
                     }
                 }
             }
@@ -1970,40 +2063,40 @@ int cc_tables_create(cc_ctx* ctx, const cc_table_desc* desc, cc_tables** out) {
         }
     }
     std::vector<DevElement> els(desc->n_elements);
-    std::vector<float> sq, rx, ra;
+    std::vector<phys> sq, rx, ra;
     std::vector<int> rbk;
     for (int e = 0; e < desc->n_elements; ++e) {
         const cc_element_desc& ed = desc->elements[e];
         if (ed.n_lines < 0 || ed.n_lines > 8) return set_error(CC_E_INVALID, "n_lines must be <= 8");
         DevElement& de = els[e];
         memset(&de, 0, sizeof(de));
-        de.k_edge = (float)ed.k_edge_kev;
-        de.k_prob = (float)ed.k_shell_prob;
-        de.omega = (float)ed.omega_k;
+        de.k_edge = (phys)ed.k_edge_kev;
+        de.k_prob = (phys)ed.k_shell_prob;
+        de.omega = (phys)ed.omega_k;
         de.n_lines = ed.n_lines;
         de.emits = ed.emits && ed.n_lines > 0;
         de.z = ed.z;
         double cum = 0.0;
         for (int k = 0; k < ed.n_lines; ++k) {
             cum += ed.line_p[k];
-            de.line_e[k] = (float)ed.line_e[k];
-            de.line_cum[k] = (float)cum;
+            de.line_e[k] = (phys)ed.line_e[k];
+            de.line_cum[k] = (phys)cum;
         }
         size_t ra_off = ra.size();
         for (int i = 0; i < TABLE_N; ++i) {
             if (i > 0 && !(ed.ray_a[i] >= ed.ray_a[i - 1]))
                 return set_error(CC_E_INVALID, "Rayleigh A(x) table must not decrease");
-            sq.push_back((float)ed.s_over_z[i]);
-            rx.push_back((float)ed.ray_x[i]);
-            ra.push_back((float)ed.ray_a[i]);
+            sq.push_back((phys)ed.s_over_z[i]);
+            rx.push_back((phys)ed.ray_x[i]);
+            ra.push_back((phys)ed.ray_a[i]);
         }
         // bucket index on the FP32 table the kernel searches
-        const float a_end = ra[ra_off + TABLE_N - 1];
+        const phys a_end = ra[ra_off + TABLE_N - 1];
         if (!(a_end > 0.0f)) return set_error(CC_E_INVALID, "Rayleigh A(x) table is empty");
-        de.ray_scale = (float)RAY_BUCKETS / a_end;
+        de.ray_scale = (phys)RAY_BUCKETS / a_end;
         int row = 0;
         for (int b = 0; b <= RAY_BUCKETS; ++b) {
-            float start = (float)b / de.ray_scale;
+            phys start = (phys)b / de.ray_scale;
             while (row + 1 < TABLE_N - 1 && ra[ra_off + row + 1] <= start) ++row;
             rbk.push_back(row);
         }
@@ -2095,26 +2188,25 @@ int cc_scene_destroy(cc_scene* s) {
     return CC_OK;
 }
 
-int cc_source_create(cc_ctx* ctx, const cc_source_desc* d, cc_source** out) {
-    if (!ctx || !d || !out) return set_error(CC_E_INVALID, "NULL argument");
-    if (d->n_energies < 1 || !d->energies_kev || !d->weights) return set_error(CC_E_INVALID, "empty spectrum");
-    if (d->field < 0 || d->field > 2) return set_error(CC_E_INVALID, "unknown field shape");
-    CC_CUDA(cudaSetDevice(ctx->device));
-    // Walker alias table built in FP64
-    int n = d->n_energies;
+// Walker alias table of a discrete spectrum, built in FP64 and appended to
+// (q, alias, energies); alias entries are indices into the appended tables.
+// Returns CC_OK or the error of a bad spectrum.
+static int append_alias_table(const double* e, const double* w, int n, std::vector<phys>& qf,
+                              std::vector<int>& alias_out, std::vector<phys>& ef) {
     double tot = 0.0;
     for (int i = 0; i < n; ++i) {
-        if (!(d->weights[i] >= 0.0)) return set_error(CC_E_INVALID, "negative spectrum weight");
-        if (!(d->energies_kev[i] >= 1.0 && d->energies_kev[i] <= 150.0))
+        if (!(w[i] >= 0.0)) return set_error(CC_E_INVALID, "negative spectrum weight");
+        if (!(e[i] >= 1.0 && e[i] <= 150.0))
             return set_error(CC_E_ENERGY_RANGE, "spectrum energy outside [1, 150] keV");
-        tot += d->weights[i];
+        tot += w[i];
     }
     if (!(tot > 0.0)) return set_error(CC_E_INVALID, "spectrum weights sum to zero");
+    const int base = (int)ef.size();
     std::vector<double> q(n);
     std::vector<int> alias(n);
     std::vector<int> small, large;
     for (int i = 0; i < n; ++i) {
-        q[i] = d->weights[i] / tot * n;
+        q[i] = w[i] / tot * n;
         alias[i] = i;
         (q[i] < 1.0 ? small : large).push_back(i);
     }
@@ -2127,8 +2219,59 @@ int cc_source_create(cc_ctx* ctx, const cc_source_desc* d, cc_source** out) {
     }
     for (int i : large) q[i] = 1.0;
     for (int i : small) q[i] = 1.0;
-    std::vector<float> qf(n), ef(n);
-    for (int i = 0; i < n; ++i) { qf[i] = (float)q[i]; ef[i] = (float)d->energies_kev[i]; }
+    for (int i = 0; i < n; ++i) {
+        qf.push_back((phys)q[i]);
+        alias_out.push_back(base + alias[i]);
+        ef.push_back((phys)e[i]);
+    }
+    return CC_OK;
+}
+
+int cc_source_create(cc_ctx* ctx, const cc_source_desc* d, cc_source** out) {
+    if (!ctx || !d || !out) return set_error(CC_E_INVALID, "NULL argument");
+    if (d->n_energies < 1 || !d->energies_kev || !d->weights) return set_error(CC_E_INVALID, "empty spectrum");
+    if (d->field < 0 || d->field > 2) return set_error(CC_E_INVALID, "unknown field shape");
+    CC_CUDA(cudaSetDevice(ctx->device));
+    int n = d->n_energies;
+    std::vector<phys> qf, ef;
+    std::vector<int> alias;
+    int rc0 = append_alias_table(d->energies_kev, d->weights, n, qf, alias, ef);
+    if (rc0 != CC_OK) return rc0;
+    // heel effect: per-bin alias tables behind one offset array
+    const cc_heel_desc* hd = d->heel;
+    std::vector<phys> hc, hf, hq, he;
+    std::vector<int> ha, hoff;
+    int heel_lo = 0, heel_hi = -1;
+    if (hd) {
+        if (d->field == CC_FIELD_PARALLEL) return set_error(CC_E_INVALID, "the heel effect needs a rect or cone field");
+        if (hd->n_bins < 1 || hd->n_bins > CC_HEEL_MAX_BINS || !hd->centers || !hd->rel_fluence || !hd->bin_sizes ||
+            !hd->energies_kev || !hd->weights || !(hd->span_cm > 0.0))
+            return set_error(CC_E_INVALID, "heel: bad bins");
+        int off = 0;
+        for (int b = 0; b < hd->n_bins; ++b) {
+            const double f = hd->rel_fluence[b];
+            if (!(f >= 0.0 && f <= 1.0)) return set_error(CC_E_INVALID, "heel: relative fluence outside [0, 1]");
+            if (b > 0 && !(hd->centers[b] > hd->centers[b - 1])) return set_error(CC_E_INVALID, "heel: centres not increasing");
+            if (f > 0.0) { if (heel_hi < 0) heel_lo = b; heel_hi = b; }
+            hc.push_back((phys)hd->centers[b]);
+            hf.push_back((phys)f);
+        }
+        if (heel_hi < 0) return set_error(CC_E_INVALID, "heel: no bin has fluence");
+        for (int b = 0; b < hd->n_bins; ++b) {
+            const int nb = hd->bin_sizes[b];
+            if (nb < 1) return set_error(CC_E_INVALID, "heel: empty bin spectrum");
+            hoff.push_back((int)he.size());
+            if (b >= heel_lo && b <= heel_hi) {
+                // photons take energies only from the bins with fluence and those between
+                int rc = append_alias_table(hd->energies_kev + off, hd->weights + off, nb, hq, ha, he);
+                if (rc != CC_OK) return rc;
+            } else {
+                for (int i = 0; i < nb; ++i) { hq.push_back((phys)1); ha.push_back((int)he.size()); he.push_back((phys)1); }
+            }
+            off += nb;
+        }
+        hoff.push_back((int)he.size());
+    }
     cc_source* s = new (std::nothrow) cc_source();
     if (!s) return set_error(CC_E_NOMEM, "out of host memory");
     s->ctx = ctx;
@@ -2138,22 +2281,41 @@ int cc_source_create(cc_ctx* ctx, const cc_source_desc* d, cc_source** out) {
     k.rot_axis = d->rot_axis;
     k.n_angles = d->n_angles;
     for (int a = 0; a < 3; ++a) {
-        k.pos[a] = (float)d->position[a];
-        k.dir[a] = (float)d->direction[a];
-        k.u[a] = (float)d->u[a];
-        k.v[a] = (float)d->v[a];
-        k.iso[a] = (float)d->isocenter[a];
+        k.pos[a] = (phys)d->position[a];
+        k.dir[a] = (phys)d->direction[a];
+        k.u[a] = (phys)d->u[a];
+        k.v[a] = (phys)d->v[a];
+        k.iso[a] = (phys)d->isocenter[a];
     }
-    k.sid = (float)d->sid_cm;
-    k.su = (float)d->size_u;
-    k.sv = (float)d->size_v;
-    k.cos_half = (float)d->cos_half_angle;
-    k.scan = (float)d->scan_length_cm;
+    k.sid = (phys)d->sid_cm;
+    k.su = (phys)d->size_u;
+    k.sv = (phys)d->size_v;
+    k.cos_half = (phys)d->cos_half_angle;
+    k.scan = (phys)d->scan_length_cm;
     k.n_e = n;
     int rc;
     if ((rc = dev_upload(s->allocs, ef, &k.e)) != CC_OK) { cc_source_destroy(s); return rc; }
     if ((rc = dev_upload(s->allocs, qf, &k.alias_p)) != CC_OK) { cc_source_destroy(s); return rc; }
     if ((rc = dev_upload(s->allocs, alias, &k.alias_i)) != CC_OK) { cc_source_destroy(s); return rc; }
+    k.heel_n = 0;
+    if (hd) {
+        k.heel_n = hd->n_bins;
+        k.heel_lo = heel_lo;
+        k.heel_hi = heel_hi;
+        k.h_u = (phys)hd->h_u;
+        k.h_v = (phys)hd->h_v;
+        k.span = (phys)hd->span_cm;
+        k.bin_w = (phys)(2.0 * hd->span_cm / hd->n_bins);
+        if ((rc = dev_upload(s->allocs, hc, &k.heel_c)) != CC_OK ||
+            (rc = dev_upload(s->allocs, hf, &k.heel_f)) != CC_OK ||
+            (rc = dev_upload(s->allocs, hoff, &k.heel_off)) != CC_OK ||
+            (rc = dev_upload(s->allocs, he, &k.heel_e)) != CC_OK ||
+            (rc = dev_upload(s->allocs, hq, &k.heel_q)) != CC_OK ||
+            (rc = dev_upload(s->allocs, ha, &k.heel_a)) != CC_OK) {
+            cc_source_destroy(s);
+            return rc;
+        }
+    }
     *out = s;
     return CC_OK;
 }
@@ -2587,7 +2749,10 @@ static int enqueue_launch(cc_ctx* c, const cc_scene* scene, const cc_tables* tab
     }
     CC_CUDA(cudaEventRecord(rec.k0, st));
     cudaError_t e;
-    if (fs && tl) e = launch_transport<true, true>(c, T, scene->k, G, S, R, smem, blocks);
+    const bool heel = fs && S.heel_n > 0;
+    if (fs && tl && heel) e = launch_transport<true, true, true>(c, T, scene->k, G, S, R, smem, blocks);
+    else if (fs && heel) e = launch_transport<true, false, true>(c, T, scene->k, G, S, R, smem, blocks);
+    else if (fs && tl) e = launch_transport<true, true>(c, T, scene->k, G, S, R, smem, blocks);
     else if (fs) e = launch_transport<true, false>(c, T, scene->k, G, S, R, smem, blocks);
     else if (tl) e = launch_transport<false, true>(c, T, scene->k, G, S, R, smem, blocks);
     else e = launch_transport<false, false>(c, T, scene->k, G, S, R, smem, blocks);
@@ -3007,24 +3172,24 @@ int cc_sample_interactions(cc_ctx* c, const cc_tables* tables, int32_t kind, int
     if (n == 0) return CC_OK;
     if (tables->ctx->device != c->device) return set_error(CC_E_INVALID, "tables belong to another device");
     CC_CUDA(cudaSetDevice(c->device));
-    std::vector<float> ef((size_t)n);
-    for (int64_t i = 0; i < n; ++i) ef[i] = (float)energy[i];
-    // [status 256 B][mat n x 4][energy n x 4][z n x 4][pad][a n x 8][b n x 8]
-    const size_t n4 = ((size_t)n * 4 + 255) / 256 * 256;
-    const size_t bytes = 256 + 3 * n4 + 2 * (size_t)n * 8;
+    std::vector<phys> ef((size_t)n);
+    for (int64_t i = 0; i < n; ++i) ef[i] = (phys)energy[i];
+    // [status 256 B][mat n x 4][energy n x 8][z n x 4][a n x 8][b n x 8], sub-arrays 256-byte aligned
+    const size_t n4 = ((size_t)n * 4 + 255) / 256 * 256, n8 = ((size_t)n * 8 + 255) / 256 * 256;
+    const size_t bytes = 256 + 2 * n4 + 3 * n8;
     char* buf = nullptr;
     CC_CUDA(cudaMalloc(&buf, bytes));
     unsigned* d_st = (unsigned*)buf;
     int* d_mat = (int*)(buf + 256);
-    float* d_e = (float*)(buf + 256 + n4);
-    int* d_z = (int*)(buf + 256 + 2 * n4);
-    double* d_a = (double*)(buf + 256 + 3 * n4);
+    phys* d_e = (phys*)(buf + 256 + n4);
+    int* d_z = (int*)(buf + 256 + n4 + n8);
+    double* d_a = (double*)(buf + 256 + 2 * n4 + n8);
     double* d_b = d_a + n;
     unsigned st = 0;
     cudaStream_t s = c->stream;
     cudaError_t e = cudaMemsetAsync(d_st, 0, sizeof(unsigned), s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(d_mat, material, (size_t)n * 4, cudaMemcpyHostToDevice, s);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(d_e, ef.data(), (size_t)n * 4, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_e, ef.data(), (size_t)n * sizeof(phys), cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) {
         const int threads = 256;
         interaction_kernel<<<(unsigned)((n + threads - 1) / threads), threads, 0, s>>>(
@@ -3215,6 +3380,7 @@ int cc_batch_create(cc_ctx* c, const cc_tables* tables, int32_t n_scenes, const 
     b->slots = slots;
     b->chunk = chunk;
     b->tally = grids != nullptr;
+    bool heel = false;               // some source carries the heel effect
     std::vector<KScene> hs(n_scenes);
     std::vector<KSource> hsrc(n_scenes);
     std::vector<KGrid> hg(n_scenes);
@@ -3225,6 +3391,7 @@ int cc_batch_create(cc_ctx* c, const cc_tables* tables, int32_t n_scenes, const 
         if (!scenes[i] || !sources[i] || n_histories[i] < 1) { batch_free(b); return set_error(CC_E_INVALID, "scene " + std::to_string(i) + ": NULL handle or no histories"); }
         hs[i] = scenes[i]->k;
         hsrc[i] = sources[i]->k;
+        if (hsrc[i].heel_n > 0) heel = true;
         memset(&hg[i], 0, sizeof(KGrid));
         if (b->tally) {
             cc_grid* g = grids[i];
@@ -3307,7 +3474,9 @@ int cc_batch_create(cc_ctx* c, const cc_tables* tables, int32_t n_scenes, const 
     if (e == cudaSuccess) e = cudaMemsetAsync(b->d_mem + o_c8, 0, total - o_c8, st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(b->d_mem + o_run, b->h_run, 2 * sizeof(unsigned long long), cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) {
-        if (b->tally) batch_kernel<true><<<b->blocks, c->block, 0, st>>>(tables->k, k, R);
+        if (b->tally && heel) batch_kernel<true, true><<<b->blocks, c->block, 0, st>>>(tables->k, k, R);
+        else if (b->tally) batch_kernel<true><<<b->blocks, c->block, 0, st>>>(tables->k, k, R);
+        else if (heel) batch_kernel<false, true><<<b->blocks, c->block, 0, st>>>(tables->k, k, R);
         else batch_kernel<false><<<b->blocks, c->block, 0, st>>>(tables->k, k, R);
         e = cudaGetLastError();
         b->launches = 1;

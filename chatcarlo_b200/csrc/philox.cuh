@@ -100,6 +100,8 @@ struct HistoryRng {
         return r;
     }
     CC_HD float uniform() { return u01_oc(next_u32()); }   // (0, 1]
+    // the same draw as an FP64 uniform in (0, 1] (exact: 32 bits fit a double)
+    CC_HD double uniform_d() { return ((double)next_u32() + 1.0) * 2.3283064365386963e-10; }
 };
 
 }  // namespace cc

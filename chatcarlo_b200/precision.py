@@ -1,11 +1,15 @@
-"""What FP32 tracking costs each tally: the same run tracked in FP64.
+"""What FP32 tracking and sampling cost each tally: the same run in FP64.
 
-The engine tracks positions, directions and distances in FP32 and
-accumulates its tallies in FP64.  ``libccb200_fp64.so`` is the same source
-built to track in FP64 (same random numbers, same FP32 physics, surface
-tolerance 1e-6 cm as in transport.py:155).  ``tally_precision`` runs one
-scene with the same seed through both and reports, for every tally
-(kerma, H*(10)), how far the FP32-tracking result is from the FP64 one:
+The engine tracks positions, directions and distances and samples its
+physics (free paths, cross-section lookups, the samplers' arithmetic) in
+FP32, with fast-math intrinsics, and accumulates its tallies in FP64.
+``libccb200_fp64.so`` is the same source built to do all of that in FP64,
+with FP64 tables and IEEE arithmetic (same 32-bit random draws, surface
+tolerance 1e-6 cm as in transport.py:155): the FP64 GPU run.
+``tally_precision`` runs one scene with the same seed through both and
+reports, for every tally (kerma, H*(10)), how far the FP32 result is from
+the FP64 one (a history whose discrete decisions flip on a rounding
+difference follows another path from there on):
 
 * relative difference per voxel (median, 99th percentile, max) over the
   voxels the FP64 run scored;

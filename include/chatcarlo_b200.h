@@ -117,6 +117,24 @@ typedef struct {
     const cc_element_desc* elements;
 } cc_table_desc;
 
+/* Heel effect of a rect or cone field (source.py:130-149,195-207): photons
+ * are kept with the relative fluence at their coordinate s along the
+ * anode-cathode axis on the SID plane (np.interp over the bin centres) and
+ * take their energy from the spectrum of s's bin.  The reference computes
+ * the bins with SpekPy (spectrum.py:88-129); the caller supplies them. */
+#define CC_HEEL_MAX_BINS 64
+typedef struct {
+    double h_u, h_v;              /* unit anode direction projected on the beam basis (source.py:42-57) */
+    double span_cm;               /* half-width of the field along the axis at the SID (source.py:60-65) */
+    int32_t n_bins;               /* 1..CC_HEEL_MAX_BINS, of width 2 span / n_bins */
+    int32_t pad;
+    const double* centers;        /* [n_bins] bin centres on the axis (cm), increasing */
+    const double* rel_fluence;    /* [n_bins] relative fluence in [0, 1], not all zero */
+    const int32_t* bin_sizes;     /* [n_bins] energies of each bin's spectrum */
+    const double* energies_kev;   /* the bins' spectra, concatenated */
+    const double* weights;        /* their weights, concatenated (normalised per bin by the engine) */
+} cc_heel_desc;
+
 /* Point source into a field, with optional CT rotation (source.py:67-210). */
 typedef struct {
     int32_t field;                /* CC_FIELD_* */
@@ -135,6 +153,8 @@ typedef struct {
     int32_t pad;
     const double* energies_kev;   /* [n_energies] */
     const double* weights;        /* [n_energies], not necessarily normalised */
+    const cc_heel_desc* heel;     /* NULL: no heel effect; else rect/cone fields only, and the bins'
+                                     spectra replace the spectrum above */
 } cc_source_desc;
 
 typedef struct {

@@ -684,8 +684,38 @@ def sample_spectrum(src, n, rng):
     return e[rng.choice(len(e), size=n, p=w)]
 
 
+def heel_spectra_for_source(src, sid, span_cm):
+    """spectrum.py:149-153: the off-axis bins of the heel effect, which the
+    reference computes with SpekPy (spectrum.py:88-129).  SpekPy is absent,
+    so this raises like the reference without it; tests replace it with
+    fixed bins (centres, per-bin (energies, weights), relative fluence,
+    absolute fluence)."""
+    raise RuntimeError("the heel effect needs SpekPy's off-axis spectra")
+
+
+def heel_axis_coeffs(src, d, u, v):
+    """source.py:42-57: anode direction projected on the beam's (u, v) basis."""
+    a = np.asarray(src["anode_direction"], dtype=float)
+    a = a - (a @ d) * d
+    norm = np.linalg.norm(a)
+    if norm < 1e-9:
+        raise ValueError("anode_direction is parallel to the beam direction")
+    a = a / norm
+    return float(a @ u), float(a @ v)
+
+
+def heel_span_cm(fld, h_u, h_v):
+    """source.py:60-65: half-width of the field along the heel axis at the SID."""
+    if fld.get("shape", "rect") == "cone":
+        return fld["diameter_cm"] / 2.0
+    w, h = fld["size_cm"]
+    return abs(h_u) * w / 2.0 + abs(h_v) * h / 2.0
+
+
 def sample_source_photons(src, n, rng):
-    """source.py:67-210 without the heel effect."""
+    """source.py:67-210, the heel effect included (fluence rejection along
+    the heel axis in draws of max(1.8 x missing, 1024), energies from the
+    photon's heel bin, source.py:130-149,195-207)."""
     from chatcarlo_b200.source import beam_basis
     pos = np.asarray(src["position"], dtype=float)
     d = np.asarray(src["direction"], dtype=float)
@@ -711,10 +741,35 @@ def sample_source_photons(src, n, rng):
         pa, da, ua, va = pos, d, u, v
         origins = np.tile(pos, (n, 1))
     shape = fld.get("shape", "rect")
+    heel = bool(src.get("heel_effect"))
+    if heel:
+        h_u, h_v = heel_axis_coeffs(src, d, u, v)
+        span = heel_span_cm(fld, h_u, h_v)
+        centers, spectra, rel_flu, _ = heel_spectra_for_source(src, float(sid), span)
+
+        def accept(draw):
+            kept, got = None, 0
+            while got < n:
+                m = max(int((n - got) * 1.8), 1024)
+                s_, *payload = draw(m)
+                keep = rng.random(m) < np.interp(s_, centers, rel_flu)
+                cols = [s_[keep]] + [c[keep] for c in payload]
+                kept = cols if kept is None else [np.concatenate([a, b]) for a, b in zip(kept, cols)]
+                got = len(kept[0])
+            return [c[:n] for c in kept]
     if shape == "cone":
         ch = np.cos(math.atan((fld["diameter_cm"] / 2.0) / fld["sid_cm"]))
-        c = rng.uniform(ch, 1.0, n)
-        ph = rng.uniform(0.0, 2.0 * np.pi, n)
+
+        def draw_cone(m):
+            c = rng.uniform(ch, 1.0, m)
+            ph = rng.uniform(0.0, 2.0 * np.pi, m)
+            s_ = sid * (np.sqrt(1.0 - c ** 2) / c) * (np.cos(ph) * h_u + np.sin(ph) * h_v) if heel else None
+            return s_, c, ph
+
+        if heel:
+            s_heel, c, ph = accept(draw_cone)
+        else:
+            _, c, ph = draw_cone(n)
         s = np.sqrt(1.0 - c ** 2)
         dirs = c[:, None] * da + (s * np.cos(ph))[:, None] * ua + (s * np.sin(ph))[:, None] * va
     elif shape == "parallel":
@@ -725,11 +780,30 @@ def sample_source_photons(src, n, rng):
         dirs = np.broadcast_to(da, (n, 3)).copy()
     else:
         w, h = fld["size_cm"]
-        su = rng.uniform(-w / 2, w / 2, n)
-        sv = rng.uniform(-h / 2, h / 2, n)
+
+        def draw_rect(m):
+            a = rng.uniform(-w / 2, w / 2, m)
+            b = rng.uniform(-h / 2, h / 2, m)
+            return (a * h_u + b * h_v if heel else None), a, b
+
+        if heel:
+            s_heel, su, sv = accept(draw_rect)
+        else:
+            _, su, sv = draw_rect(n)
         tgt = pa + da * sid + su[:, None] * ua + sv[:, None] * va
         dirs = tgt - origins
         dirs /= np.linalg.norm(dirs, axis=1, keepdims=True)
+    if heel:
+        bin_w = 2.0 * span / len(centers)
+        bins = np.clip(((s_heel + span) / bin_w).astype(int), 0, len(centers) - 1)
+        nz = np.where(rel_flu > 0)[0]
+        bins = np.clip(bins, nz.min(), nz.max())
+        energies = np.empty(n)
+        for b in np.unique(bins):
+            m = bins == b
+            e_b, w_b = spectra[b]
+            energies[m] = e_b[rng.choice(len(e_b), size=int(m.sum()), p=w_b)]
+        return origins, dirs, energies
     return origins, dirs, sample_spectrum(src, n, rng)
 
 

@@ -240,6 +240,57 @@ def case_source():
     return out
 
 
+HEEL_VARIANTS = {
+    "rect": {"field": {"shape": "rect", "size_cm": [35, 43], "sid_cm": 100}, "anode_direction": [1.0, 0.3, 0.0]},
+    "cone": {"field": {"shape": "cone", "diameter_cm": 30, "sid_cm": 100}, "anode_direction": [0.0, 1.0, 0.2]},
+    "rot": {"field": {"shape": "rect", "size_cm": [50, 4], "sid_cm": 100}, "anode_direction": [1.0, 0.0, 0.0],
+            "rotation": {"isocenter": [0, 0, 50], "axis": "y", "scan_length_cm": 20}},
+}
+
+
+def heel_bins(span_cm, n_bins=15):
+    """Fixed heel-axis bins standing in for SpekPy's off-axis spectra: the
+    reference's bin centres (spectrum.py:103), relative fluence falling
+    towards the anode side with its last bin cut off (zero), and Kramers
+    spectra (the reference's own fallback, spectrum.py:55-62) hardened by
+    0.4 mm Al more per bin towards the anode."""
+    from chatcarlo.spectrum import _kramers_fallback_spectrum
+    centers = (np.arange(n_bins) + 0.5) / n_bins * 2.0 * span_cm - span_cm
+    rel = np.clip(1.0 - 0.9 * (np.arange(n_bins) / (n_bins - 1)) ** 2, 0.0, None)
+    rel[-1] = 0.0
+    spectra = tuple(_kramers_fallback_spectrum(80.0, 2.5 + 0.4 * i, n_bins=75) for i in range(n_bins))
+    return centers, spectra, rel, rel * 1e6
+
+
+def case_heel():
+    """source.py:130-149,195-207 run by the reference itself, with its
+    SpekPy-only heel_spectra_for_source replaced by fixed bins; the bins are
+    stored with the outputs."""
+    out = {}
+    base = {"position": [0, -100, 50], "direction": [0, 1, 0], "heel_effect": True, "kvp": 80}
+    saved = rsrc.heel_spectra_for_source
+    try:
+        for k, extra in HEEL_VARIANTS.items():
+            src = dict(base, **extra)
+            seen = {}
+
+            def fake(src_, sid, span, seen=seen):
+                seen["span"] = span
+                return heel_bins(span)
+            rsrc.heel_spectra_for_source = fake
+            p, d, e = rsrc.sample_source_photons(src, 3000, np.random.default_rng(23))
+            out[f"{k}_pos"], out[f"{k}_dir"], out[f"{k}_e"] = p, d, e
+            centers, spectra, rel, _ = heel_bins(seen["span"])
+            out[f"{k}_span"] = np.array(seen["span"])
+            out[f"{k}_centers"] = centers
+            out[f"{k}_rel"] = rel
+            out[f"{k}_spec_e"] = np.stack([a for a, _ in spectra])
+            out[f"{k}_spec_w"] = np.stack([b for _, b in spectra])
+    finally:
+        rsrc.heel_spectra_for_source = saved
+    return out
+
+
 CT_SOURCE = {"position": [0.0, -60.0, 0.0], "direction": [0.0, 1.0, 0.0],
              "field": {"shape": "rect", "size_cm": [50.0, 4.0], "sid_cm": 60.0},
              "rotation": {"isocenter": [0.0, 0.0, 0.0], "axis": "z", "scan_length_cm": 10.0},
@@ -293,7 +344,7 @@ def case_maps():
 
 CASES = {"geometry": case_geometry, "materials": case_materials, "samplers": case_samplers,
          "tally": case_tally, "transport": case_transport, "run": case_run, "source": case_source,
-         "ctdi": case_ctdi, "maps": case_maps}
+         "ctdi": case_ctdi, "maps": case_maps, "heel": case_heel}
 
 
 def main(names=None):

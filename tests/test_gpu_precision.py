@@ -1,6 +1,6 @@
-"""FP32 tracking against the same engine tracking in FP64 (same seed, same
-random numbers): every tally's difference must vanish next to its own
-Monte Carlo noise."""
+"""The FP32 engine against the same engine tracking and sampling in FP64
+(FP64 tables, IEEE arithmetic; same seed, same random draws): every
+tally's difference must vanish next to its own Monte Carlo noise."""
 import pytest
 
 from chatcarlo_b200 import workloads as W

@@ -119,8 +119,8 @@ def test_source_spec_fields():
         np.testing.assert_allclose(m @ m.T, np.eye(3), atol=1e-12)
     spec = SourceSpec(W.room()["source"])
     assert spec.desc.n_energies == 75 and spec.desc.sid_cm == 180.0
-    with pytest.raises(RuntimeError):
-        SourceSpec(dict(W.room()["source"], heel_effect=True))
+    with pytest.raises(ValueError):
+        SourceSpec(dict(W.room()["source"], heel_effect=True))      # no anode_direction
 
 
 def test_cli_parser():
@@ -351,3 +351,32 @@ def test_denoiser_volume_shapes():
     for bad in (12, (16, 30, 8), (16, 16), (0, 8, 8)):
         with pytest.raises(ValueError):
             UNet3D._side3(bad)
+
+
+def test_heel_effect_without_spekpy_raises():
+    """Without SpekPy's off-axis spectra the heel effect cannot be set up;
+    the reference raises the same way (spectrum.py:97-99)."""
+    from chatcarlo_b200.source import SourceSpec
+    src = {"position": [0, -100, 50], "direction": [0, 1, 0], "heel_effect": True, "kvp": 80,
+           "field": {"shape": "rect", "size_cm": [35, 43], "sid_cm": 100}, "anode_direction": [1.0, 0.3, 0.0]}
+    with pytest.raises(RuntimeError):
+        SourceSpec(src)
+
+
+def test_heel_descriptor_from_supplied_bins(monkeypatch):
+    """With bins supplied (as SpekPy would give them), the source descriptor
+    carries the heel axis, span and the concatenated per-bin spectra."""
+    import chatcarlo_b200.source as S
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "heel.npz"))
+    spectra = tuple((a, b) for a, b in zip(g["rect_spec_e"], g["rect_spec_w"]))
+    bins = (g["rect_centers"], spectra, g["rect_rel"], g["rect_rel"])
+    monkeypatch.setattr(S, "heel_spectra_for_source", lambda src, sid, span, n_bins=15: bins)
+    src = {"position": [0, -100, 50], "direction": [0, 1, 0], "heel_effect": True, "kvp": 80,
+           "field": {"shape": "rect", "size_cm": [35, 43], "sid_cm": 100}, "anode_direction": [1.0, 0.3, 0.0]}
+    spec = S.SourceSpec(src)
+    h = spec.desc.heel.contents
+    assert h.n_bins == 15 and h.span_cm == pytest.approx(float(g["rect_span"]))
+    assert h.h_u ** 2 + h.h_v ** 2 == pytest.approx(1.0)
+    assert sum(h.bin_sizes[i] for i in range(15)) == sum(len(e) for e, _ in spectra)
+    with pytest.raises(ValueError):
+        S.SourceSpec(dict(src, field={"shape": "parallel", "size_cm": [10, 10]}))

@@ -251,3 +251,32 @@ def test_voxel_fixtures_are_consistent():
             assert np.all(f[f"{tag}_mean"] > 0)
             assert np.all(f[f"{tag}_rel"].astype(float) < float(f["rel_cut"]) + 1e-3)
             assert np.all(np.flatnonzero(mask) % int(f["keep_every"]) == 0)
+
+
+HEEL_VARIANTS = {
+    "rect": {"field": {"shape": "rect", "size_cm": [35, 43], "sid_cm": 100}, "anode_direction": [1.0, 0.3, 0.0]},
+    "cone": {"field": {"shape": "cone", "diameter_cm": 30, "sid_cm": 100}, "anode_direction": [0.0, 1.0, 0.2]},
+    "rot": {"field": {"shape": "rect", "size_cm": [50, 4], "sid_cm": 100}, "anode_direction": [1.0, 0.0, 0.0],
+            "rotation": {"isocenter": [0, 0, 50], "axis": "y", "scan_length_cm": 20}},
+}
+
+
+def heel_bins_from_golden(g, k):
+    """The fixed heel bins a golden heel case was made with."""
+    spectra = tuple((a, b) for a, b in zip(g[f"{k}_spec_e"], g[f"{k}_spec_w"]))
+    return g[f"{k}_centers"], spectra, g[f"{k}_rel"], g[f"{k}_rel"] * 1e6
+
+
+def test_heel_effect_sampling_matches_reference(golden, monkeypatch):
+    """source.py:130-149,195-207 (fluence rejection along the heel axis,
+    energies from the photon's heel bin) through the oracle, with the bins
+    the reference ran with: identical photons."""
+    g = golden("heel")
+    base = {"position": [0, -100, 50], "direction": [0, 1, 0], "heel_effect": True, "kvp": 80}
+    for k, extra in HEEL_VARIANTS.items():
+        bins = heel_bins_from_golden(g, k)
+        monkeypatch.setattr(O, "heel_spectra_for_source", lambda src, sid, span, b=bins: b)
+        p, d, e = O.sample_source_photons(dict(base, **extra), 3000, np.random.default_rng(23))
+        np.testing.assert_array_equal(p, g[f"{k}_pos"], err_msg=k)
+        np.testing.assert_array_equal(d, g[f"{k}_dir"], err_msg=k)
+        np.testing.assert_array_equal(e, g[f"{k}_e"], err_msg=k)
