@@ -281,6 +281,111 @@ def DN_inference_s(model, n_phantoms: int) -> float:
 
 
 # ---------------------------------------------------------------------------
+# side measurements
+# ---------------------------------------------------------------------------
+
+def fp64_reduction_ceiling(eng, n_cells: int, repeats: int = 5) -> dict:
+    """Measured rate of the tally's scoring pattern with nothing else in the
+    kernel (cc_measure_fp64_reductions): two FP64 reductions into one
+    16-byte cell per visit, cells spread uniformly over n_cells."""
+    import ctypes as C
+    import torch
+    from chatcarlo_b200 import _native as N
+    buf = torch.zeros(2 * n_cells, dtype=torch.float64, device=f"cuda:{eng.device}")
+    v = C.c_double()
+    N.check(eng.lib.cc_measure_fp64_reductions(eng.device, C.c_void_p(buf.data_ptr()), n_cells, 0,
+                                               eng_sm_count(eng) * 8, 256, 256, 0, 0, 0, repeats, C.byref(v)),
+            eng.lib)
+    del buf
+    return {"visits_per_s": v.value, "reductions_per_s": 2.0 * v.value, "cells": n_cells,
+            "pattern": f"uniform over {n_cells} 16-byte cells ({n_cells * 16 / 2**20:.0f} MiB)"}
+
+
+def eng_sm_count(eng) -> int:
+    import torch
+    return torch.cuda.get_device_properties(eng.device).multi_processor_count
+
+
+def side_measurements(eng, args, flush, n_vox_per_hist: float, hist_per_s_kernel: float) -> dict:
+    import ctypes as C
+    import torch
+    from chatcarlo_b200 import _native as N
+    from chatcarlo_b200 import workloads as W
+    from chatcarlo_b200.geometry import Geometry
+    from chatcarlo_b200.source import SourceSpec
+    from chatcarlo_b200.transport import DeviceGrid
+    out = {}
+    # the atomics ceiling for the headline workload: the room grid's cells
+    # times the batches a launch keeps in flight (8 slots of 384,000 cells,
+    # 49 MB, L2-resident like the tally's scratch)
+    ceil = fp64_reduction_ceiling(eng, 8 * 384_000)
+    achieved = 2.0 * n_vox_per_hist * hist_per_s_kernel
+    out["atomics"] = {"ceiling_per_s": ceil["reductions_per_s"], "ceiling_pattern": ceil["pattern"],
+                      "frac": achieved / ceil["reductions_per_s"]}
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    # CT dosimetry configuration (15.4M voxels of 1 mm, batch statistics)
+    raw = W.ct()
+    geom = Geometry(raw["geometry"])
+    ts, th = eng.tables(geom.materials(), need_muen=True)
+    sh = eng.scene(geom, ts)
+    srch = eng.source(SourceSpec(raw["source"]))
+    g = W.make_grid(W.CT_GRID, track_uncertainty=True)
+    dg = DeviceGrid(eng, g, stats=True)
+    edep = np.zeros(len(ts.names))
+    edep2 = np.zeros(len(ts.names))
+    S = int(args.histories_per_step)
+    try:
+        ms, outs = [], []
+        for i in range(3 + 3):
+            flush.zero_()
+            torch.cuda.synchronize()
+            o = N.RunOut()
+            ev0.record()
+            N.check(eng.lib.cc_run(eng.ctx, sh, th, srch, dg.handle, S, BATCH, 777, i * S, 1, N.dptr(edep),
+                                   N.dptr(edep2), C.byref(o)))
+            ev1.record()
+            torch.cuda.synchronize()
+            if i >= 3:
+                ms.append(ev0.elapsed_time(ev1))
+                outs.append(o)
+        n = S * len(ms)
+        out["ct"] = {"metric": METRIC, "value": n / (float(np.sum(ms)) / 1e3), "unit": "histories/s",
+                     "workload": WORKLOAD_CT, "histories_per_step": S, "steps": len(ms), "batch_size": BATCH,
+                     "transport_ms_per_step": sum(o.transport_ms for o in outs) / len(ms),
+                     "segments_per_history": sum(o.n_steps for o in outs) / n,
+                     "voxel_visits_per_history": sum(o.n_voxel_visits for o in outs) / n,
+                     "gpu_launches_per_step": sum(o.gpu_launches for o in outs) / len(ms)}
+    finally:
+        dg.close()
+        eng.lib.cc_source_destroy(srch)
+        eng.lib.cc_scene_destroy(sh)
+    # the batched configuration: 256 random scenes, log-uniform 1e5-1e7
+    # histories each, 64^3 grids, one persistent launch replayed from a CUDA
+    # graph (launch shape from the autotuner)
+    from chatcarlo_b200.batched import BatchedRun, autotune
+    scenes, specs, counts = W.batched_scenes()
+    shape = autotune(scenes, specs, counts, engine=eng)
+    br = BatchedRun(scenes, specs, counts, engine=eng, shape=shape)
+    try:
+        br.run(seed=1)
+        ms = []
+        for i in range(3):
+            br.reset()
+            flush.zero_()
+            torch.cuda.synchronize()
+            ms.append(br.run(seed=2 + i)[1].elapsed_ms)
+    finally:
+        br.close()
+    total = int(sum(counts))
+    out["batched"] = {"metric": METRIC, "value": total / (float(np.median(ms)) / 1e3), "unit": "histories/s",
+                      "workload": "256 random scenes (1-12 primitives, 7 materials, mono 20-140 keV or 60-140 kVp "
+                                  "spectra), log-uniform 1e5-1e7 histories each, 64^3 kerma grids, one launch",
+                      "histories": total, "launch_ms_median": float(np.median(ms)), "replays": len(ms),
+                      "shape": shape}
+    return out
+
+
+# ---------------------------------------------------------------------------
 # engine arm
 # ---------------------------------------------------------------------------
 
@@ -302,6 +407,8 @@ def main():
                     help="skip the side measurement with FP32 tally scratch cells")
     ap.add_argument("--no-denoiser", action="store_true", help="skip the denoised time-to-2 %% measurements")
     ap.add_argument("--denoiser-phantoms", type=int, default=8)
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the side measurements of the CT and batched configurations and the atomics ceiling")
     ap.add_argument("--workload", choices=["room", "ct"], default="room",
                     help="room-scale (the headline configuration) or CT dosimetry")
     args = ap.parse_args()
@@ -388,14 +495,13 @@ def main():
             step_ms.append(ev0.elapsed_time(ev1))
         red_ms = 0.0
         if world > 1:
-            # the one exchange step: sum the tally grids and their batch
-            # statistics over ranks (totals, sums of squares and hit counts
-            # are additive, as when the reference merges its workers)
-            dg.download(grid)
-            t = torch.from_numpy(np.stack([grid.kerma_keV, grid.h10_track_pSv_cm3, grid.kerma_sum2, grid.h10_sum2,
-                                           grid.n_batches_hit.astype(np.float64)])).cuda()
+            # the one exchange step: sum the device-resident tally grids and
+            # their batch statistics over ranks in place (totals, sums of
+            # squares and hit counts are additive, as when the reference
+            # merges its workers); the time covers every collective of it
+            from chatcarlo_b200.distributed import allreduce_device_grid
             ev0.record()
-            dist.all_reduce(t)
+            allreduce_device_grid(dg)
             ev1.record()
             torch.cuda.synchronize()
             red_ms = ev0.elapsed_time(ev1)
@@ -532,6 +638,13 @@ def main():
         denoise = denoiser_metric(eng, args.denoiser_phantoms)
         ct_denoise = ct_denoiser_metric(eng)
 
+    # side measurements under the same clock record: the CT configuration's
+    # plain MC and the batched configuration's one-launch run, and the
+    # measured ceiling of the tally's FP64 reductions
+    extras = {}
+    if rank == 0 and world == 1 and not args.no_extras:
+        extras = side_measurements(eng, args, flush, n_vox_per_hist=n_vox, hist_per_s_kernel=n_h / (tr_ms / 1e3))
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         per_core = args.cpu_histories_per_process
@@ -557,11 +670,12 @@ def main():
                              "avg_launch_ms": tr_ms / max(tr_launch, 1),
                              "histories_per_launch": hist_per_launch,
                              # the tally's atomic bound: two FP64 reductions (kerma, H*(10)) per voxel visit
-                             "atomics": {"per_history": 2.0 * n_vox,
-                                         "achieved_per_s": 2.0 * n_vox * n_h / (tr_ms / 1e3),
-                                         "cells": "fp64"}},
+                             "atomics": dict({"per_history": 2.0 * n_vox,
+                                              "achieved_per_s": 2.0 * n_vox * n_h / (tr_ms / 1e3),
+                                              "cells": "fp64"}, **extras.get("atomics", {}))},
                 "cpu_baseline": cpu, "e2e": e2e, "e2e_photons": e2e_photons, "precision": precision,
                 "denoiser": denoise, "denoiser_ct": ct_denoise, "tally_fp32_cells": fp32_cells,
+                "ct": extras.get("ct"), "batched": extras.get("batched"),
                 "clocks": clocks,
                 "gpu_launches": int(launches),
                 "reduce_ms": red_ms}
