@@ -66,7 +66,7 @@ def engine_run(engine, name, n, batch, seed):
     return _RUNS[key]
 
 
-def voxel_z(grid, tag, fx):
+def voxel_z(grid, tag, fx, report: bool = False):
     T = grid.kerma_keV if tag == "kerma" else grid.h10_track_pSv_cm3
     Q = grid.kerma_sum2 if tag == "kerma" else grid.h10_sum2
     mean_g = T.ravel() / grid.n_histories
@@ -75,6 +75,12 @@ def voxel_z(grid, tag, fx):
     with np.errstate(divide="ignore", invalid="ignore"):
         ok = mask & (mean_g > 0) & (se_g / mean_g < REL_CUT) & (se_o / mean_o < REL_CUT)
     z = (mean_g[ok] - mean_o[ok]) / np.sqrt(se_g[ok] ** 2 + se_o[ok] ** 2)
+    if report:
+        idx = np.flatnonzero(ok)
+        for j in np.argsort(-np.abs(z))[:6]:
+            v = int(idx[j])
+            print(f"  voxel {np.unravel_index(v, grid.shape)}: engine {mean_g[v]:.6g} +- {se_g[v]:.2g}, "
+                  f"oracle {mean_o[v]:.6g} +- {se_o[v]:.2g}, z {z[j]:+.2f}")
     return z
 
 
@@ -88,7 +94,7 @@ CONFIGS = [("plain", 200_000_000, 2_000_000, 101), ("room", 240_000_000, 2_400_0
 def test_voxel_tallies_match_the_reference_method(engine, name, n, batch, seed, tag):
     fx = load_fixture(name)
     g, _ = engine_run(engine, name, n, batch, seed)
-    z = voxel_z(g, tag, fx)
+    z = voxel_z(g, tag, fx, report=True)
     chi2 = float(np.mean(z ** 2))
     print(f"{name} {tag}: {z.size} voxels, chi2/dof {chi2:.3f}, max |z| {np.max(np.abs(z)):.2f}, "
           f"|z|>3 {np.mean(np.abs(z) > 3):.4f}, mean z {np.mean(z):+.3f}")
