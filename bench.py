@@ -301,6 +301,30 @@ def fp64_reduction_ceiling(eng, n_cells: int, repeats: int = 5) -> dict:
             "pattern": f"uniform over {n_cells} 16-byte cells ({n_cells * 16 / 2**20:.0f} MiB)"}
 
 
+def atomics_sweep(eng) -> None:
+    """The FP64-reduction ceiling over the patterns a tally produces: cells
+    spread over an L2-resident region (the room grid, 8 of its batch slots)
+    and over one beyond L2 (a CT slot), a few hot cells (a beam's busiest
+    voxels), and runs of 16 cells `stride` apart (a photon crossing a row,
+    a column or a plane of voxels).  One JSON line per case."""
+    import ctypes as C
+    import torch
+    from chatcarlo_b200 import _native as N
+    sms = eng_sm_count(eng)
+    for n_cells, label in ((384_000, "room grid, 6 MiB"), (8 * 384_000, "8 room slots, 47 MiB"),
+                           (15_360_000, "CT grid, 234 MiB")):
+        buf = torch.zeros(2 * n_cells, dtype=torch.float64, device=f"cuda:{eng.device}")
+        for mode, hot, run, stride in ((0, 0, 0, 0), (1, 32, 0, 0), (1, 4096, 0, 0), (2, 0, 16, 1), (2, 0, 16, 80),
+                                       (2, 0, 16, 6400)):
+            v = C.c_double()
+            N.check(eng.lib.cc_measure_fp64_reductions(eng.device, C.c_void_p(buf.data_ptr()), n_cells, mode,
+                                                       sms * 8, 256, 256, hot, run, stride, 5, C.byref(v)), eng.lib)
+            pattern = {0: "uniform", 1: f"{hot} hot cells", 2: f"runs of {run}, stride {stride}"}[mode]
+            print(json.dumps({"region": label, "pattern": pattern, "reductions_per_s": 2.0 * v.value}), flush=True)
+        del buf
+        torch.cuda.empty_cache()
+
+
 def eng_sm_count(eng) -> int:
     import torch
     return torch.cuda.get_device_properties(eng.device).multi_processor_count
@@ -407,6 +431,8 @@ def main():
                     help="skip the side measurement with FP32 tally scratch cells")
     ap.add_argument("--no-denoiser", action="store_true", help="skip the denoised time-to-2 %% measurements")
     ap.add_argument("--denoiser-phantoms", type=int, default=8)
+    ap.add_argument("--atomics-sweep", action="store_true",
+                    help="only print the FP64-reduction ceiling for several scoring patterns (JSON lines)")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the side measurements of the CT and batched configurations and the atomics ceiling")
     ap.add_argument("--workload", choices=["room", "ct"], default="room",
@@ -454,6 +480,10 @@ def main():
     device = local if world > 1 else 0
     torch.cuda.set_device(device)
     eng = Engine(device)
+    if args.atomics_sweep:
+        if rank == 0:
+            atomics_sweep(eng)
+        return 0
     raw, gspec, desc = workload(args.workload)
     geom = Geometry(raw["geometry"])
     ts, th = eng.tables(geom.materials(), need_muen=True)

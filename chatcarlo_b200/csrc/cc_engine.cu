@@ -642,11 +642,22 @@ __device__ __forceinline__ int visit_estimate(const KGrid& G, const real p[3], c
 // One axis of the traversal: the entry voxel i, the step s (-1, 0, 1), the
 // ray parameter tm of the next face crossing and the spacing td of those
 // crossings.  A point that rounds onto the far side of a face gets a
-// zero-length first cell and steps back in.
+// zero-length first cell and steps back in.  Along an axis the ray does
+// not move on, the point's side of the neighbouring faces is decided by
+// comparing its coordinate with the faces' own: the offset from the grid
+// origin keeps only ~1e-7 of the origin's magnitude in FP32, which would
+// move the face by up to half an ulp of the grid's extent -- harmless for
+// rays that cross faces at random positions, but a beam that runs along a
+// face (a pencil beam on a voxel boundary) would have a systematic share of
+// its photons scored on the wrong side of it.
 __device__ __forceinline__ void walk_axis(real o, real h, real inv_h, int n, real p, real d, real t0, int& i,
                                           int& s, real& tm, real& td) {
     real x = (p + d * t0 - o) * inv_h;
     i = max(0, min(n - 1, (int)floor(x)));
+    if (!(fabs(d) > (real)P(1e-12))) {
+        if (i > 0 && p < o + (real)i * h) --i;
+        else if (i < n - 1 && p >= o + (real)(i + 1) * h) ++i;
+    }
     if (d > P(1e-12)) {
         real inv = P(1.0) / d;
         s = 1;

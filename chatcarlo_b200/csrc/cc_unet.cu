@@ -564,6 +564,170 @@ __global__ void __launch_bounds__(THREADS) conv_halo_kernel(const ConvP P) {
 }
 
 // ---------------------------------------------------------------------------
+// forward / backward-data convolution streaming z-planes through a halo ring
+// ---------------------------------------------------------------------------
+
+// A persistent version of the halo kernel.  A work item is a column of
+// output tiles (16 y x 8 x, one z each) over ZSEG consecutive z of one
+// volume; the CTA keeps the layer's packed weights in shared memory for all
+// its items and a ring of four 18 x 10 halo planes, so each input plane is
+// loaded once per column instead of three times, and the weights once per
+// CTA instead of once per tile.  Per output plane z: one thread issues the
+// 27 x cin/16 MMAs of z into one of two tensor-memory accumulators, then
+// all threads wait for the MMAs of z - 1, copy plane z + 2 into the ring
+// slot that plane z - 2 held, and store z - 1's outputs from the other
+// accumulator -- loads, MMAs and epilogue of neighbouring planes overlap.
+// The ring slot of plane p of an item starting at zs is (p - zs + 1) & 3;
+// the operand descriptors are the halo kernel's (8 x voxels per core
+// matrix row, SBO one halo row, LBO one 8-channel plane).
+constexpr int ZSEG = 16;
+constexpr int RING_V = HALO_Y * HALO_X;               // voxels of one halo plane
+
+__host__ __device__ constexpr uint32_t stream_acc_cols(int n) { return n <= 32 ? 32u : 64u; }
+__host__ __device__ constexpr uint32_t stream_tmem_cols(int n) { return 2u * stream_acc_cols(n); }
+__host__ __device__ constexpr uint32_t stream_smem_bytes(int n, int cin) {
+    return 4u * (uint32_t)(cin / 8) * RING_V * 16 + (uint32_t)((27 * cin + KS - 1) / KS) * 8 * n * 16;
+}
+
+template <int N>
+__global__ void __launch_bounds__(THREADS) conv_stream_kernel(const ConvP P, int n_items) {
+    extern __shared__ __align__(128) uint8_t smem[];
+    __shared__ uint64_t bar[2];
+    __shared__ uint32_t s_tmem;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const Src& S = P.src;
+    const int cin = S.ca + S.cb, c8n = cin / 8;
+    const int tiles_x = S.W / 8, tiles_y = S.H / 16, n_seg = (S.D + ZSEG - 1) / ZSEG;
+    const uint32_t ring_bytes = 4u * (uint32_t)c8n * RING_V * 16;
+    const int w_chunks = ((27 * cin + KS - 1) / KS) * 8 * N;
+    constexpr uint32_t ACC = stream_acc_cols(N);
+
+    if (warp == 0) tmem_alloc(&s_tmem, stream_tmem_cols(N));
+    if (tid == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        mbar_init_fence();
+    }
+    const uint32_t sbase = smem_u32(smem), swt = sbase + ring_bytes;
+    for (int i = tid; i < w_chunks; i += THREADS) cp_async16(swt + (uint32_t)i * 16, P.w + (size_t)i * 8, 16u);
+    cp_async_commit();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = s_tmem;
+    constexpr uint32_t IDESC = idesc_bf16(TILE_M, N, 0, 0);
+    const int q = warp & 3, half = warp >> 2;
+
+    // copies of input plane zz (zero outside the volume) of column (n, y0, x0) into ring slot
+    auto load_plane = [&](int n, int y0, int x0, int zz, int slot) {
+        const uint32_t base = sbase + (uint32_t)slot * c8n * RING_V * 16;
+        for (int i = tid; i < c8n * RING_V; i += THREADS) {
+            const int c8 = i / RING_V, hv = i - c8 * RING_V;
+            const int yy = y0 + hv / HALO_X - 1, xx = x0 + hv % HALO_X - 1;
+            const int ch = c8 * 8;
+            uint32_t bytes = 0;
+            const void* src = S.a;
+            if ((unsigned)zz < (unsigned)S.D && (unsigned)yy < (unsigned)S.H && (unsigned)xx < (unsigned)S.W) {
+                bytes = 16;
+                if (ch < S.ca) {
+                    src = S.a + ((((size_t)n * S.D + zz) * S.H + yy) * S.W + xx) * S.ca + ch;
+                } else {
+                    const size_t cv =
+                        (((size_t)n * (S.D >> 1) + (zz >> 1)) * (S.H >> 1) + (yy >> 1)) * (S.W >> 1) + (xx >> 1);
+                    src = S.b + cv * S.cb + (ch - S.ca);
+                }
+            }
+            cp_async16(base + (uint32_t)(c8 * RING_V + hv) * 16, src, bytes);
+        }
+    };
+    // outputs of plane z of the column from the accumulator of commit k
+    auto store_plane = [&](int n, int y0, int x0, int z, uint32_t k) {
+        const uint32_t acc = tmem + (k & 1u) * ACC;
+        const int m = q * 32 + lane;
+        const long long v = (((long long)n * S.D + z) * S.H + y0 + (m >> 3)) * S.W + x0 + (m & 7);
+        for (int c0 = half * 8; c0 < N; c0 += 16) {
+            float f[8];
+            tmem_ld8(acc + ((uint32_t)(q * 32) << 16) + (uint32_t)c0, f);
+            conv_store(P, v, c0, N, f);
+        }
+    };
+
+    bool ok = true;
+    uint32_t commits = 0;                      // MMA groups committed by this CTA (bar[k & 1], phase k >> 1)
+    for (int item = blockIdx.x; item < n_items && ok; item += gridDim.x) {
+        int t = item;
+        const int seg = t % n_seg;
+        t /= n_seg;
+        const int x0 = (t % tiles_x) * 8;
+        t /= tiles_x;
+        const int y0 = (t % tiles_y) * 16;
+        const int n = t / tiles_y;
+        const int zs = seg * ZSEG, ze = min(zs + ZSEG, S.D);
+        for (int r = 0; r < 3; ++r) load_plane(n, y0, x0, zs - 1 + r, r);
+        cp_async_commit();
+        cp_async_wait<0>();
+        fence_proxy_async();
+        tc_fence_before();
+        __syncthreads();
+        tc_fence_after();
+        for (int z = zs; z < ze; ++z) {
+            const int i = z - zs;
+            const uint32_t k = commits++;
+            if (tid == 0) {
+                const uint32_t acc = tmem + (k & 1u) * ACC;
+                for (int tap = 0; tap < 27; ++tap) {
+                    const int slot = (i + tap / 9) & 3;
+                    const uint32_t off = (uint32_t)(((tap / 3) % 3) * HALO_X + tap % 3) * 16;
+                    for (int j = 0; j < c8n / 2; ++j) {
+                        uint64_t ad = smem_desc(sbase + (uint32_t)(slot * c8n + 2 * j) * RING_V * 16 + off,
+                                                RING_V * 16, HALO_X * 16);
+                        uint64_t bd = smem_desc(swt + (uint32_t)(tap * c8n + 2 * j) * N * 16, N * 16, 128);
+                        mma_bf16(acc, ad, bd, IDESC, (tap > 0 || j > 0) ? 1u : 0u);
+                    }
+                }
+                mma_commit(&bar[k & 1u]);
+            }
+            if (i > 0) {
+                // the MMAs of z - 1: their accumulator is ready and plane z - 2 is free
+                const bool w = mbar_wait(&bar[(k - 1) & 1u], ((k - 1) >> 1) & 1u);
+                ok = __syncthreads_and(ok && w) != 0;      // uniform before the warp-collective loads
+                tc_fence_after();
+                if (!ok) break;
+            }
+            if (z + 2 <= ze) load_plane(n, y0, x0, z + 2, (i + 3) & 3);
+            cp_async_commit();
+            if (i > 0) store_plane(n, y0, x0, z - 1, k - 1);
+            cp_async_wait<0>();
+            fence_proxy_async();
+            tc_fence_before();
+            ok = __syncthreads_and(ok) != 0;
+            tc_fence_after();
+            if (!ok) break;
+        }
+        if (!ok) break;
+        // the last plane of the item
+        const uint32_t k = commits - 1;
+        const bool w = mbar_wait(&bar[k & 1u], (k >> 1) & 1u);
+        ok = __syncthreads_and(w) != 0;
+        tc_fence_after();
+        if (!ok) break;
+        store_plane(n, y0, x0, ze - 1, k);
+        tc_fence_before();
+        ok = __syncthreads_and(ok) != 0;
+        tc_fence_after();
+    }
+    if (!ok) {
+        // every committed MMA group has finished (or its wait ran out) before the memory is freed
+        if (commits > 0) mbar_wait(&bar[(commits - 1) & 1u], ((commits - 1) >> 1) & 1u);
+        if (tid == 0) atomicOr(&g_status, 1u);
+    }
+    cp_async_wait<0>();
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) tmem_dealloc(tmem, stream_tmem_cols(N));
+}
+
+// ---------------------------------------------------------------------------
 // weight gradient: dW[tap][co][ci] += sum_v dz[v][co] * X[v + off(tap)][ci]
 // ---------------------------------------------------------------------------
 
@@ -1121,12 +1285,43 @@ int launch_conv(const ConvP& P, cudaStream_t st) {
     return CCU_OK;
 }
 
-int g_conv_path = 0;      // 0: halo kernel where it applies, 1: always the gathering kernel
+// 0: the streaming halo kernel where it applies, 1: always the gathering
+// kernel, 2: the one-tile halo kernel where it applies
+int g_conv_path = 0;
 
 bool halo_applies(const ConvP& P, int n_out) {
     const int cin = P.src.ca + P.src.cb;
-    return g_conv_path == 0 && P.src.H % 16 == 0 && P.src.W % 8 == 0 && cin <= 48 && n_out <= 48 &&
+    return g_conv_path == 2 && P.src.H % 16 == 0 && P.src.W % 8 == 0 && cin <= 48 && n_out <= 48 &&
            halo_smem_bytes(n_out, cin) <= 160 * 1024;
+}
+
+bool stream_applies(const ConvP& P, int n_out) {
+    const int cin = P.src.ca + P.src.cb;
+    return g_conv_path == 0 && P.src.H % 16 == 0 && P.src.W % 8 == 0 && cin <= 48 && n_out <= 48 &&
+           stream_smem_bytes(n_out, cin) <= 200 * 1024;
+}
+
+template <int N>
+int launch_conv_stream(const ConvP& P, cudaStream_t st) {
+    const int cin = P.src.ca + P.src.cb;
+    size_t smem = 0;
+    int rc = tc_launch_smem(conv_stream_kernel<N>, stream_smem_bytes(N, cin), stream_tmem_cols(N), smem);
+    if (rc != CCU_OK) return rc;
+    const long long items =
+        (long long)P.src.B * (P.src.H / 16) * (P.src.W / 8) * ((P.src.D + ZSEG - 1) / ZSEG);
+    if (items >= (1LL << 31)) return set_error(CCU_E_INVALID, "volume too large");
+    // resident CTAs per SM: shared memory (1 KB of it reserved per CTA), the
+    // 512 tensor-memory columns and 2048 threads per SM
+    int dev = 0, sms = 0, per_sm = 0;
+    CU_CHECK(cudaGetDevice(&dev));
+    CU_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    CU_CHECK(cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
+    const int resident = std::max(1, std::min({(int)((size_t)per_sm / (smem + 1024)),
+                                               (int)(512u / stream_tmem_cols(N)), 2048 / THREADS}));
+    const long long grid = std::min<long long>(items, (long long)sms * resident);
+    conv_stream_kernel<N><<<(unsigned)grid, THREADS, smem, st>>>(P, (int)items);
+    CU_CHECK(cudaGetLastError());
+    return CCU_OK;
 }
 
 template <int N>
@@ -1201,6 +1396,14 @@ int ccu_conv3d(const void* a, int ca, const void* b, int cb, int batch, int d, i
     P.split = split;
     P.out1 = (__nv_bfloat16*)out1;
     cudaStream_t st = (cudaStream_t)stream;
+    if (stream_applies(P, cout)) {
+        switch (cout) {
+            case 16: return launch_conv_stream<16>(P, st);
+            case 32: return launch_conv_stream<32>(P, st);
+            case 48: return launch_conv_stream<48>(P, st);
+            default: break;
+        }
+    }
     if (halo_applies(P, cout)) {
         switch (cout) {
             case 16: return launch_conv_halo<16>(P, st);
@@ -1343,7 +1546,9 @@ int ccu_pack_weights(const float* w32, int cout, int cin, void* w, void* wt, voi
 }
 
 int ccu_set_conv_path(int path) {
-    if (path < 0 || path > 1) return set_error(CCU_E_INVALID, "path must be 0 (automatic) or 1 (gathering kernel)");
+    if (path < 0 || path > 2)
+        return set_error(CCU_E_INVALID, "path must be 0 (streaming halo kernel where it applies), 1 (gathering "
+                                        "kernel) or 2 (one-tile halo kernel where it applies)");
     g_conv_path = path;
     return CCU_OK;
 }

@@ -159,29 +159,38 @@ def test_pool_upsample_bias_helpers(U):
     torch.testing.assert_close(db, gfull.float().sum(dim=(0, 1, 2, 3)), rtol=1e-4, atol=1e-2)
 
 
-def test_halo_and_gathering_kernels_agree(U):
-    """The two forward kernels on the same inputs (the halo one applies to
-    this shape; path 1 forces the gathering one)."""
-    gen = torch.Generator().manual_seed(77)
-    B, D, H, W, ca, cb, cout = 2, 4, 32, 16, 16, 32, 48
+@pytest.mark.parametrize("B,D,H,W,ca,cb,cout", [(2, 4, 32, 16, 16, 32, 48), (1, 37, 16, 8, 16, 0, 16),
+                                                (3, 18, 32, 24, 16, 0, 32), (1, 5, 16, 16, 32, 0, 16)])
+def test_halo_and_gathering_kernels_agree(U, B, D, H, W, ca, cb, cout):
+    """The three forward kernels on the same inputs: the streaming halo
+    kernel (path 0; depths that are not a multiple of its 16-plane segment
+    and several volumes), the gathering kernel (path 1) and the one-tile
+    halo kernel (path 2)."""
+    gen = torch.Generator().manual_seed(77 + D)
     a = _bf((B, D, H, W, ca), gen)
-    b = _bf((B, D // 2, H // 2, W // 2, cb), gen)
+    b = _bf((B, D // 2, H // 2, W // 2, cb), gen) if cb else None
     w32 = (torch.randn(27 * cout * (ca + cb), generator=gen) * 0.1).cuda()
     w = torch.empty(U.lib().ccu_packed_weight_elems(cout, ca + cb), dtype=torch.bfloat16, device="cuda")
     U.check(U.lib().ccu_pack_weights(_ptr(w32), cout, ca + cb, _ptr(w), None, None))
     outs = []
     try:
-        for path in (0, 1):
+        for path in (0, 1, 2):
             U.check(U.lib().ccu_set_conv_path(path))
             o = torch.empty(B, D, H, W, cout, dtype=torch.bfloat16, device="cuda")
-            U.check(U.lib().ccu_conv3d(_ptr(a), ca, _ptr(b), cb, B, D, H, W, _ptr(w), None, cout, 0, _ptr(o), cout,
-                                       None, None, None))
+            U.check(U.lib().ccu_conv3d(_ptr(a), ca, _ptr(b) if b is not None else None, cb, B, D, H, W, _ptr(w),
+                                       None, cout, 0, _ptr(o), cout, None, None, None))
             outs.append(o.float())
     finally:
         U.check(U.lib().ccu_set_conv_path(0))
     torch.cuda.synchronize()
     assert U.status() == 0
     torch.testing.assert_close(outs[0], outs[1], rtol=1.6e-2, atol=1e-2)
+    torch.testing.assert_close(outs[2], outs[1], rtol=1.6e-2, atol=1e-2)
+    x = _to_ncdhw(a)
+    if cb:
+        x = torch.cat([x, _up(_to_ncdhw(b))], dim=1)
+    ref = torch.nn.functional.conv3d(x, _torch_w(w32.to(torch.bfloat16), cout, ca + cb), padding=1)
+    torch.testing.assert_close(outs[0], ref.permute(0, 2, 3, 4, 1), rtol=1.6e-2, atol=1e-2)
 
 
 def test_adam_with_adaptive_clipping(U):
