@@ -579,7 +579,9 @@ __global__ void __launch_bounds__(THREADS) conv_halo_kernel(const ConvP P) {
 // accumulator -- loads, MMAs and epilogue of neighbouring planes overlap.
 // The ring slot of plane p of an item starting at zs is (p - zs + 1) & 3;
 // the operand descriptors are the halo kernel's (8 x voxels per core
-// matrix row, SBO one halo row, LBO one 8-channel plane).
+// matrix row, SBO one halo row, LBO one 8-channel plane).  The issuing
+// thread starts plane z's MMAs once those of z - 1 are done, so that its
+// issue overlaps the other warps' copies and epilogue.
 constexpr int ZSEG = 16;
 constexpr int RING_V = HALO_Y * HALO_X;               // voxels of one halo plane
 
@@ -597,7 +599,9 @@ __global__ void __launch_bounds__(THREADS) conv_stream_kernel(const ConvP P, int
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const Src& S = P.src;
     const int cin = S.ca + S.cb, c8n = cin / 8;
-    const int tiles_x = S.W / 8, tiles_y = S.H / 16, n_seg = (S.D + ZSEG - 1) / ZSEG;
+    // edge tiles reach past the volume: their halo reads zeros there and
+    // their outputs outside it are not stored
+    const int tiles_x = (S.W + 7) / 8, tiles_y = (S.H + 15) / 16, n_seg = (S.D + ZSEG - 1) / ZSEG;
     const uint32_t ring_bytes = 4u * (uint32_t)c8n * RING_V * 16;
     const int w_chunks = ((27 * cin + KS - 1) / KS) * 8 * N;
     constexpr uint32_t ACC = stream_acc_cols(N);
@@ -644,11 +648,12 @@ __global__ void __launch_bounds__(THREADS) conv_stream_kernel(const ConvP P, int
     auto store_plane = [&](int n, int y0, int x0, int z, uint32_t k) {
         const uint32_t acc = tmem + (k & 1u) * ACC;
         const int m = q * 32 + lane;
-        const long long v = (((long long)n * S.D + z) * S.H + y0 + (m >> 3)) * S.W + x0 + (m & 7);
+        const int y = y0 + (m >> 3), x = x0 + (m & 7);
+        const long long v = (((long long)n * S.D + z) * S.H + y) * S.W + x;
         for (int c0 = half * 8; c0 < N; c0 += 16) {
             float f[8];
-            tmem_ld8(acc + ((uint32_t)(q * 32) << 16) + (uint32_t)c0, f);
-            conv_store(P, v, c0, N, f);
+            tmem_ld8(acc + ((uint32_t)(q * 32) << 16) + (uint32_t)c0, f);   // every lane: warp-collective
+            if (y < S.H && x < S.W) conv_store(P, v, c0, N, f);
         }
     };
 
@@ -672,27 +677,32 @@ __global__ void __launch_bounds__(THREADS) conv_stream_kernel(const ConvP P, int
         tc_fence_after();
         for (int z = zs; z < ze; ++z) {
             const int i = z - zs;
-            const uint32_t k = commits++;
-            if (tid == 0) {
-                const uint32_t acc = tmem + (k & 1u) * ACC;
-                for (int tap = 0; tap < 27; ++tap) {
-                    const int slot = (i + tap / 9) & 3;
-                    const uint32_t off = (uint32_t)(((tap / 3) % 3) * HALO_X + tap % 3) * 16;
-                    for (int j = 0; j < c8n / 2; ++j) {
-                        uint64_t ad = smem_desc(sbase + (uint32_t)(slot * c8n + 2 * j) * RING_V * 16 + off,
-                                                RING_V * 16, HALO_X * 16);
-                        uint64_t bd = smem_desc(swt + (uint32_t)(tap * c8n + 2 * j) * N * 16, N * 16, 128);
-                        mma_bf16(acc, ad, bd, IDESC, (tap > 0 || j > 0) ? 1u : 0u);
-                    }
-                }
-                mma_commit(&bar[k & 1u]);
-            }
             if (i > 0) {
                 // the MMAs of z - 1: their accumulator is ready and plane z - 2 is free
-                const bool w = mbar_wait(&bar[(k - 1) & 1u], ((k - 1) >> 1) & 1u);
+                const uint32_t kp = commits - 1;
+                const bool w = mbar_wait(&bar[kp & 1u], (kp >> 1) & 1u);
                 ok = __syncthreads_and(ok && w) != 0;      // uniform before the warp-collective loads
                 tc_fence_after();
                 if (!ok) break;
+            }
+            const uint32_t k = commits++;
+            if (tid == 0) {
+                // the 27 x cin/16 MMAs of plane z; the descriptors differ from
+                // the first one by their start addresses only (in 16-byte units)
+                const uint32_t acc = tmem + (k & 1u) * ACC;
+                const uint64_t a0 = smem_desc(sbase, RING_V * 16, HALO_X * 16);
+                const uint64_t b0 = smem_desc(swt, N * 16, 128);
+                const uint32_t slot16 = (uint32_t)c8n * RING_V;
+                const uint32_t so[3] = {(uint32_t)(i & 3) * slot16, (uint32_t)((i + 1) & 3) * slot16,
+                                        (uint32_t)((i + 2) & 3) * slot16};
+#pragma unroll
+                for (int tap = 0; tap < 27; ++tap) {
+                    const uint32_t ta = so[tap / 9] + (uint32_t)(((tap / 3) % 3) * HALO_X + tap % 3);
+                    for (int j = 0; j < c8n / 2; ++j)
+                        mma_bf16(acc, a0 + ta + (uint32_t)(2 * j * RING_V), b0 + (uint32_t)((tap * c8n + 2 * j) * N),
+                                 IDESC, (tap > 0 || j > 0) ? 1u : 0u);
+                }
+                mma_commit(&bar[k & 1u]);
             }
             if (z + 2 <= ze) load_plane(n, y0, x0, z + 2, (i + 3) & 3);
             cp_async_commit();
@@ -1297,8 +1307,7 @@ bool halo_applies(const ConvP& P, int n_out) {
 
 bool stream_applies(const ConvP& P, int n_out) {
     const int cin = P.src.ca + P.src.cb;
-    return g_conv_path == 0 && P.src.H % 16 == 0 && P.src.W % 8 == 0 && cin <= 48 && n_out <= 48 &&
-           stream_smem_bytes(n_out, cin) <= 200 * 1024;
+    return g_conv_path == 0 && cin <= 48 && n_out <= 48 && stream_smem_bytes(n_out, cin) <= 200 * 1024;
 }
 
 template <int N>
@@ -1307,8 +1316,8 @@ int launch_conv_stream(const ConvP& P, cudaStream_t st) {
     size_t smem = 0;
     int rc = tc_launch_smem(conv_stream_kernel<N>, stream_smem_bytes(N, cin), stream_tmem_cols(N), smem);
     if (rc != CCU_OK) return rc;
-    const long long items =
-        (long long)P.src.B * (P.src.H / 16) * (P.src.W / 8) * ((P.src.D + ZSEG - 1) / ZSEG);
+    const long long items = (long long)P.src.B * ((P.src.H + 15) / 16) * ((P.src.W + 7) / 8) *
+                            ((P.src.D + ZSEG - 1) / ZSEG);
     if (items >= (1LL << 31)) return set_error(CCU_E_INVALID, "volume too large");
     // resident CTAs per SM: shared memory (1 KB of it reserved per CTA), the
     // 512 tensor-memory columns and 2048 threads per SM

@@ -109,9 +109,10 @@ int ccu_pack_weights(const float* w32, int cout, int cin, void* w, void* wt, voi
 
 /* Which convolution kernel ccu_conv3d uses: 0 (default) the persistent
  * halo kernel that streams z-planes through a shared-memory ring where it
- * applies (input and output channels <= 48, h % 16 == 0, w % 8 == 0) and
- * the gathering kernel elsewhere; 1 always the gathering kernel; 2 the
- * one-tile halo kernel where it applies (for comparisons).  Process-wide. */
+ * applies (input and output channels <= 48) and the gathering kernel
+ * elsewhere; 1 always the gathering kernel; 2 the one-tile halo kernel where
+ * it applies (channels <= 48, h % 16 == 0, w % 8 == 0; for comparisons).
+ * Process-wide. */
 int ccu_set_conv_path(int path);
 
 /* cudaMemsetAsync(p, 0, bytes) on the stream (gradient buffers). */

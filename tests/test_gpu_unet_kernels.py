@@ -160,7 +160,9 @@ def test_pool_upsample_bias_helpers(U):
 
 
 @pytest.mark.parametrize("B,D,H,W,ca,cb,cout", [(2, 4, 32, 16, 16, 32, 48), (1, 37, 16, 8, 16, 0, 16),
-                                                (3, 18, 32, 24, 16, 0, 32), (1, 5, 16, 16, 32, 0, 16)])
+                                                (3, 18, 32, 24, 16, 0, 32), (1, 5, 16, 16, 32, 0, 16),
+                                                # edge tiles of the streaming kernel (h % 16, w % 8 != 0)
+                                                (2, 6, 10, 12, 16, 32, 32), (1, 20, 38, 19, 16, 0, 16)])
 def test_halo_and_gathering_kernels_agree(U, B, D, H, W, ca, cb, cout):
     """The three forward kernels on the same inputs: the streaming halo
     kernel (path 0; depths that are not a multiple of its 16-plane segment
