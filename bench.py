@@ -174,7 +174,7 @@ def _ref_init(root):
 # learned denoiser leg
 # ---------------------------------------------------------------------------
 
-def denoiser_metric(eng, n_phantoms: int, levels=(500_000, 1_000_000, 2_000_000), n_ref: int = 400_000_000,
+def denoiser_metric(eng, n_phantoms: int, levels=(500_000, 1_000_000, 2_000_000), n_ref: int = 1_000_000_000,
                     seed: int = 1001) -> dict:
     """Time to a 2 % median voxel-kerma error per phantom: plain batched
     Monte Carlo (its error from its own batch statistics, 1/sqrt(n)) against
@@ -221,7 +221,7 @@ def denoiser_metric(eng, n_phantoms: int, levels=(500_000, 1_000_000, 2_000_000)
             "network": meta.get("trained_by")}
 
 
-def ct_denoiser_metric(eng, levels=(1_000_000, 3_000_000, 10_000_000), n_ref: int = 2_000_000_000) -> dict:
+def ct_denoiser_metric(eng, levels=(1_000_000, 3_000_000, 10_000_000), n_ref: int = 10_000_000_000) -> dict:
     """The same measurement on the CT configuration (1 mm voxels,
     320x320x150): its own phantom, never seen by the shipped CT network,
     denoised as one whole volume in a single pass of the network, against an
@@ -234,7 +234,7 @@ def ct_denoiser_metric(eng, levels=(1_000_000, 3_000_000, 10_000_000), n_ref: in
     grid = W.make_grid(W.CT_GRID, track_uncertainty=True, pinned=True)
     sc = W.ct()
     mat, dens = PH.voxel_maps(sc, W.CT_GRID, CD.CT_MATERIALS)
-    k_ref, rel_ref, ms_ref = CD.scan(sc, n_ref, 7, eng, grid, batches=20)
+    k_ref, rel_ref, ms_ref = CD.scan(sc, n_ref, 7, eng, grid, batches=100)
     sel = (mat != 0) & (k_ref > 0)
     ref_noise = float(np.median(0.6745 * np.nan_to_num(rel_ref[sel], nan=0.0)))
     rate = n_ref / (ms_ref * 1e-3)

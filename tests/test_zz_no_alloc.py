@@ -5,8 +5,10 @@ library allocate device memory (an application that owns every device
 allocation, or a pipeline that forbids cudaMalloc/cudaFree while it runs).
 Its scratch is a static device array shared by all calls, so this test
 calls it twice in a row and compares both results with
-cc_transport_photons_device on the same photons and seed.  It lives in its
-own file, collected last, and runs alone in a fresh process too.
+cc_transport_photons_device on the same photons and seed; the second call
+runs on a stream of the caller's, and the device's free memory must not
+change across it.  It lives in its own file, collected last, and runs
+alone in a fresh process too.
 """
 import ctypes as C
 
@@ -65,10 +67,17 @@ def test_noalloc_matches_allocating_entry_point():
             nsc, absd, esc = _outputs(torch, n)
             edep = np.zeros(len(ts.names))
             nfl = C.c_int64()
+            # call 0 on the legacy default stream, call 1 on a stream of the
+            # caller's; the second call allocates nothing on the device
+            stream = torch.cuda.Stream() if call == 1 else None
+            torch.cuda.synchronize()
+            free_before = torch.cuda.mem_get_info()[0]
             N.check(lib.cc_transport_photons_device_noalloc(
                 sh, th, n, ptr(pos), ptr(dirv), ptr(en), seed, 0, 1, ptr(nsc), ptr(absd), ptr(esc),
-                N.dptr(edep), C.byref(nfl), None))
+                N.dptr(edep), C.byref(nfl), C.c_void_p(stream.cuda_stream) if stream is not None else None))
             torch.cuda.synchronize()
+            if call == 1:
+                assert torch.cuda.mem_get_info()[0] == free_before
             # same kernel code and the same per-history Philox streams: identical photons
             assert torch.equal(pos, ref_pos), call
             assert torch.equal(dirv, ref_dir), call
