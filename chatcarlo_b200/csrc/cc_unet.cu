@@ -33,6 +33,7 @@
 #include <stdint.h>
 #include <string.h>
 
+#include <mutex>
 #include <string>
 
 #include "../../include/chatcarlo_b200_unet.h"
@@ -99,6 +100,27 @@ __device__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
     while (true) {
         if (mbar_try_wait(bar, parity)) return true;
         if (global_ns() - t0 > WAIT_NS) return false;
+    }
+}
+
+// One arrival on an mbarrier (release semantics, CTA scope).
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared::cta.b64 st, [%0];\n\t}" ::"r"(smem_u32(bar))
+                 : "memory");
+}
+
+// mbar_wait that also gives up once another thread of the CTA has set
+// *fail (its own wait ran out); sets *fail itself when its WAIT_NS run out.
+__device__ bool mbar_wait_or_fail(uint64_t* bar, uint32_t parity, volatile int* fail) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const unsigned long long t0 = global_ns();
+    while (true) {
+        if (mbar_try_wait(bar, parity)) return true;
+        if (*fail) return false;
+        if (global_ns() - t0 > WAIT_NS) {
+            *fail = 1;
+            return false;
+        }
     }
 }
 
@@ -738,6 +760,469 @@ __global__ void __launch_bounds__(THREADS) conv_stream_kernel(const ConvP P, int
 }
 
 // ---------------------------------------------------------------------------
+// the same streaming convolution with warp roles and no block-wide barriers
+// ---------------------------------------------------------------------------
+
+// The work unit is conv_stream_kernel's (output planes of one 16 x 8 column,
+// fed by a ring of halo planes, the packed weights resident), but:
+//  - each CTA takes one contiguous range of the (column, plane) sequence,
+//    T / gridDim.x planes, so that every CTA has the same work to within one
+//    plane; the range is cut into segments at column ends;
+//  - the ring holds `ring` planes (4 .. WS_RING_MAX), so that the copies run
+//    up to ring - 3 planes ahead of the MMAs;
+//  - the CTA's warps take fixed roles that hand work to each other through
+//    mbarriers instead of meeting at __syncthreads:
+//      warp 0, one thread: waits for the three input planes of output plane
+//        z and for a free accumulator, issues the 27 x cin/16 MMAs, commits
+//        to "accumulator full" and to "plane free" of the planes z's MMAs
+//        read last;
+//      warps 1-3: copy input planes into the ring as slots come free (each
+//        thread waits for its own copies, fences them for the tensor core
+//        and arrives on the slot's "plane full");
+//      warps 4-7: one output row per thread (the four warps are the four
+//        tensor-memory lane quarters), read an accumulator, store it and
+//        arrive on "accumulator free".
+// Plane L of the CTA's sequence (the planes zs - 1 .. ze of each segment in
+// turn) lives in ring slot L % ring; the MMAs of output plane z read planes
+// base + i .. base + i + 2 (i = z - zs, base the segment's first plane); z
+// is the last reader of plane base + i, and of the segment's last two
+// planes when z is its last output.
+constexpr int WS_RING_MAX = 12;
+constexpr int WS_LOADERS = 96;              // warps 1-3
+
+__host__ __device__ constexpr uint32_t ws_smem_bytes(int n, int cin, int ring) {
+    return (uint32_t)ring * (uint32_t)(cin / 8) * RING_V * 16 + (uint32_t)((27 * cin + KS - 1) / KS) * 8 * n * 16;
+}
+
+// Segment of the CTA's plane range that starts at sequence position g (g <
+// end): column (n, y0, x0), output planes [zs, ze).
+struct WsSeg {
+    int n, y0, x0, zs, ze;
+};
+__device__ __forceinline__ WsSeg ws_segment(const Src& S, long long g, long long end, int tiles_x, int tiles_y) {
+    WsSeg q;
+    const long long col = g / S.D;
+    q.zs = (int)(g - col * S.D);
+    q.ze = (int)min((long long)S.D, (long long)q.zs + (end - g));
+    q.x0 = (int)(col % tiles_x) * 8;
+    const long long r = col / tiles_x;
+    q.y0 = (int)(r % tiles_y) * 16;
+    q.n = (int)(r / tiles_y);
+    return q;
+}
+
+template <int N>
+__global__ void __launch_bounds__(THREADS, 4) conv_ws_kernel(const ConvP P, int ring) {
+    extern __shared__ __align__(128) uint8_t smem[];
+    __shared__ uint64_t full[WS_RING_MAX], empty[WS_RING_MAX], accf[2], acce[2];
+    __shared__ uint32_t s_tmem;
+    __shared__ int s_fail;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const Src& S = P.src;
+    const int cin = S.ca + S.cb, c8n = cin / 8;
+    const int tiles_x = (S.W + 7) / 8, tiles_y = (S.H + 15) / 16;
+    const long long total = (long long)S.B * tiles_y * tiles_x * S.D;
+    const long long g_begin = total * blockIdx.x / gridDim.x, g_end = total * (blockIdx.x + 1) / gridDim.x;
+    const uint32_t R = (uint32_t)ring;
+    const uint32_t slot16 = (uint32_t)c8n * RING_V;           // one ring slot, 16-byte units
+    const uint32_t ring_bytes = R * slot16 * 16;
+    const int w_chunks = ((27 * cin + KS - 1) / KS) * 8 * N;
+    constexpr uint32_t ACC = stream_acc_cols(N);
+    volatile int* fail = &s_fail;
+
+    if (warp == 0) tmem_alloc(&s_tmem, stream_tmem_cols(N));
+    if (tid == 0) {
+        for (uint32_t r = 0; r < R; ++r) {
+            mbar_init(&full[r], WS_LOADERS);
+            mbar_init(&empty[r], 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(&accf[b], 1);
+            mbar_init(&acce[b], 128);
+        }
+        s_fail = 0;
+        mbar_init_fence();
+    }
+    const uint32_t sbase = smem_u32(smem), swt = sbase + ring_bytes;
+    for (int i = tid; i < w_chunks; i += THREADS) cp_async16(swt + (uint32_t)i * 16, P.w + (size_t)i * 8, 16u);
+    cp_async_commit();
+    cp_async_wait<0>();
+    fence_proxy_async();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = s_tmem;
+
+    if (warp >= 1 && warp <= 3) {
+        // ---- loaders ----
+        const int lt = tid - 32;
+        uint32_t L = 0;                       // planes issued by this CTA
+        bool pending = false;                 // plane L - 1 issued but not yet published
+        for (long long g = g_begin; g < g_end && !*fail;) {
+            const WsSeg q = ws_segment(S, g, g_end, tiles_x, tiles_y);
+            g += q.ze - q.zs;
+            for (int zz = q.zs - 1; zz <= q.ze && !*fail; ++zz, ++L) {
+                const uint32_t slot = L % R;
+                if (L >= R) {
+                    const uint32_t par = ((L / R) - 1) & 1u;
+                    if (!mbar_try_wait(&empty[slot], par)) {
+                        // the slot is still read: publish the previous plane first
+                        if (pending) {
+                            cp_async_wait<0>();
+                            fence_proxy_async();
+                            mbar_arrive(&full[(L - 1) % R]);
+                            pending = false;
+                        }
+                        if (!mbar_wait_or_fail(&empty[slot], par, fail)) break;
+                    }
+                }
+                const uint32_t base = sbase + slot * slot16 * 16;
+                for (int i = lt; i < c8n * RING_V; i += WS_LOADERS) {
+                    const int c8 = i / RING_V, hv = i - c8 * RING_V;
+                    const int yy = q.y0 + hv / HALO_X - 1, xx = q.x0 + hv % HALO_X - 1;
+                    const int ch = c8 * 8;
+                    uint32_t bytes = 0;
+                    const void* src = S.a;
+                    if ((unsigned)zz < (unsigned)S.D && (unsigned)yy < (unsigned)S.H && (unsigned)xx < (unsigned)S.W) {
+                        bytes = 16;
+                        if (ch < S.ca) {
+                            src = S.a + ((((size_t)q.n * S.D + zz) * S.H + yy) * S.W + xx) * S.ca + ch;
+                        } else {
+                            const size_t cv = (((size_t)q.n * (S.D >> 1) + (zz >> 1)) * (S.H >> 1) + (yy >> 1)) *
+                                                  (S.W >> 1) + (xx >> 1);
+                            src = S.b + cv * S.cb + (ch - S.ca);
+                        }
+                    }
+                    cp_async16(base + (uint32_t)i * 16, src, bytes);
+                }
+                cp_async_commit();
+                // the previous plane's copies of this thread have landed: publish them
+                if (pending) {
+                    cp_async_wait<1>();
+                    fence_proxy_async();
+                    mbar_arrive(&full[(L - 1) % R]);
+                }
+                pending = true;
+            }
+        }
+        cp_async_wait<0>();
+        fence_proxy_async();
+        if (pending && !*fail) mbar_arrive(&full[(L - 1) % R]);
+    } else if (warp == 0 && lane == 0) {
+        // ---- MMA issuer ----
+        uint32_t K = 0, waited = 0, base = 0;     // output planes issued, input planes seen full, segment's first plane
+        const uint64_t a0 = smem_desc(sbase, RING_V * 16, HALO_X * 16);
+        const uint64_t b0 = smem_desc(swt, N * 16, 128);
+        constexpr uint32_t IDESC = idesc_bf16(TILE_M, N, 0, 0);
+        for (long long g = g_begin; g < g_end && !*fail;) {
+            const WsSeg q = ws_segment(S, g, g_end, tiles_x, tiles_y);
+            g += q.ze - q.zs;
+            for (int z = q.zs; z < q.ze && !*fail; ++z, ++K) {
+                const uint32_t p0 = base + (uint32_t)(z - q.zs);          // plane z - 1
+                bool ok = true;
+                while (ok && waited <= p0 + 2) {
+                    ok = mbar_wait_or_fail(&full[waited % R], (waited / R) & 1u, fail);
+                    ++waited;
+                }
+                if (ok && K >= 2) ok = mbar_wait_or_fail(&acce[K & 1u], ((K >> 1) - 1) & 1u, fail);
+                if (!ok) break;
+                tc_fence_after();
+                const uint32_t acc = tmem + (K & 1u) * ACC;
+                const uint32_t s0 = (p0 % R) * slot16, s1 = ((p0 + 1) % R) * slot16, s2 = ((p0 + 2) % R) * slot16;
+                for (int dz = 0; dz < 3; ++dz) {
+                    const uint32_t so = dz == 0 ? s0 : (dz == 1 ? s1 : s2);
+#pragma unroll
+                    for (int t = 0; t < 9; ++t) {
+                        const int tap = dz * 9 + t;
+                        const uint32_t ta = so + (uint32_t)((t / 3) * HALO_X + t % 3);
+                        for (int j = 0; j < c8n / 2; ++j)
+                            mma_bf16(acc, a0 + ta + (uint32_t)(2 * j * RING_V),
+                                     b0 + (uint32_t)((tap * c8n + 2 * j) * N), IDESC, (tap > 0 || j > 0) ? 1u : 0u);
+                    }
+                }
+                mma_commit(&accf[K & 1u]);
+                mma_commit(&empty[p0 % R]);
+                if (z == q.ze - 1) {
+                    mma_commit(&empty[(p0 + 1) % R]);
+                    mma_commit(&empty[(p0 + 2) % R]);
+                }
+            }
+            base += (uint32_t)(q.ze - q.zs) + 2;
+        }
+        // every issued MMA has finished before the tensor memory can be freed
+        if (K > 0) mbar_wait(&accf[(K - 1) & 1u], ((K - 1) >> 1) & 1u);
+    } else if (warp >= 4) {
+        // ---- epilogue: row m of the tile, lane quarter warp - 4 ----
+        const int qw = warp - 4, m = qw * 32 + lane;
+        uint32_t K = 0;
+        for (long long g = g_begin; g < g_end && !*fail;) {
+            const WsSeg q = ws_segment(S, g, g_end, tiles_x, tiles_y);
+            g += q.ze - q.zs;
+            const int y = q.y0 + (m >> 3), x = q.x0 + (m & 7);
+            for (int z = q.zs; z < q.ze; ++z, ++K) {
+                // one waiter per warp keeps the warp-collective loads uniform
+                int w = 1;
+                if (lane == 0) w = mbar_wait_or_fail(&accf[K & 1u], (K >> 1) & 1u, fail) ? 1 : 0;
+                if (!__shfl_sync(0xffffffffu, w, 0)) break;
+                tc_fence_after();
+                const uint32_t acc = tmem + (K & 1u) * ACC + ((uint32_t)(qw * 32) << 16);
+                const long long v = (((long long)q.n * S.D + z) * S.H + y) * S.W + x;
+#pragma unroll
+                for (int c0 = 0; c0 < N; c0 += 8) {
+                    float f[8];
+                    tmem_ld8(acc + (uint32_t)c0, f);
+                    if (y < S.H && x < S.W) conv_store(P, v, c0, N, f);
+                }
+                tc_fence_before();
+                mbar_arrive(&acce[K & 1u]);
+            }
+        }
+    }
+    __syncthreads();
+    if (tid == 0 && s_fail) atomicOr(&g_status, 1u);
+    tc_fence_after();
+    if (warp == 0) tmem_dealloc(tmem, stream_tmem_cols(N));
+}
+
+// ---------------------------------------------------------------------------
+// plane-stationary streaming convolution (16 or 32 output channels)
+// ---------------------------------------------------------------------------
+
+// A tcgen05.mma that accumulates into the accumulator of the previous one
+// waits for it: a chain of MMAs on one accumulator runs at one MMA per
+// ~125 cycles (A in shared memory) whatever N is, so 16 or 32 output
+// channels per MMA leave the tensor core mostly idle.  Here each input
+// plane p is read by ONE chain of 9 x cin/16 MMAs (the in-plane taps dy,
+// dx) against the three weight planes dz stacked along N (N = 3 x cout):
+//     D_p[m][dz * cout + co] = sum_{dy, dx, ci} W[dz, dy, dx][co][ci] x_p(m + (dy, dx))[ci]
+// and output plane z is D_{z-1}[.., 0 | ..] + D_z[.., 1 | ..] + D_{z+1}[.., 2 | ..],
+// summed in FP32 by the epilogue from three tensor-memory regions.  A is
+// read a third as often as by the output-stationary kernels, and N is
+// three times wider.  Q = 4 regions of 3 x cout columns (at 64- or 128-
+// column steps): the MMAs of plane p + 1 overlap the epilogue of output
+// p - 1.
+// Work split, ring of halo planes, warp roles and loader as conv_ws_kernel;
+// the barriers are: full / empty per ring slot (one MMA group reads each
+// plane), rfull per region (the plane's MMAs are done) and rfree per region
+// (the last output that reads the region, z + 1 for D_z, is stored).
+// Channel passes: the kernel reads input channel groups [c8_lo, c8_hi) (8
+// channels each) and the matching weight rows only, so that layers whose
+// weights do not fit shared memory run as several passes: every pass but
+// the last adds into an FP32 partial sum [v][cout] (part_out), the last adds
+// the partial (part_in) before bias, ReLU, mask and the BF16 store.
+constexpr int PS_REGIONS = 4;
+
+// tensor-memory columns of one region (3 x cout, rounded up to 64 / 128) and of a CTA
+__host__ __device__ constexpr uint32_t ps_region_cols(int n) { return n <= 16 ? 64u : 128u; }
+__host__ __device__ constexpr uint32_t ps_tmem_cols(int n) { return PS_REGIONS * ps_region_cols(n); }
+__host__ __device__ constexpr uint32_t ps_weight_bytes(int n, int c8p) { return 9u * (uint32_t)c8p * 3u * n * 16u; }
+__host__ __device__ constexpr uint32_t ps_smem_bytes(int n, int c8p, int ring) {
+    return (uint32_t)ring * (uint32_t)c8p * RING_V * 16 + ps_weight_bytes(n, c8p);
+}
+
+struct PsPass {
+    int c8_lo, c8_hi;          // input channel groups of this pass
+    const float* part_in;      // FP32 partial sums [v][cout] to add, or null
+    float* part_out;           // FP32 sums [v][cout] out (no bias / ReLU / BF16), or null
+};
+
+template <int NO>
+__global__ void __launch_bounds__(THREADS, 1) conv_ps_kernel(const ConvP P, const PsPass Q, int ring) {
+    constexpr int NP = 3 * NO;                                // MMA N: the three dz weight planes
+    constexpr uint32_t RC = ps_region_cols(NO);
+    extern __shared__ __align__(128) uint8_t smem[];
+    __shared__ uint64_t full[WS_RING_MAX], empty[WS_RING_MAX], rfull[PS_REGIONS], rfree[PS_REGIONS];
+    __shared__ uint32_t s_tmem;
+    __shared__ int s_fail;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const Src& S = P.src;
+    const int c8n = (S.ca + S.cb) / 8, c8p = Q.c8_hi - Q.c8_lo;
+    const int tiles_x = (S.W + 7) / 8, tiles_y = (S.H + 15) / 16;
+    const long long total = (long long)S.B * tiles_y * tiles_x * S.D;
+    const long long g_begin = total * blockIdx.x / gridDim.x, g_end = total * (blockIdx.x + 1) / gridDim.x;
+    const uint32_t R = (uint32_t)ring;
+    const uint32_t slot16 = (uint32_t)c8p * RING_V;           // one ring slot, 16-byte units
+    volatile int* fail = &s_fail;
+
+    if (warp == 0) tmem_alloc(&s_tmem, ps_tmem_cols(NO));
+    if (tid == 0) {
+        for (uint32_t r = 0; r < R; ++r) {
+            mbar_init(&full[r], WS_LOADERS);
+            mbar_init(&empty[r], 1);
+        }
+        for (int r = 0; r < PS_REGIONS; ++r) {
+            mbar_init(&rfull[r], 1);
+            mbar_init(&rfree[r], 128);
+        }
+        s_fail = 0;
+        mbar_init_fence();
+    }
+    // weights: packed chunk (tap * c8n + c8, co) -> (t9 * c8p + c8 - c8_lo, dz * NO + co)
+    const uint32_t sbase = smem_u32(smem), swt = sbase + R * slot16 * 16;
+    for (int i = tid; i < 9 * c8p * NP; i += THREADS) {
+        const int r = i % NP, g = i / NP;
+        const int t9 = g / c8p, c8 = Q.c8_lo + g % c8p, dz = r / NO, co = r % NO;
+        const int src = ((dz * 9 + t9) * c8n + c8) * NO + co;
+        cp_async16(swt + (uint32_t)i * 16, P.w + (size_t)src * 8, 16u);
+    }
+    cp_async_commit();
+    cp_async_wait<0>();
+    fence_proxy_async();
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = s_tmem;
+
+    if (warp >= 1 && warp <= 3) {
+        // ---- loaders: planes zs - 1 .. ze of each segment, channel groups of the pass ----
+        const int lt = tid - 32;
+        uint32_t L = 0;
+        bool pending = false;
+        for (long long g = g_begin; g < g_end && !*fail;) {
+            const WsSeg q = ws_segment(S, g, g_end, tiles_x, tiles_y);
+            g += q.ze - q.zs;
+            for (int zz = q.zs - 1; zz <= q.ze && !*fail; ++zz, ++L) {
+                const uint32_t slot = L % R;
+                if (L >= R) {
+                    const uint32_t par = ((L / R) - 1) & 1u;
+                    if (!mbar_try_wait(&empty[slot], par)) {
+                        if (pending) {
+                            cp_async_wait<0>();
+                            fence_proxy_async();
+                            mbar_arrive(&full[(L - 1) % R]);
+                            pending = false;
+                        }
+                        if (!mbar_wait_or_fail(&empty[slot], par, fail)) break;
+                    }
+                }
+                const uint32_t base = sbase + slot * slot16 * 16;
+                for (int i = lt; i < c8p * RING_V; i += WS_LOADERS) {
+                    const int c8 = i / RING_V, hv = i - c8 * RING_V;
+                    const int yy = q.y0 + hv / HALO_X - 1, xx = q.x0 + hv % HALO_X - 1;
+                    const int ch = (Q.c8_lo + c8) * 8;
+                    uint32_t bytes = 0;
+                    const void* src = S.a;
+                    if ((unsigned)zz < (unsigned)S.D && (unsigned)yy < (unsigned)S.H && (unsigned)xx < (unsigned)S.W) {
+                        bytes = 16;
+                        if (ch < S.ca) {
+                            src = S.a + ((((size_t)q.n * S.D + zz) * S.H + yy) * S.W + xx) * S.ca + ch;
+                        } else {
+                            const size_t cv = (((size_t)q.n * (S.D >> 1) + (zz >> 1)) * (S.H >> 1) + (yy >> 1)) *
+                                                  (S.W >> 1) + (xx >> 1);
+                            src = S.b + cv * S.cb + (ch - S.ca);
+                        }
+                    }
+                    cp_async16(base + (uint32_t)i * 16, src, bytes);
+                }
+                cp_async_commit();
+                if (pending) {
+                    cp_async_wait<1>();
+                    fence_proxy_async();
+                    mbar_arrive(&full[(L - 1) % R]);
+                }
+                pending = true;
+            }
+        }
+        cp_async_wait<0>();
+        fence_proxy_async();
+        if (pending && !*fail) mbar_arrive(&full[(L - 1) % R]);
+    } else if (warp == 0 && lane == 0) {
+        // ---- MMA issuer: one chain of 9 x c8p / 2 MMAs per input plane ----
+        const uint64_t a0 = smem_desc(sbase, RING_V * 16, HALO_X * 16);
+        const uint64_t b0 = smem_desc(swt, NP * 16, 128);
+        constexpr uint32_t IDESC = idesc_bf16(TILE_M, NP, 0, 0);
+        uint32_t L = 0;
+        for (long long g = g_begin; g < g_end && !*fail;) {
+            const WsSeg q = ws_segment(S, g, g_end, tiles_x, tiles_y);
+            g += q.ze - q.zs;
+            bool ok = true;
+            for (int zz = q.zs - 1; zz <= q.ze && ok; ++zz, ++L) {
+                const uint32_t rg = L % PS_REGIONS;
+                ok = mbar_wait_or_fail(&full[L % R], (L / R) & 1u, fail);
+                if (ok && L >= PS_REGIONS) ok = mbar_wait_or_fail(&rfree[rg], ((L / PS_REGIONS) - 1) & 1u, fail);
+                if (!ok) break;
+                tc_fence_after();
+                const uint32_t d = tmem + rg * RC;
+                const uint32_t so = (L % R) * slot16;
+#pragma unroll
+                for (int t9 = 0; t9 < 9; ++t9) {
+                    const uint32_t ta = so + (uint32_t)((t9 / 3) * HALO_X + t9 % 3);
+                    for (int j = 0; j < c8p / 2; ++j)
+                        mma_bf16(d, a0 + ta + (uint32_t)(2 * j * RING_V), b0 + (uint32_t)((t9 * c8p + 2 * j) * NP),
+                                 IDESC, (t9 > 0 || j > 0) ? 1u : 0u);
+                }
+                mma_commit(&rfull[rg]);
+                mma_commit(&empty[L % R]);
+            }
+            if (!ok) break;
+        }
+        // every issued MMA has finished before the tensor memory can be freed
+        if (L > 0) mbar_wait(&rfull[(L - 1) % PS_REGIONS], ((L - 1) / PS_REGIONS) & 1u);
+    } else if (warp >= 4) {
+        // ---- epilogue: output z = D_{z-1}[dz 0] + D_z[dz 1] + D_{z+1}[dz 2]; row m, lane quarter warp - 4 ----
+        const int qw = warp - 4, m = qw * 32 + lane;
+        const uint32_t lq = (uint32_t)(qw * 32) << 16;
+        uint32_t base = 0;                                     // sequence index of the segment's plane zs - 1
+        for (long long g = g_begin; g < g_end && !*fail;) {
+            const WsSeg q = ws_segment(S, g, g_end, tiles_x, tiles_y);
+            g += q.ze - q.zs;
+            const int y = q.y0 + (m >> 3), x = q.x0 + (m & 7);
+            const bool in = y < S.H && x < S.W;
+            bool ok = true;
+            for (int z = q.zs; z < q.ze; ++z) {
+                const uint32_t L1 = base + (uint32_t)(z - q.zs) + 2;        // plane z + 1
+                int w = 1;
+                if (lane == 0) w = mbar_wait_or_fail(&rfull[L1 % PS_REGIONS], (L1 / PS_REGIONS) & 1u, fail) ? 1 : 0;
+                if (!__shfl_sync(0xffffffffu, w, 0)) {
+                    ok = false;
+                    break;
+                }
+                tc_fence_after();
+                const uint32_t rm = tmem + ((L1 - 2) % PS_REGIONS) * RC + lq;
+                const uint32_t r0 = tmem + ((L1 - 1) % PS_REGIONS) * RC + NO + lq;
+                const uint32_t rp = tmem + (L1 % PS_REGIONS) * RC + 2 * NO + lq;
+                const long long v = (((long long)q.n * S.D + z) * S.H + y) * S.W + x;
+#pragma unroll
+                for (int c0 = 0; c0 < NO; c0 += 8) {
+                    float f[8], f1[8], f2[8];
+                    tmem_ld8(rm + (uint32_t)c0, f);
+                    tmem_ld8(r0 + (uint32_t)c0, f1);
+                    tmem_ld8(rp + (uint32_t)c0, f2);
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) f[j] = (f[j] + f1[j]) + f2[j];
+                    if (!in) continue;
+                    if (Q.part_in) {
+                        const float4* pi = reinterpret_cast<const float4*>(Q.part_in + (size_t)v * NO + c0);
+                        const float4 u0 = __ldg(pi), u1 = __ldg(pi + 1);
+                        f[0] += u0.x, f[1] += u0.y, f[2] += u0.z, f[3] += u0.w;
+                        f[4] += u1.x, f[5] += u1.y, f[6] += u1.z, f[7] += u1.w;
+                    }
+                    if (Q.part_out) {
+                        float4* po = reinterpret_cast<float4*>(Q.part_out + (size_t)v * NO + c0);
+                        po[0] = make_float4(f[0], f[1], f[2], f[3]);
+                        po[1] = make_float4(f[4], f[5], f[6], f[7]);
+                    } else {
+                        conv_store(P, v, c0, NO, f);
+                    }
+                }
+                tc_fence_before();
+                mbar_arrive(&rfree[(L1 - 2) % PS_REGIONS]);             // plane z - 1: last reader done
+                if (z == q.ze - 1) {
+                    mbar_arrive(&rfree[(L1 - 1) % PS_REGIONS]);
+                    mbar_arrive(&rfree[L1 % PS_REGIONS]);
+                }
+            }
+            if (!ok) break;
+            base += (uint32_t)(q.ze - q.zs) + 2;
+        }
+    }
+    __syncthreads();
+    if (tid == 0 && s_fail) atomicOr(&g_status, 1u);
+    tc_fence_after();
+    if (warp == 0) tmem_dealloc(tmem, ps_tmem_cols(NO));
+}
+
+// ---------------------------------------------------------------------------
 // weight gradient: dW[tap][co][ci] += sum_v dz[v][co] * X[v + off(tap)][ci]
 // ---------------------------------------------------------------------------
 
@@ -1295,8 +1780,11 @@ int launch_conv(const ConvP& P, cudaStream_t st) {
     return CCU_OK;
 }
 
-// 0: the streaming halo kernel where it applies, 1: always the gathering
-// kernel, 2: the one-tile halo kernel where it applies
+// 0: the plane-stationary kernel where it applies, else the streaming halo
+// kernel where it applies, else the gathering kernel; 1: always the
+// gathering kernel; 2: the one-tile halo kernel where it applies; 3: the
+// warp-role streaming kernel where the streaming kernel applies; 4: path 0
+// without the plane-stationary kernel
 int g_conv_path = 0;
 
 bool halo_applies(const ConvP& P, int n_out) {
@@ -1307,29 +1795,155 @@ bool halo_applies(const ConvP& P, int n_out) {
 
 bool stream_applies(const ConvP& P, int n_out) {
     const int cin = P.src.ca + P.src.cb;
-    return g_conv_path == 0 && cin <= 48 && n_out <= 48 && stream_smem_bytes(n_out, cin) <= 200 * 1024;
+    return (g_conv_path == 0 || g_conv_path == 3 || g_conv_path == 4) && cin <= 48 && n_out <= 48 &&
+           stream_smem_bytes(n_out, cin) <= 200 * 1024;
 }
+
+// Channel passes of the plane-stationary kernel for cin input channels: the
+// fewest passes of equal 16-channel-aligned groups whose weights and a
+// ring of 3 planes fit 200 KB of shared memory (0: does not apply).
+int ps_passes(int n_out, int cin) {
+    if (g_conv_path != 0 || (n_out != 16 && n_out != 32) || cin % 16) return 0;
+    const int c16 = cin / 16;
+    for (int passes = 1; passes <= c16; ++passes) {
+        const int c8p = 2 * ((c16 + passes - 1) / passes);
+        if (ps_smem_bytes(n_out, c8p, 3) <= 200 * 1024) return passes;
+    }
+    return 0;
+}
+
+// Resident CTAs per SM of a kernel launched with THREADS threads and this
+// dynamic shared memory: shared memory (1 KB of it reserved per CTA), the
+// registers of its threads, the 512 tensor-memory columns and the 2048
+// threads of an SM.
+template <typename Kern>
+int resident_ctas(Kern kernel, size_t smem, uint32_t cols, int& resident) {
+    int dev = 0, per_sm = 0;
+    CU_CHECK(cudaGetDevice(&dev));
+    CU_CHECK(cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
+    cudaFuncAttributes fa;
+    CU_CHECK(cudaFuncGetAttributes(&fa, kernel));
+    const int regs = ((std::max(fa.numRegs, 1) + 7) / 8) * 8;      // allocated per thread in steps of 8
+    resident = std::max(1, std::min({(int)((size_t)per_sm / (smem + 1024)), 65536 / (regs * THREADS),
+                                     (int)(512u / cols), 2048 / THREADS}));
+    return CCU_OK;
+}
+
+// ring depth of the warp-role kernel (0: chosen per layer)
+int g_conv_ring = 0;
 
 template <int N>
 int launch_conv_stream(const ConvP& P, cudaStream_t st) {
     const int cin = P.src.ca + P.src.cb;
+    int dev = 0, sms = 0;
+    CU_CHECK(cudaGetDevice(&dev));
+    CU_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     size_t smem = 0;
-    int rc = tc_launch_smem(conv_stream_kernel<N>, stream_smem_bytes(N, cin), stream_tmem_cols(N), smem);
+    int rc = CCU_OK, resident = 1;
+    if (g_conv_path == 3) {
+        // deepest useful ring: most planes in flight per SM (resident CTAs x
+        // the ring - 3 planes each copies ahead of its MMAs)
+        const long long planes = (long long)P.src.B * ((P.src.H + 15) / 16) * ((P.src.W + 7) / 8) * P.src.D;
+        int ring = g_conv_ring;
+        if (ring == 0) {
+            int per_sm = 0, best = -1;
+            CU_CHECK(cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
+            // tc_launch_smem's floor: no more CTAs per SM than the tensor memory holds
+            const size_t floor_smem = (size_t)per_sm / (512u / stream_tmem_cols(N) + 1) + 1024;
+            for (int r = 4; r <= WS_RING_MAX && ws_smem_bytes(N, cin, r) <= 200 * 1024; ++r) {
+                int res = 1;
+                rc = resident_ctas(conv_ws_kernel<N>, std::max<size_t>(ws_smem_bytes(N, cin, r), floor_smem),
+                                   stream_tmem_cols(N), res);
+                if (rc != CCU_OK) return rc;
+                if (res * (r - 3) > best) best = res * (r - 3), ring = r;
+            }
+        }
+        if (ws_smem_bytes(N, cin, ring) > 200 * 1024) return set_error(CCU_E_INVALID, "ring too deep for this layer");
+        rc = tc_launch_smem(conv_ws_kernel<N>, ws_smem_bytes(N, cin, ring), stream_tmem_cols(N), smem);
+        if (rc != CCU_OK) return rc;
+        if ((rc = resident_ctas(conv_ws_kernel<N>, smem, stream_tmem_cols(N), resident)) != CCU_OK) return rc;
+        const long long grid = std::min<long long>(planes, (long long)sms * resident);
+        conv_ws_kernel<N><<<(unsigned)grid, THREADS, smem, st>>>(P, ring);
+        CU_CHECK(cudaGetLastError());
+        return CCU_OK;
+    }
+    rc = tc_launch_smem(conv_stream_kernel<N>, stream_smem_bytes(N, cin), stream_tmem_cols(N), smem);
     if (rc != CCU_OK) return rc;
     const long long items = (long long)P.src.B * ((P.src.H + 15) / 16) * ((P.src.W + 7) / 8) *
                             ((P.src.D + ZSEG - 1) / ZSEG);
     if (items >= (1LL << 31)) return set_error(CCU_E_INVALID, "volume too large");
-    // resident CTAs per SM: shared memory (1 KB of it reserved per CTA), the
-    // 512 tensor-memory columns and 2048 threads per SM
-    int dev = 0, sms = 0, per_sm = 0;
-    CU_CHECK(cudaGetDevice(&dev));
-    CU_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    CU_CHECK(cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
-    const int resident = std::max(1, std::min({(int)((size_t)per_sm / (smem + 1024)),
-                                               (int)(512u / stream_tmem_cols(N)), 2048 / THREADS}));
+    if ((rc = resident_ctas(conv_stream_kernel<N>, smem, stream_tmem_cols(N), resident)) != CCU_OK) return rc;
     const long long grid = std::min<long long>(items, (long long)sms * resident);
     conv_stream_kernel<N><<<(unsigned)grid, THREADS, smem, st>>>(P, (int)items);
     CU_CHECK(cudaGetLastError());
+    return CCU_OK;
+}
+
+// FP32 partial sums of multi-pass plane-stationary convolutions: one
+// buffer per device, grown on demand (the stream is drained before an
+// older, smaller buffer is freed) and kept for the process.
+std::mutex g_ws_mu;
+void* g_ws[64] = {};
+size_t g_ws_bytes[64] = {};
+
+int ps_workspace(size_t bytes, cudaStream_t st, float*& ws) {
+    int dev = 0;
+    CU_CHECK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return set_error(CCU_E_INVALID, "device index out of range");
+    std::lock_guard<std::mutex> lk(g_ws_mu);
+    if (g_ws_bytes[dev] < bytes) {
+        if (g_ws[dev]) {
+            CU_CHECK(cudaStreamSynchronize(st));
+            CU_CHECK(cudaFree(g_ws[dev]));
+            g_ws[dev] = nullptr;
+            g_ws_bytes[dev] = 0;
+        }
+        CU_CHECK(cudaMalloc(&g_ws[dev], bytes));
+        g_ws_bytes[dev] = bytes;
+    }
+    ws = (float*)g_ws[dev];
+    return CCU_OK;
+}
+
+template <int NO>
+int launch_conv_ps(const ConvP& P, int passes, cudaStream_t st) {
+    const int c8n = (P.src.ca + P.src.cb) / 8;
+    const int c8p_max = 2 * ((c8n / 2 + passes - 1) / passes);
+    int dev = 0, sms = 0;
+    CU_CHECK(cudaGetDevice(&dev));
+    CU_CHECK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const long long planes = (long long)P.src.B * ((P.src.H + 15) / 16) * ((P.src.W + 7) / 8) * P.src.D;
+    float* ws = nullptr;
+    if (passes > 1) {
+        const int rc = ps_workspace((size_t)P.n_vox * NO * sizeof(float), st, ws);
+        if (rc != CCU_OK) return rc;
+    }
+    for (int k = 0, lo = 0; lo < c8n; ++k, lo += c8p_max) {
+        PsPass Q;
+        Q.c8_lo = lo;
+        Q.c8_hi = std::min(c8n, lo + c8p_max);
+        Q.part_in = k > 0 ? ws : nullptr;
+        Q.part_out = Q.c8_hi < c8n ? ws : nullptr;
+        const int c8p = Q.c8_hi - Q.c8_lo;
+        // deepest ring (2 .. WS_RING_MAX planes) that keeps the CTAs per SM the tensor memory allows
+        int ring = 0, best_res = 0;
+        size_t smem = 0;
+        for (int r = 2; r <= WS_RING_MAX && ps_smem_bytes(NO, c8p, r) <= 200 * 1024; ++r) {
+            int res = 1;
+            const int rc = resident_ctas(conv_ps_kernel<NO>, (size_t)ps_smem_bytes(NO, c8p, r) + 1024,
+                                         ps_tmem_cols(NO), res);
+            if (rc != CCU_OK) return rc;
+            if (res >= best_res) best_res = res, ring = r;
+        }
+        if (ring == 0) return set_error(CCU_E_INVALID, "plane-stationary pass does not fit shared memory");
+        int rc = tc_launch_smem(conv_ps_kernel<NO>, ps_smem_bytes(NO, c8p, ring), ps_tmem_cols(NO), smem);
+        if (rc != CCU_OK) return rc;
+        int resident = 1;
+        if ((rc = resident_ctas(conv_ps_kernel<NO>, smem, ps_tmem_cols(NO), resident)) != CCU_OK) return rc;
+        const long long grid = std::min<long long>(planes, (long long)sms * resident);
+        conv_ps_kernel<NO><<<(unsigned)grid, THREADS, smem, st>>>(P, Q, ring);
+        CU_CHECK(cudaGetLastError());
+    }
     return CCU_OK;
 }
 
@@ -1405,6 +2019,10 @@ int ccu_conv3d(const void* a, int ca, const void* b, int cb, int batch, int d, i
     P.split = split;
     P.out1 = (__nv_bfloat16*)out1;
     cudaStream_t st = (cudaStream_t)stream;
+    if (const int passes = ps_passes(cout, ca + cb)) {
+        if (cout == 16) return launch_conv_ps<16>(P, passes, st);
+        return launch_conv_ps<32>(P, passes, st);
+    }
     if (stream_applies(P, cout)) {
         switch (cout) {
             case 16: return launch_conv_stream<16>(P, st);
@@ -1555,10 +2173,19 @@ int ccu_pack_weights(const float* w32, int cout, int cin, void* w, void* wt, voi
 }
 
 int ccu_set_conv_path(int path) {
-    if (path < 0 || path > 2)
-        return set_error(CCU_E_INVALID, "path must be 0 (streaming halo kernel where it applies), 1 (gathering "
-                                        "kernel) or 2 (one-tile halo kernel where it applies)");
+    if (path < 0 || path > 4)
+        return set_error(CCU_E_INVALID, "path must be 0 (plane-stationary, else streaming, else gathering kernel), "
+                                        "1 (gathering kernel), 2 (one-tile halo kernel where it applies), 3 (the "
+                                        "streaming kernel with warp roles) or 4 (path 0 without the "
+                                        "plane-stationary kernel)");
     g_conv_path = path;
+    return CCU_OK;
+}
+
+int ccu_set_conv_ring(int ring) {
+    if (ring != 0 && (ring < 4 || ring > WS_RING_MAX))
+        return set_error(CCU_E_INVALID, "ring must be 0 (chosen per layer) or 4 .. 12 planes");
+    g_conv_ring = ring;
     return CCU_OK;
 }
 

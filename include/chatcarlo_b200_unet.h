@@ -107,13 +107,25 @@ long long ccu_packed_weight_elems(int n, int c);
  * c = cout; taps flipped, channels transposed). */
 int ccu_pack_weights(const float* w32, int cout, int cin, void* w, void* wt, void* stream);
 
-/* Which convolution kernel ccu_conv3d uses: 0 (default) the persistent
- * halo kernel that streams z-planes through a shared-memory ring where it
- * applies (input and output channels <= 48) and the gathering kernel
- * elsewhere; 1 always the gathering kernel; 2 the one-tile halo kernel where
- * it applies (channels <= 48, h % 16 == 0, w % 8 == 0; for comparisons).
- * Process-wide. */
+/* Which convolution kernel ccu_conv3d uses: 0 (default) the
+ * plane-stationary kernel for 16 or 32 output channels (in channel passes
+ * with an FP32 partial sum when the weights do not fit shared memory at
+ * once; the partial lives in a per-device workspace of n_vox x cout x 4
+ * bytes that the first such call allocates and the process keeps), else the
+ * persistent halo kernel that streams z-planes through a shared-memory ring
+ * where it applies (input and output channels <= 48), else the gathering
+ * kernel; 1 always the gathering kernel; 2 the one-tile halo kernel where
+ * it applies (channels <= 48, h % 16 == 0, w % 8 == 0; for comparisons);
+ * 3 the streaming kernel with warp roles (loader, MMA and epilogue warps
+ * handing off through mbarriers) where the streaming kernel applies; 4
+ * path 0 without the plane-stationary kernel.  Process-wide. */
 int ccu_set_conv_path(int path);
+
+/* Ring depth (input planes held in shared memory) of path 3: 0 (default)
+ * chosen per layer to keep the most planes in flight per SM, else 4 .. 12
+ * (a ring that does not fit a layer's shared memory makes ccu_conv3d fail
+ * with CCU_E_INVALID).  Process-wide. */
+int ccu_set_conv_ring(int ring);
 
 /* cudaMemsetAsync(p, 0, bytes) on the stream (gradient buffers). */
 int ccu_zero(void* p, long long bytes, void* stream);

@@ -58,7 +58,12 @@ def _up(x):
                                              (128, 0, 128, (1, 5, 3, 7)), (16, 0, 192, (1, 4, 4, 4)),
                                              # shapes of the shared-memory halo kernel (H % 16, W % 8)
                                              (16, 0, 16, (2, 3, 16, 8)), (16, 32, 48, (1, 4, 32, 16)),
-                                             (32, 0, 32, (1, 2, 16, 24)), (16, 32, 16, (2, 2, 16, 16))])
+                                             (32, 0, 32, (1, 2, 16, 24)), (16, 32, 16, (2, 2, 16, 16)),
+                                             # plane-stationary kernel: 2 and 3 channel passes (FP32
+                                             # partial sums), split outputs with fine and coarse
+                                             # channels in one pass, edge tiles
+                                             (32, 64, 32, (1, 6, 8, 8)), (64, 128, 32, (1, 4, 6, 8)),
+                                             (16, 16, 32, (2, 6, 12, 10)), (16, 0, 16, (1, 1, 19, 9))])
 def test_conv3d_forward(U, ca, cb, cout, dims):
     gen = torch.Generator().manual_seed(ca * 1000 + cb * 10 + cout)
     B, D, H, W = dims
@@ -164,10 +169,12 @@ def test_pool_upsample_bias_helpers(U):
                                                 # edge tiles of the streaming kernel (h % 16, w % 8 != 0)
                                                 (2, 6, 10, 12, 16, 32, 32), (1, 20, 38, 19, 16, 0, 16)])
 def test_halo_and_gathering_kernels_agree(U, B, D, H, W, ca, cb, cout):
-    """The three forward kernels on the same inputs: the streaming halo
-    kernel (path 0; depths that are not a multiple of its 16-plane segment
-    and several volumes), the gathering kernel (path 1) and the one-tile
-    halo kernel (path 2)."""
+    """The forward kernels on the same inputs: the default path 0 (the
+    plane-stationary kernel for 16 and 32 output channels), the gathering
+    kernel (path 1), the one-tile halo kernel (path 2), the streaming kernel
+    with warp roles (path 3) and the streaming halo kernel (path 4; depths
+    that are not a multiple of its 16-plane segment, several volumes); paths
+    3 and 4 issue the same MMAs in the same order and agree bit for bit."""
     gen = torch.Generator().manual_seed(77 + D)
     a = _bf((B, D, H, W, ca), gen)
     b = _bf((B, D // 2, H // 2, W // 2, cb), gen) if cb else None
@@ -176,7 +183,7 @@ def test_halo_and_gathering_kernels_agree(U, B, D, H, W, ca, cb, cout):
     U.check(U.lib().ccu_pack_weights(_ptr(w32), cout, ca + cb, _ptr(w), None, None))
     outs = []
     try:
-        for path in (0, 1, 2):
+        for path in (0, 1, 2, 3, 4):
             U.check(U.lib().ccu_set_conv_path(path))
             o = torch.empty(B, D, H, W, cout, dtype=torch.bfloat16, device="cuda")
             U.check(U.lib().ccu_conv3d(_ptr(a), ca, _ptr(b) if b is not None else None, cb, B, D, H, W, _ptr(w),
@@ -186,13 +193,57 @@ def test_halo_and_gathering_kernels_agree(U, B, D, H, W, ca, cb, cout):
         U.check(U.lib().ccu_set_conv_path(0))
     torch.cuda.synchronize()
     assert U.status() == 0
-    torch.testing.assert_close(outs[0], outs[1], rtol=1.6e-2, atol=1e-2)
-    torch.testing.assert_close(outs[2], outs[1], rtol=1.6e-2, atol=1e-2)
+    for k in (0, 2, 4):
+        torch.testing.assert_close(outs[k], outs[1], rtol=1.6e-2, atol=1e-2)
+    torch.testing.assert_close(outs[3], outs[4], rtol=0, atol=0)
     x = _to_ncdhw(a)
     if cb:
         x = torch.cat([x, _up(_to_ncdhw(b))], dim=1)
     ref = torch.nn.functional.conv3d(x, _torch_w(w32.to(torch.bfloat16), cout, ca + cb), padding=1)
-    torch.testing.assert_close(outs[0], ref.permute(0, 2, 3, 4, 1), rtol=1.6e-2, atol=1e-2)
+    for k in (0, 4):
+        torch.testing.assert_close(outs[k], ref.permute(0, 2, 3, 4, 1), rtol=1.6e-2, atol=1e-2)
+
+
+@pytest.mark.parametrize("B,D,H,W,ca,cb,cout", [(1, 37, 16, 8, 16, 0, 16), (2, 6, 10, 12, 16, 32, 32),
+                                                (1, 3, 40, 24, 16, 0, 48), (3, 1, 16, 16, 32, 0, 16)])
+def test_warp_role_kernel_ring_depths(U, B, D, H, W, ca, cb, cout):
+    """Path 3 with every ring depth that fits the layer, bit for bit equal to
+    path 4 (the same MMAs in the same order); a ring that does not fit the
+    layer's shared memory is an error, not a silent fallback."""
+    gen = torch.Generator().manual_seed(5 + D + cout)
+    a = _bf((B, D, H, W, ca), gen)
+    b = _bf((B, max(D // 2, 1), H // 2, W // 2, cb), gen) if cb else None
+    cin = ca + cb
+    w32 = (torch.randn(27 * cout * cin, generator=gen) * 0.1).cuda()
+    w = torch.empty(U.lib().ccu_packed_weight_elems(cout, cin), dtype=torch.bfloat16, device="cuda")
+    U.check(U.lib().ccu_pack_weights(_ptr(w32), cout, cin, _ptr(w), None, None))
+
+    def conv():
+        o = torch.empty(B, D, H, W, cout, dtype=torch.bfloat16, device="cuda")
+        rc = U.lib().ccu_conv3d(_ptr(a), ca, _ptr(b) if b is not None else None, cb, B, D, H, W, _ptr(w), None,
+                                cout, 0, _ptr(o), cout, None, None, None)
+        return rc, o
+
+    slot, wbytes = cin // 8 * 180 * 16, -(-27 * cin // 64) * 8 * cout * 16
+    try:
+        U.check(U.lib().ccu_set_conv_path(4))
+        rc, ref = conv()
+        U.check(rc)
+        U.check(U.lib().ccu_set_conv_path(3))
+        for ring in (0, 4, 5, 7, 12):
+            U.check(U.lib().ccu_set_conv_ring(ring))
+            rc, o = conv()
+            if ring and ring * slot + wbytes > 200 * 1024:
+                assert rc != 0
+                continue
+            U.check(rc)
+            torch.cuda.synchronize()
+            assert torch.equal(o, ref), ring
+    finally:
+        U.check(U.lib().ccu_set_conv_ring(0))
+        U.check(U.lib().ccu_set_conv_path(0))
+    assert U.status() == 0
+    assert U.lib().ccu_set_conv_ring(3) != 0
 
 
 def test_adam_with_adaptive_clipping(U):
