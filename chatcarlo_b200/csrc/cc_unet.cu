@@ -124,6 +124,13 @@ __device__ bool mbar_wait_or_fail(uint64_t* bar, uint32_t parity, volatile int* 
     }
 }
 
+// The mbarrier receives one arrival when all of this thread's earlier
+// cp.async copies have landed (the arrival is not counted in advance: the
+// barrier's expected count includes it).
+__device__ __forceinline__ void cp_async_arrive_noinc(uint64_t* bar) {
+    asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
 __device__ __forceinline__ void fence_proxy_async() {
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
 }
@@ -185,6 +192,14 @@ __device__ __forceinline__ void tmem_ld8(uint32_t taddr, float f[8]) {
     for (int j = 0; j < 8; ++j) f[j] = __uint_as_float(r[j]);
 }
 
+// tmem_ld8 without the wait: several loads in flight, then tmem_wait_ld()
+__device__ __forceinline__ void tmem_ld8_nw(uint32_t taddr, uint32_t r[8]) {
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+                 : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
 __device__ __forceinline__ uint4 pack_bf16x8(const float f[8]) {
     uint4 u;
     __nv_bfloat162 h0 = __floats2bfloat162_rn(f[0], f[1]), h1 = __floats2bfloat162_rn(f[2], f[3]);
@@ -238,6 +253,11 @@ __device__ __forceinline__ void voxel_coords(long long v, const Src& s, int& n, 
 // (the zero padding outside the volume) without reading src.
 __device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, uint32_t src_bytes) {
     asm volatile("cp.async.ca.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(src_bytes) : "memory");
+}
+// cp_async16 that bypasses L1 (cached in L2 only): for streamed data read
+// once per CTA, where shared memory leaves L1 little room
+__device__ __forceinline__ void cp_async16_cg(uint32_t dst, const void* src, uint32_t src_bytes) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(src_bytes) : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 template <int PENDING>
@@ -1075,26 +1095,17 @@ __global__ void __launch_bounds__(THREADS, 1) conv_ps_kernel(const ConvP P, cons
 
     if (warp >= 1 && warp <= 3) {
         // ---- loaders: planes zs - 1 .. ze of each segment, channel groups of the pass ----
+        // Each thread's copies of a plane arrive on the slot's "full" barrier
+        // when they land, so the loaders never wait for their own copies:
+        // as many planes are in flight as the ring has free slots.
         const int lt = tid - 32;
         uint32_t L = 0;
-        bool pending = false;
         for (long long g = g_begin; g < g_end && !*fail;) {
             const WsSeg q = ws_segment(S, g, g_end, tiles_x, tiles_y);
             g += q.ze - q.zs;
             for (int zz = q.zs - 1; zz <= q.ze && !*fail; ++zz, ++L) {
                 const uint32_t slot = L % R;
-                if (L >= R) {
-                    const uint32_t par = ((L / R) - 1) & 1u;
-                    if (!mbar_try_wait(&empty[slot], par)) {
-                        if (pending) {
-                            cp_async_wait<0>();
-                            fence_proxy_async();
-                            mbar_arrive(&full[(L - 1) % R]);
-                            pending = false;
-                        }
-                        if (!mbar_wait_or_fail(&empty[slot], par, fail)) break;
-                    }
-                }
+                if (L >= R && !mbar_wait_or_fail(&empty[slot], ((L / R) - 1) & 1u, fail)) break;
                 const uint32_t base = sbase + slot * slot16 * 16;
                 for (int i = lt; i < c8p * RING_V; i += WS_LOADERS) {
                     const int c8 = i / RING_V, hv = i - c8 * RING_V;
@@ -1112,20 +1123,12 @@ __global__ void __launch_bounds__(THREADS, 1) conv_ps_kernel(const ConvP P, cons
                             src = S.b + cv * S.cb + (ch - S.ca);
                         }
                     }
-                    cp_async16(base + (uint32_t)i * 16, src, bytes);
+                    cp_async16_cg(base + (uint32_t)i * 16, src, bytes);
                 }
-                cp_async_commit();
-                if (pending) {
-                    cp_async_wait<1>();
-                    fence_proxy_async();
-                    mbar_arrive(&full[(L - 1) % R]);
-                }
-                pending = true;
+                cp_async_arrive_noinc(&full[slot]);
             }
         }
         cp_async_wait<0>();
-        fence_proxy_async();
-        if (pending && !*fail) mbar_arrive(&full[(L - 1) % R]);
     } else if (warp == 0 && lane == 0) {
         // ---- MMA issuer: one chain of 9 x c8p / 2 MMAs per input plane ----
         const uint64_t a0 = smem_desc(sbase, RING_V * 16, HALO_X * 16);
@@ -1141,6 +1144,7 @@ __global__ void __launch_bounds__(THREADS, 1) conv_ps_kernel(const ConvP P, cons
                 ok = mbar_wait_or_fail(&full[L % R], (L / R) & 1u, fail);
                 if (ok && L >= PS_REGIONS) ok = mbar_wait_or_fail(&rfree[rg], ((L / PS_REGIONS) - 1) & 1u, fail);
                 if (!ok) break;
+                fence_proxy_async();          // the loaders' copies, seen through the barrier, to the tensor core
                 tc_fence_after();
                 const uint32_t d = tmem + rg * RC;
                 const uint32_t so = (L % R) * slot16;
@@ -1182,27 +1186,39 @@ __global__ void __launch_bounds__(THREADS, 1) conv_ps_kernel(const ConvP P, cons
                 const uint32_t r0 = tmem + ((L1 - 1) % PS_REGIONS) * RC + NO + lq;
                 const uint32_t rp = tmem + (L1 % PS_REGIONS) * RC + 2 * NO + lq;
                 const long long v = (((long long)q.n * S.D + z) * S.H + y) * S.W + x;
+                // the three regions' loads of 16 channels in flight together
 #pragma unroll
-                for (int c0 = 0; c0 < NO; c0 += 8) {
-                    float f[8], f1[8], f2[8];
-                    tmem_ld8(rm + (uint32_t)c0, f);
-                    tmem_ld8(r0 + (uint32_t)c0, f1);
-                    tmem_ld8(rp + (uint32_t)c0, f2);
-#pragma unroll
-                    for (int j = 0; j < 8; ++j) f[j] = (f[j] + f1[j]) + f2[j];
+                for (int c0 = 0; c0 < NO; c0 += 16) {
+                    uint32_t u[6][8];
+                    tmem_ld8_nw(rm + (uint32_t)c0, u[0]);
+                    tmem_ld8_nw(r0 + (uint32_t)c0, u[1]);
+                    tmem_ld8_nw(rp + (uint32_t)c0, u[2]);
+                    tmem_ld8_nw(rm + (uint32_t)c0 + 8, u[3]);
+                    tmem_ld8_nw(r0 + (uint32_t)c0 + 8, u[4]);
+                    tmem_ld8_nw(rp + (uint32_t)c0 + 8, u[5]);
+                    tmem_wait_ld();
                     if (!in) continue;
-                    if (Q.part_in) {
-                        const float4* pi = reinterpret_cast<const float4*>(Q.part_in + (size_t)v * NO + c0);
-                        const float4 u0 = __ldg(pi), u1 = __ldg(pi + 1);
-                        f[0] += u0.x, f[1] += u0.y, f[2] += u0.z, f[3] += u0.w;
-                        f[4] += u1.x, f[5] += u1.y, f[6] += u1.z, f[7] += u1.w;
-                    }
-                    if (Q.part_out) {
-                        float4* po = reinterpret_cast<float4*>(Q.part_out + (size_t)v * NO + c0);
-                        po[0] = make_float4(f[0], f[1], f[2], f[3]);
-                        po[1] = make_float4(f[4], f[5], f[6], f[7]);
-                    } else {
-                        conv_store(P, v, c0, NO, f);
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        const int c = c0 + 8 * h;
+                        float f[8];
+#pragma unroll
+                        for (int j = 0; j < 8; ++j)
+                            f[j] = (__uint_as_float(u[3 * h][j]) + __uint_as_float(u[3 * h + 1][j])) +
+                                   __uint_as_float(u[3 * h + 2][j]);
+                        if (Q.part_in) {
+                            const float4* pi = reinterpret_cast<const float4*>(Q.part_in + (size_t)v * NO + c);
+                            const float4 u0 = __ldg(pi), u1 = __ldg(pi + 1);
+                            f[0] += u0.x, f[1] += u0.y, f[2] += u0.z, f[3] += u0.w;
+                            f[4] += u1.x, f[5] += u1.y, f[6] += u1.z, f[7] += u1.w;
+                        }
+                        if (Q.part_out) {
+                            float4* po = reinterpret_cast<float4*>(Q.part_out + (size_t)v * NO + c);
+                            po[0] = make_float4(f[0], f[1], f[2], f[3]);
+                            po[1] = make_float4(f[4], f[5], f[6], f[7]);
+                        } else {
+                            conv_store(P, v, c, NO, f);
+                        }
                     }
                 }
                 tc_fence_before();
