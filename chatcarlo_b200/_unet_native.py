@@ -17,7 +17,8 @@ LIB_PATH = Path(os.environ.get("CHATCARLO_B200_UNET_LIB") or
 EXPORTED = [
     "ccu_version", "ccu_last_error", "ccu_status", "ccu_conv3d", "ccu_conv3d_wgrad", "ccu_bias_grad",
     "ccu_avgpool", "ccu_pool_backward", "ccu_up_reduce", "ccu_head", "ccu_input", "ccu_adam", "ccu_adam_clipped",
-    "ccu_packed_weight_elems", "ccu_pack_weights", "ccu_set_conv_path", "ccu_set_conv_ring", "ccu_zero", "ccu_gemm_test",
+    "ccu_packed_weight_elems", "ccu_pack_weights", "ccu_set_conv_path", "ccu_set_conv_ring",
+    "ccu_set_conv_group", "ccu_zero", "ccu_gemm_test",
 ]
 
 P = C.c_void_p
@@ -44,6 +45,7 @@ _SIGS = {
     "ccu_pack_weights": ([P, I, I, P, P, P], I),
     "ccu_set_conv_path": ([I], I),
     "ccu_set_conv_ring": ([I], I),
+    "ccu_set_conv_group": ([I], I),
     "ccu_zero": ([P, LL, P], I),
     "ccu_gemm_test": ([P, P, P, I, I, I, I, I, P], I),
 }

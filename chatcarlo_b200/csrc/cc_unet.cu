@@ -1025,19 +1025,37 @@ __global__ void __launch_bounds__(THREADS, 4) conv_ws_kernel(const ConvP P, int 
 // the barriers are: full / empty per ring slot (one MMA group reads each
 // plane), rfull per region (the plane's MMAs are done) and rfree per region
 // (the last output that reads the region, z + 1 for D_z, is stored).
+// Issue groups: the MMA thread takes G consecutive planes at once and
+// interleaves their chains tap by tap, so that G independent accumulator
+// chains are in flight per CTA (one per plane); the CTA then holds
+// 2 G + 2 regions (4 for G = 1).
 // Channel passes: the kernel reads input channel groups [c8_lo, c8_hi) (8
 // channels each) and the matching weight rows only, so that layers whose
 // weights do not fit shared memory run as several passes: every pass but
 // the last adds into an FP32 partial sum [v][cout] (part_out), the last adds
 // the partial (part_in) before bias, ReLU, mask and the BF16 store.
-constexpr int PS_REGIONS = 4;
+constexpr int PS_REGIONS_MAX = 8;
+constexpr int PS_GROUP_MAX = 3;
 
-// tensor-memory columns of one region (3 x cout, rounded up to 64 / 128) and of a CTA
+// tensor-memory columns of one region (3 x cout, rounded up to 64 / 128)
 __host__ __device__ constexpr uint32_t ps_region_cols(int n) { return n <= 16 ? 64u : 128u; }
-__host__ __device__ constexpr uint32_t ps_tmem_cols(int n) { return PS_REGIONS * ps_region_cols(n); }
+// regions for issue groups of g planes: 4 for g = 1, else 2 g + 2 (the
+// next group's MMAs overlap the outputs of the last); columns allocated
+__host__ __device__ constexpr int ps_regions(int g) { return g <= 1 ? 4 : 2 * g + 2; }
+__host__ __device__ constexpr uint32_t ps_tmem_cols(int n, int g) {
+    return (uint32_t)ps_regions(g) * ps_region_cols(n) <= 256u ? 256u : 512u;
+}
 __host__ __device__ constexpr uint32_t ps_weight_bytes(int n, int c8p) { return 9u * (uint32_t)c8p * 3u * n * 16u; }
 __host__ __device__ constexpr uint32_t ps_smem_bytes(int n, int c8p, int ring) {
     return (uint32_t)ring * (uint32_t)c8p * RING_V * 16 + ps_weight_bytes(n, c8p);
+}
+
+// next index of a ring of n entries, flipping the phase bit on wrap-around
+__device__ __forceinline__ void ring_next(uint32_t& i, uint32_t& phase, uint32_t n) {
+    if (++i == n) {
+        i = 0;
+        phase ^= 1u;
+    }
 }
 
 struct PsPass {
@@ -1046,12 +1064,14 @@ struct PsPass {
     float* part_out;           // FP32 sums [v][cout] out (no bias / ReLU / BF16), or null
 };
 
-template <int NO>
+template <int NO, int G>
 __global__ void __launch_bounds__(THREADS, 1) conv_ps_kernel(const ConvP P, const PsPass Q, int ring) {
     constexpr int NP = 3 * NO;                                // MMA N: the three dz weight planes
     constexpr uint32_t RC = ps_region_cols(NO);
+    constexpr uint32_t NQ = (uint32_t)ps_regions(G), TCOLS = ps_tmem_cols(NO, G);
+    static_assert(NQ <= PS_REGIONS_MAX && NQ * RC <= 512, "issue group too large for the tensor memory");
     extern __shared__ __align__(128) uint8_t smem[];
-    __shared__ uint64_t full[WS_RING_MAX], empty[WS_RING_MAX], rfull[PS_REGIONS], rfree[PS_REGIONS];
+    __shared__ uint64_t full[WS_RING_MAX], empty[WS_RING_MAX], rfull[PS_REGIONS_MAX], rfree[PS_REGIONS_MAX];
     __shared__ uint32_t s_tmem;
     __shared__ int s_fail;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -1064,13 +1084,13 @@ __global__ void __launch_bounds__(THREADS, 1) conv_ps_kernel(const ConvP P, cons
     const uint32_t slot16 = (uint32_t)c8p * RING_V;           // one ring slot, 16-byte units
     volatile int* fail = &s_fail;
 
-    if (warp == 0) tmem_alloc(&s_tmem, ps_tmem_cols(NO));
+    if (warp == 0) tmem_alloc(&s_tmem, TCOLS);
     if (tid == 0) {
         for (uint32_t r = 0; r < R; ++r) {
             mbar_init(&full[r], WS_LOADERS);
             mbar_init(&empty[r], 1);
         }
-        for (int r = 0; r < PS_REGIONS; ++r) {
+        for (uint32_t r = 0; r < NQ; ++r) {
             mbar_init(&rfull[r], 1);
             mbar_init(&rfree[r], 128);
         }
@@ -1099,13 +1119,12 @@ __global__ void __launch_bounds__(THREADS, 1) conv_ps_kernel(const ConvP P, cons
         // when they land, so the loaders never wait for their own copies:
         // as many planes are in flight as the ring has free slots.
         const int lt = tid - 32;
-        uint32_t L = 0;
+        uint32_t L = 0, slot = 0, ph = 0;             // plane, its ring slot and the slot's phase
         for (long long g = g_begin; g < g_end && !*fail;) {
             const WsSeg q = ws_segment(S, g, g_end, tiles_x, tiles_y);
             g += q.ze - q.zs;
-            for (int zz = q.zs - 1; zz <= q.ze && !*fail; ++zz, ++L) {
-                const uint32_t slot = L % R;
-                if (L >= R && !mbar_wait_or_fail(&empty[slot], ((L / R) - 1) & 1u, fail)) break;
+            for (int zz = q.zs - 1; zz <= q.ze && !*fail; ++zz, ++L, ring_next(slot, ph, R)) {
+                if (L >= R && !mbar_wait_or_fail(&empty[slot], ph ^ 1u, fail)) break;
                 const uint32_t base = sbase + slot * slot16 * 16;
                 for (int i = lt; i < c8p * RING_V; i += WS_LOADERS) {
                     const int c8 = i / RING_V, hv = i - c8 * RING_V;
@@ -1130,61 +1149,94 @@ __global__ void __launch_bounds__(THREADS, 1) conv_ps_kernel(const ConvP P, cons
         }
         cp_async_wait<0>();
     } else if (warp == 0 && lane == 0) {
-        // ---- MMA issuer: one chain of 9 x c8p / 2 MMAs per input plane ----
+        // ---- MMA issuer: per input plane one chain of 9 x c8p / 2 MMAs; the chains of a
+        // group of planes are issued tap by tap in turn ----
         const uint64_t a0 = smem_desc(sbase, RING_V * 16, HALO_X * 16);
         const uint64_t b0 = smem_desc(swt, NP * 16, 128);
         constexpr uint32_t IDESC = idesc_bf16(TILE_M, NP, 0, 0);
-        uint32_t L = 0;
-        for (long long g = g_begin; g < g_end && !*fail;) {
+        uint32_t n_planes = 0;                       // planes of the CTA's sequence: each segment's zs - 1 .. ze
+        for (long long g = g_begin; g < g_end;) {
             const WsSeg q = ws_segment(S, g, g_end, tiles_x, tiles_y);
             g += q.ze - q.zs;
-            bool ok = true;
-            for (int zz = q.zs - 1; zz <= q.ze && ok; ++zz, ++L) {
-                const uint32_t rg = L % PS_REGIONS;
-                ok = mbar_wait_or_fail(&full[L % R], (L / R) & 1u, fail);
-                if (ok && L >= PS_REGIONS) ok = mbar_wait_or_fail(&rfree[rg], ((L / PS_REGIONS) - 1) & 1u, fail);
-                if (!ok) break;
-                fence_proxy_async();          // the loaders' copies, seen through the barrier, to the tensor core
-                tc_fence_after();
-                const uint32_t d = tmem + rg * RC;
-                const uint32_t so = (L % R) * slot16;
+            n_planes += (uint32_t)(q.ze - q.zs) + 2;
+        }
+        // plane L's ring slot and region with their phases, advanced without divisions
+        uint32_t L = 0, fs = 0, fph = 0, rs = 0, rph = 0;
+        bool ok = true;
+        while (L < n_planes && ok && !*fail) {
+            const uint32_t gn = min((uint32_t)G, n_planes - L);      // G but for the CTA's last group
+            uint32_t d[G], so[G], fsk[G], rsk[G];
+            {
+                uint32_t f = fs, fp = fph, r = rs, rp = rph;
 #pragma unroll
-                for (int t9 = 0; t9 < 9; ++t9) {
-                    const uint32_t ta = so + (uint32_t)((t9 / 3) * HALO_X + t9 % 3);
-                    for (int j = 0; j < c8p / 2; ++j)
-                        mma_bf16(d, a0 + ta + (uint32_t)(2 * j * RING_V), b0 + (uint32_t)((t9 * c8p + 2 * j) * NP),
-                                 IDESC, (t9 > 0 || j > 0) ? 1u : 0u);
+                for (int k = 0; k < G; ++k) {
+                    fsk[k] = f;
+                    rsk[k] = r;
+                    d[k] = tmem + r * RC;
+                    so[k] = f * slot16;
+                    if (G == 1 || (uint32_t)k < gn) {
+                        if (ok) ok = mbar_wait_or_fail(&full[f], fp, fail);
+                        if (ok && L + k >= NQ) ok = mbar_wait_or_fail(&rfree[r], rp ^ 1u, fail);
+                    }
+                    ring_next(f, fp, R);
+                    ring_next(r, rp, NQ);
                 }
-                mma_commit(&rfull[rg]);
-                mma_commit(&empty[L % R]);
             }
             if (!ok) break;
+            fence_proxy_async();              // the loaders' copies, seen through the barrier, to the tensor core
+            tc_fence_after();
+#pragma unroll
+            for (int t9 = 0; t9 < 9; ++t9) {
+                const uint32_t ta = (uint32_t)((t9 / 3) * HALO_X + t9 % 3);
+                for (int j = 0; j < c8p / 2; ++j) {
+                    const uint64_t bd = b0 + (uint32_t)((t9 * c8p + 2 * j) * NP);
+                    const uint32_t acc = (t9 > 0 || j > 0) ? 1u : 0u;
+#pragma unroll
+                    for (int k = 0; k < G; ++k)
+                        if (G == 1 || (uint32_t)k < gn)
+                            mma_bf16(d[k], a0 + so[k] + ta + (uint32_t)(2 * j * RING_V), bd, IDESC, acc);
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < G; ++k)
+                if (G == 1 || (uint32_t)k < gn) {
+                    mma_commit(&rfull[rsk[k]]);
+                    mma_commit(&empty[fsk[k]]);
+                }
+            for (uint32_t k = 0; k < gn; ++k) {
+                ring_next(fs, fph, R);
+                ring_next(rs, rph, NQ);
+            }
+            L += gn;
         }
-        // every issued MMA has finished before the tensor memory can be freed
-        if (L > 0) mbar_wait(&rfull[(L - 1) % PS_REGIONS], ((L - 1) / PS_REGIONS) & 1u);
+        // every issued MMA has finished before the tensor memory can be freed: plane L - 1's phase
+        if (L > 0) mbar_wait(&rfull[rs == 0 ? NQ - 1 : rs - 1], rs == 0 ? rph ^ 1u : rph);
     } else if (warp >= 4) {
         // ---- epilogue: output z = D_{z-1}[dz 0] + D_z[dz 1] + D_{z+1}[dz 2]; row m, lane quarter warp - 4 ----
         const int qw = warp - 4, m = qw * 32 + lane;
         const uint32_t lq = (uint32_t)(qw * 32) << 16;
-        uint32_t base = 0;                                     // sequence index of the segment's plane zs - 1
+        // region and phase of plane z + 1, and the regions of planes z and z - 1
+        uint32_t r1 = 0, ph1 = 0;
+        ring_next(r1, ph1, NQ);
+        ring_next(r1, ph1, NQ);                                // the first output reads planes 0, 1, 2
         for (long long g = g_begin; g < g_end && !*fail;) {
             const WsSeg q = ws_segment(S, g, g_end, tiles_x, tiles_y);
             g += q.ze - q.zs;
             const int y = q.y0 + (m >> 3), x = q.x0 + (m & 7);
             const bool in = y < S.H && x < S.W;
             bool ok = true;
-            for (int z = q.zs; z < q.ze; ++z) {
-                const uint32_t L1 = base + (uint32_t)(z - q.zs) + 2;        // plane z + 1
+            for (int z = q.zs; z < q.ze; ++z, ring_next(r1, ph1, NQ)) {
+                const uint32_t r0i = r1 == 0 ? NQ - 1 : r1 - 1, rmi = r0i == 0 ? NQ - 1 : r0i - 1;
                 int w = 1;
-                if (lane == 0) w = mbar_wait_or_fail(&rfull[L1 % PS_REGIONS], (L1 / PS_REGIONS) & 1u, fail) ? 1 : 0;
+                if (lane == 0) w = mbar_wait_or_fail(&rfull[r1], ph1, fail) ? 1 : 0;
                 if (!__shfl_sync(0xffffffffu, w, 0)) {
                     ok = false;
                     break;
                 }
                 tc_fence_after();
-                const uint32_t rm = tmem + ((L1 - 2) % PS_REGIONS) * RC + lq;
-                const uint32_t r0 = tmem + ((L1 - 1) % PS_REGIONS) * RC + NO + lq;
-                const uint32_t rp = tmem + (L1 % PS_REGIONS) * RC + 2 * NO + lq;
+                const uint32_t rm = tmem + rmi * RC + lq;
+                const uint32_t r0 = tmem + r0i * RC + NO + lq;
+                const uint32_t rp = tmem + r1 * RC + 2 * NO + lq;
                 const long long v = (((long long)q.n * S.D + z) * S.H + y) * S.W + x;
                 // the three regions' loads of 16 channels in flight together
 #pragma unroll
@@ -1222,20 +1274,22 @@ __global__ void __launch_bounds__(THREADS, 1) conv_ps_kernel(const ConvP P, cons
                     }
                 }
                 tc_fence_before();
-                mbar_arrive(&rfree[(L1 - 2) % PS_REGIONS]);             // plane z - 1: last reader done
+                mbar_arrive(&rfree[rmi]);                               // plane z - 1: last reader done
                 if (z == q.ze - 1) {
-                    mbar_arrive(&rfree[(L1 - 1) % PS_REGIONS]);
-                    mbar_arrive(&rfree[L1 % PS_REGIONS]);
+                    mbar_arrive(&rfree[r0i]);
+                    mbar_arrive(&rfree[r1]);
                 }
             }
             if (!ok) break;
-            base += (uint32_t)(q.ze - q.zs) + 2;
+            // the next segment's first output reads its planes 0 .. 2: two planes on
+            ring_next(r1, ph1, NQ);
+            ring_next(r1, ph1, NQ);
         }
     }
     __syncthreads();
     if (tid == 0 && s_fail) atomicOr(&g_status, 1u);
     tc_fence_after();
-    if (warp == 0) tmem_dealloc(tmem, ps_tmem_cols(NO));
+    if (warp == 0) tmem_dealloc(tmem, TCOLS);
 }
 
 // ---------------------------------------------------------------------------
@@ -1847,6 +1901,8 @@ int resident_ctas(Kern kernel, size_t smem, uint32_t cols, int& resident) {
 
 // ring depth of the warp-role kernel (0: chosen per layer)
 int g_conv_ring = 0;
+// issue group of the plane-stationary kernel (0: chosen per layer)
+int g_conv_group = 0;
 
 template <int N>
 int launch_conv_stream(const ConvP& P, cudaStream_t st) {
@@ -1921,8 +1977,8 @@ int ps_workspace(size_t bytes, cudaStream_t st, float*& ws) {
     return CCU_OK;
 }
 
-template <int NO>
-int launch_conv_ps(const ConvP& P, int passes, cudaStream_t st) {
+template <int NO, int G>
+int launch_conv_ps_g(const ConvP& P, int passes, cudaStream_t st) {
     const int c8n = (P.src.ca + P.src.cb) / 8;
     const int c8p_max = 2 * ((c8n / 2 + passes - 1) / passes);
     int dev = 0, sms = 0;
@@ -1941,26 +1997,38 @@ int launch_conv_ps(const ConvP& P, int passes, cudaStream_t st) {
         Q.part_in = k > 0 ? ws : nullptr;
         Q.part_out = Q.c8_hi < c8n ? ws : nullptr;
         const int c8p = Q.c8_hi - Q.c8_lo;
-        // deepest ring (2 .. WS_RING_MAX planes) that keeps the CTAs per SM the tensor memory allows
+        const uint32_t cols = ps_tmem_cols(NO, G);
+        // deepest ring (group + 1 .. WS_RING_MAX planes) that keeps the CTAs per SM the tensor memory allows
         int ring = 0, best_res = 0;
         size_t smem = 0;
-        for (int r = 2; r <= WS_RING_MAX && ps_smem_bytes(NO, c8p, r) <= 200 * 1024; ++r) {
+        for (int r = G + 1; r <= WS_RING_MAX && ps_smem_bytes(NO, c8p, r) <= 200 * 1024; ++r) {
             int res = 1;
-            const int rc = resident_ctas(conv_ps_kernel<NO>, (size_t)ps_smem_bytes(NO, c8p, r) + 1024,
-                                         ps_tmem_cols(NO), res);
+            const int rc = resident_ctas(conv_ps_kernel<NO, G>, (size_t)ps_smem_bytes(NO, c8p, r) + 1024, cols, res);
             if (rc != CCU_OK) return rc;
             if (res >= best_res) best_res = res, ring = r;
         }
         if (ring == 0) return set_error(CCU_E_INVALID, "plane-stationary pass does not fit shared memory");
-        int rc = tc_launch_smem(conv_ps_kernel<NO>, ps_smem_bytes(NO, c8p, ring), ps_tmem_cols(NO), smem);
+        int rc = tc_launch_smem(conv_ps_kernel<NO, G>, ps_smem_bytes(NO, c8p, ring), cols, smem);
         if (rc != CCU_OK) return rc;
         int resident = 1;
-        if ((rc = resident_ctas(conv_ps_kernel<NO>, smem, ps_tmem_cols(NO), resident)) != CCU_OK) return rc;
+        if ((rc = resident_ctas(conv_ps_kernel<NO, G>, smem, cols, resident)) != CCU_OK) return rc;
         const long long grid = std::min<long long>(planes, (long long)sms * resident);
-        conv_ps_kernel<NO><<<(unsigned)grid, THREADS, smem, st>>>(P, Q, ring);
+        conv_ps_kernel<NO, G><<<(unsigned)grid, THREADS, smem, st>>>(P, Q, ring);
         CU_CHECK(cudaGetLastError());
     }
     return CCU_OK;
+}
+
+// The requested issue group (by default 1: for 16 output channels one chain
+// on each of two CTAs per SM measured 1.4x faster than three interleaved
+// chains on one CTA), down to the largest whose regions fit 512
+// tensor-memory columns (1 for 32 output channels).
+template <int NO>
+int launch_conv_ps(const ConvP& P, int passes, cudaStream_t st) {
+    const int group = g_conv_group > 0 ? g_conv_group : 1;
+    if (NO == 16 && group == 3) return launch_conv_ps_g<16, 3>(P, passes, st);
+    if (NO == 16 && group == 2) return launch_conv_ps_g<16, 2>(P, passes, st);
+    return launch_conv_ps_g<NO, 1>(P, passes, st);
 }
 
 template <int N>
@@ -2202,6 +2270,13 @@ int ccu_set_conv_ring(int ring) {
     if (ring != 0 && (ring < 4 || ring > WS_RING_MAX))
         return set_error(CCU_E_INVALID, "ring must be 0 (chosen per layer) or 4 .. 12 planes");
     g_conv_ring = ring;
+    return CCU_OK;
+}
+
+int ccu_set_conv_group(int group) {
+    if (group < 0 || group > PS_GROUP_MAX)
+        return set_error(CCU_E_INVALID, "group must be 0 (chosen per layer) or 1 .. 3 planes");
+    g_conv_group = group;
     return CCU_OK;
 }
 

@@ -127,6 +127,14 @@ int ccu_set_conv_path(int path);
  * with CCU_E_INVALID).  Process-wide. */
 int ccu_set_conv_ring(int ring);
 
+/* Issue group of the plane-stationary kernel (path 0, 16 or 32 output
+ * channels): 0 (default) chosen per layer, else 1 .. 3 input planes whose
+ * MMA chains one thread interleaves (more independent accumulators in
+ * flight, fewer CTAs per SM), reduced per layer to the largest group whose
+ * tensor-memory regions fit 512 columns (3 for 16 output channels, 1 for
+ * 32).  Process-wide. */
+int ccu_set_conv_group(int group);
+
 /* cudaMemsetAsync(p, 0, bytes) on the stream (gradient buffers). */
 int ccu_zero(void* p, long long bytes, void* stream);
 

@@ -246,6 +246,40 @@ def test_warp_role_kernel_ring_depths(U, B, D, H, W, ca, cb, cout):
     assert U.lib().ccu_set_conv_ring(3) != 0
 
 
+@pytest.mark.parametrize("B,D,H,W,ca,cb,cout", [(1, 37, 16, 8, 16, 0, 16), (2, 6, 10, 12, 16, 32, 16),
+                                                (1, 10, 24, 16, 32, 64, 32), (3, 1, 16, 16, 32, 0, 16)])
+def test_plane_stationary_issue_groups(U, B, D, H, W, ca, cb, cout):
+    """Path 0 with issue groups 1, 2 and 3 (chains of consecutive planes
+    interleaved tap by tap; clamped to 1 for 32 output channels): the same
+    MMAs per plane in the same order, so every group gives the same bits."""
+    gen = torch.Generator().manual_seed(11 + D + cout)
+    a = _bf((B, D, H, W, ca), gen)
+    b = _bf((B, max(D // 2, 1), H // 2, W // 2, cb), gen) if cb else None
+    cin = ca + cb
+    w32 = (torch.randn(27 * cout * cin, generator=gen) * 0.1).cuda()
+    w = torch.empty(U.lib().ccu_packed_weight_elems(cout, cin), dtype=torch.bfloat16, device="cuda")
+    U.check(U.lib().ccu_pack_weights(_ptr(w32), cout, cin, _ptr(w), None, None))
+    outs = []
+    try:
+        for group in (1, 2, 3):
+            U.check(U.lib().ccu_set_conv_group(group))
+            o = torch.empty(B, D, H, W, cout, dtype=torch.bfloat16, device="cuda")
+            U.check(U.lib().ccu_conv3d(_ptr(a), ca, _ptr(b) if b is not None else None, cb, B, D, H, W, _ptr(w),
+                                       None, cout, 0, _ptr(o), cout, None, None, None))
+            outs.append(o)
+    finally:
+        U.check(U.lib().ccu_set_conv_group(0))
+    torch.cuda.synchronize()
+    assert U.status() == 0
+    assert torch.equal(outs[0], outs[1]) and torch.equal(outs[0], outs[2])
+    x = _to_ncdhw(a)
+    if cb:
+        x = torch.cat([x, _up(_to_ncdhw(b))], dim=1)
+    ref = torch.nn.functional.conv3d(x, _torch_w(w32.to(torch.bfloat16), cout, cin), padding=1)
+    torch.testing.assert_close(outs[0].float(), ref.permute(0, 2, 3, 4, 1), rtol=1.6e-2, atol=1e-2)
+    assert U.lib().ccu_set_conv_group(4) != 0
+
+
 def test_adam_with_adaptive_clipping(U):
     """ccu_adam_clipped against a NumPy restatement: the first gradient sets
     the running norm, a ten times larger one is cut to 3x that mean, and
