@@ -258,7 +258,36 @@ def main(argv=None) -> None:
     ap.add_argument("--load", default=None,
                     help="evaluate a saved network (save_params file, e.g. the shipped denoiser_ct64.npz) "
                          "instead of training one")
-    print(json.dumps(run(ap.parse_args(argv))))
+    ap.add_argument("--layer-times", type=int, nargs=3, metavar=("X", "Y", "Z"), default=None,
+                    help="only time each convolution of the shipped CT network on a random volume of this shape "
+                         "(the whole CT grid: 320 320 152)")
+    args = ap.parse_args(argv)
+    if args.layer_times:
+        print(json.dumps(layer_times(tuple(args.layer_times))))
+        return
+    print(json.dumps(run(args)))
+
+
+def layer_times(shape: tuple[int, int, int], repeats: int = 3) -> dict:
+    """Per-convolution device time of CT-volume inference with the shipped
+    network on random inputs of `shape` (every side a multiple of 8), and
+    the whole prediction (forward and head) timed with CUDA events."""
+    import torch
+    model = DN.UNet3D(params=DN.load_params(CT_PRETRAINED)[0])
+    rng = np.random.default_rng(0)
+    x = rng.normal(size=(1,) + shape).astype(np.float32)
+    m = rng.integers(0, len(CT_MATERIALS), size=(1,) + shape).astype(np.uint8)
+    model.set_input(x, np.ones((1,) + shape, np.float32), m, 1, shape, unc=np.full((1,) + shape, 0.1, np.float32))
+    layers = model.layer_times(repeats)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    for _ in range(repeats):
+        ev[0].record()
+        model.predict()
+        ev[1].record()
+    torch.cuda.synchronize()
+    model.check_status()
+    return {"shape": list(shape), "predict_ms": round(ev[0].elapsed_time(ev[1]), 3),
+            "conv_ms": round(sum(r["ms"] for r in layers), 3), "layers": layers}
 
 
 if __name__ == "__main__":

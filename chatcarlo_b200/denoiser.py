@@ -330,6 +330,39 @@ class UNet3D:
                        self.p.numel(), lr, b1, b2, eps, self.step_n, wd, self._stream())
         self.pack()
 
+    def layer_times(self, repeats: int = 3) -> list[dict]:
+        """Device time of each convolution of a forward pass on the current
+        input (CUDA events around every layer, the last of `repeats`
+        passes); FLOPs = 2 x 27 x cin x cout x voxels of the layer's level."""
+        torch = self.torch
+        rec = []
+        conv = self._conv
+
+        def timed(L, a, b, out):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            conv(L, a, b, out)
+            e1.record()
+            rec.append((L, e0, e1))
+
+        self._conv = timed
+        try:
+            for _ in range(repeats):
+                rec.clear()
+                self.forward()
+            torch.cuda.synchronize()
+        finally:
+            del self._conv
+        self.check_status()
+        out = []
+        for L, e0, e1 in rec:
+            B, d, h, w = self._dims(L.level)
+            ms = e0.elapsed_time(e1)
+            flops = 2.0 * 27 * L.cin * L.cout * B * d * h * w
+            out.append({"layer": L.name, "level": L.level, "cin": L.cin, "cout": L.cout, "ms": round(ms, 4),
+                        "tflops": round(flops / ms / 1e9, 1)})
+        return out
+
     def check_status(self) -> None:
         st = U.status(reset=True)
         if st:

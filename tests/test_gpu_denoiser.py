@@ -233,3 +233,14 @@ def test_whole_volume_pass_equals_the_oracle_on_a_non_cubic_volume():
     got = model.a["e0a"].float().cpu().numpy().reshape(y.shape)
     assert np.all(np.isfinite(out))
     assert float(np.linalg.norm(got - y) / np.linalg.norm(y)) < 3e-3
+
+
+def test_layer_times_cover_every_convolution():
+    """ct_denoise.layer_times: one entry per convolution of the network,
+    positive device times and FLOP rates, and a timed whole prediction."""
+    from chatcarlo_b200 import ct_denoise as CD
+    from chatcarlo_b200 import denoiser as DN
+    r = CD.layer_times((64, 48, 16), repeats=2)
+    assert [x["layer"] for x in r["layers"]] == [L.name for L in DN.LAYERS]
+    assert all(x["ms"] > 0 and x["tflops"] > 0 for x in r["layers"])
+    assert r["predict_ms"] > 0 and r["conv_ms"] > 0
