@@ -1032,8 +1032,10 @@ __global__ void __launch_bounds__(THREADS, 4) conv_ws_kernel(const ConvP P, int 
 // Channel passes: the kernel reads input channel groups [c8_lo, c8_hi) (8
 // channels each) and the matching weight rows only, so that layers whose
 // weights do not fit shared memory run as several passes: every pass but
-// the last adds into an FP32 partial sum [v][cout] (part_out), the last adds
+// the last adds into an FP32 partial sum [v][NO] (part_out), the last adds
 // the partial (part_in) before bias, ReLU, mask and the BF16 store.
+// Output slices: a launch computes output channels [co_lo, co_lo + NO) of
+// a layer with more (64 output channels: two slices of 32).
 constexpr int PS_REGIONS_MAX = 8;
 constexpr int PS_GROUP_MAX = 3;
 
@@ -1060,8 +1062,9 @@ __device__ __forceinline__ void ring_next(uint32_t& i, uint32_t& phase, uint32_t
 
 struct PsPass {
     int c8_lo, c8_hi;          // input channel groups of this pass
-    const float* part_in;      // FP32 partial sums [v][cout] to add, or null
-    float* part_out;           // FP32 sums [v][cout] out (no bias / ReLU / BF16), or null
+    int co_lo, n_out;          // output channels [co_lo, co_lo + NO) of the layer's n_out
+    const float* part_in;      // FP32 partial sums [v][NO] to add, or null
+    float* part_out;           // FP32 sums [v][NO] out (no bias / ReLU / BF16), or null
 };
 
 template <int NO, int G>
@@ -1097,12 +1100,12 @@ __global__ void __launch_bounds__(THREADS, 1) conv_ps_kernel(const ConvP P, cons
         s_fail = 0;
         mbar_init_fence();
     }
-    // weights: packed chunk (tap * c8n + c8, co) -> (t9 * c8p + c8 - c8_lo, dz * NO + co)
+    // weights: packed chunk (tap * c8n + c8, co_lo + co) -> (t9 * c8p + c8 - c8_lo, dz * NO + co)
     const uint32_t sbase = smem_u32(smem), swt = sbase + R * slot16 * 16;
     for (int i = tid; i < 9 * c8p * NP; i += THREADS) {
         const int r = i % NP, g = i / NP;
         const int t9 = g / c8p, c8 = Q.c8_lo + g % c8p, dz = r / NO, co = r % NO;
-        const int src = ((dz * 9 + t9) * c8n + c8) * NO + co;
+        const int src = ((dz * 9 + t9) * c8n + c8) * Q.n_out + Q.co_lo + co;
         cp_async16(swt + (uint32_t)i * 16, P.w + (size_t)src * 8, 16u);
     }
     cp_async_commit();
@@ -1269,7 +1272,7 @@ __global__ void __launch_bounds__(THREADS, 1) conv_ps_kernel(const ConvP P, cons
                             po[0] = make_float4(f[0], f[1], f[2], f[3]);
                             po[1] = make_float4(f[4], f[5], f[6], f[7]);
                         } else {
-                            conv_store(P, v, c, NO, f);
+                            conv_store(P, v, Q.co_lo + c, Q.n_out, f);
                         }
                     }
                 }
@@ -1872,12 +1875,20 @@ bool stream_applies(const ConvP& P, int n_out) {
 // Channel passes of the plane-stationary kernel for cin input channels: the
 // fewest passes of equal 16-channel-aligned groups whose weights and a
 // ring of 3 planes fit 200 KB of shared memory (0: does not apply).
+// Output slices of the plane-stationary kernel: one of 16 or 32 channels,
+// two of 32 for 64 (0: does not apply).
+int ps_slice(int n_out) {
+    if (g_conv_path != 0) return 0;
+    return n_out == 16 ? 16 : (n_out == 32 || n_out == 64) ? 32 : 0;
+}
+
 int ps_passes(int n_out, int cin) {
-    if (g_conv_path != 0 || (n_out != 16 && n_out != 32) || cin % 16) return 0;
+    const int no = ps_slice(n_out);
+    if (!no || cin % 16) return 0;
     const int c16 = cin / 16;
     for (int passes = 1; passes <= c16; ++passes) {
         const int c8p = 2 * ((c16 + passes - 1) / passes);
-        if (ps_smem_bytes(n_out, c8p, 3) <= 200 * 1024) return passes;
+        if (ps_smem_bytes(no, c8p, 3) <= 200 * 1024) return passes;
     }
     return 0;
 }
@@ -1978,7 +1989,7 @@ int ps_workspace(size_t bytes, cudaStream_t st, float*& ws) {
 }
 
 template <int NO, int G>
-int launch_conv_ps_g(const ConvP& P, int passes, cudaStream_t st) {
+int launch_conv_ps_g(const ConvP& P, int n_out, int passes, cudaStream_t st) {
     const int c8n = (P.src.ca + P.src.cb) / 8;
     const int c8p_max = 2 * ((c8n / 2 + passes - 1) / passes);
     int dev = 0, sms = 0;
@@ -1990,8 +2001,12 @@ int launch_conv_ps_g(const ConvP& P, int passes, cudaStream_t st) {
         const int rc = ps_workspace((size_t)P.n_vox * NO * sizeof(float), st, ws);
         if (rc != CCU_OK) return rc;
     }
+    // output slices one after the other (they share the partial-sum workspace), channel passes within each
+    for (int co_lo = 0; co_lo < n_out; co_lo += NO)
     for (int k = 0, lo = 0; lo < c8n; ++k, lo += c8p_max) {
         PsPass Q;
+        Q.co_lo = co_lo;
+        Q.n_out = n_out;
         Q.c8_lo = lo;
         Q.c8_hi = std::min(c8n, lo + c8p_max);
         Q.part_in = k > 0 ? ws : nullptr;
@@ -2024,11 +2039,11 @@ int launch_conv_ps_g(const ConvP& P, int passes, cudaStream_t st) {
 // chains on one CTA), down to the largest whose regions fit 512
 // tensor-memory columns (1 for 32 output channels).
 template <int NO>
-int launch_conv_ps(const ConvP& P, int passes, cudaStream_t st) {
+int launch_conv_ps(const ConvP& P, int n_out, int passes, cudaStream_t st) {
     const int group = g_conv_group > 0 ? g_conv_group : 1;
-    if (NO == 16 && group == 3) return launch_conv_ps_g<16, 3>(P, passes, st);
-    if (NO == 16 && group == 2) return launch_conv_ps_g<16, 2>(P, passes, st);
-    return launch_conv_ps_g<NO, 1>(P, passes, st);
+    if (NO == 16 && group == 3) return launch_conv_ps_g<16, 3>(P, n_out, passes, st);
+    if (NO == 16 && group == 2) return launch_conv_ps_g<16, 2>(P, n_out, passes, st);
+    return launch_conv_ps_g<NO, 1>(P, n_out, passes, st);
 }
 
 template <int N>
@@ -2104,8 +2119,8 @@ int ccu_conv3d(const void* a, int ca, const void* b, int cb, int batch, int d, i
     P.out1 = (__nv_bfloat16*)out1;
     cudaStream_t st = (cudaStream_t)stream;
     if (const int passes = ps_passes(cout, ca + cb)) {
-        if (cout == 16) return launch_conv_ps<16>(P, passes, st);
-        return launch_conv_ps<32>(P, passes, st);
+        if (ps_slice(cout) == 16) return launch_conv_ps<16>(P, cout, passes, st);
+        return launch_conv_ps<32>(P, cout, passes, st);
     }
     if (stream_applies(P, cout)) {
         switch (cout) {
