@@ -1018,9 +1018,8 @@ __global__ void __launch_bounds__(THREADS, 4) conv_ws_kernel(const ConvP P, int 
 // and output plane z is D_{z-1}[.., 0 | ..] + D_z[.., 1 | ..] + D_{z+1}[.., 2 | ..],
 // summed in FP32 by the epilogue from three tensor-memory regions.  A is
 // read a third as often as by the output-stationary kernels, and N is
-// three times wider.  Q = 4 regions of 3 x cout columns (at 64- or 128-
-// column steps): the MMAs of plane p + 1 overlap the epilogue of output
-// p - 1.
+// three times wider.  Q = 5 regions of 3 x cout columns: the MMAs of
+// plane p + 1 and p + 2 overlap the epilogue of output p - 1.
 // Work split, ring of halo planes, warp roles and loader as conv_ws_kernel;
 // the barriers are: full / empty per ring slot (one MMA group reads each
 // plane), rfull per region (the plane's MMAs are done) and rfree per region
@@ -1039,11 +1038,13 @@ __global__ void __launch_bounds__(THREADS, 4) conv_ws_kernel(const ConvP P, int 
 constexpr int PS_REGIONS_MAX = 8;
 constexpr int PS_GROUP_MAX = 3;
 
-// tensor-memory columns of one region (3 x cout, rounded up to 64 / 128)
-__host__ __device__ constexpr uint32_t ps_region_cols(int n) { return n <= 16 ? 64u : 128u; }
-// regions for issue groups of g planes: 4 for g = 1, else 2 g + 2 (the
-// next group's MMAs overlap the outputs of the last); columns allocated
-__host__ __device__ constexpr int ps_regions(int g) { return g <= 1 ? 4 : 2 * g + 2; }
+// tensor-memory columns of one region: 3 x cout
+__host__ __device__ constexpr uint32_t ps_region_cols(int n) { return 3u * (uint32_t)n; }
+// regions for issue groups of g planes: 5 for g = 1 (plane L's MMAs need
+// the region of plane L - 5, released once plane L - 3's MMAs are done:
+// the issuing thread runs two planes ahead of the epilogue), else 2 g + 2;
+// columns allocated
+__host__ __device__ constexpr int ps_regions(int g) { return g <= 1 ? 5 : 2 * g + 2; }
 __host__ __device__ constexpr uint32_t ps_tmem_cols(int n, int g) {
     return (uint32_t)ps_regions(g) * ps_region_cols(n) <= 256u ? 256u : 512u;
 }
