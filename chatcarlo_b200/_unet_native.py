@@ -15,7 +15,8 @@ LIB_PATH = Path(os.environ.get("CHATCARLO_B200_UNET_LIB") or
                 Path(__file__).resolve().parent / "lib" / "libccunet.so")
 
 EXPORTED = [
-    "ccu_version", "ccu_last_error", "ccu_status", "ccu_conv3d", "ccu_conv3d_wgrad", "ccu_bias_grad",
+    "ccu_version", "ccu_last_error", "ccu_status", "ccu_conv3d", "ccu_conv3d_head", "ccu_conv3d_wgrad",
+    "ccu_bias_grad",
     "ccu_avgpool", "ccu_pool_backward", "ccu_up_reduce", "ccu_head", "ccu_input", "ccu_adam", "ccu_adam_clipped",
     "ccu_packed_weight_elems", "ccu_pack_weights", "ccu_set_conv_path", "ccu_set_conv_ring",
     "ccu_set_conv_group", "ccu_zero", "ccu_gemm_test",
@@ -31,6 +32,7 @@ _SIGS = {
     "ccu_last_error": ([], C.c_char_p),
     "ccu_status": ([C.POINTER(C.c_uint), I], I),
     "ccu_conv3d": ([P, I, P, I, I, I, I, I, P, P, I, I, P, I, P, P, P], I),
+    "ccu_conv3d_head": ([P, I, I, I, I, I, P, P, P, P, P, P, I, P], I),
     "ccu_conv3d_wgrad": ([P, I, P, I, I, I, I, I, P, I, P, I, P], I),
     "ccu_bias_grad": ([P, LL, I, P, P], I),
     "ccu_avgpool": ([P, I, I, I, I, I, P, P], I),

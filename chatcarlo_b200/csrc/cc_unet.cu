@@ -322,9 +322,16 @@ struct ConvP {
     const __nv_bfloat16* mask0;
     int split;
     __nv_bfloat16* out1;
+    // the network's 1 x 1 x 1 head on a 16-channel layer (plane-stationary
+    // kernel only): head_out[v] = head_x[v] + head[16] + sum_j head[j] a_j,
+    // a_j the BF16 activations; out0 may then be null (not stored)
+    const float* head;
+    const float* head_x;
+    float* head_out;
 };
 
-// Bias, ReLU, mask and BF16 store of output channels [c0, c0 + 8) of voxel v.
+// Bias, ReLU, mask and BF16 store of output channels [c0, c0 + 8) of voxel v
+// (f returns the activations before the BF16 rounding).
 __device__ __forceinline__ void conv_store(const ConvP& P, long long v, int c0, int n_out, float f[8]) {
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
@@ -339,7 +346,7 @@ __device__ __forceinline__ void conv_store(const ConvP& P, long long v, int c0, 
 #pragma unroll
             for (int j = 0; j < 8; ++j) f[j] = mk[j] > 0.0f ? f[j] : 0.0f;
         }
-        *reinterpret_cast<uint4*>(P.out0 + o) = pack_bf16x8(f);
+        if (P.out0) *reinterpret_cast<uint4*>(P.out0 + o) = pack_bf16x8(f);
     } else {
         const size_t o = (size_t)v * (n_out - P.split) + (c0 - P.split);
         *reinterpret_cast<uint4*>(P.out1 + o) = pack_bf16x8(f);
@@ -1242,6 +1249,9 @@ __global__ void __launch_bounds__(THREADS, 1) conv_ps_kernel(const ConvP P, cons
                 const uint32_t r0 = tmem + r0i * RC + NO + lq;
                 const uint32_t rp = tmem + r1 * RC + 2 * NO + lq;
                 const long long v = (((long long)q.n * S.D + z) * S.H + y) * S.W + x;
+                // the head: x + b, then + w_j a_j in channel order (the head kernel's FP32 sequence)
+                const bool head = NO == 16 && P.head && in;
+                float hsum = head ? P.head_x[v] + __ldg(P.head + 16) : 0.0f;
                 // the three regions' loads of 16 channels in flight together
 #pragma unroll
                 for (int c0 = 0; c0 < NO; c0 += 16) {
@@ -1274,9 +1284,16 @@ __global__ void __launch_bounds__(THREADS, 1) conv_ps_kernel(const ConvP P, cons
                             po[1] = make_float4(f[4], f[5], f[6], f[7]);
                         } else {
                             conv_store(P, v, Q.co_lo + c, Q.n_out, f);
+                            if (head) {
+#pragma unroll
+                                for (int j = 0; j < 8; ++j)
+                                    hsum = fmaf(__ldg(P.head + c + j), __bfloat162float(__float2bfloat16_rn(f[j])),
+                                                hsum);
+                            }
                         }
                     }
                 }
+                if (head) P.head_out[v] = hsum;
                 tc_fence_before();
                 mbar_arrive(&rfree[rmi]);                               // plane z - 1: last reader done
                 if (z == q.ze - 1) {
@@ -2118,6 +2135,9 @@ int ccu_conv3d(const void* a, int ca, const void* b, int cb, int batch, int d, i
     P.mask0 = (const __nv_bfloat16*)mask0;
     P.split = split;
     P.out1 = (__nv_bfloat16*)out1;
+    P.head = nullptr;
+    P.head_x = nullptr;
+    P.head_out = nullptr;
     cudaStream_t st = (cudaStream_t)stream;
     if (const int passes = ps_passes(cout, ca + cb)) {
         if (ps_slice(cout) == 16) return launch_conv_ps<16>(P, cout, passes, st);
@@ -2149,6 +2169,38 @@ int ccu_conv3d(const void* a, int ca, const void* b, int cb, int batch, int d, i
         case 192: return launch_conv<192>(P, st);
         default: return set_error(CCU_E_INVALID, "output channels must be one of 16, 32, 48, 64, 96, 128, 192");
     }
+}
+
+int ccu_conv3d_head(const void* a, int ca, int batch, int d, int h, int w, const void* weight, const float* bias,
+                    const float* head, const float* xlog, float* out, void* act, int store_act, void* stream) {
+    int rc = check_src(a, ca, nullptr, 0, batch, d, h, w);
+    if (rc != CCU_OK) return rc;
+    if (!weight || !head || !xlog || !out || (store_act && !act))
+        return set_error(CCU_E_INVALID, "bad fused-head arguments");
+    if (!aligned16(weight) || (act && !aligned16(act))) return set_error(CCU_E_INVALID, "tensors must be 16-byte aligned");
+    const long long n_vox = (long long)batch * d * h * w;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (ps_passes(16, ca) == 1) {
+        ConvP P;
+        P.src = Src{(const __nv_bfloat16*)a, nullptr, ca, 0, batch, d, h, w};
+        P.w = (const __nv_bfloat16*)weight;
+        P.bias = bias;
+        P.relu = 1;
+        P.n_vox = n_vox;
+        P.out0 = store_act ? (__nv_bfloat16*)act : nullptr;
+        P.mask0 = nullptr;
+        P.split = 16;
+        P.out1 = nullptr;
+        P.head = head;
+        P.head_x = xlog;
+        P.head_out = out;
+        return launch_conv_ps<16>(P, 16, 1, st);
+    }
+    // not fusable (another convolution path): the convolution into act, then the head kernel
+    if (!act) return set_error(CCU_E_INVALID, "the activation buffer is needed when the head is not fused");
+    rc = ccu_conv3d(a, ca, nullptr, 0, batch, d, h, w, weight, bias, 16, 1, act, 16, nullptr, nullptr, stream);
+    if (rc != CCU_OK) return rc;
+    return ccu_head(act, xlog, nullptr, nullptr, head, 0.0f, n_vox, out, nullptr, nullptr, nullptr, stream);
 }
 
 int ccu_conv3d_wgrad(const void* a, int ca, const void* b, int cb, int batch, int d, int h, int w, const void* dz,

@@ -223,7 +223,9 @@ class UNet3D:
                    self._ptr(un) if un is not None else None, n0, self._ptr(self.a["x0"]), self._stream())
         self._keep = (de, ma, un)
 
-    def forward(self) -> None:
+    def forward(self, last: bool = True) -> None:
+        """All convolutions; `last` = False stops before the final one (d0),
+        which predict() runs fused with the head."""
         a, lib, st = self.a, U.lib(), self._stream()
         L = {x.name: x for x in LAYERS}
         self._conv(L["e0a"], a["x0"], None, a["e0a"])
@@ -245,7 +247,8 @@ class UNet3D:
         self._conv(L["d1a"], a["e1"], a["d2"], a["d1a"])
         self._conv(L["d1"], a["d1a"], None, a["d1"])
         self._conv(L["d0a"], a["e0"], a["d1"], a["d0a"])
-        self._conv(L["d0"], a["d0a"], None, a["d0"])
+        if last:
+            self._conv(L["d0"], a["d0a"], None, a["d0"])
 
     def _head(self, target=None, weight=None, inv_wsum: float = 0.0, backward: bool = False) -> None:
         n0 = int(np.prod(self.shape))
@@ -258,9 +261,18 @@ class UNet3D:
                    self._stream())
 
     def predict(self) -> "torch.Tensor":
-        """Forward pass and head; returns the predicted log map (device)."""
-        self.forward()
-        self._head()
+        """Forward pass and head; returns the predicted log map (device).
+        The last convolution runs with the head in its epilogue
+        (ccu_conv3d_head: the same values as the convolution and ccu_head,
+        without storing its activations)."""
+        self.forward(last=False)
+        L = next(x for x in LAYERS if x.name == "d0")
+        _, _, bo, _ = self.lay["d0"]
+        ho, _, _, _ = self.lay["head"]
+        B, d, h, w = self._dims(0)
+        self._call(U.lib().ccu_conv3d_head, self._ptr(self.a["d0a"]), L.cin, B, d, h, w, self._ptr(self.w["d0"]),
+                   self._ptr(self.p, bo), self._ptr(self.p, ho), self._ptr(self.xlog), self._ptr(self.out),
+                   self._ptr(self.a["d0"]), 0, self._stream())
         return self.out
 
     # -- backward ---------------------------------------------------------

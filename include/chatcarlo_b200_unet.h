@@ -44,6 +44,16 @@ int ccu_conv3d(const void* a, int ca, const void* b, int cb, int batch, int d, i
                const float* bias, int cout, int relu, void* out0, int split, const void* mask0, void* out1,
                void* stream);
 
+/* The network's last convolution and its 1 x 1 x 1 head in one pass: a
+ * ReLU convolution of a [v][ca] (no second input) to 16 channels, and
+ * out[v] = xlog[v] + head[16] + sum_j head[j] * bf16(act_j) -- the values
+ * ccu_conv3d followed by ccu_head would give.  With the plane-stationary
+ * kernel (path 0, weights in one pass) the head runs in its epilogue and the
+ * activations are stored to act only when store_act is set; otherwise the
+ * two calls are made, which needs act. */
+int ccu_conv3d_head(const void* a, int ca, int batch, int d, int h, int w, const void* weight, const float* bias,
+                    const float* head, const float* xlog, float* out, void* act, int store_act, void* stream);
+
 /* Weight gradient of ccu_conv3d: dw[27][cout][ca + cb] (FP32) +=
  * sum over voxels of dz[v][co] * input[v + tap][ci].  The voxels are split
  * into `slices` ranges reduced with atomics.  cout in {16, 32, 64, 128}. */

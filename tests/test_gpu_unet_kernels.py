@@ -280,6 +280,45 @@ def test_plane_stationary_issue_groups(U, B, D, H, W, ca, cb, cout):
     assert U.lib().ccu_set_conv_group(4) != 0
 
 
+@pytest.mark.parametrize("path", [0, 1])
+def test_last_convolution_with_the_head_fused(U, path):
+    """ccu_conv3d_head equals ccu_conv3d + ccu_head bit for bit: on path 0
+    the head runs in the plane-stationary kernel's epilogue (activations
+    stored or not), on path 1 it falls back to the two calls."""
+    gen = torch.Generator().manual_seed(31 + path)
+    B, D, H, W = 2, 6, 20, 12
+    a = _bf((B, D, H, W, 16), gen)
+    w32 = (torch.randn(27 * 16 * 16, generator=gen) * 0.1).cuda()
+    w = torch.empty(U.lib().ccu_packed_weight_elems(16, 16), dtype=torch.bfloat16, device="cuda")
+    U.check(U.lib().ccu_pack_weights(_ptr(w32), 16, 16, _ptr(w), None, None))
+    bias = (torch.randn(16, generator=gen) * 0.1).cuda()
+    head = (torch.randn(17, generator=gen) * 0.3).cuda()
+    xlog = torch.randn(B * D * H * W, generator=gen).cuda()
+    n = B * D * H * W
+    try:
+        U.check(U.lib().ccu_set_conv_path(path))
+        act_ref = torch.empty(B, D, H, W, 16, dtype=torch.bfloat16, device="cuda")
+        out_ref = torch.empty(n, device="cuda")
+        U.check(U.lib().ccu_conv3d(_ptr(a), 16, None, 0, B, D, H, W, _ptr(w), _ptr(bias), 16, 1, _ptr(act_ref), 16,
+                                   None, None, None))
+        U.check(U.lib().ccu_head(_ptr(act_ref), _ptr(xlog), None, None, _ptr(head), 0.0, n, _ptr(out_ref), None,
+                                 None, None, None))
+        for store in (0, 1):
+            act = torch.zeros(B, D, H, W, 16, dtype=torch.bfloat16, device="cuda")
+            out = torch.empty(n, device="cuda")
+            U.check(U.lib().ccu_conv3d_head(_ptr(a), 16, B, D, H, W, _ptr(w), _ptr(bias), _ptr(head), _ptr(xlog),
+                                            _ptr(out), _ptr(act), store, None))
+            torch.cuda.synchronize()
+            assert torch.equal(out, out_ref), store
+            if store or path == 1:
+                assert torch.equal(act, act_ref)
+            else:
+                assert not bool(act.abs().sum())        # not stored
+    finally:
+        U.check(U.lib().ccu_set_conv_path(0))
+    assert U.status() == 0
+
+
 def test_adam_with_adaptive_clipping(U):
     """ccu_adam_clipped against a NumPy restatement: the first gradient sets
     the running norm, a ten times larger one is cut to 3x that mean, and
