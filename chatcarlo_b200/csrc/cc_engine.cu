@@ -592,8 +592,14 @@ __device__ __forceinline__ void isotropic(real d[3], HistoryRng& rng) {
 // slot that sums at most FP32_SLOT_HISTORIES histories holds FP32 partial
 // sums instead, both scored by one 8-byte vector reduction.  Every slot is
 // folded into the FP64 totals after its launch.
+// The cell kind is a template parameter where the launch knows it, so that
+// a kernel holds only the reduction it issues; CELL_RUNTIME reads the grid's
+// flag (kernels that serve grids of both kinds).
+constexpr int CELL_FP64 = 0, CELL_FP32 = 1, CELL_RUNTIME = 2;
+
+template <int CELL>
 __device__ __forceinline__ void score(double* tally, int tally32, int v, real wk_len, real wh_len) {
-    if (tally32) {
+    if (CELL == CELL_FP32 || (CELL == CELL_RUNTIME && tally32)) {
         asm volatile("red.global.add.v2.f32 [%0], {%1, %2};" ::"l"(reinterpret_cast<float*>(tally + 2 * v)),
                      "f"((float)wk_len), "f"((float)wh_len)
                      : "memory");
@@ -680,6 +686,7 @@ __device__ __forceinline__ void walk_axis(real o, real h, real inv_h, int n, rea
 // per-axis state is held in scalars and the crossing axis picked by
 // selects: a register array indexed by the crossing axis would live in
 // local memory.
+template <int CELL = CELL_RUNTIME>
 __device__ __forceinline__ int walk_range(const KGrid& G, double* tally, const real p[3], const real d[3],
                                           real t0, real t1, phys wk, phys wh) {
     int ix, iy, iz, sx, sy, sz;
@@ -702,7 +709,7 @@ __device__ __forceinline__ int walk_range(const KGrid& G, double* tally, const r
         real tn = fmin(ax0 ? mx : (ax1 ? my : mz), t1);
         real len = tn - t;
         if (len > P(0.0)) {
-            score(tally, G.tally32, v, wk * len, wh * len);
+            score<CELL>(tally, G.tally32, v, wk * len, wh * len);
             ++visits;
         }
         t = tn;
@@ -895,6 +902,7 @@ __device__ __forceinline__ void piece_range(real t0, real t1, int m, int k, real
 // The warp scores its segments together: lane l's segment (if m > 0) is in
 // seg[l]; every segment is cut into m pieces and the lanes walk all pieces
 // round-robin, so every lane walks about the same number of voxels.
+template <int CELL = CELL_RUNTIME>
 __device__ __forceinline__ void score_warp_segments(const KGrid& G, const SegRec* seg, int* pre, int lane, int m,
                                                     unsigned& c_vox) {
     int incl = warp_inclusive_scan(m, lane);
@@ -912,7 +920,7 @@ __device__ __forceinline__ void score_warp_segments(const KGrid& G, const SegRec
         const int k = u - pre[lo];
         real ta, tz;
         piece_range(q.t0, q.t1, q.m, k, ta, tz);
-        int nv = walk_range(G, G.tally + (size_t)q.batch * 2 * G.nvox, q.p, q.d, ta, tz, q.wk, q.wh);
+        int nv = walk_range<CELL>(G, G.tally + (size_t)q.batch * 2 * G.nvox, q.p, q.d, ta, tz, q.wk, q.wh);
         c_vox += max(nv - (k > 0 ? 1 : 0), 0);   // a cut voxel is one visit
     }
     __syncwarp();
@@ -940,7 +948,13 @@ __device__ __forceinline__ void score_warp_segments(const KGrid& G, const SegRec
 #define CC_MIN_BLOCKS 4
 #endif
 
-template <bool FROM_SOURCE, bool TALLY, bool HEEL = false>
+// The tally variant TV of a launch: CELL_FP64 or CELL_FP32 scores inline
+// with that one reduction; TV_DEFER queues the segments (the fallback walk
+// reads the grid's cell flag).  Each instantiation holds one copy of the
+// voxel walk, which keeps the loop's code small.
+constexpr int TV_DEFER = 3;
+
+template <bool FROM_SOURCE, bool TALLY, bool HEEL = false, int TV = CELL_FP64>
 __global__ void __launch_bounds__(BLOCK, CC_MIN_BLOCKS)
 transport_kernel(const KTables T, const KScene S, const KGrid G, const KSource SRC, const KRun R) {
     extern __shared__ double s_edep[];             // [n_scratch][n_mat]
@@ -1053,7 +1067,7 @@ transport_kernel(const KTables T, const KScene S, const KGrid G, const KSource S
         }
 
         // ---- phase 2: the warp scores its segments, or queues them ----
-        if (TALLY && R.defer) {
+        if (TALLY && TV == TV_DEFER) {
             const bool has = tal_n > 0;
             const unsigned mask = __ballot_sync(FULL, has);
             if (mask) {
@@ -1088,7 +1102,7 @@ transport_kernel(const KTables T, const KScene S, const KGrid G, const KSource S
                     r.d[0] = d[0]; r.d[1] = d[1]; r.d[2] = d[2];
                     r.t0 = t0; r.t1 = t1; r.wk = wk; r.wh = wh; r.batch = batch; r.m = m;
                 }
-                score_warp_segments(G, s_seg[warp], s_pre[warp], lane, m, c_vox);
+                score_warp_segments<TV == TV_DEFER ? CELL_RUNTIME : TV>(G, s_seg[warp], s_pre[warp], lane, m, c_vox);
             }
         }
         if (TALLY && c_vox >= COUNTER_FLUSH) {
@@ -1906,7 +1920,16 @@ static int dev_upload(std::vector<void*>& allocs, const std::vector<T>& v, const
 template <bool FS, bool TL, bool HEEL = false>
 static cudaError_t launch_transport(cc_ctx* c, const KTables& T, const KScene& S, const KGrid& G,
                                     const KSource& SRC, const KRun& R, size_t smem, int grid_blocks) {
-    transport_kernel<FS, TL, HEEL><<<grid_blocks, c->block, smem, c->stream>>>(T, S, G, SRC, R);
+    if constexpr (TL) {
+        if (R.defer)
+            transport_kernel<FS, TL, HEEL, TV_DEFER><<<grid_blocks, c->block, smem, c->stream>>>(T, S, G, SRC, R);
+        else if (G.tally32)
+            transport_kernel<FS, TL, HEEL, CELL_FP32><<<grid_blocks, c->block, smem, c->stream>>>(T, S, G, SRC, R);
+        else
+            transport_kernel<FS, TL, HEEL, CELL_FP64><<<grid_blocks, c->block, smem, c->stream>>>(T, S, G, SRC, R);
+    } else {
+        transport_kernel<FS, TL, HEEL><<<grid_blocks, c->block, smem, c->stream>>>(T, S, G, SRC, R);
+    }
     return cudaGetLastError();
 }
 
