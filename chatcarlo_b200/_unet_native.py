@@ -18,7 +18,7 @@ EXPORTED = [
     "ccu_version", "ccu_last_error", "ccu_status", "ccu_conv3d", "ccu_conv3d_head", "ccu_conv3d_wgrad",
     "ccu_bias_grad",
     "ccu_avgpool", "ccu_pool_backward", "ccu_up_reduce", "ccu_head", "ccu_input", "ccu_adam", "ccu_adam_clipped",
-    "ccu_packed_weight_elems", "ccu_pack_weights", "ccu_set_conv_path", "ccu_set_conv_ring",
+    "ccu_packed_weight_elems", "ccu_pack_weights", "ccu_set_conv_path", "ccu_set_wgrad_path", "ccu_set_conv_ring",
     "ccu_set_conv_group", "ccu_zero", "ccu_gemm_test",
 ]
 
@@ -46,6 +46,7 @@ _SIGS = {
     "ccu_packed_weight_elems": ([I, I], LL),
     "ccu_pack_weights": ([P, I, I, P, P, P], I),
     "ccu_set_conv_path": ([I], I),
+    "ccu_set_wgrad_path": ([I], I),
     "ccu_set_conv_ring": ([I], I),
     "ccu_set_conv_group": ([I], I),
     "ccu_zero": ([P, LL, P], I),

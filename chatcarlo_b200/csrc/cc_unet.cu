@@ -28,6 +28,8 @@
 // sets a status bit that the host reads, and the CTA still frees its tensor
 // memory before it returns.
 #include <algorithm>
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 #include <cuda_bf16.h>
 #include <stdint.h>
@@ -129,6 +131,25 @@ __device__ bool mbar_wait_or_fail(uint64_t* bar, uint32_t parity, volatile int* 
 // barrier's expected count includes it).
 __device__ __forceinline__ void cp_async_arrive_noinc(uint64_t* bar) {
     asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// One arrival on an mbarrier that also raises the bytes its phase waits
+// for by `bytes` (the tensor-memory-accelerator copies that complete on it).
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+
+// Tile load of one box of a 5D tensor map into this CTA's shared memory,
+// completing on an mbarrier (no multicast).  Coordinates outside the tensor
+// read zeros; the innermost coordinate must be 16-byte aligned.
+__device__ __forceinline__ void tma_load_5d(uint32_t dst, const CUtensorMap* map, uint64_t* bar, int c0, int c1,
+                                            int c2, int c3, int c4) {
+    asm volatile(
+        "cp.async.bulk.tensor.5d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5, "
+        "%6}], [%7];" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4), "r"(smem_u32(bar))
+        : "memory");
 }
 
 __device__ __forceinline__ void fence_proxy_async() {
@@ -1465,6 +1486,156 @@ __global__ void __launch_bounds__(THREADS) wgrad_kernel(const WgradP P) {
 }
 
 // ---------------------------------------------------------------------------
+// weight gradient from tensor-memory-accelerator tile loads
+// ---------------------------------------------------------------------------
+
+// The GEMM of wgrad_kernel -- M = 128 (tap, ci) rows, N = output channels,
+// K = voxels -- for inputs that are not concatenated, with both operands
+// copied by the tensor memory accelerator instead of gathered by threads.
+// A K stage is a block of bx x by = 64 voxels at one z (bx a power of two
+// that divides W).  The A tile of row group g (channels ci0 .. ci0 + 7 of
+// tap (dz, dy, dx)) is one box {8 channels, bx, by, 1, 1} of the input at
+// the stage's coordinates shifted by the tap; it lands as 64 rows of 16
+// bytes in voxel order, i.e. eight MN-major core matrices along K, 128 bytes
+// apart, and the M tile's 16 row groups follow each other 1 KB apart.
+// Coordinates outside the volume read zeros, which is the convolution's
+// zero padding.  The output-gradient tile is the same box of dz at the
+// unshifted coordinates, one per 8 output channels, so K runs over the same
+// voxels in the same order in both operands.  Warp 0 issues the copies
+// (lane g: row group g; lanes 16 .. 16 + N / 8 - 1: the dz groups) once lane
+// 0 has set the stage's expected bytes; one thread of warp 1 issues the
+// MMAs and commits the stage's "empty" barrier; every warp then reads the
+// accumulator and adds it into dw.
+struct WgradT {
+    float* dw;                   // [27][N][cin], accumulated
+    int cin, rows;               // input channels, 27 x cin
+    int D, ny_blk, nx_blk;       // depth, y blocks (of by), x blocks (of bx)
+    int bx, by;                  // a stage's voxels along x and y (bx x by = KSTAGE)
+    long long stages;            // volumes x D x ny_blk x nx_blk
+};
+
+__host__ __device__ constexpr int wgrad_tma_stages(int n) { return n <= 16 ? 6 : (n <= 32 ? 5 : (n <= 64 ? 4 : 3)); }
+
+template <int N>
+__global__ void __launch_bounds__(THREADS) wgrad_tma_kernel(const __grid_constant__ CUtensorMap xmap,
+                                                            const __grid_constant__ CUtensorMap zmap,
+                                                            const WgradT P) {
+    constexpr int NS = wgrad_tma_stages(N);
+    constexpr uint32_t A_BYTES = TILE_M * KSTAGE * 2, STAGE = wgrad_stage_bytes(N);
+    static_assert(A_BYTES == 16 * 1024 && STAGE % 1024 == 0, "row groups of 1 KB");
+    extern __shared__ __align__(128) uint8_t smem[];
+    __shared__ uint64_t full[NS], empty[NS], done;
+    __shared__ uint32_t s_tmem;
+    __shared__ int s_fail;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int r0 = blockIdx.x * TILE_M;
+    const long long s_begin = P.stages * blockIdx.y / gridDim.y;
+    const int n_st = (int)(P.stages * (blockIdx.y + 1) / gridDim.y - s_begin);
+    volatile int* fail = &s_fail;
+
+    if (warp == 0) tmem_alloc(&s_tmem, tmem_cols(N));
+    if (tid == 0) {
+        for (int i = 0; i < NS; ++i) {
+            mbar_init(&full[i], 1);
+            mbar_init(&empty[i], 1);
+        }
+        mbar_init(&done, 1);
+        s_fail = 0;
+        mbar_init_fence();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = s_tmem;
+    const uint32_t sbase = (smem_u32(smem) + 1023u) & ~1023u;     // the launch adds 1 KB of slack
+
+    if (warp == 0) {
+        // ---- copies: this lane's box, fixed for the CTA ----
+        int kind = 0, c0 = 0, ox = 0, oy = 0, oz = 0;
+        uint32_t dst = 0;
+        if (lane < 16) {
+            const int r = r0 + 8 * lane;
+            if (r < P.rows) {
+                const int tap = r / P.cin;
+                kind = 1;
+                c0 = r - tap * P.cin;
+                oz = tap / 9 - 1;
+                oy = (tap / 3) % 3 - 1;
+                ox = tap % 3 - 1;
+                dst = (uint32_t)lane * 1024u;
+            }
+        } else if (lane < 16 + N / 8) {
+            kind = 2;
+            c0 = (lane - 16) * 8;
+            dst = A_BYTES + (uint32_t)(lane - 16) * 1024u;
+        }
+        const CUtensorMap* map = kind == 2 ? &zmap : &xmap;
+        const uint32_t bytes = (uint32_t)__popc(__ballot_sync(0xffffffffu, kind != 0)) * 1024u;
+        int issued = 0;
+        for (int s = 0; s < n_st; ++s) {
+            const int slot = s % NS;
+            int ok = 1;
+            // the slot's previous stage has been read by its MMAs
+            if (lane == 0 && s >= NS) ok = mbar_wait_or_fail(&empty[slot], (uint32_t)((s / NS) - 1) & 1u, fail);
+            if (!__shfl_sync(0xffffffffu, ok, 0)) break;
+            long long q = s_begin + s;
+            const int xb = (int)(q % P.nx_blk);
+            q /= P.nx_blk;
+            const int yb = (int)(q % P.ny_blk);
+            q /= P.ny_blk;
+            const int z = (int)(q % P.D), n = (int)(q / P.D);
+            if (lane == 0) mbar_arrive_expect_tx(&full[slot], bytes);
+            __syncwarp();
+            if (kind != 0)
+                tma_load_5d(sbase + (uint32_t)slot * STAGE + dst, map, &full[slot], c0, xb * P.bx + ox,
+                            yb * P.by + oy, z + oz, n);
+            issued = s + 1;
+        }
+        // after a failure, the copies still in flight land before the CTA ends
+        if (lane == 0 && *fail)
+            for (int s = max(0, issued - NS); s < issued; ++s) mbar_wait(&full[s % NS], (uint32_t)(s / NS) & 1u);
+    } else if (warp == 1 && lane == 0) {
+        // ---- MMAs: four of K = 16 voxels per stage ----
+        constexpr uint32_t IDESC = idesc_bf16(TILE_M, N, 1, 1);
+        for (int s = 0; s < n_st; ++s) {
+            const int slot = s % NS;
+            if (!mbar_wait_or_fail(&full[slot], (uint32_t)(s / NS) & 1u, fail)) break;
+            tc_fence_after();
+            const uint32_t a0 = sbase + (uint32_t)slot * STAGE, b0 = a0 + A_BYTES;
+#pragma unroll
+            for (int k = 0; k < KSTAGE / 16; ++k)
+                mma_bf16(tmem, smem_desc(a0 + k * 256, 128, 1024), smem_desc(b0 + k * 256, 128, 1024), IDESC,
+                         (s > 0 || k > 0) ? 1u : 0u);
+            mma_commit(&empty[slot]);
+        }
+        mma_commit(&done);          // arrives once every MMA issued above has finished
+    }
+    // ---- epilogue: the accumulator into dw ----
+    if (lane == 0) mbar_wait_or_fail(&done, 0u, fail);
+    __syncthreads();
+    tc_fence_after();
+    const bool good = !*fail && n_st > 0;
+    if (good) {
+        const int q = warp & 3, half = warp >> 2;
+        const int rr = r0 + q * 32 + lane;
+        const int tp = rr / P.cin, cc = rr - tp * P.cin;
+        for (int c0 = half * 8; c0 < N; c0 += 16) {
+            float f[8];
+            tmem_ld8(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)c0, f);
+            if (rr < P.rows) {
+#pragma unroll
+                for (int j = 0; j < 8; ++j) atomicAdd(P.dw + ((size_t)tp * N + c0 + j) * P.cin + cc, f[j]);
+            }
+        }
+    } else if (*fail && tid == 0) {
+        atomicOr(&g_status, 1u);
+    }
+    tc_fence_before();
+    __syncthreads();
+    if (warp == 0) tmem_dealloc(tmem, tmem_cols(N));
+}
+
+// ---------------------------------------------------------------------------
 // memory-bound helpers (CUDA cores)
 // ---------------------------------------------------------------------------
 
@@ -2087,6 +2258,76 @@ int launch_wgrad(const WgradP& P, int slices, int cin, cudaStream_t st) {
     return CCU_OK;
 }
 
+// cuTensorMapEncodeTiled from the driver (the runtime is linked statically,
+// the driver API is reached through its entry point).
+using TensorMapEncodeFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                       const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                       CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+TensorMapEncodeFn tensor_map_encoder() {
+    static std::once_flag once;
+    static TensorMapEncodeFn fn = nullptr;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (TensorMapEncodeFn)p;
+    });
+    return fn;
+}
+
+// 5D map of a [batch][d][h][w][c] BF16 tensor with boxes {8, bx, by, 1, 1};
+// coordinates outside it read zeros.
+int volume_map(CUtensorMap* m, const void* base, int c, int batch, int d, int h, int w, int bx, int by) {
+    TensorMapEncodeFn enc = tensor_map_encoder();
+    if (!enc) return set_error(CCU_E_DEVICE, "cuTensorMapEncodeTiled is not available from the driver");
+    const cuuint64_t dims[5] = {(cuuint64_t)c, (cuuint64_t)w, (cuuint64_t)h, (cuuint64_t)d, (cuuint64_t)batch};
+    const cuuint64_t strides[4] = {(cuuint64_t)c * 2, (cuuint64_t)w * c * 2, (cuuint64_t)h * w * c * 2,
+                                   (cuuint64_t)d * h * w * c * 2};
+    const cuuint32_t box[5] = {8u, (cuuint32_t)bx, (cuuint32_t)by, 1u, 1u};
+    const cuuint32_t estride[5] = {1u, 1u, 1u, 1u, 1u};
+    const CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<void*>(base), dims, strides, box,
+                           estride, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return set_error(CCU_E_INVALID, "cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
+    return CCU_OK;
+}
+
+template <int N>
+int launch_wgrad_tma(const void* a, int ca, int batch, int d, int h, int w, const void* dz, float* dw, int slices,
+                     cudaStream_t st) {
+    int bx = KSTAGE;
+    while (w % bx) bx >>= 1;                        // >= 8: checked by the caller
+    const int by = KSTAGE / bx;
+    CUtensorMap xmap, zmap;
+    int rc = volume_map(&xmap, a, ca, batch, d, h, w, bx, by);
+    if (rc == CCU_OK) rc = volume_map(&zmap, dz, N, batch, d, h, w, bx, by);
+    if (rc != CCU_OK) return rc;
+    WgradT P;
+    P.dw = dw;
+    P.cin = ca;
+    P.rows = 27 * ca;
+    P.D = d;
+    P.bx = bx;
+    P.by = by;
+    P.nx_blk = w / bx;
+    P.ny_blk = (h + by - 1) / by;
+    P.stages = (long long)batch * d * P.ny_blk * P.nx_blk;
+    size_t smem = 0;
+    rc = tc_launch_smem(wgrad_tma_kernel<N>, (size_t)wgrad_tma_stages(N) * wgrad_stage_bytes(N) + 1024, tmem_cols(N),
+                        smem);
+    if (rc != CCU_OK) return rc;
+    const long long splits = std::max(1LL, std::min<long long>(slices, P.stages));
+    dim3 grid((unsigned)((P.rows + TILE_M - 1) / TILE_M), (unsigned)splits);
+    wgrad_tma_kernel<N><<<grid, THREADS, smem, st>>>(xmap, zmap, P);
+    CU_CHECK(cudaGetLastError());
+    return CCU_OK;
+}
+
+int g_wgrad_path = 0;       // 0: tile loads where they apply, 1: the gathering kernel
+
 int check_src(const void* a, int ca, const void* b, int cb, int batch, int d, int h, int w) {
     if (!a || ca <= 0 || ca % 16 || cb < 0 || cb % 16 || (cb > 0 && !b))
         return set_error(CCU_E_INVALID, "channels must be positive multiples of 16 (the second input optional)");
@@ -2208,6 +2449,16 @@ int ccu_conv3d_wgrad(const void* a, int ca, const void* b, int cb, int batch, in
     int rc = check_src(a, ca, b, cb, batch, d, h, w);
     if (rc != CCU_OK) return rc;
     if (!dz || !dw || !aligned16(dz) || slices <= 0) return set_error(CCU_E_INVALID, "bad gradient arguments");
+    cudaStream_t st = (cudaStream_t)stream;
+    if (g_wgrad_path == 0 && cb == 0 && w % 8 == 0) {
+        switch (cout) {
+            case 16: return launch_wgrad_tma<16>(a, ca, batch, d, h, w, dz, dw, slices, st);
+            case 32: return launch_wgrad_tma<32>(a, ca, batch, d, h, w, dz, dw, slices, st);
+            case 64: return launch_wgrad_tma<64>(a, ca, batch, d, h, w, dz, dw, slices, st);
+            case 128: return launch_wgrad_tma<128>(a, ca, batch, d, h, w, dz, dw, slices, st);
+            default: return set_error(CCU_E_INVALID, "output channels must be one of 16, 32, 64, 128");
+        }
+    }
     WgradP P;
     P.src = Src{(const __nv_bfloat16*)a, (const __nv_bfloat16*)b, ca, cb, batch, d, h, w};
     P.dz = (const __nv_bfloat16*)dz;
@@ -2217,7 +2468,6 @@ int ccu_conv3d_wgrad(const void* a, int ca, const void* b, int cb, int batch, in
     P.vox_per_cta = per;
     slices = (int)((P.n_vox + per - 1) / per);
     P.dw = dw;
-    cudaStream_t st = (cudaStream_t)stream;
     const int cin = ca + cb;
     switch (cout) {
         case 16: return launch_wgrad<16>(P, slices, cin, st);
@@ -2331,6 +2581,13 @@ int ccu_set_conv_path(int path) {
                                         "streaming kernel with warp roles) or 4 (path 0 without the "
                                         "plane-stationary kernel)");
     g_conv_path = path;
+    return CCU_OK;
+}
+
+int ccu_set_wgrad_path(int path) {
+    if (path < 0 || path > 1)
+        return set_error(CCU_E_INVALID, "path must be 0 (tile loads where they apply) or 1 (the gathering kernel)");
+    g_wgrad_path = path;
     return CCU_OK;
 }
 

@@ -56,7 +56,10 @@ int ccu_conv3d_head(const void* a, int ca, int batch, int d, int h, int w, const
 
 /* Weight gradient of ccu_conv3d: dw[27][cout][ca + cb] (FP32) +=
  * sum over voxels of dz[v][co] * input[v + tap][ci].  The voxels are split
- * into `slices` ranges reduced with atomics.  cout in {16, 32, 64, 128}. */
+ * into `slices` ranges reduced with atomics.  cout in {16, 32, 64, 128}.
+ * An input without a second (upsampled) part and with w % 8 == 0 is read by
+ * tensor-memory-accelerator tile loads, others by the gathering kernel
+ * (ccu_set_wgrad_path). */
 int ccu_conv3d_wgrad(const void* a, int ca, const void* b, int cb, int batch, int d, int h, int w, const void* dz,
                      int cout, float* dw, int slices, void* stream);
 
@@ -130,6 +133,10 @@ int ccu_pack_weights(const float* w32, int cout, int cin, void* w, void* wt, voi
  * handing off through mbarriers) where the streaming kernel applies; 4
  * path 0 without the plane-stationary kernel.  Process-wide. */
 int ccu_set_conv_path(int path);
+
+/* Kernel of ccu_conv3d_wgrad: 0 (default) tile loads where they apply, else
+ * the gathering kernel; 1 the gathering kernel always.  Process-wide. */
+int ccu_set_wgrad_path(int path);
 
 /* Ring depth (input planes held in shared memory) of path 3: 0 (default)
  * chosen per layer to keep the most planes in flight per SM, else 4 .. 12
