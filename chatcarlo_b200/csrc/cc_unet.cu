@@ -181,6 +181,13 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint3
            ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
 }
 
+// The same with a swizzled layout: type 6 (32-byte rows), 4 (64) or 2 (128),
+// bits 61-63; for MN-major operands lbo is then the byte offset between
+// swizzle-atom columns along M/N and sbo between groups of 8 rows along K.
+__device__ __forceinline__ uint64_t smem_desc_sw(uint32_t addr, uint32_t lbo, uint32_t sbo, uint32_t layout) {
+    return smem_desc(addr, lbo, sbo) | ((uint64_t)(layout & 7u) << 61);
+}
+
 // Instruction descriptor of kind::f16: FP32 accumulator, BF16 A and B,
 // A/B K-major (0) or MN-major (1), N >> 3, M >> 4.
 __host__ __device__ constexpr uint32_t idesc_bf16(int m, int n, int a_mn, int b_mn) {
@@ -1493,36 +1500,43 @@ __global__ void __launch_bounds__(THREADS) wgrad_kernel(const WgradP P) {
 // K = voxels -- for inputs that are not concatenated, with both operands
 // copied by the tensor memory accelerator instead of gathered by threads.
 // A K stage is a block of bx x by = 64 voxels at one z (bx a power of two
-// that divides W).  The A tile of row group g (channels ci0 .. ci0 + 7 of
-// tap (dz, dy, dx)) is one box {8 channels, bx, by, 1, 1} of the input at
-// the stage's coordinates shifted by the tap; it lands as 64 rows of 16
-// bytes in voxel order, i.e. eight MN-major core matrices along K, 128 bytes
-// apart, and the M tile's 16 row groups follow each other 1 KB apart.
-// Coordinates outside the volume read zeros, which is the convolution's
-// zero padding.  The output-gradient tile is the same box of dz at the
-// unshifted coordinates, one per 8 output channels, so K runs over the same
-// voxels in the same order in both operands.  Warp 0 issues the copies
-// (lane g: row group g; lanes 16 .. 16 + N / 8 - 1: the dz groups) once lane
-// 0 has set the stage's expected bytes; one thread of warp 1 issues the
-// MMAs and commits the stage's "empty" barrier; every warp then reads the
-// accumulator and adds it into dw.
+// that divides W).  A box {c channels, bx, by, 1, 1} of the input, c =
+// min(cin, 64), at the stage's coordinates shifted by one tap holds the
+// A operand of c rows (tap, ci0 .. ci0 + c - 1) of the M tile: 64 voxel
+// rows of 2c bytes, written with the 32-, 64- or 128-byte swizzle that
+// matches its row length, which is the MN-major swizzled layout of the MMA
+// (the M tile's 128 / c boxes are its atom columns, 128 c bytes apart; K
+// groups of 8 rows are 16 c bytes apart).  The copy engine handles a box
+// row per cycle or so, so rows of whole voxels (32 bytes and more) move
+// more bytes per row than 16-byte channel groups would.  Coordinates
+// outside the volume read zeros, the convolution's zero padding.  The
+// output-gradient operand is the same kind of box of dz at the unshifted
+// coordinates (min(N, 64) channels), so K runs over the same voxels in the
+// same order in both.  Warp 0 issues the copies (lanes 0 .. 7: A boxes;
+// lanes 16, 17: dz boxes) once lane 0 has set the stage's expected bytes;
+// one thread of warp 1 issues the MMAs and commits the stage's "empty"
+// barrier; every warp then reads the accumulator and adds it into dw.
 struct WgradT {
     float* dw;                   // [27][N][cin], accumulated
     int cin, rows;               // input channels, 27 x cin
+    int a_ch;                    // channels of an A box: min(cin, 64)
     int D, ny_blk, nx_blk;       // depth, y blocks (of by), x blocks (of bx)
     int bx, by;                  // a stage's voxels along x and y (bx x by = KSTAGE)
     long long stages;            // volumes x D x ny_blk x nx_blk
 };
 
 __host__ __device__ constexpr int wgrad_tma_stages(int n) { return n <= 16 ? 6 : (n <= 32 ? 5 : (n <= 64 ? 4 : 3)); }
+// descriptor layout type of rows of `bytes` (32, 64 or 128)
+__host__ __device__ constexpr uint32_t swizzle_layout(int bytes) { return bytes == 32 ? 6u : (bytes == 64 ? 4u : 2u); }
 
 template <int N>
 __global__ void __launch_bounds__(THREADS) wgrad_tma_kernel(const __grid_constant__ CUtensorMap xmap,
                                                             const __grid_constant__ CUtensorMap zmap,
                                                             const WgradT P) {
     constexpr int NS = wgrad_tma_stages(N);
+    constexpr int B_CH = N < 64 ? N : 64;                      // channels of a dz box
     constexpr uint32_t A_BYTES = TILE_M * KSTAGE * 2, STAGE = wgrad_stage_bytes(N);
-    static_assert(A_BYTES == 16 * 1024 && STAGE % 1024 == 0, "row groups of 1 KB");
+    static_assert(STAGE % 1024 == 0, "stages keep the 1 KB alignment of the swizzle patterns");
     extern __shared__ __align__(128) uint8_t smem[];
     __shared__ uint64_t full[NS], empty[NS], done;
     __shared__ uint32_t s_tmem;
@@ -1551,26 +1565,27 @@ __global__ void __launch_bounds__(THREADS) wgrad_tma_kernel(const __grid_constan
 
     if (warp == 0) {
         // ---- copies: this lane's box, fixed for the CTA ----
-        int kind = 0, c0 = 0, ox = 0, oy = 0, oz = 0;
-        uint32_t dst = 0;
-        if (lane < 16) {
-            const int r = r0 + 8 * lane;
+        int c0 = 0, ox = 0, oy = 0, oz = 0;
+        uint32_t dst = 0, box = 0;                                // box bytes, 0: no box
+        const CUtensorMap* map = &xmap;
+        if (lane < TILE_M / P.a_ch) {
+            const int r = r0 + lane * P.a_ch;
             if (r < P.rows) {
                 const int tap = r / P.cin;
-                kind = 1;
                 c0 = r - tap * P.cin;
                 oz = tap / 9 - 1;
                 oy = (tap / 3) % 3 - 1;
                 ox = tap % 3 - 1;
-                dst = (uint32_t)lane * 1024u;
+                box = (uint32_t)(KSTAGE * 2 * P.a_ch);
+                dst = (uint32_t)lane * box;
             }
-        } else if (lane < 16 + N / 8) {
-            kind = 2;
-            c0 = (lane - 16) * 8;
-            dst = A_BYTES + (uint32_t)(lane - 16) * 1024u;
+        } else if (lane >= 16 && lane < 16 + N / B_CH) {
+            c0 = (lane - 16) * B_CH;
+            box = (uint32_t)(KSTAGE * 2 * B_CH);
+            dst = A_BYTES + (uint32_t)(lane - 16) * box;
+            map = &zmap;
         }
-        const CUtensorMap* map = kind == 2 ? &zmap : &xmap;
-        const uint32_t bytes = (uint32_t)__popc(__ballot_sync(0xffffffffu, kind != 0)) * 1024u;
+        const uint32_t bytes = __reduce_add_sync(0xffffffffu, box);
         int issued = 0;
         for (int s = 0; s < n_st; ++s) {
             const int slot = s % NS;
@@ -1586,7 +1601,7 @@ __global__ void __launch_bounds__(THREADS) wgrad_tma_kernel(const __grid_constan
             const int z = (int)(q % P.D), n = (int)(q / P.D);
             if (lane == 0) mbar_arrive_expect_tx(&full[slot], bytes);
             __syncwarp();
-            if (kind != 0)
+            if (box)
                 tma_load_5d(sbase + (uint32_t)slot * STAGE + dst, map, &full[slot], c0, xb * P.bx + ox,
                             yb * P.by + oy, z + oz, n);
             issued = s + 1;
@@ -1597,6 +1612,8 @@ __global__ void __launch_bounds__(THREADS) wgrad_tma_kernel(const __grid_constan
     } else if (warp == 1 && lane == 0) {
         // ---- MMAs: four of K = 16 voxels per stage ----
         constexpr uint32_t IDESC = idesc_bf16(TILE_M, N, 1, 1);
+        const uint32_t ar = 2u * (uint32_t)P.a_ch, al = swizzle_layout((int)ar);      // A row bytes, layout
+        constexpr uint32_t BR = 2u * B_CH, BL = swizzle_layout(2 * B_CH);
         for (int s = 0; s < n_st; ++s) {
             const int slot = s % NS;
             if (!mbar_wait_or_fail(&full[slot], (uint32_t)(s / NS) & 1u, fail)) break;
@@ -1604,8 +1621,8 @@ __global__ void __launch_bounds__(THREADS) wgrad_tma_kernel(const __grid_constan
             const uint32_t a0 = sbase + (uint32_t)slot * STAGE, b0 = a0 + A_BYTES;
 #pragma unroll
             for (int k = 0; k < KSTAGE / 16; ++k)
-                mma_bf16(tmem, smem_desc(a0 + k * 256, 128, 1024), smem_desc(b0 + k * 256, 128, 1024), IDESC,
-                         (s > 0 || k > 0) ? 1u : 0u);
+                mma_bf16(tmem, smem_desc_sw(a0 + k * 16 * ar, KSTAGE * ar, 8 * ar, al),
+                         smem_desc_sw(b0 + k * 16 * BR, KSTAGE * BR, 8 * BR, BL), IDESC, (s > 0 || k > 0) ? 1u : 0u);
             mma_commit(&empty[slot]);
         }
         mma_commit(&done);          // arrives once every MMA issued above has finished
@@ -2278,18 +2295,21 @@ TensorMapEncodeFn tensor_map_encoder() {
     return fn;
 }
 
-// 5D map of a [batch][d][h][w][c] BF16 tensor with boxes {8, bx, by, 1, 1};
-// coordinates outside it read zeros.
-int volume_map(CUtensorMap* m, const void* base, int c, int batch, int d, int h, int w, int bx, int by) {
+// 5D map of a [batch][d][h][w][c] BF16 tensor with boxes {bc, bx, by, 1, 1}
+// (bc = 16, 32 or 64 channels: rows of 32, 64 or 128 bytes, written with the
+// swizzle of that width); coordinates outside it read zeros.
+int volume_map(CUtensorMap* m, const void* base, int c, int batch, int d, int h, int w, int bc, int bx, int by) {
     TensorMapEncodeFn enc = tensor_map_encoder();
     if (!enc) return set_error(CCU_E_DEVICE, "cuTensorMapEncodeTiled is not available from the driver");
     const cuuint64_t dims[5] = {(cuuint64_t)c, (cuuint64_t)w, (cuuint64_t)h, (cuuint64_t)d, (cuuint64_t)batch};
     const cuuint64_t strides[4] = {(cuuint64_t)c * 2, (cuuint64_t)w * c * 2, (cuuint64_t)h * w * c * 2,
                                    (cuuint64_t)d * h * w * c * 2};
-    const cuuint32_t box[5] = {8u, (cuuint32_t)bx, (cuuint32_t)by, 1u, 1u};
+    const cuuint32_t box[5] = {(cuuint32_t)bc, (cuuint32_t)bx, (cuuint32_t)by, 1u, 1u};
     const cuuint32_t estride[5] = {1u, 1u, 1u, 1u, 1u};
+    const CUtensorMapSwizzle sw = bc == 16 ? CU_TENSOR_MAP_SWIZZLE_32B
+                                           : (bc == 32 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_128B);
     const CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<void*>(base), dims, strides, box,
-                           estride, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                           estride, CU_TENSOR_MAP_INTERLEAVE_NONE, sw,
                            CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return set_error(CCU_E_INVALID, "cuTensorMapEncodeTiled failed: " + std::to_string((int)r));
     return CCU_OK;
@@ -2301,14 +2321,16 @@ int launch_wgrad_tma(const void* a, int ca, int batch, int d, int h, int w, cons
     int bx = KSTAGE;
     while (w % bx) bx >>= 1;                        // >= 8: checked by the caller
     const int by = KSTAGE / bx;
+    const int a_ch = std::min(ca, 64);             // ca: 16, 32 or a multiple of 64, checked by the caller
     CUtensorMap xmap, zmap;
-    int rc = volume_map(&xmap, a, ca, batch, d, h, w, bx, by);
-    if (rc == CCU_OK) rc = volume_map(&zmap, dz, N, batch, d, h, w, bx, by);
+    int rc = volume_map(&xmap, a, ca, batch, d, h, w, a_ch, bx, by);
+    if (rc == CCU_OK) rc = volume_map(&zmap, dz, N, batch, d, h, w, std::min(N, 64), bx, by);
     if (rc != CCU_OK) return rc;
     WgradT P;
     P.dw = dw;
     P.cin = ca;
     P.rows = 27 * ca;
+    P.a_ch = a_ch;
     P.D = d;
     P.bx = bx;
     P.by = by;
@@ -2319,8 +2341,12 @@ int launch_wgrad_tma(const void* a, int ca, int batch, int d, int h, int w, cons
     rc = tc_launch_smem(wgrad_tma_kernel<N>, (size_t)wgrad_tma_stages(N) * wgrad_stage_bytes(N) + 1024, tmem_cols(N),
                         smem);
     if (rc != CCU_OK) return rc;
-    const long long splits = std::max(1LL, std::min<long long>(slices, P.stages));
-    dim3 grid((unsigned)((P.rows + TILE_M - 1) / TILE_M), (unsigned)splits);
+    // at least four CTAs per SM over the M tiles when the stages allow it
+    // (the deep levels have few voxels), else the caller's split
+    const int mtiles = (P.rows + TILE_M - 1) / TILE_M;
+    const long long want = std::max<long long>(slices, (4LL * sm_count() + mtiles - 1) / mtiles);
+    const long long splits = std::max(1LL, std::min<long long>(want, P.stages));
+    dim3 grid((unsigned)mtiles, (unsigned)splits);
     wgrad_tma_kernel<N><<<grid, THREADS, smem, st>>>(xmap, zmap, P);
     CU_CHECK(cudaGetLastError());
     return CCU_OK;
@@ -2450,7 +2476,7 @@ int ccu_conv3d_wgrad(const void* a, int ca, const void* b, int cb, int batch, in
     if (rc != CCU_OK) return rc;
     if (!dz || !dw || !aligned16(dz) || slices <= 0) return set_error(CCU_E_INVALID, "bad gradient arguments");
     cudaStream_t st = (cudaStream_t)stream;
-    if (g_wgrad_path == 0 && cb == 0 && w % 8 == 0) {
+    if (g_wgrad_path == 0 && cb == 0 && w % 8 == 0 && (ca == 16 || ca == 32 || ca % 64 == 0)) {
         switch (cout) {
             case 16: return launch_wgrad_tma<16>(a, ca, batch, d, h, w, dz, dw, slices, st);
             case 32: return launch_wgrad_tma<32>(a, ca, batch, d, h, w, dz, dw, slices, st);
