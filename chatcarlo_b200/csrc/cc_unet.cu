@@ -1517,8 +1517,9 @@ __global__ void __launch_bounds__(THREADS) wgrad_kernel(const WgradP P) {
 // one thread of warp 1 issues the MMAs and commits the stage's "empty"
 // barrier; every warp then reads the accumulator and adds it into dw.
 struct WgradT {
-    float* dw;                   // [27][N][cin], accumulated
-    int cin, rows;               // input channels, 27 x cin
+    float* dw;                   // [27][N][ld], accumulated at columns c_off .. c_off + cin - 1
+    int ld, c_off;               // columns of dw (all input channels of the layer), first column here
+    int cin, rows;               // input channels of this operand, 27 x cin
     int a_ch;                    // channels of an A box: min(cin, 64)
     int D, ny_blk, nx_blk;       // depth, y blocks (of by), x blocks (of bx)
     int bx, by;                  // a stage's voxels along x and y (bx x by = KSTAGE)
@@ -1641,7 +1642,8 @@ __global__ void __launch_bounds__(THREADS) wgrad_tma_kernel(const __grid_constan
             tmem_ld8(tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)c0, f);
             if (rr < P.rows) {
 #pragma unroll
-                for (int j = 0; j < 8; ++j) atomicAdd(P.dw + ((size_t)tp * N + c0 + j) * P.cin + cc, f[j]);
+                for (int j = 0; j < 8; ++j)
+                    atomicAdd(P.dw + ((size_t)tp * N + c0 + j) * P.ld + P.c_off + cc, f[j]);
             }
         }
     } else if (*fail && tid == 0) {
@@ -1650,6 +1652,26 @@ __global__ void __launch_bounds__(THREADS) wgrad_tma_kernel(const __grid_constan
     tc_fence_before();
     __syncthreads();
     if (warp == 0) tmem_dealloc(tmem, tmem_cols(N));
+}
+
+// Nearest 2x upsampling, channels-last: out[n][z][y][x] = b[n][z/2][y/2][x/2]
+// (the second input of a concatenated layer, spelled out for the tile loads).
+__global__ void upsample_kernel(const uint4* __restrict__ b, uint4* __restrict__ out, int batch, int d, int h,
+                                int w, int c8) {
+    const long long total = (long long)batch * d * h * w * c8;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        const int c = (int)(i % c8);
+        long long v = i / c8;
+        const int x = (int)(v % w);
+        v /= w;
+        const int y = (int)(v % h);
+        v /= h;
+        const int z = (int)(v % d);
+        const long long n = v / d;
+        const long long cv = ((n * (d >> 1) + (z >> 1)) * (h >> 1) + (y >> 1)) * (w >> 1) + (x >> 1);
+        out[i] = __ldg(b + cv * c8 + c);
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -2171,27 +2193,38 @@ int launch_conv_stream(const ConvP& P, cudaStream_t st) {
 // FP32 partial sums of multi-pass plane-stationary convolutions: one
 // buffer per device, grown on demand (the stream is drained before an
 // older, smaller buffer is freed) and kept for the process.
-std::mutex g_ws_mu;
-void* g_ws[64] = {};
-size_t g_ws_bytes[64] = {};
+struct DevBuffers {
+    std::mutex mu;
+    void* p[64] = {};
+    size_t bytes[64] = {};
+};
+DevBuffers g_ws;          // FP32 partial sums of channel passes
+DevBuffers g_up_ws;       // the upsampled input of a weight gradient
 
-int ps_workspace(size_t bytes, cudaStream_t st, float*& ws) {
+int grow_buffer(DevBuffers& b, size_t bytes, cudaStream_t st, void*& out) {
     int dev = 0;
     CU_CHECK(cudaGetDevice(&dev));
     if (dev < 0 || dev >= 64) return set_error(CCU_E_INVALID, "device index out of range");
-    std::lock_guard<std::mutex> lk(g_ws_mu);
-    if (g_ws_bytes[dev] < bytes) {
-        if (g_ws[dev]) {
+    std::lock_guard<std::mutex> lk(b.mu);
+    if (b.bytes[dev] < bytes) {
+        if (b.p[dev]) {
             CU_CHECK(cudaStreamSynchronize(st));
-            CU_CHECK(cudaFree(g_ws[dev]));
-            g_ws[dev] = nullptr;
-            g_ws_bytes[dev] = 0;
+            CU_CHECK(cudaFree(b.p[dev]));
+            b.p[dev] = nullptr;
+            b.bytes[dev] = 0;
         }
-        CU_CHECK(cudaMalloc(&g_ws[dev], bytes));
-        g_ws_bytes[dev] = bytes;
+        CU_CHECK(cudaMalloc(&b.p[dev], bytes));
+        b.bytes[dev] = bytes;
     }
-    ws = (float*)g_ws[dev];
+    out = b.p[dev];
     return CCU_OK;
+}
+
+int ps_workspace(size_t bytes, cudaStream_t st, float*& ws) {
+    void* p = nullptr;
+    const int rc = grow_buffer(g_ws, bytes, st, p);
+    ws = (float*)p;
+    return rc;
 }
 
 template <int NO, int G>
@@ -2316,8 +2349,8 @@ int volume_map(CUtensorMap* m, const void* base, int c, int batch, int d, int h,
 }
 
 template <int N>
-int launch_wgrad_tma(const void* a, int ca, int batch, int d, int h, int w, const void* dz, float* dw, int slices,
-                     cudaStream_t st) {
+int launch_wgrad_tma(const void* a, int ca, int batch, int d, int h, int w, const void* dz, float* dw, int ld,
+                     int c_off, int slices, cudaStream_t st) {
     int bx = KSTAGE;
     while (w % bx) bx >>= 1;                        // >= 8: checked by the caller
     const int by = KSTAGE / bx;
@@ -2328,6 +2361,8 @@ int launch_wgrad_tma(const void* a, int ca, int batch, int d, int h, int w, cons
     if (rc != CCU_OK) return rc;
     WgradT P;
     P.dw = dw;
+    P.ld = ld;
+    P.c_off = c_off;
     P.cin = ca;
     P.rows = 27 * ca;
     P.a_ch = a_ch;
@@ -2476,14 +2511,31 @@ int ccu_conv3d_wgrad(const void* a, int ca, const void* b, int cb, int batch, in
     if (rc != CCU_OK) return rc;
     if (!dz || !dw || !aligned16(dz) || slices <= 0) return set_error(CCU_E_INVALID, "bad gradient arguments");
     cudaStream_t st = (cudaStream_t)stream;
-    if (g_wgrad_path == 0 && cb == 0 && w % 8 == 0 && (ca == 16 || ca == 32 || ca % 64 == 0)) {
-        switch (cout) {
-            case 16: return launch_wgrad_tma<16>(a, ca, batch, d, h, w, dz, dw, slices, st);
-            case 32: return launch_wgrad_tma<32>(a, ca, batch, d, h, w, dz, dw, slices, st);
-            case 64: return launch_wgrad_tma<64>(a, ca, batch, d, h, w, dz, dw, slices, st);
-            case 128: return launch_wgrad_tma<128>(a, ca, batch, d, h, w, dz, dw, slices, st);
-            default: return set_error(CCU_E_INVALID, "output channels must be one of 16, 32, 64, 128");
-        }
+    auto box_channels = [](int c) { return c == 16 || c == 32 || c % 64 == 0; };
+    if (g_wgrad_path == 0 && w % 8 == 0 && box_channels(ca) && (cb == 0 || box_channels(cb))) {
+        if (cout != 16 && cout != 32 && cout != 64 && cout != 128)
+            return set_error(CCU_E_INVALID, "output channels must be one of 16, 32, 64, 128");
+        auto run = [&](const void* x, int cx, int c_off) {
+            switch (cout) {
+                case 16: return launch_wgrad_tma<16>(x, cx, batch, d, h, w, dz, dw, ca + cb, c_off, slices, st);
+                case 32: return launch_wgrad_tma<32>(x, cx, batch, d, h, w, dz, dw, ca + cb, c_off, slices, st);
+                case 64: return launch_wgrad_tma<64>(x, cx, batch, d, h, w, dz, dw, ca + cb, c_off, slices, st);
+                default: return launch_wgrad_tma<128>(x, cx, batch, d, h, w, dz, dw, ca + cb, c_off, slices, st);
+            }
+        };
+        if (cb == 0) return run(a, ca, 0);
+        // a concatenated layer: the skip part from a, the upsampled part
+        // from its full-resolution copy in a per-device buffer
+        void* up = nullptr;
+        const long long n_vox = (long long)batch * d * h * w;
+        rc = grow_buffer(g_up_ws, (size_t)n_vox * cb * 2, st, up);
+        if (rc != CCU_OK) return rc;
+        upsample_kernel<<<grid_for(n_vox * (cb / 8), 256), 256, 0, st>>>((const uint4*)b, (uint4*)up, batch, d, h, w,
+                                                                        cb / 8);
+        CU_CHECK(cudaGetLastError());
+        rc = run(a, ca, 0);
+        if (rc != CCU_OK) return rc;
+        return run(up, cb, ca);
     }
     WgradP P;
     P.src = Src{(const __nv_bfloat16*)a, (const __nv_bfloat16*)b, ca, cb, batch, d, h, w};

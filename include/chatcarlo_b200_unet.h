@@ -57,8 +57,10 @@ int ccu_conv3d_head(const void* a, int ca, int batch, int d, int h, int w, const
 /* Weight gradient of ccu_conv3d: dw[27][cout][ca + cb] (FP32) +=
  * sum over voxels of dz[v][co] * input[v + tap][ci].  The voxels are split
  * into `slices` ranges reduced with atomics.  cout in {16, 32, 64, 128}.
- * An input without a second (upsampled) part and with w % 8 == 0 is read by
- * tensor-memory-accelerator tile loads, others by the gathering kernel
+ * With w % 8 == 0 and ca, cb each 16, 32 or a multiple of 64 the input is
+ * read by tensor-memory-accelerator tile loads (a second input is first
+ * upsampled into a per-device buffer that the first such call allocates,
+ * synchronously, and the process keeps), otherwise by the gathering kernel
  * (ccu_set_wgrad_path). */
 int ccu_conv3d_wgrad(const void* a, int ca, const void* b, int cb, int batch, int d, int h, int w, const void* dz,
                      int cout, float* dw, int slices, void* stream);

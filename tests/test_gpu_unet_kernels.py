@@ -164,35 +164,42 @@ def test_pool_upsample_bias_helpers(U):
     torch.testing.assert_close(db, gfull.float().sum(dim=(0, 1, 2, 3)), rtol=1e-4, atol=1e-2)
 
 
-@pytest.mark.parametrize("ca,cout,dims", [(16, 16, (2, 5, 12, 64)),     # x runs of 64, one y row per stage
-                                           (32, 32, (1, 3, 10, 24)),     # 8 x 8 stages, a partial y block
-                                           (64, 64, (2, 4, 6, 16)),      # 16 x 4 stages
-                                           (16, 128, (1, 3, 5, 40)),     # 432 rows: a partial M tile
-                                           (128, 64, (1, 2, 4, 32)),     # 27 M tiles
-                                           (16, 16, (1, 4, 16, 8))])
-def test_weight_gradient_tile_loads(U, ca, cout, dims):
+@pytest.mark.parametrize("ca,cb,cout,dims", [(16, 0, 16, (2, 5, 12, 64)),    # x runs of 64, one y row per stage
+                                              (32, 0, 32, (1, 3, 10, 24)),    # 8 x 8 stages, a partial y block
+                                              (64, 0, 64, (2, 4, 6, 16)),     # 16 x 4 stages
+                                              (16, 0, 128, (1, 3, 5, 40)),    # 432 rows: a partial M tile
+                                              (128, 0, 64, (1, 2, 4, 32)),    # 27 M tiles
+                                              (16, 0, 16, (1, 4, 16, 8)),
+                                              # concatenated inputs: the upsampled part from its copy
+                                              (16, 32, 16, (1, 4, 8, 16)), (32, 64, 32, (2, 2, 4, 8)),
+                                              (64, 128, 64, (1, 2, 6, 8))])
+def test_weight_gradient_tile_loads(U, ca, cb, cout, dims):
     """The weight gradient from tensor-memory-accelerator tile loads (the
-    default for inputs without an upsampled part and w % 8 == 0) against
-    torch autograd and against the gathering kernel (wgrad path 1), with
-    more splits than some volumes have stages."""
-    gen = torch.Generator().manual_seed(11 * ca + cout + dims[3])
+    default for w % 8 == 0 and 16, 32 or 64k channels per input part)
+    against torch autograd and against the gathering kernel (wgrad path 1),
+    with more splits than some volumes have stages."""
+    gen = torch.Generator().manual_seed(11 * ca + 3 * cb + cout + dims[3])
     B, D, H, W = dims
+    cin = ca + cb
     a = torch.relu(_bf((B, D, H, W, ca), gen).float()).to(torch.bfloat16)
+    b = torch.relu(_bf((B, D // 2, H // 2, W // 2, cb), gen).float()).to(torch.bfloat16) if cb else None
     dz = _bf((B, D, H, W, cout), gen)
     got = []
     try:
         for path, slices in ((0, 7), (0, 1000), (1, 7)):
             U.check(U.lib().ccu_set_wgrad_path(path))
-            dw = torch.zeros(27 * cout * ca, dtype=torch.float32, device="cuda")
-            U.check(U.lib().ccu_conv3d_wgrad(_ptr(a), ca, None, 0, B, D, H, W, _ptr(dz), cout, _ptr(dw), slices,
-                                             None))
+            dw = torch.zeros(27 * cout * cin, dtype=torch.float32, device="cuda")
+            U.check(U.lib().ccu_conv3d_wgrad(_ptr(a), ca, _ptr(b) if b is not None else None, cb, B, D, H, W,
+                                             _ptr(dz), cout, _ptr(dw), slices, None))
             got.append(dw)
     finally:
         U.check(U.lib().ccu_set_wgrad_path(0))
     torch.cuda.synchronize()
     assert U.status() == 0
-    x = _to_ncdhw(a).requires_grad_(False)
-    wt_ref = torch.zeros(cout, ca, 3, 3, 3, device="cuda", requires_grad=True)
+    x = _to_ncdhw(a)
+    if cb:
+        x = torch.cat([x, _up(_to_ncdhw(b))], dim=1)
+    wt_ref = torch.zeros(cout, cin, 3, 3, 3, device="cuda", requires_grad=True)
     y = torch.nn.functional.conv3d(x, wt_ref, None, padding=1)
     y.backward(_to_ncdhw(dz))
     ref = wt_ref.grad.permute(2, 3, 4, 0, 1).reshape(-1)
