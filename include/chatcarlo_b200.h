@@ -178,6 +178,10 @@ int cc_version(void);
 const char* cc_last_error(void);
 int cc_ctx_create(int device, cc_ctx** out);
 int cc_ctx_destroy(cc_ctx* ctx);
+/* Launch shape of the transport kernels: blocks_per_sm = 0 (default) runs
+ * as many blocks of 256 per SM as fit (four), or one on a grid whose batch
+ * slot exceeds 32 MB, where fewer histories in flight keep fewer slots in
+ * L2.  No reference counterpart (launch tuning). */
 int cc_ctx_set_launch(cc_ctx* ctx, int block_size, int blocks_per_sm);
 /* Transport steps a photon may take before the call fails with
  * CC_E_TIMEOUT (a guard against runaway histories; default 100000);
