@@ -58,3 +58,14 @@ def test_denoiser_library_exports_every_declared_symbol():
     # invalid sizes are rejected on the host
     assert lib.ccu_conv3d(None, 16, None, 0, 1, 8, 8, 8, None, None, 16, 1, None, 16, None, None, None) == -1
     assert lib.ccu_gemm_test(None, None, None, 100, 16, 64, 0, 0, None) == -1
+
+
+def test_kernel_path_setters_reject_unknown_paths_without_gpu():
+    from chatcarlo_b200 import _unet_native as U
+    lib = U.lib()
+    assert lib.ccu_set_wgrad_path(2) == -1
+    assert lib.ccu_set_wgrad_path(-1) == -1
+    assert lib.ccu_set_wgrad_path(0) == 0
+    assert lib.ccu_set_conv_path(5) == -1
+    # the weight gradient checks its arguments on the host
+    assert lib.ccu_conv3d_wgrad(None, 16, None, 0, 1, 8, 8, 8, None, 16, None, 1, None) == -1
